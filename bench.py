@@ -1,0 +1,384 @@
+#!/usr/bin/env python3
+"""Benchmark of the path-tracing hot path on B200.
+
+Default workload (the one the headline is quoted on): the closest-hit query
+set -- 1,000,000 fp32 triangles (uniform centroids in [0,1]^3, N(0, 0.005^2)
+vertex jitter) in the reference's SAH BVH, 4,194,304 rays from a radius-2
+sphere towards uniform points of the cube. One step = one closest-hit pass
+over all rays (BVHAccel::Intersect semantics, bit-exact hit IDs).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line. Under torchrun (N > 1) every rank traces its own copy of
+the query set on its own GPU with no collective on the data path (weak
+scaling); the step time is the max over ranks.
+
+--impl reference times the reference's own CPU implementation of the same
+query (its sources compiled in place with its shipped -O3 -ffast-math flags
+and OpenMP, oracle/_ref/libprr_ref_fast.so; the C restatement if that library
+is absent) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_TRIS = 1_000_000
+N_RAYS = 4_194_304
+WORKLOAD = "closest-hit query set: 1,000,000 fp32 triangles, 4,194,304 rays"
+METRIC = "Mrays/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, local):
+    import torch
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return world > 1
+
+
+def barrier(on):
+    if on:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, on):
+    if not on:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """dram bytes per launch recorded by the ncu capture summarised under
+    profiles/ (a `traffic_bytes_per_launch: N` line), or None."""
+    for f in sorted((ROOT / "profiles").glob(f"{kernel}*.md")):
+        for line in f.read_text().splitlines():
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].strip().split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+def workload_arrays():
+    from photorealisticrender4610_b200 import scenes
+    return scenes.query_set(N_TRIS, N_RAYS, seed=1)
+
+
+def parse_launch(text):
+    """'block=128,persistent=1' -> launch config dict."""
+    out = {}
+    for kv in filter(None, (text or "").split(",")):
+        k, v = kv.split("=")
+        out[{"block": "block_size"}.get(k, k)] = int(v)
+    return out
+
+
+def traversal_work(verts, o, d, threads):
+    """Mean interior visits I and triangle tests T per ray, counted by the
+    oracle's traversal on the same rays (sample of 2^20 rays)."""
+    from oracle.loader import PortOracle
+    port = PortOracle()
+    m = port.mesh(verts)
+    k = min(len(o), 1 << 20)
+    _, _, _, vis, tst = m.intersect(o[:k], d[:k], threads=threads, stats=True)
+    return float(vis.mean()), float(tst.mean())
+
+
+_CPU_MESH = {}
+
+
+def cpu_reference_rate(verts, o, d, n_sample, threads):
+    """Reference CPU closest-hit throughput (Mrays/s) on n_sample rays (the
+    BVH is built once, untimed, like the reference's own timer excludes
+    nothing but we exclude construction from a traversal rate)."""
+    from oracle import loader
+    if "run" in _CPU_MESH:
+        run, kind = _CPU_MESH["run"], _CPU_MESH["kind"]
+        t0 = time.perf_counter()
+        run(o[:n_sample], d[:n_sample])
+        return n_sample / (time.perf_counter() - t0) / 1e6, kind
+    if loader.reference_available(fast=True):
+        ref = loader.ReferenceOracle(fast=True)
+        kind = "reference"
+        mesh = ref.mesh(verts)
+        run = lambda a, b: mesh.intersect(a, b, threads=threads)  # noqa: E731
+    else:
+        port = loader.PortOracle()
+        kind = "port"
+        mesh = port.mesh(verts)
+        run = lambda a, b: mesh.intersect(a, b, threads=threads)  # noqa: E731
+    run(o[:4096], d[:4096])
+    _CPU_MESH.update(run=run, kind=kind, mesh=mesh)
+    t0 = time.perf_counter()
+    run(o[:n_sample], d[:n_sample])
+    dt = time.perf_counter() - t0
+    return n_sample / dt / 1e6, kind
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    verts, o, d = workload_arrays()
+    sample = min(N_RAYS, 1 << 20)
+    for _ in range(args.warmup):
+        cpu_reference_rate(verts, o, d, 1 << 16, threads)
+    rates = []
+    kind = None
+    t_all = time.perf_counter()
+    for k in range(args.steps):
+        r, kind = cpu_reference_rate(verts, o, d, sample, threads)
+        rates.append(r)
+    total = time.perf_counter() - t_all
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / max(1, args.steps) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": sample, "threads": threads},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                         "sample": f"{sample} of the {N_RAYS} query rays per step"},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, on):
+    import torch
+    import photorealisticrender4610_b200 as prr
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    verts, o, d = workload_arrays()
+    scene = prr.Scene.single_mesh(verts)
+    O = torch.from_numpy(o).to(dev)
+    D = torch.from_numpy(d).to(dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    # autotune the launch shape on this scene (untimed)
+    configs = [{"block_size": 128}, {"block_size": 64}, {"block_size": 256},
+               {"block_size": 128, "persistent": 1}, {"block_size": 64, "persistent": 1}]
+    if args.launch:
+        configs = [parse_launch(args.launch)]
+    best, best_ms = None, math.inf
+    for cfg in configs if len(configs) > 1 else []:
+        times = []
+        for _ in range(2):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            scene.mesh_intersect(0, O, D, config=cfg)
+            e.record()
+            torch.cuda.synchronize()
+            times.append(s.elapsed_time(e))
+        if min(times) < best_ms:
+            best, best_ms = cfg, min(times)
+    if best is None:
+        best = configs[0]
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        scene.mesh_intersect(0, O, D, config=best)
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(dev.index if world == 1 else int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        barrier(on)
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record()
+            hid, t = scene.mesh_intersect(0, O, D, config=best)
+            ends[k].record()
+        torch.cuda.synchronize()
+        barrier(on)
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms_step = max_over_ranks(float(np.mean(kernel_ms)), on)
+    value = N_RAYS * world / (ms_step * 1e-3) / 1e6
+
+    assert int((hid >= 0).sum().item()) > 0.99 * N_RAYS
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"kernel_ms": kernel_ms, "launch": best, "mrays_s": value}))
+        return 0
+
+    # end to end through the host-buffer C ABI call (pinned host arrays)
+    ho = torch.from_numpy(o).pin_memory().numpy()
+    hd = torch.from_numpy(d).pin_memory().numpy()
+    hid_h = torch.empty(N_RAYS, dtype=torch.int32).pin_memory().numpy()
+    t_h = torch.empty(N_RAYS, dtype=torch.float32).pin_memory().numpy()
+    scene.mesh_intersect_host(0, ho, hd, hid_h, t_h)
+    e2e_ms = []
+    for _ in range(max(3, min(args.steps, 10))):
+        barrier(on)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        scene.mesh_intersect_host(0, ho, hd, hid_h, t_h)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = max_over_ranks(float(np.median(e2e_ms)), on)
+    e2e_value = N_RAYS * world / (e2e_step * 1e-3) / 1e6
+    assert np.array_equal(hid_h, hid.cpu().numpy())
+
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    I, T = traversal_work(verts, o, d, threads)
+    bytes_per_ray = 24 + 8 + 64 * I + 36 * T
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_ray * N_RAYS / (float(np.mean(kernel_ms)) * 1e-3) / 1e9
+    traffic = profiled_traffic("k_mesh_closest")
+    cpu_rate, cpu_kind = cpu_reference_rate(verts, o, d, N_RAYS, threads)
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": N_RAYS, "triangles": N_TRIS,
+                   "seed": 1, "l2": "flushed (512 MB write) before every timed step",
+                   "launch": best, "parallelism": f"replica x{world}" if world > 1 else "1 GPU"},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 24,
+                "d2h_bytes_per_step": N_RAYS * 8},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "bytes_per_ray": bytes_per_ray, "interior_visits": I, "tri_tests": T},
+        "cpu_baseline": {"value": cpu_rate, "unit": "Mrays/s", "cores": threads,
+                         "kind": cpu_kind, "sample": f"all {N_RAYS} query rays, one pass"},
+        "clocks": clocks,
+        "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--launch", default="", help="fixed launch shape, e.g. block=128,persistent=0")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the kernel only (no e2e, no CPU baseline): profiling runs")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if world > 1 and rank != 0:
+            return 0
+        return run_reference(args, rank, world)
+    on = init_dist(world, local)
+    try:
+        return run_ours(args, rank, world, on)
+    finally:
+        if on:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,155 @@
+/*
+ * prr.h -- C ABI of libprr, the B200 (sm_100a) Monte Carlo path-tracing hot
+ * path of the PhotoRealisticRender4610 CPU renderer.
+ *
+ * The reference has no plugin or FFI layer: its interface is a set of C++
+ * classes compiled into one executable (Scene, BVHAccel, Integrator, Renderer,
+ * tonemap). Each entry point below names the reference member it replaces
+ * (file:line in the reference tree). The C++ drop-in classes in prr_dropin.hpp
+ * forward to these calls with the reference's own class and method names.
+ *
+ * Conventions
+ *   - Every call returns an int status: PRR_OK (0) or a negative PRR_ERR_*;
+ *     prr_last_error() gives the calling thread's message for the last failure.
+ *   - Handles are opaque. A scene is immutable after prr_scene_build() and may
+ *     then be used from several host threads and streams at once.
+ *   - Unless a name ends in _host, array arguments are DEVICE pointers owned by
+ *     the caller and the call is asynchronous on `stream` (a cudaStream_t, NULL
+ *     for the legacy default stream). _host variants take host pointers and
+ *     return when the results are in host memory.
+ *   - Rays are n x 3 float arrays of origins and of directions (x,y,z per ray).
+ */
+#ifndef PRR_H
+#define PRR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRR_ABI_VERSION 1
+
+#define PRR_OK 0
+#define PRR_ERR_INVALID_ARGUMENT (-1)
+#define PRR_ERR_CUDA (-2)
+#define PRR_ERR_OUT_OF_MEMORY (-3)
+#define PRR_ERR_NOT_BUILT (-4)
+#define PRR_ERR_UNSUPPORTED (-5)
+#define PRR_ERR_TIMEOUT (-6)
+#define PRR_ERR_BUDGET (-7)
+#define PRR_ERR_INTERNAL (-8)
+
+/* Material kinds: DiffuseMaterial, EmissiveMaterial, MirrorMaterial,
+ * GlassMaterial (Material.hpp:120-183). */
+#define PRR_MAT_DIFFUSE 0
+#define PRR_MAT_EMISSIVE 1
+#define PRR_MAT_MIRROR 2
+#define PRR_MAT_GLASS 3
+
+typedef struct prr_scene prr_scene;
+
+/* Camera fields of Camera::create + aperture/focusDistance (Camera.hpp:10-31). */
+typedef struct prr_camera {
+    float eye[3], target[3], up[3];
+    float fovv, fovh;
+    float aperture;
+    float focus_distance; /* < 0: distance eye -> target (Camera.hpp:51-54) */
+} prr_camera;
+
+/* Traversal launch shape (chosen by the autotuner; zero fields = defaults). */
+typedef struct prr_trace_config {
+    int block_size;   /* threads per block (multiple of 32) */
+    int persistent;   /* 1: grid of SMs x blocks_per_sm pulling ray batches */
+    int blocks_per_sm;
+    int batch;        /* rays fetched per warp per atomic when persistent */
+} prr_trace_config;
+
+typedef struct prr_scene_stats {
+    int64_t n_objects, n_triangles, n_nodes;
+    int32_t tlas_depth, blas_depth;
+    int64_t device_bytes;
+    float total_emit_area;
+} prr_scene_stats;
+
+/* ---- library ---------------------------------------------------------- */
+int prr_abi_version(void);
+/* Copies the calling thread's last error message (NUL-terminated). Returns
+ * its full length. */
+int prr_last_error(char *buf, size_t len);
+
+/* ---- BVH construction alone (BVHAccel ctor, BVH.cpp:13-54) --------------
+ * Host-only: builds the reference's binned-SAH tree over n primitives given
+ * their bounds (n x 6: minX,minY,minZ,maxX,maxY,maxZ) and areas, with
+ * maxPrimsInNode clamped to 255, and writes the flattened layout (BVHNode
+ * bounds interleaved per axis, first_child, meta, nodeAreas, orderedPrims).
+ * Outputs must hold 2n-1 nodes; any may be NULL. Returns the node count. */
+int64_t prr_bvh_build(const float *prim_bounds, const float *prim_areas, int64_t n,
+                      int max_prims_in_node, float *bounds, uint32_t *first_child,
+                      uint32_t *meta, float *areas, int32_t *ordered, int32_t *max_depth);
+
+/* ---- scene (Scene, Scene.hpp:15-41) ------------------------------------ */
+int prr_scene_create(prr_scene **out);
+int prr_scene_destroy(prr_scene *scene);
+/* params: baseColor[3], roughness, metallic, ior, emission[3]
+ * (Material fields, Material.hpp:40-44). */
+int prr_scene_add_material(prr_scene *scene, int kind, const float params[9], int *out_id);
+/* MeshTriangle(tris, bounds, mat) (Triangle.hpp:116-124) + Scene::Add:
+ * verts = ntri x 9 host floats (v0, v1, v2). The mesh gets its own BVH with
+ * maxPrimsInNode 4 (Triangle.hpp:173-179). */
+int prr_scene_add_mesh(prr_scene *scene, const float *verts, int64_t ntri, int material,
+                       int *out_object);
+/* Sphere(center, radius, mat) (Sphere.hpp:14-16) + Scene::Add. */
+int prr_scene_add_sphere(prr_scene *scene, const float center[3], float radius, int material,
+                         int *out_object);
+/* Scene::backgroundColor (Scene.hpp:17). */
+int prr_scene_set_background(prr_scene *scene, const float rgb[3]);
+/* EnvMap pixels (EnvMap.hpp:35-56 after decoding): w*h*3 host floats. */
+int prr_scene_set_env(prr_scene *scene, const float *rgb, int width, int height);
+/* Camera::init(width, height) (Camera.hpp:43-56). */
+int prr_scene_set_camera(prr_scene *scene, const prr_camera *camera, int width, int height);
+/* Scene::buildBVH (Scene.cpp:15-27): per-mesh SAH BVHs, the scene BVH over
+ * objects (maxPrimsInNode 1), the emitter list, the env-map CDF (built on the
+ * device, EnvMap.hpp:189-224), and the upload of everything. */
+int prr_scene_build(prr_scene *scene, void *stream);
+int prr_scene_stats_get(const prr_scene *scene, prr_scene_stats *out);
+/* The reference-layout flattened tree of one mesh (object >= 0) or of the
+ * scene BVH (object == -1): BVHNode bounds/first_child/meta, nodeAreas and
+ * orderedPrims (BVH.hpp:34-67, :129-135). Any output may be NULL. Returns the
+ * node count, or a negative status. */
+int64_t prr_scene_export_nodes(const prr_scene *scene, int object, float *bounds,
+                               uint32_t *first_child, uint32_t *meta, float *areas,
+                               int32_t *ordered);
+
+/* ---- batch ray queries ------------------------------------------------- */
+/* BVHAccel::Intersect on one mesh's BVH (BVH.cpp:311-415, Triangle.hpp:46-64):
+ * out_id = input-order index of the closest triangle (-1 on a miss), out_t its
+ * fp32 distance (+inf on a miss). out_t64 (optional) re-solves the winner's t
+ * in fp64 from the input vertices (NaN on a miss). cfg may be NULL. */
+int prr_mesh_intersect(const prr_scene *scene, int object, const float *o, const float *d,
+                       int64_t n, int32_t *out_id, float *out_t, double *out_t64,
+                       const prr_trace_config *cfg, void *stream);
+/* The same with host buffers: copies in, traces, copies out, synchronises. */
+int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const float *d,
+                            int64_t n, int32_t *out_id, float *out_t, void *stream);
+/* BVHAccel::IntersectP on one mesh (BVH.cpp:421-473, Triangle.hpp:75-92):
+ * out_hit[i] = 1 if an occluder lies within tmax[i]. */
+int prr_mesh_occluded(const prr_scene *scene, int object, const float *o, const float *d,
+                      const float *tmax, int64_t n, uint8_t *out_hit, void *stream);
+/* Scene::intersect (Scene.cpp:29-31, BVH.cpp:359-369 over MeshTriangle and
+ * Sphere leaves): out_obj = object index (-1 miss), out_prim = triangle index
+ * within the mesh (0 for a sphere), out_t = tnear; out_geo (optional, n x 6) =
+ * hit coords and geometric normal as Intersection carries them. */
+int prr_scene_intersect(const prr_scene *scene, const float *o, const float *d, int64_t n,
+                        int32_t *out_obj, int32_t *out_prim, float *out_t, float *out_geo,
+                        void *stream);
+/* Scene::intersectP (Scene.cpp:33-35, BVH.cpp:421-473 over MeshTriangle /
+ * Sphere intersectT). */
+int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
+                       const float *tmax, int64_t n, uint8_t *out_hit, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PRR_H */

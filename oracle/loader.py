@@ -1,0 +1,475 @@
+"""Test infrastructure only: ctypes bindings to the oracle libraries.
+
+Two oracles live here:
+
+* ``ReferenceOracle`` -- the reference renderer's own C++ sources compiled in
+  place by ``oracle/Makefile`` into ``oracle/_ref/libprr_ref.so`` (IEEE flags,
+  the parity oracle) and ``libprr_ref_fast.so`` (the reference's shipped
+  ``-O3 -ffast-math`` flags, the timed CPU baseline), driven through
+  ``oracle/ref/harness.cpp``.
+* ``PortOracle`` -- the plain-C restatement ``oracle/prr_oracle.c``.
+
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use
+this module, always as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+PORT_LIB = HERE / "libprr_oracle.so"
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def build_port() -> Path:
+    """Compile the C restatement (gcc only; works on any host with the image)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "port"], check=True)
+    return PORT_LIB
+
+
+def build_reference(ref_root: str | None = None) -> bool:
+    """Compile the reference sources in place into oracle/_ref/ (needs the
+    reference tree, which exists only on the build host)."""
+    root = ref_root or os.environ.get("PRR_REFERENCE_ROOT", "/root/reference")
+    if not Path(root, "BVH.cpp").exists():
+        return False
+    subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", f"REF={root}"], check=True)
+    return True
+
+
+def reference_available(fast: bool = False) -> bool:
+    return (REF_DIR / ("libprr_ref_fast.so" if fast else "libprr_ref.so")).exists()
+
+
+class PortOracle:
+    """The C restatement (oracle/prr_oracle.c)."""
+
+    def __init__(self):
+        if not PORT_LIB.exists():
+            build_port()
+        L = C.CDLL(str(PORT_LIB))
+        L.prr_oracle_rng_stream.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, _f32p]
+        L.prr_oracle_bvh_build.restype = C.c_int64
+        L.prr_oracle_bvh_build.argtypes = [_f32p, _f32p, C.c_int64, C.c_int, _f32p, _u32p, _u32p,
+                                           _f32p, _i32p]
+        L.prr_oracle_triangle_prims.argtypes = [_f32p, C.c_int64, _f32p, _f32p]
+        L.prr_oracle_mesh_new.restype = C.c_void_p
+        L.prr_oracle_mesh_new.argtypes = [_f32p, C.c_int64]
+        L.prr_oracle_mesh_free.argtypes = [C.c_void_p]
+        L.prr_oracle_mesh_nodes.restype = C.c_int64
+        L.prr_oracle_mesh_nodes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]
+        L.prr_oracle_mesh_intersect.argtypes = [C.c_void_p, _f32p, _f32p, C.c_int64, _i32p, _f32p,
+                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.prr_oracle_mesh_occluded.argtypes = [C.c_void_p, _f32p, _f32p, _f32p, C.c_int64, _u8p,
+                                               C.c_int]
+        L.prr_oracle_tonemap.argtypes = [C.c_int, C.c_float, _f32p, C.c_int64, _f32p, _u8p]
+        L.prr_oracle_env_cdf.argtypes = [_f32p, C.c_int, C.c_int, _f32p, _f32p,
+                                         C.POINTER(C.c_float)]
+        L.prr_oracle_photon_estimate.argtypes = [_f32p, C.c_int64, C.c_float, _f32p, C.c_int64,
+                                                 _f32p, C.POINTER(C.c_int32)]
+        self.L = L
+
+    def rng_stream(self, seed, stream, index, n):
+        out = np.empty(n, np.float32)
+        self.L.prr_oracle_rng_stream(seed, stream, index, n, out)
+        return out
+
+    def mesh(self, verts):
+        return PortMesh(self, _c(verts, np.float32).reshape(-1, 9))
+
+    def tonemap(self, mapper, rgb, exposure=1.0):
+        rgb = _c(rgb, np.float32).reshape(-1, 3)
+        out = np.empty_like(rgb)
+        u8 = np.empty(rgb.shape, np.uint8)
+        self.L.prr_oracle_tonemap(mapper, exposure, rgb, len(rgb), out, u8)
+        return out, u8
+
+    def env_cdf(self, rgb):
+        rgb = _c(rgb, np.float32)
+        h, w = rgb.shape[:2]
+        cdf = np.empty(h * w, np.float32)
+        marg = np.empty(h, np.float32)
+        tot = C.c_float()
+        self.L.prr_oracle_env_cdf(rgb.reshape(-1), w, h, cdf, marg, C.byref(tot))
+        return cdf, marg, tot.value
+
+    def photon_estimate(self, rec, radius, q):
+        rec = _c(rec, np.float32).reshape(-1, 9)
+        q = _c(q, np.float32).reshape(-1, 3)
+        out = np.empty((len(q), 3), np.float32)
+        res = C.c_int32()
+        self.L.prr_oracle_photon_estimate(rec, len(rec), radius, q, len(q), out, C.byref(res))
+        return out, res.value
+
+
+class PortMesh:
+    def __init__(self, port: PortOracle, verts):
+        self.port = port
+        self.n = len(verts)
+        self.h = port.L.prr_oracle_mesh_new(verts, self.n)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.port.L.prr_oracle_mesh_free(self.h)
+            self.h = None
+
+    def nodes(self):
+        L = self.port.L
+        nn = L.prr_oracle_mesh_nodes(self.h, None, None, None, None, None)
+        b = np.empty((nn, 6), np.float32)
+        fc = np.empty(nn, np.uint32)
+        meta = np.empty(nn, np.uint32)
+        area = np.empty(nn, np.float32)
+        order = np.empty(self.n, np.int32)
+        L.prr_oracle_mesh_nodes(self.h, b.ctypes.data, fc.ctypes.data, meta.ctypes.data,
+                                area.ctypes.data, order.ctypes.data)
+        return dict(bounds=b, first_child=fc, meta=meta, area=area, ordered=order)
+
+    def intersect(self, o, d, threads=0, stats=False):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        n = len(o)
+        hid = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        t64 = np.empty(n, np.float64)
+        vis = np.empty(n, np.int32) if stats else None
+        tst = np.empty(n, np.int32) if stats else None
+        self.port.L.prr_oracle_mesh_intersect(
+            self.h, o, d, n, hid, t, t64.ctypes.data,
+            vis.ctypes.data if stats else None, tst.ctypes.data if stats else None,
+            threads or os.cpu_count())
+        if stats:
+            return hid, t, t64, vis, tst
+        return hid, t, t64
+
+    def occluded(self, o, d, tmax, threads=0):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        tmax = _c(tmax, np.float32).reshape(-1)
+        out = np.empty(len(o), np.uint8)
+        self.port.L.prr_oracle_mesh_occluded(self.h, o, d, tmax, len(o), out,
+                                             threads or os.cpu_count())
+        return out
+
+
+class ReferenceOracle:
+    """The reference's own code (oracle/_ref/libprr_ref*.so via harness.cpp)."""
+
+    def __init__(self, fast: bool = False):
+        path = REF_DIR / ("libprr_ref_fast.so" if fast else "libprr_ref.so")
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (oracle/Makefile ref)")
+        L = C.CDLL(str(path))
+        vp = C.c_void_p
+        L.prr_ref_rng_stream.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, _f32p]
+        L.prr_ref_max_threads.restype = C.c_int
+        L.prr_ref_mesh_new.restype = vp
+        L.prr_ref_mesh_new.argtypes = [_f32p, C.c_int64]
+        L.prr_ref_mesh_free.argtypes = [vp]
+        L.prr_ref_mesh_nodes.restype = C.c_int64
+        L.prr_ref_mesh_nodes.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.prr_ref_mesh_area.restype = C.c_float
+        L.prr_ref_mesh_area.argtypes = [vp, C.POINTER(C.c_float)]
+        L.prr_ref_mesh_intersect.argtypes = [vp, _f32p, _f32p, C.c_int64, _i32p, _f32p, vp, vp,
+                                             C.c_int]
+        L.prr_ref_mesh_occluded.argtypes = [vp, _f32p, _f32p, _f32p, C.c_int64, _u8p, C.c_int]
+        L.prr_ref_scene_new.restype = vp
+        L.prr_ref_scene_free.argtypes = [vp]
+        L.prr_ref_scene_add_material.restype = C.c_int
+        L.prr_ref_scene_add_material.argtypes = [vp, C.c_int, _f32p]
+        L.prr_ref_scene_add_mesh.restype = C.c_int
+        L.prr_ref_scene_add_mesh.argtypes = [vp, _f32p, C.c_int64, C.c_int]
+        L.prr_ref_scene_add_sphere.restype = C.c_int
+        L.prr_ref_scene_add_sphere.argtypes = [vp, _f32p, C.c_float, C.c_int]
+        L.prr_ref_scene_set_background.argtypes = [vp, _f32p]
+        L.prr_ref_scene_set_env.restype = C.c_int
+        L.prr_ref_scene_set_env.argtypes = [vp, _f32p, C.c_int, C.c_int, C.c_char_p]
+        L.prr_ref_scene_env_export.restype = C.c_int
+        L.prr_ref_scene_env_export.argtypes = [vp, vp, vp, vp, vp]
+        L.prr_ref_env_eval.argtypes = [vp, _f32p, C.c_int64, _f32p, _f32p]
+        L.prr_ref_env_importance.argtypes = [vp, C.c_uint64, C.c_int64, _f32p, _f32p]
+        L.prr_ref_scene_set_camera.argtypes = [vp, _f32p, _f32p, _f32p, C.c_float, C.c_float,
+                                               C.c_float, C.c_float, C.c_int, C.c_int]
+        L.prr_ref_scene_build.argtypes = [vp]
+        L.prr_ref_scene_tlas_nodes.restype = C.c_int64
+        L.prr_ref_scene_tlas_nodes.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.prr_ref_scene_object_nodes.restype = C.c_int64
+        L.prr_ref_scene_object_nodes.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
+        L.prr_ref_scene_emit_area.restype = C.c_float
+        L.prr_ref_scene_emit_area.argtypes = [vp]
+        L.prr_ref_scene_intersect.argtypes = [vp, _f32p, _f32p, C.c_int64, _i32p, _i32p, _f32p,
+                                              vp, C.c_int]
+        L.prr_ref_scene_occluded.argtypes = [vp, _f32p, _f32p, _f32p, C.c_int64, _u8p, C.c_int]
+        L.prr_ref_scene_sample_light.argtypes = [vp, C.c_uint64, C.c_int64, _f32p, _f32p, _f32p]
+        L.prr_ref_render.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                     C.c_int, C.c_int, C.c_int, C.c_int, _f32p, vp, C.c_int]
+        L.prr_ref_cast_samples.argtypes = [vp, C.c_int, C.c_uint64, _i32p, _i32p, _i32p,
+                                           C.c_int64, _f32p, vp, C.c_int]
+        L.prr_ref_camera_rays.argtypes = [vp, _i32p, _i32p, _f32p, _f32p, C.c_int64, _f32p, _f32p]
+        L.prr_ref_tonemap.argtypes = [C.c_int, C.c_float, _f32p, C.c_int64, _f32p, _u8p]
+        L.prr_ref_photon_emit.restype = vp
+        L.prr_ref_photon_emit.argtypes = [vp, C.c_int64, C.c_uint64, C.c_int, C.c_int]
+        L.prr_ref_photon_export.restype = C.c_int64
+        L.prr_ref_photon_export.argtypes = [vp, vp, vp]
+        L.prr_ref_photon_free.argtypes = [vp]
+        L.prr_ref_photon_estimate.argtypes = [_f32p, C.c_int64, C.c_float, _f32p, C.c_int64,
+                                              _f32p, C.POINTER(C.c_int32), C.c_int]
+        self.L = L
+        self.fast = fast
+
+    def max_threads(self):
+        return self.L.prr_ref_max_threads()
+
+    def rng_stream(self, seed, stream, index, n):
+        out = np.empty(n, np.float32)
+        self.L.prr_ref_rng_stream(seed, stream, index, n, out)
+        return out
+
+    def mesh(self, verts):
+        return RefMesh(self, _c(verts, np.float32).reshape(-1, 9))
+
+    def scene(self, desc):
+        return RefScene(self, desc)
+
+    def tonemap(self, mapper, rgb, exposure=1.0):
+        rgb = _c(rgb, np.float32).reshape(-1, 3)
+        out = np.empty_like(rgb)
+        u8 = np.empty(rgb.shape, np.uint8)
+        self.L.prr_ref_tonemap(mapper, exposure, rgb, len(rgb), out, u8)
+        return out, u8
+
+    def photon_estimate(self, rec, radius, q, threads=0):
+        rec = _c(rec, np.float32).reshape(-1, 9)
+        q = _c(q, np.float32).reshape(-1, 3)
+        out = np.empty((len(q), 3), np.float32)
+        res = C.c_int32()
+        self.L.prr_ref_photon_estimate(rec, len(rec), radius, q, len(q), out, C.byref(res),
+                                       threads)
+        return out, res.value
+
+
+class RefMesh:
+    def __init__(self, ref: ReferenceOracle, verts):
+        self.ref = ref
+        self.n = len(verts)
+        self.h = ref.L.prr_ref_mesh_new(verts, self.n)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.L.prr_ref_mesh_free(self.h)
+            self.h = None
+
+    def nodes(self):
+        L = self.ref.L
+        nn = L.prr_ref_mesh_nodes(self.h, None, None, None, None, None)
+        b = np.empty((nn, 6), np.float32)
+        fc = np.empty(nn, np.uint32)
+        meta = np.empty(nn, np.uint32)
+        area = np.empty(nn, np.float32)
+        order = np.empty(self.n, np.int32)
+        L.prr_ref_mesh_nodes(self.h, b.ctypes.data, fc.ctypes.data, meta.ctypes.data,
+                             area.ctypes.data, order.ctypes.data)
+        return dict(bounds=b, first_child=fc, meta=meta, area=area, ordered=order)
+
+    def areas(self):
+        tot = C.c_float()
+        a = self.ref.L.prr_ref_mesh_area(self.h, C.byref(tot))
+        return a, tot.value
+
+    def intersect(self, o, d, threads=0, uv=False):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        n = len(o)
+        hid = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        u = np.empty(n, np.float32) if uv else None
+        v = np.empty(n, np.float32) if uv else None
+        self.ref.L.prr_ref_mesh_intersect(self.h, o, d, n, hid, t,
+                                          u.ctypes.data if uv else None,
+                                          v.ctypes.data if uv else None, threads)
+        return (hid, t, u, v) if uv else (hid, t)
+
+    def occluded(self, o, d, tmax, threads=0):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        tmax = _c(tmax, np.float32).reshape(-1)
+        out = np.empty(len(o), np.uint8)
+        self.ref.L.prr_ref_mesh_occluded(self.h, o, d, tmax, len(o), out, threads)
+        return out
+
+
+class RefScene:
+    """A reference Scene built from a photorealisticrender4610_b200 SceneDesc."""
+
+    def __init__(self, ref: ReferenceOracle, desc, env_tmp: str | None = None):
+        L = ref.L
+        self.ref = ref
+        self.desc = desc
+        self.h = L.prr_ref_scene_new()
+        for m in desc.materials:
+            L.prr_ref_scene_add_material(self.h, int(m.kind), _c(m.params(), np.float32))
+        for obj in desc.objects:
+            if obj.kind == "mesh":
+                v = _c(obj.verts, np.float32).reshape(-1, 9)
+                L.prr_ref_scene_add_mesh(self.h, v, len(v), obj.material)
+            else:
+                L.prr_ref_scene_add_sphere(self.h, _c(obj.center, np.float32), float(obj.radius),
+                                           obj.material)
+        L.prr_ref_scene_set_background(self.h, _c(desc.background, np.float32))
+        if desc.env is not None:
+            import tempfile
+            fd, path = tempfile.mkstemp(suffix=".hdr")
+            os.close(fd)
+            try:
+                env = _c(desc.env, np.float32)
+                rc = L.prr_ref_scene_set_env(self.h, env.reshape(-1), env.shape[1], env.shape[0],
+                                             path.encode())
+                if rc != 0:
+                    raise RuntimeError(f"reference EnvMap::load failed ({rc})")
+            finally:
+                os.unlink(path)
+        cam = desc.camera
+        L.prr_ref_scene_set_camera(self.h, _c(cam.eye, np.float32), _c(cam.target, np.float32),
+                                   _c(cam.up, np.float32), cam.fovv, cam.fovh, cam.aperture,
+                                   cam.focus_distance, desc.width, desc.height)
+        L.prr_ref_scene_build(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.L.prr_ref_scene_free(self.h)
+            self.h = None
+
+    def env_export(self):
+        e = self.desc.env
+        h, w = e.shape[:2]
+        px = np.empty((h, w, 3), np.float32)
+        cdf = np.empty(h * w, np.float32)
+        marg = np.empty(h, np.float32)
+        tot = np.empty(1, np.float32)
+        self.ref.L.prr_ref_scene_env_export(self.h, px.ctypes.data, cdf.ctypes.data,
+                                            marg.ctypes.data, tot.ctypes.data)
+        return px, cdf, marg, float(tot[0])
+
+    def env_eval(self, dirs):
+        dirs = _c(dirs, np.float32).reshape(-1, 3)
+        rgb = np.empty_like(dirs)
+        pdf = np.empty(len(dirs), np.float32)
+        self.ref.L.prr_ref_env_eval(self.h, dirs, len(dirs), rgb, pdf)
+        return rgb, pdf
+
+    def env_importance(self, seed, n):
+        dirs = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.ref.L.prr_ref_env_importance(self.h, seed, n, dirs, pdf)
+        return dirs, pdf
+
+    def nodes(self, obj=-1):
+        L = self.ref.L
+        if obj < 0:
+            nn = L.prr_ref_scene_tlas_nodes(self.h, None, None, None, None, None)
+            nprim = len(self.desc.objects)
+        else:
+            nn = L.prr_ref_scene_object_nodes(self.h, obj, None, None, None, None, None)
+            nprim = len(self.desc.objects[obj].verts)
+        b = np.empty((nn, 6), np.float32)
+        fc = np.empty(nn, np.uint32)
+        meta = np.empty(nn, np.uint32)
+        area = np.empty(nn, np.float32)
+        order = np.empty(nprim, np.int32)
+        if obj < 0:
+            L.prr_ref_scene_tlas_nodes(self.h, b.ctypes.data, fc.ctypes.data, meta.ctypes.data,
+                                       area.ctypes.data, order.ctypes.data)
+        else:
+            L.prr_ref_scene_object_nodes(self.h, obj, b.ctypes.data, fc.ctypes.data,
+                                         meta.ctypes.data, area.ctypes.data, order.ctypes.data)
+        return dict(bounds=b, first_child=fc, meta=meta, area=area, ordered=order)
+
+    def emit_area(self):
+        return self.ref.L.prr_ref_scene_emit_area(self.h)
+
+    def intersect(self, o, d, threads=0, geo=False):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        n = len(o)
+        obj = np.empty(n, np.int32)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        g = np.zeros((n, 6), np.float32) if geo else None
+        self.ref.L.prr_ref_scene_intersect(self.h, o, d, n, obj, prim, t,
+                                           g.ctypes.data if geo else None, threads)
+        return (obj, prim, t, g) if geo else (obj, prim, t)
+
+    def occluded(self, o, d, tmax, threads=0):
+        o = _c(o, np.float32).reshape(-1, 3)
+        d = _c(d, np.float32).reshape(-1, 3)
+        tmax = _c(tmax, np.float32).reshape(-1)
+        out = np.empty(len(o), np.uint8)
+        self.ref.L.prr_ref_scene_occluded(self.h, o, d, tmax, len(o), out, threads)
+        return out
+
+    def sample_light(self, seed, n):
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        pdf = np.empty(n, np.float32)
+        self.ref.L.prr_ref_scene_sample_light(self.h, seed, n, pos, nrm, pdf)
+        return pos, nrm, pdf
+
+    def render(self, max_depth, spp, seed, window=None, min_spp=None, threshold=0.05,
+               threads=0):
+        W, H = self.desc.width, self.desc.height
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        out = np.empty(((y1 - y0) * (x1 - x0), 3), np.float32)
+        cnt = np.empty((y1 - y0) * (x1 - x0), np.int32)
+        self.ref.L.prr_ref_render(self.h, max_depth, spp if min_spp is None else min_spp, spp,
+                                  threshold, seed, x0, y0, x1, y1, out, cnt.ctypes.data, threads)
+        return out.reshape(y1 - y0, x1 - x0, 3), cnt.reshape(y1 - y0, x1 - x0)
+
+    def cast_samples(self, max_depth, seed, px, py, sample, threads=0):
+        px = _c(px, np.int32)
+        py = _c(py, np.int32)
+        sample = _c(sample, np.int32)
+        n = len(px)
+        out = np.empty((n, 3), np.float32)
+        draws = np.empty(n, np.int32)
+        self.ref.L.prr_ref_cast_samples(self.h, max_depth, seed, px, py, sample, n, out,
+                                        draws.ctypes.data, threads)
+        return out, draws
+
+    def camera_rays(self, px, py, xo, yo):
+        px = _c(px, np.int32)
+        py = _c(py, np.int32)
+        xo = _c(xo, np.float32)
+        yo = _c(yo, np.float32)
+        n = len(px)
+        o = np.empty((n, 3), np.float32)
+        d = np.empty((n, 3), np.float32)
+        self.ref.L.prr_ref_camera_rays(self.h, px, py, xo, yo, n, o, d)
+        return o, d
+
+    def photon_emit(self, n_photons, seed, max_depth=30, threads=0):
+        L = self.ref.L
+        ph = L.prr_ref_photon_emit(self.h, n_photons, seed, max_depth, threads)
+        try:
+            n = L.prr_ref_photon_export(ph, None, None)
+            rec = np.empty((n, 9), np.float32)
+            owner = np.empty(n, np.int32)
+            L.prr_ref_photon_export(ph, rec.ctypes.data, owner.ctypes.data)
+        finally:
+            L.prr_ref_photon_free(ph)
+        return rec, owner

@@ -1,0 +1,757 @@
+// Test infrastructure only (the oracle): a C ABI over the reference renderer's
+// own C++ code, compiled in place from the reference sources by
+// oracle/Makefile. Tests and the CPU-baseline leg of bench.py load the
+// resulting oracle/_ref/libprr_ref*.so with ctypes; nothing in the product
+// links it.
+//
+// What it wraps (reference file:line):
+//   MeshTriangle(tris, bounds, mat)      Triangle.hpp:116-124 -> BVHAccel(ptrs, 4)
+//   BVHAccel::Intersect / IntersectP     BVH.cpp:311-415 / :421-473
+//   Scene::Add / buildBVH / intersect    Scene.hpp:15-41, Scene.cpp:15-35
+//   Camera::create / init / generateRay  Camera.hpp:23-56, :75-95
+//   Integrator::castRay                  Integrator.cpp:104-263
+//   Renderer per-pixel sample loop       Renderer.cpp:63-99 (restated below: the
+//                                        reference keeps the linear framebuffer
+//                                        local to Render and only writes 8-bit files)
+//   EnvMap::load / sample / importance*  EnvMap.hpp:35-169
+//   PhotonMap::emit / trace / build      Photon.cpp:96-188 (emit restated so that
+//                                        each photon draws from its own RNG stream)
+//   PhotonGrid / estimateIrradiance      Photon.cpp:24-94
+//   tonemap::apply + exposure            ToneMapping.hpp:267-279, Renderer.cpp:149-171
+//
+// Random numbers: prelude.hpp renames the reference's thread-local SplitMix64
+// (global.hpp:35-50) and routes every call site to get_random_float() below,
+// a SplitMix64 whose state is set per path from (seed, stream, index).
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cassert>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <numeric>
+#include <queue>
+#include <random>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+#include <omp.h>
+
+// Private members needed by the oracle: BVHAccel's flattened nodes (to diff
+// the device tree node for node) and PhotonMap::trace (to key each photon's RNG
+// stream by its index).
+#define private public
+#include "Camera.hpp"
+#include "EnvMap.hpp"
+#include "Integrator.hpp"
+#include "Material.hpp"
+#include "Renderer.hpp"
+#include "Scene.hpp"
+#include "Sphere.hpp"
+#include "ToneMapping.hpp"
+#include "Triangle.hpp"
+#undef private
+
+#include "stb_image_write.h"
+
+// ---------------------------------------------------------------------------
+// Counter-keyed SplitMix64 stream (the replacement for global.hpp:35-50).
+// path state = mix(mix(seed ^ K0) ^ (stream << 32 | index)); each draw adds
+// the golden gamma and returns the top 24 bits of the finalised value, the
+// same output form as the reference generator.
+// ---------------------------------------------------------------------------
+static inline uint64_t ref_mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+static inline uint64_t ref_path_state(uint64_t seed, uint32_t stream, uint32_t index) {
+    return ref_mix64(ref_mix64(seed ^ 0x6A09E667F3BCC909ULL) ^
+                     (((uint64_t) stream << 32) | (uint64_t) index));
+}
+
+static thread_local uint64_t g_rng_state = 0;
+static thread_local uint64_t g_rng_draws = 0;
+
+float get_random_float() {
+    uint64_t z = (g_rng_state += 0x9E3779B97F4A7C15ULL);
+    z = ref_mix64(z);
+    g_rng_draws++;
+    return (z >> 40) * 0x1p-24f;
+}
+
+static inline void ref_set_path(uint64_t seed, uint32_t stream, uint32_t index) {
+    g_rng_state = ref_path_state(seed, stream, index);
+    g_rng_draws = 0;
+}
+
+extern "C" {
+
+void prr_ref_rng_stream(uint64_t seed, uint32_t stream, uint32_t index, int n, float *out) {
+    ref_set_path(seed, stream, index);
+    for (int i = 0; i < n; i++)
+        out[i] = get_random_float();
+}
+
+int prr_ref_max_threads(void) {
+    return omp_get_max_threads();
+}
+
+// ---------------------------------------------------------------------------
+// Single mesh: MeshTriangle + its BVHAccel(maxPrimsInNode = 4).
+// ---------------------------------------------------------------------------
+struct RefMesh {
+    DiffuseMaterial mat;
+    MeshTriangle *mesh = nullptr;
+};
+
+static Bounds3 vertex_bounds(const float *v, int64_t ntri) {
+    // Same bounds the OBJ constructor computes (Triangle.cpp:12-30).
+    Vector3f minVert(std::numeric_limits<float>::infinity());
+    Vector3f maxVert(-std::numeric_limits<float>::infinity());
+    for (int64_t i = 0; i < ntri * 3; i++) {
+        Vector3f p(v[i * 3 + 0], v[i * 3 + 1], v[i * 3 + 2]);
+        minVert = Vector3f(std::min(minVert.x, p.x), std::min(minVert.y, p.y),
+                           std::min(minVert.z, p.z));
+        maxVert = Vector3f(std::max(maxVert.x, p.x), std::max(maxVert.y, p.y),
+                           std::max(maxVert.z, p.z));
+    }
+    return Bounds3(minVert, maxVert);
+}
+
+static std::vector<Triangle> make_tris(const float *v, int64_t ntri, Material *m) {
+    std::vector<Triangle> tris;
+    tris.reserve(ntri);
+    for (int64_t i = 0; i < ntri; i++) {
+        const float *p = v + i * 9;
+        tris.emplace_back(Vector3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]),
+                          Vector3f(p[6], p[7], p[8]), m);
+    }
+    return tris;
+}
+
+void *prr_ref_mesh_new(const float *verts, int64_t ntri) {
+    RefMesh *rm = new RefMesh();
+    rm->mesh = new MeshTriangle(make_tris(verts, ntri, &rm->mat), vertex_bounds(verts, ntri),
+                                &rm->mat);
+    return rm;
+}
+
+void prr_ref_mesh_free(void *h) {
+    RefMesh *rm = (RefMesh *) h;
+    if (!rm)
+        return;
+    delete rm->mesh->bvh;
+    delete rm->mesh;
+    delete rm;
+}
+
+static int64_t export_bvh(const BVHAccel *bvh, const Object *first_prim, size_t prim_size,
+                          float *bounds, uint32_t *first_child, uint32_t *meta, float *areas,
+                          int32_t *ordered) {
+    int64_t n = (int64_t) bvh->nodes.size();
+    for (int64_t i = 0; i < n; i++) {
+        const BVHNode &nd = bvh->nodes[i];
+        if (bounds)
+            for (int k = 0; k < 6; k++)
+                bounds[i * 6 + k] = nd.bounds[k];
+        if (first_child)
+            first_child[i] = nd.first_child;
+        if (meta)
+            meta[i] = nd.meta;
+        if (areas)
+            areas[i] = bvh->nodeAreas[i];
+    }
+    if (ordered)
+        for (size_t i = 0; i < bvh->orderedPrims.size(); i++)
+            ordered[i] = (int32_t) (((const char *) bvh->orderedPrims[i] -
+                                     (const char *) first_prim) /
+                                    (ptrdiff_t) prim_size);
+    return n;
+}
+
+int64_t prr_ref_mesh_nodes(void *h, float *bounds, uint32_t *first_child, uint32_t *meta,
+                           float *areas, int32_t *ordered) {
+    RefMesh *rm = (RefMesh *) h;
+    return export_bvh(rm->mesh->bvh, &rm->mesh->triangles[0], sizeof(Triangle), bounds,
+                      first_child, meta, areas, ordered);
+}
+
+float prr_ref_mesh_area(void *h, float *bvh_total_area) {
+    RefMesh *rm = (RefMesh *) h;
+    if (bvh_total_area)
+        *bvh_total_area = rm->mesh->bvh->totalArea;
+    return rm->mesh->area;
+}
+
+// Closest hit through BVHAccel::Intersect on the mesh BVH (the config-2
+// micro-path). id = index of the hit triangle in input order, -1 on a miss.
+void prr_ref_mesh_intersect(void *h, const float *o, const float *d, int64_t n, int32_t *id,
+                            float *t, float *u, float *v, int nthreads) {
+    RefMesh *rm = (RefMesh *) h;
+    const Triangle *base = &rm->mesh->triangles[0];
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; i++) {
+        Ray ray(Vector3f(o[i * 3], o[i * 3 + 1], o[i * 3 + 2]),
+                Vector3f(d[i * 3], d[i * 3 + 1], d[i * 3 + 2]));
+        Intersection in = rm->mesh->bvh->Intersect(ray);
+        if (in.happened) {
+            id[i] = (int32_t) ((const Triangle *) in.obj - base);
+            t[i] = (float) in.tnear;
+            if (u || v) {
+                // finalize() keeps only the interpolated uv; recompute the
+                // barycentrics of the winning triangle with its own hitTest.
+                Triangle::TriHit hh = ((const Triangle *) in.obj)->hitTest(ray);
+                if (u)
+                    u[i] = hh.u;
+                if (v)
+                    v[i] = hh.v;
+            }
+        } else {
+            id[i] = -1;
+            t[i] = std::numeric_limits<float>::infinity();
+            if (u)
+                u[i] = 0.f;
+            if (v)
+                v[i] = 0.f;
+        }
+    }
+}
+
+void prr_ref_mesh_occluded(void *h, const float *o, const float *d, const float *tmax, int64_t n,
+                           uint8_t *hit, int nthreads) {
+    RefMesh *rm = (RefMesh *) h;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; i++) {
+        Ray ray(Vector3f(o[i * 3], o[i * 3 + 1], o[i * 3 + 2]),
+                Vector3f(d[i * 3], d[i * 3 + 1], d[i * 3 + 2]));
+        hit[i] = rm->mesh->bvh->IntersectP(ray, tmax[i]) ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scene: materials, meshes, spheres, env map, camera.
+// ---------------------------------------------------------------------------
+enum { REF_MAT_DIFFUSE = 0, REF_MAT_EMISSIVE = 1, REF_MAT_MIRROR = 2, REF_MAT_GLASS = 3 };
+
+struct RefScene {
+    Scene scene;
+    std::vector<Material *> materials;
+    std::vector<Object *> objects;
+    std::vector<int> object_kind; // 0 mesh, 1 sphere
+    int width = 0, height = 0;
+};
+
+void *prr_ref_scene_new(void) {
+    return new RefScene();
+}
+
+void prr_ref_scene_free(void *h) {
+    RefScene *rs = (RefScene *) h;
+    if (!rs)
+        return;
+    for (size_t i = 0; i < rs->objects.size(); i++) {
+        if (rs->object_kind[i] == 0) {
+            MeshTriangle *m = (MeshTriangle *) rs->objects[i];
+            delete m->bvh;
+            delete m;
+        } else {
+            delete (Sphere *) rs->objects[i];
+        }
+    }
+    for (auto *m : rs->materials)
+        delete m;
+    delete rs->scene.bvh;
+    delete rs;
+}
+
+// params: baseColor[3], roughness, metallic, ior, emission[3]
+int prr_ref_scene_add_material(void *h, int type, const float *p) {
+    RefScene *rs = (RefScene *) h;
+    Material *m = nullptr;
+    switch (type) {
+    case REF_MAT_DIFFUSE:
+        m = new DiffuseMaterial();
+        break;
+    case REF_MAT_EMISSIVE:
+        m = new EmissiveMaterial();
+        break;
+    case REF_MAT_MIRROR:
+        m = new MirrorMaterial();
+        break;
+    case REF_MAT_GLASS:
+        m = new GlassMaterial();
+        break;
+    default:
+        return -1;
+    }
+    m->baseColor = Vector3f(p[0], p[1], p[2]);
+    m->roughness = p[3];
+    m->metallic = p[4];
+    m->ior = p[5];
+    m->m_emission = Vector3f(p[6], p[7], p[8]);
+    rs->materials.push_back(m);
+    return (int) rs->materials.size() - 1;
+}
+
+int prr_ref_scene_add_mesh(void *h, const float *verts, int64_t ntri, int mat) {
+    RefScene *rs = (RefScene *) h;
+    Material *m = rs->materials.at(mat);
+    MeshTriangle *mesh = new MeshTriangle(make_tris(verts, ntri, m), vertex_bounds(verts, ntri), m);
+    rs->scene.Add(mesh);
+    rs->objects.push_back(mesh);
+    rs->object_kind.push_back(0);
+    return (int) rs->objects.size() - 1;
+}
+
+int prr_ref_scene_add_sphere(void *h, const float *c, float r, int mat) {
+    RefScene *rs = (RefScene *) h;
+    Sphere *s = new Sphere(Vector3f(c[0], c[1], c[2]), r, rs->materials.at(mat));
+    rs->scene.Add(s);
+    rs->objects.push_back(s);
+    rs->object_kind.push_back(1);
+    return (int) rs->objects.size() - 1;
+}
+
+void prr_ref_scene_set_background(void *h, const float *rgb) {
+    RefScene *rs = (RefScene *) h;
+    rs->scene.backgroundColor = Vector3f(rgb[0], rgb[1], rgb[2]);
+}
+
+// EnvMap can only be filled through load(path) (buildCDF is private,
+// EnvMap.hpp:189). Write the pixels as Radiance .hdr with the vendored stb
+// writer, then load them back through the reference's own loader.
+int prr_ref_scene_set_env(void *h, const float *rgb, int w, int hgt, const char *tmp_path) {
+    RefScene *rs = (RefScene *) h;
+    if (!stbi_write_hdr(tmp_path, w, hgt, 3, rgb))
+        return -1;
+    return rs->scene.envMap.load(tmp_path) ? 0 : -2;
+}
+
+int prr_ref_scene_env_export(void *h, float *pixels, float *cdf, float *marginal, float *total) {
+    RefScene *rs = (RefScene *) h;
+    const EnvMap &e = rs->scene.envMap;
+    if (!e.loaded)
+        return -1;
+    int64_t n = (int64_t) e.width * e.height;
+    if (pixels)
+        for (int64_t i = 0; i < n; i++) {
+            pixels[i * 3 + 0] = e.pixels[i].x;
+            pixels[i * 3 + 1] = e.pixels[i].y;
+            pixels[i * 3 + 2] = e.pixels[i].z;
+        }
+    if (cdf)
+        std::memcpy(cdf, e.cdf.data(), sizeof(float) * n);
+    if (marginal)
+        std::memcpy(marginal, e.marginalCdf.data(), sizeof(float) * e.height);
+    if (total)
+        *total = e.totalLuminance;
+    return 0;
+}
+
+// EnvMap lookups for unit parity: sample(dir) -> rgb, importanceSamplePdf(dir).
+void prr_ref_env_eval(void *h, const float *dirs, int64_t n, float *rgb, float *pdf) {
+    RefScene *rs = (RefScene *) h;
+    const EnvMap &e = rs->scene.envMap;
+    for (int64_t i = 0; i < n; i++) {
+        Vector3f d(dirs[i * 3], dirs[i * 3 + 1], dirs[i * 3 + 2]);
+        Vector3f c = e.sample(d);
+        rgb[i * 3 + 0] = c.x;
+        rgb[i * 3 + 1] = c.y;
+        rgb[i * 3 + 2] = c.z;
+        pdf[i] = e.importanceSamplePdf(d);
+    }
+}
+
+// EnvMap::importanceSample with the stream (seed, i, 0) per sample.
+void prr_ref_env_importance(void *h, uint64_t seed, int64_t n, float *dirs, float *pdf) {
+    RefScene *rs = (RefScene *) h;
+    const EnvMap &e = rs->scene.envMap;
+    for (int64_t i = 0; i < n; i++) {
+        ref_set_path(seed, (uint32_t) i, 0u);
+        float p;
+        Vector3f d = e.importanceSample(p);
+        dirs[i * 3 + 0] = d.x;
+        dirs[i * 3 + 1] = d.y;
+        dirs[i * 3 + 2] = d.z;
+        pdf[i] = p;
+    }
+}
+
+void prr_ref_scene_set_camera(void *h, const float *eye, const float *target, const float *up,
+                              float fovv, float fovh, float aperture, float focus, int W, int H) {
+    RefScene *rs = (RefScene *) h;
+    Camera c = Camera::create(Vector3f(eye[0], eye[1], eye[2]),
+                              Vector3f(target[0], target[1], target[2]),
+                              Vector3f(up[0], up[1], up[2]), fovv, fovh);
+    c.aperture = aperture;
+    c.focusDistance = focus;
+    rs->scene.camera = c;
+    rs->scene.camera.init(W, H);
+    rs->width = W;
+    rs->height = H;
+}
+
+void prr_ref_scene_build(void *h) {
+    RefScene *rs = (RefScene *) h;
+    rs->scene.buildBVH();
+}
+
+int64_t prr_ref_scene_tlas_nodes(void *h, float *bounds, uint32_t *first_child, uint32_t *meta,
+                                 float *areas, int32_t *ordered) {
+    RefScene *rs = (RefScene *) h;
+    const BVHAccel *bvh = rs->scene.bvh;
+    int64_t n = export_bvh(bvh, nullptr, 1, bounds, first_child, meta, areas, nullptr);
+    if (ordered)
+        for (size_t i = 0; i < bvh->orderedPrims.size(); i++) {
+            int idx = -1;
+            for (size_t k = 0; k < rs->objects.size(); k++)
+                if (rs->objects[k] == bvh->orderedPrims[i])
+                    idx = (int) k;
+            ordered[i] = idx;
+        }
+    return n;
+}
+
+int64_t prr_ref_scene_object_nodes(void *h, int obj, float *bounds, uint32_t *first_child,
+                                   uint32_t *meta, float *areas, int32_t *ordered) {
+    RefScene *rs = (RefScene *) h;
+    if (rs->object_kind.at(obj) != 0)
+        return -1;
+    MeshTriangle *m = (MeshTriangle *) rs->objects[obj];
+    return export_bvh(m->bvh, &m->triangles[0], sizeof(Triangle), bounds, first_child, meta,
+                      areas, ordered);
+}
+
+float prr_ref_scene_emit_area(void *h) {
+    return ((RefScene *) h)->scene.totalEmitArea;
+}
+
+// Map an Intersection back to (object index, triangle index in that mesh).
+static void locate_hit(const RefScene *rs, const Intersection &in, int32_t *obj, int32_t *prim) {
+    *obj = -1;
+    *prim = -1;
+    for (size_t k = 0; k < rs->objects.size(); k++) {
+        if (rs->object_kind[k] == 1) {
+            if (in.obj == rs->objects[k]) {
+                *obj = (int32_t) k;
+                *prim = 0;
+                return;
+            }
+        } else {
+            const MeshTriangle *m = (const MeshTriangle *) rs->objects[k];
+            const Triangle *b = &m->triangles[0];
+            const Triangle *e = b + m->triangles.size();
+            const Triangle *t = (const Triangle *) in.obj;
+            if (t >= b && t < e) {
+                *obj = (int32_t) k;
+                *prim = (int32_t) (t - b);
+                return;
+            }
+        }
+    }
+}
+
+// Scene::intersect (two-level: scene BVH over objects, mesh BVHs below).
+// geo[i*6..] = hit coords and normal.
+void prr_ref_scene_intersect(void *h, const float *o, const float *d, int64_t n, int32_t *obj,
+                             int32_t *prim, float *t, float *geo, int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; i++) {
+        Ray ray(Vector3f(o[i * 3], o[i * 3 + 1], o[i * 3 + 2]),
+                Vector3f(d[i * 3], d[i * 3 + 1], d[i * 3 + 2]));
+        Intersection in = rs->scene.intersect(ray);
+        if (in.happened) {
+            locate_hit(rs, in, &obj[i], &prim[i]);
+            t[i] = (float) in.tnear;
+            if (geo) {
+                geo[i * 6 + 0] = in.coords.x;
+                geo[i * 6 + 1] = in.coords.y;
+                geo[i * 6 + 2] = in.coords.z;
+                geo[i * 6 + 3] = in.normal.x;
+                geo[i * 6 + 4] = in.normal.y;
+                geo[i * 6 + 5] = in.normal.z;
+            }
+        } else {
+            obj[i] = -1;
+            prim[i] = -1;
+            t[i] = std::numeric_limits<float>::infinity();
+        }
+    }
+}
+
+void prr_ref_scene_occluded(void *h, const float *o, const float *d, const float *tmax, int64_t n,
+                            uint8_t *hit, int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; i++) {
+        Ray ray(Vector3f(o[i * 3], o[i * 3 + 1], o[i * 3 + 2]),
+                Vector3f(d[i * 3], d[i * 3 + 1], d[i * 3 + 2]));
+        hit[i] = rs->scene.intersectP(ray, tmax[i]) ? 1 : 0;
+    }
+}
+
+// Scene::sampleLight with stream (seed, i, 0) per sample: coords, normal, pdf.
+void prr_ref_scene_sample_light(void *h, uint64_t seed, int64_t n, float *pos, float *nrm,
+                                float *pdf) {
+    RefScene *rs = (RefScene *) h;
+    for (int64_t i = 0; i < n; i++) {
+        ref_set_path(seed, (uint32_t) i, 0u);
+        Intersection li;
+        float p = 0.f;
+        rs->scene.sampleLight(li, p);
+        pos[i * 3 + 0] = li.coords.x;
+        pos[i * 3 + 1] = li.coords.y;
+        pos[i * 3 + 2] = li.coords.z;
+        nrm[i * 3 + 0] = li.normal.x;
+        nrm[i * 3 + 1] = li.normal.y;
+        nrm[i * 3 + 2] = li.normal.z;
+        pdf[i] = p;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rendering: the Renderer.cpp:63-99 per-pixel loop, restated so the linear
+// framebuffer is returned. Pixel m = i + j*W draws from stream (seed, m, n)
+// for its n-th sample. Window [x0,x1) x [y0,y1); out is (y1-y0)*(x1-x0)*3.
+// min_spp == max_spp gives the fixed-spp mode; otherwise the Welford
+// confidence-interval stop of Renderer.cpp:88-95 applies.
+// ---------------------------------------------------------------------------
+void prr_ref_render(void *h, int max_depth, int min_spp, int max_spp, float threshold,
+                    uint64_t seed, int x0, int y0, int x1, int y1, float *out_rgb,
+                    int32_t *out_spp, int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    const int W = rs->width, H = rs->height;
+    Integrator integrator(rs->scene, max_depth, 0.8f);
+    const int ww = x1 - x0, wh = y1 - y0;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t q = 0; q < (int64_t) ww * wh; q++) {
+        int i = x0 + (int) (q % ww);
+        int j = y0 + (int) (q / ww);
+        int m = i + j * W;
+        Welford wR, wG, wB;
+        Vector3f acc(0.f);
+        int n = 0;
+        while (n < max_spp) {
+            ref_set_path(seed, (uint32_t) m, (uint32_t) n);
+            float xOffset = get_random_float();
+            float yOffset = get_random_float();
+            Ray ray = rs->scene.camera.generateRay(i, j, W, H, xOffset, yOffset);
+            Vector3f s = integrator.castRay(ray);
+            if (std::isnan(s.x) || std::isnan(s.y) || std::isnan(s.z))
+                s = Vector3f(0.f);
+            acc += s;
+            n++;
+            wR.update(s.x);
+            wG.update(s.y);
+            wB.update(s.z);
+            if (n >= min_spp) {
+                if (wR.ci() < threshold && wG.ci() < threshold && wB.ci() < threshold)
+                    break;
+            }
+        }
+        acc = acc / (float) n;
+        out_rgb[q * 3 + 0] = acc.x;
+        out_rgb[q * 3 + 1] = acc.y;
+        out_rgb[q * 3 + 2] = acc.z;
+        if (out_spp)
+            out_spp[q] = n;
+    }
+}
+
+// One path per (pixel, sample) pair: the radiance castRay returns and the
+// number of random numbers the path drew (for lockstep checks).
+void prr_ref_cast_samples(void *h, int max_depth, uint64_t seed, const int32_t *px,
+                          const int32_t *py, const int32_t *sample, int64_t n, float *out_rgb,
+                          int32_t *out_draws, int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    const int W = rs->width, H = rs->height;
+    Integrator integrator(rs->scene, max_depth, 0.8f);
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t k = 0; k < n; k++) {
+        int i = px[k], j = py[k];
+        ref_set_path(seed, (uint32_t) (i + j * W), (uint32_t) sample[k]);
+        float xOffset = get_random_float();
+        float yOffset = get_random_float();
+        Ray ray = rs->scene.camera.generateRay(i, j, W, H, xOffset, yOffset);
+        Vector3f s = integrator.castRay(ray);
+        if (std::isnan(s.x) || std::isnan(s.y) || std::isnan(s.z))
+            s = Vector3f(0.f);
+        out_rgb[k * 3 + 0] = s.x;
+        out_rgb[k * 3 + 1] = s.y;
+        out_rgb[k * 3 + 2] = s.z;
+        if (out_draws)
+            out_draws[k] = (int32_t) g_rng_draws;
+    }
+}
+
+// Camera::generateRay for (pixel, offsets): origin and direction.
+void prr_ref_camera_rays(void *h, const int32_t *px, const int32_t *py, const float *xo,
+                         const float *yo, int64_t n, float *o, float *d) {
+    RefScene *rs = (RefScene *) h;
+    for (int64_t k = 0; k < n; k++) {
+        Ray r = rs->scene.camera.generateRay(px[k], py[k], rs->width, rs->height, xo[k], yo[k]);
+        o[k * 3 + 0] = r.origin.x;
+        o[k * 3 + 1] = r.origin.y;
+        o[k * 3 + 2] = r.origin.z;
+        d[k * 3 + 0] = r.direction.x;
+        d[k * 3 + 1] = r.direction.y;
+        d[k * 3 + 2] = r.direction.z;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Display transform: exposure + sanitise (Renderer.cpp:149-161), operator
+// (ToneMapping.hpp:267-279), 8-bit quantise (Renderer.cpp:169-171).
+// mapper: 0 Raw, 1 Standard, 2 AgX, 3 PBRNeutral.
+// ---------------------------------------------------------------------------
+void prr_ref_tonemap(int mapper, float exposure, const float *in_rgb, int64_t n, float *out_rgb,
+                     uint8_t *out_u8) {
+    for (int64_t i = 0; i < n; i++) {
+        Vector3f c = Vector3f(in_rgb[i * 3], in_rgb[i * 3 + 1], in_rgb[i * 3 + 2]) * exposure;
+        if (!std::isfinite(c.x))
+            c.x = 0.f;
+        if (!std::isfinite(c.y))
+            c.y = 0.f;
+        if (!std::isfinite(c.z))
+            c.z = 0.f;
+        c.x = std::max(0.f, c.x);
+        c.y = std::max(0.f, c.y);
+        c.z = std::max(0.f, c.z);
+        Vector3f co = tonemap::apply((tonemap::ToneMapper) mapper, c);
+        if (out_rgb) {
+            out_rgb[i * 3 + 0] = co.x;
+            out_rgb[i * 3 + 1] = co.y;
+            out_rgb[i * 3 + 2] = co.z;
+        }
+        if (out_u8) {
+            out_u8[i * 3 + 0] = (unsigned char) (std::clamp(co.x, 0.f, 1.f) * 255.f + 0.5f);
+            out_u8[i * 3 + 1] = (unsigned char) (std::clamp(co.y, 0.f, 1.f) * 255.f + 0.5f);
+            out_u8[i * 3 + 2] = (unsigned char) (std::clamp(co.z, 0.f, 1.f) * 255.f + 0.5f);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Caustic photons. The emit loop of Photon.cpp:156-188 is restated so photon i
+// draws from stream (seed, i, 0xFFFFFFFF); each photon's stored records are
+// kept in trace order and concatenated in photon order, so the output order
+// is canonical (photon index, then depth). Returns the number of photons
+// stored; with out == nullptr only counts. Record layout (11 floats + 2 ints):
+// position[3], direction[3], power[3], and in the int arrays photon index and
+// the running record index within that photon.
+// ---------------------------------------------------------------------------
+struct RefPhotons {
+    std::vector<Photon> photons;
+    std::vector<int32_t> owner;
+};
+
+void *prr_ref_photon_emit(void *h, int64_t num_photons, uint64_t seed, int max_depth,
+                          int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    PhotonMap pm;
+    pm.maxDepth = max_depth;
+    std::vector<std::vector<Photon>> per(num_photons);
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 100)
+    for (int64_t i = 0; i < num_photons; i++) {
+        ref_set_path(seed, (uint32_t) i, 0xFFFFFFFFu);
+        Intersection lightPoint;
+        float light_pdf;
+        rs->scene.sampleLight(lightPoint, light_pdf);
+        float area = 1.0f / light_pdf;
+        Vector3f dir = sampleCosineHemisphere(lightPoint.normal);
+        Vector3f power = lightPoint.material->m_emission * area / num_photons;
+        Photon p;
+        p.position = lightPoint.coords + lightPoint.normal * EPSILON;
+        p.direction = dir;
+        p.power = power;
+        p.is_caustic = false;
+        pm.trace(p, 0, per[i], rs->scene);
+    }
+    RefPhotons *out = new RefPhotons();
+    for (int64_t i = 0; i < num_photons; i++)
+        for (auto &p : per[i]) {
+            out->photons.push_back(p);
+            out->owner.push_back((int32_t) i);
+        }
+    return out;
+}
+
+int64_t prr_ref_photon_export(void *ph, float *rec, int32_t *owner) {
+    RefPhotons *p = (RefPhotons *) ph;
+    int64_t n = (int64_t) p->photons.size();
+    if (rec)
+        for (int64_t i = 0; i < n; i++) {
+            const Photon &q = p->photons[i];
+            float *r = rec + i * 9;
+            r[0] = q.position.x;
+            r[1] = q.position.y;
+            r[2] = q.position.z;
+            r[3] = q.direction.x;
+            r[4] = q.direction.y;
+            r[5] = q.direction.z;
+            r[6] = q.power.x;
+            r[7] = q.power.y;
+            r[8] = q.power.z;
+        }
+    if (owner)
+        std::memcpy(owner, p->owner.data(), sizeof(int32_t) * n);
+    return n;
+}
+
+void prr_ref_photon_free(void *ph) {
+    delete (RefPhotons *) ph;
+}
+
+// PhotonGrid::build + PhotonMap::estimateIrradiance on a given photon array
+// (rec = n x 9 floats as above), radius r, at nq query points.
+void prr_ref_photon_estimate(const float *rec, int64_t n, float radius, const float *q,
+                             int64_t nq, float *out_rgb, int32_t *grid_res, int nthreads) {
+    PhotonMap pm;
+    pm.photon_radius = radius;
+    pm.caustic_map.resize(n);
+    for (int64_t i = 0; i < n; i++) {
+        const float *r = rec + i * 9;
+        pm.caustic_map[i].position = Vector3f(r[0], r[1], r[2]);
+        pm.caustic_map[i].direction = Vector3f(r[3], r[4], r[5]);
+        pm.caustic_map[i].power = Vector3f(r[6], r[7], r[8]);
+        pm.caustic_map[i].is_caustic = true;
+    }
+    pm.build();
+    if (grid_res)
+        *grid_res = pm.caustic_grid.resolution;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t k = 0; k < nq; k++) {
+        Vector3f e = pm.estimateIrradiance(Vector3f(q[k * 3], q[k * 3 + 1], q[k * 3 + 2]),
+                                           Vector3f(0, 1, 0));
+        out_rgb[k * 3 + 0] = e.x;
+        out_rgb[k * 3 + 1] = e.y;
+        out_rgb[k * 3 + 2] = e.z;
+    }
+}
+
+} // extern "C"

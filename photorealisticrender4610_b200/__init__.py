@@ -1,0 +1,10 @@
+"""B200-native (sm_100a) Monte Carlo path-tracing hot path of the
+PhotoRealisticRender4610 renderer: SAH-BVH traversal, the path integrator,
+environment-map importance sampling, caustic photons and tone mapping as
+hand-written CUDA behind a C ABI (include/prr.h), with a Python mirror of the
+reference's Scene / BVHAccel / Integrator / Renderer interface."""
+from ._lib import PrrError, header_symbols, load  # noqa: F401
+from . import scenes  # noqa: F401
+from .api import Scene  # noqa: F401
+
+__all__ = ["Scene", "PrrError", "load", "header_symbols", "scenes"]

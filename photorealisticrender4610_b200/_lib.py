@@ -1,0 +1,125 @@
+"""ctypes binding to libprr.so (the C ABI declared in include/prr.h).
+
+The library is built in-tree (``photorealisticrender4610_b200/build.py``).
+Loading fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libprr.so"
+HEADER_DIR = PKG.parent / "include"
+
+PRR_OK = 0
+ERRORS = {
+    -1: "PRR_ERR_INVALID_ARGUMENT", -2: "PRR_ERR_CUDA", -3: "PRR_ERR_OUT_OF_MEMORY",
+    -4: "PRR_ERR_NOT_BUILT", -5: "PRR_ERR_UNSUPPORTED", -6: "PRR_ERR_TIMEOUT",
+    -7: "PRR_ERR_BUDGET", -8: "PRR_ERR_INTERNAL",
+}
+
+
+class PrrError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class prr_camera(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3),
+                ("fovv", C.c_float), ("fovh", C.c_float), ("aperture", C.c_float),
+                ("focus_distance", C.c_float)]
+
+
+class prr_trace_config(C.Structure):
+    _fields_ = [("block_size", C.c_int), ("persistent", C.c_int), ("blocks_per_sm", C.c_int),
+                ("batch", C.c_int)]
+
+
+class prr_scene_stats(C.Structure):
+    _fields_ = [("n_objects", C.c_int64), ("n_triangles", C.c_int64), ("n_nodes", C.c_int64),
+                ("tlas_depth", C.c_int32), ("blas_depth", C.c_int32),
+                ("device_bytes", C.c_int64), ("total_emit_area", C.c_float)]
+
+
+class prr_render_settings(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("min_spp", C.c_int),
+                ("max_spp", C.c_int), ("max_depth", C.c_int), ("variance_threshold", C.c_float),
+                ("seed", C.c_uint64), ("mode", C.c_int), ("x0", C.c_int), ("y0", C.c_int),
+                ("x1", C.c_int), ("y1", C.c_int), ("sample_offset", C.c_int),
+                ("reserved", C.c_int * 3)]
+
+
+_vp = C.c_void_p
+_SIGS = {
+    "prr_abi_version": (C.c_int, []),
+    "prr_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "prr_bvh_build": (C.c_int64, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp, _vp, _vp, _vp,
+                                  C.POINTER(C.c_int32)]),
+    "prr_scene_create": (C.c_int, [C.POINTER(_vp)]),
+    "prr_scene_destroy": (C.c_int, [_vp]),
+    "prr_scene_add_material": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
+    "prr_scene_add_mesh": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, C.POINTER(C.c_int)]),
+    "prr_scene_add_sphere": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_float, C.c_int,
+                                       C.POINTER(C.c_int)]),
+    "prr_scene_set_background": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "prr_scene_set_env": (C.c_int, [_vp, _vp, C.c_int, C.c_int]),
+    "prr_scene_set_camera": (C.c_int, [_vp, C.POINTER(prr_camera), C.c_int, C.c_int]),
+    "prr_scene_build": (C.c_int, [_vp, _vp]),
+    "prr_scene_stats_get": (C.c_int, [_vp, C.POINTER(prr_scene_stats)]),
+    "prr_scene_export_nodes": (C.c_int64, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "prr_mesh_intersect": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int64, _vp, _vp, _vp,
+                                     C.POINTER(prr_trace_config), _vp]),
+    "prr_mesh_intersect_host": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int64, _vp, _vp, _vp]),
+    "prr_mesh_occluded": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
+    "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Every function declared in include/*.h."""
+    names = []
+    for h in sorted(HEADER_DIR.glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        names += re.findall(r"\b(prr_\w+)\s*\(", text)
+    seen = []
+    for n in names:
+        if n not in seen:
+            seen.append(n)
+    return seen
+
+
+def load() -> C.CDLL:
+    """Load libprr.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: run photorealisticrender4610_b200/build.py "
+                          "(nvcc, sm_100a). There is no CPU fallback.")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in _SIGS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    lib = load()
+    buf = C.create_string_buffer(1024)
+    lib.prr_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int) -> int:
+    if rc < 0:
+        raise PrrError(rc, last_error())
+    return rc

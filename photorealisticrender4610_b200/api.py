@@ -1,0 +1,213 @@
+"""Python mirror of the reference's host interface over libprr's C ABI.
+
+``Scene`` follows Scene (Scene.hpp:15-41): ``add_material`` / ``add_mesh`` /
+``add_sphere`` (MeshTriangle, Sphere + Scene::Add), ``set_env`` (EnvMap),
+``set_camera`` (Camera::init), ``buildBVH`` (Scene::buildBVH), and the batch
+forms of ``intersect`` / ``intersectP`` (Scene::intersect / intersectP) and of
+the mesh-level ``BVHAccel::Intersect`` / ``IntersectP``. Device arrays are torch
+CUDA tensors (torch supplies memory and streams only); ``*_host`` calls take
+numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, prr_camera, prr_scene_stats, prr_trace_config
+
+
+def _ptr(t):
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _f3(x):
+    return (C.c_float * 3)(*[float(v) for v in x])
+
+
+def _rays(o, d):
+    import torch
+    o = o.to(torch.float32).contiguous()
+    d = d.to(torch.float32).contiguous()
+    if not o.is_cuda or not d.is_cuda:
+        raise ValueError("device calls take CUDA tensors; use the *_host forms for host arrays")
+    if o.shape != d.shape or o.shape[-1] != 3:
+        raise ValueError("rays must be (n, 3) origins and directions")
+    return o.reshape(-1, 3), d.reshape(-1, 3)
+
+
+class Scene:
+    def __init__(self):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.prr_scene_create(C.byref(h)))
+        self.h = h
+        self.objects = []
+        self.desc = None
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.prr_scene_destroy(h)
+            self.h = None
+
+    # ---- construction ----
+    def add_material(self, kind: int, params) -> int:
+        p = (C.c_float * 9)(*[float(x) for x in params])
+        out = C.c_int()
+        check(self.lib.prr_scene_add_material(self.h, kind, p, C.byref(out)))
+        return out.value
+
+    def add_mesh(self, verts, material: int) -> int:
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 9)
+        out = C.c_int()
+        check(self.lib.prr_scene_add_mesh(self.h, C.c_void_p(v.ctypes.data), len(v), material,
+                                          C.byref(out)))
+        self.objects.append(("mesh", len(v)))
+        return out.value
+
+    def add_sphere(self, center, radius: float, material: int) -> int:
+        out = C.c_int()
+        check(self.lib.prr_scene_add_sphere(self.h, _f3(center), float(radius), material,
+                                            C.byref(out)))
+        self.objects.append(("sphere", 1))
+        return out.value
+
+    def set_background(self, rgb):
+        check(self.lib.prr_scene_set_background(self.h, _f3(rgb)))
+
+    def set_env(self, rgb):
+        e = np.ascontiguousarray(rgb, np.float32)
+        h, w = e.shape[:2]
+        check(self.lib.prr_scene_set_env(self.h, C.c_void_p(e.ctypes.data), w, h))
+
+    def set_camera(self, cam, width: int, height: int):
+        c = prr_camera()
+        c.eye[:] = list(map(float, cam.eye))
+        c.target[:] = list(map(float, cam.target))
+        c.up[:] = list(map(float, cam.up))
+        c.fovv = cam.fovv
+        c.fovh = cam.fovh
+        c.aperture = cam.aperture
+        c.focus_distance = cam.focus_distance
+        check(self.lib.prr_scene_set_camera(self.h, C.byref(c), width, height))
+
+    def buildBVH(self, stream=None):
+        check(self.lib.prr_scene_build(self.h, _stream(stream)))
+        return self
+
+    @classmethod
+    def from_desc(cls, desc, build: bool = True) -> "Scene":
+        s = cls()
+        s.desc = desc
+        for m in desc.materials:
+            s.add_material(int(m.kind), m.params())
+        for o in desc.objects:
+            if o.kind == "mesh":
+                s.add_mesh(o.verts, o.material)
+            else:
+                s.add_sphere(o.center, o.radius, o.material)
+        s.set_background(desc.background)
+        if desc.env is not None:
+            s.set_env(desc.env)
+        s.set_camera(desc.camera, desc.width, desc.height)
+        if build:
+            s.buildBVH()
+        return s
+
+    @classmethod
+    def single_mesh(cls, verts) -> "Scene":
+        """One MeshTriangle (its own BVHAccel(ptrs, 4)) and nothing else."""
+        s = cls()
+        m = s.add_material(0, [0.8, 0.8, 0.8, 0.5, 0.0, 1.5, 0.0, 0.0, 0.0])
+        s.add_mesh(verts, m)
+        return s.buildBVH()
+
+    # ---- inspection ----
+    def stats(self) -> dict:
+        st = prr_scene_stats()
+        check(self.lib.prr_scene_stats_get(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def export_nodes(self, obj: int = -1) -> dict:
+        n = check(self.lib.prr_scene_export_nodes(self.h, obj, None, None, None, None, None))
+        nprim = len(self.objects) if obj < 0 else self.objects[obj][1]
+        b = np.empty((n, 6), np.float32)
+        fc = np.empty(n, np.uint32)
+        meta = np.empty(n, np.uint32)
+        area = np.empty(n, np.float32)
+        order = np.empty(nprim, np.int32)
+        check(self.lib.prr_scene_export_nodes(self.h, obj, b.ctypes.data, fc.ctypes.data,
+                                              meta.ctypes.data, area.ctypes.data,
+                                              order.ctypes.data))
+        return dict(bounds=b, first_child=fc, meta=meta, area=area, ordered=order)
+
+    # ---- batch queries (device) ----
+    def mesh_intersect(self, obj: int, o, d, t64: bool = False, config: dict | None = None,
+                       stream=None):
+        """BVHAccel::Intersect on one mesh: (id int32, t float32[, t64 float64])."""
+        import torch
+        o, d = _rays(o, d)
+        n = o.shape[0]
+        hid = torch.empty(n, dtype=torch.int32, device=o.device)
+        t = torch.empty(n, dtype=torch.float32, device=o.device)
+        tt = torch.empty(n, dtype=torch.float64, device=o.device) if t64 else None
+        cfg = None
+        if config:
+            cfg = prr_trace_config(config.get("block_size", 0), config.get("persistent", 0),
+                                   config.get("blocks_per_sm", 0), config.get("batch", 0))
+        check(self.lib.prr_mesh_intersect(self.h, obj, _ptr(o), _ptr(d), n, _ptr(hid), _ptr(t),
+                                          _ptr(tt), C.byref(cfg) if cfg else None,
+                                          _stream(stream)))
+        return (hid, t, tt) if t64 else (hid, t)
+
+    def mesh_intersect_host(self, obj: int, o, d, out_id=None, out_t=None, stream=None):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = len(o)
+        hid = out_id if out_id is not None else np.empty(n, np.int32)
+        t = out_t if out_t is not None else np.empty(n, np.float32)
+        check(self.lib.prr_mesh_intersect_host(self.h, obj, C.c_void_p(o.ctypes.data),
+                                               C.c_void_p(d.ctypes.data), n,
+                                               C.c_void_p(hid.ctypes.data),
+                                               C.c_void_p(t.ctypes.data), _stream(stream)))
+        return hid, t
+
+    def mesh_occluded(self, obj: int, o, d, tmax, stream=None):
+        import torch
+        o, d = _rays(o, d)
+        tmax = tmax.to(torch.float32).contiguous()
+        out = torch.empty(o.shape[0], dtype=torch.uint8, device=o.device)
+        check(self.lib.prr_mesh_occluded(self.h, obj, _ptr(o), _ptr(d), _ptr(tmax), o.shape[0],
+                                         _ptr(out), _stream(stream)))
+        return out
+
+    def intersect(self, o, d, geo: bool = False, stream=None):
+        """Scene::intersect: (obj, prim, t[, geo (n,6)])."""
+        import torch
+        o, d = _rays(o, d)
+        n = o.shape[0]
+        obj = torch.empty(n, dtype=torch.int32, device=o.device)
+        prim = torch.empty(n, dtype=torch.int32, device=o.device)
+        t = torch.empty(n, dtype=torch.float32, device=o.device)
+        g = torch.empty((n, 6), dtype=torch.float32, device=o.device) if geo else None
+        check(self.lib.prr_scene_intersect(self.h, _ptr(o), _ptr(d), n, _ptr(obj), _ptr(prim),
+                                           _ptr(t), _ptr(g), _stream(stream)))
+        return (obj, prim, t, g) if geo else (obj, prim, t)
+
+    def intersectP(self, o, d, tmax, stream=None):
+        """Scene::intersectP: uint8 per ray."""
+        import torch
+        o, d = _rays(o, d)
+        tmax = tmax.to(torch.float32).contiguous()
+        out = torch.empty(o.shape[0], dtype=torch.uint8, device=o.device)
+        check(self.lib.prr_scene_occluded(self.h, _ptr(o), _ptr(d), _ptr(tmax), o.shape[0],
+                                          _ptr(out), _stream(stream)))
+        return out

@@ -1,0 +1,115 @@
+// Device-resident scene layout shared by the host builder and the kernels.
+//
+// BVH nodes. The reference flattens its SAH tree into 32-byte nodes and, at
+// every interior step, reads both children from two unrelated addresses
+// (left = idx+1, right = first_child; BVH.cpp:263-280, :370-373). Here each
+// interior node of that same tree becomes one 64-byte record holding the two
+// CHILD boxes, so one interior step is one aligned 64-byte fetch (two 32-byte
+// sectors) instead of two scattered 32-byte ones. Leaves need no record: a
+// child reference with the top bit set points straight at the leaf's first
+// triangle, and that triangle carries the leaf's primitive count.
+//
+// The slab test reads the same float bounds and does the same operations in
+// the same order as BVHAccel::nodeIntersect (BVH.hpp:115-124), so entry
+// distances, traversal order and tie-breaks are those of the reference tree.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define PRR_HD __host__ __device__
+#else
+#define PRR_HD
+#endif
+
+namespace prr {
+
+constexpr uint32_t kLeafBit = 0x80000000u;
+
+// One interior node: boxes of its left (reference idx+1) and right
+// (reference first_child) children, interleaved [minX,maxX,minY,maxY,minZ,maxZ]
+// like BVHNode::bounds, plus the child references.
+struct alignas(64) WNode {
+    float lb[6];        // left child bounds
+    float rb[6];        // right child bounds
+    uint32_t left;      // interior: WNode index; leaf: kLeafBit | first triangle
+    uint32_t right;
+    uint32_t axis;      // split axis of this node (IntersectP near-child choice, BVH.cpp:384-391)
+    float left_area;    // nodeAreas[idx+1] (light-sampling descent, BVH.cpp:488-496)
+};
+static_assert(sizeof(WNode) == 64, "WNode must be 64 bytes");
+
+// One triangle in leaf order (orderedPrims order): v0, e1 = v1-v0, e2 = v2-v0
+// exactly as Triangle's constructor computes them (Triangle.hpp:27-31).
+struct alignas(16) Tri {
+    float v0x, v0y, v0z, e1x;
+    float e1y, e1z, e2x, e2y;
+    float e2z;
+    int32_t id;         // index of the triangle in its mesh's input order
+    uint32_t leaf_count;// primitive count of the leaf this triangle starts (0 inside a leaf)
+    float area;         // Triangle::area (Triangle.hpp:31)
+};
+static_assert(sizeof(Tri) == 48, "Tri must be 48 bytes");
+
+enum ObjectKind : int32_t { kObjMesh = 0, kObjSphere = 1 };
+enum MaterialKind : int32_t { kMatDiffuse = 0, kMatEmissive = 1, kMatMirror = 2, kMatGlass = 3 };
+
+// Scene-level primitive (an entry of Scene::objects).
+struct alignas(16) DevObject {
+    int32_t kind;
+    int32_t material;
+    uint32_t root;      // mesh: root reference into nodes/tris
+    int32_t tri_base;   // mesh: first triangle (global index)
+    float root_box[6];  // own bounds (IntersectP tests the root box first)
+    float area;         // MeshTriangle::area or Sphere::area
+    float bvh_area;     // mesh: BVHAccel::totalArea (root->area)
+    float cx, cy, cz, radius, radius2;
+    int32_t ntri;
+    int32_t depth;      // max leaf depth of the mesh BVH (stack bound)
+    int32_t pad;
+};
+
+struct alignas(16) DevMaterial {
+    int32_t kind;
+    float base[3];
+    float roughness, metallic, ior;
+    float emission[3];
+    int32_t has_emission; // Material::hasEmission: |m_emission| > EPSILON
+    float pad[2];
+};
+
+struct DevCamera {
+    float eye[3], forward[3], right[3], up[3];
+    float focal_px;     // (W*0.5) / tan(halfFovH) (Camera.hpp:76)
+    float aperture, focus_distance;
+    int32_t width, height;
+};
+
+struct DevEnv {
+    const float4 *pixels; // rgb + pad, row-major
+    const float *cdf;     // width*height conditional CDFs
+    const float *marginal;// height
+    int32_t width, height;
+    float total;          // totalLuminance
+    int32_t loaded;
+};
+
+struct DevScene {
+    const WNode *nodes;
+    const Tri *tris;
+    const float *verts;   // original v0,v1,v2 per triangle, leaf order (sampling, fp64 re-solve)
+    const float *normals; // Triangle::normal per triangle, leaf order
+    const DevObject *objects;
+    const DevMaterial *materials;
+    const int32_t *emissives; // Scene::emissives, in object order
+    int32_t n_objects, n_materials, n_emissives;
+    float total_emit_area;
+    uint32_t tlas_root;
+    float tlas_box[6];
+    int32_t tlas_depth;
+    int32_t blas_depth;   // max over meshes
+    float background[3];
+    DevCamera camera;
+    DevEnv env;
+};
+
+} // namespace prr

@@ -1,0 +1,317 @@
+// Batch ray-query kernels: mesh closest hit / any hit (the BVHAccel::Intersect
+// and IntersectP micro-path, BVH.cpp:311-473) and scene-level closest hit /
+// any hit (Scene::intersect / intersectP, Scene.cpp:29-35).
+//
+// One thread traces one ray. Stacks are columns of a dynamic shared-memory
+// array sized from the tree depth measured at build time, so the stack bound is
+// proven rather than guessed (a push only happens at an interior node and at
+// most one entry per tree level is outstanding).
+//
+// Two launch shapes: a plain grid (one ray per thread) and a persistent grid
+// sized to the SM count in which each warp pulls 32-ray batches from a global
+// counter; the autotuner picks per scene.
+#include "prr_internal.h"
+#include "trace.cuh"
+
+#include <algorithm>
+
+namespace prr {
+
+namespace {
+
+__device__ __forceinline__ RayD load_ray(const float *__restrict__ O, const float *__restrict__ D,
+                                         int64_t i) {
+    RayD r;
+    r.ox = __ldg(O + i * 3 + 0);
+    r.oy = __ldg(O + i * 3 + 1);
+    r.oz = __ldg(O + i * 3 + 2);
+    r.dx = __ldg(D + i * 3 + 0);
+    r.dy = __ldg(D + i * 3 + 1);
+    r.dz = __ldg(D + i * 3 + 2);
+    return r;
+}
+
+// Möller-Trumbore in fp64 on the input vertices: the winner's t re-solved for
+// the 1e-6-relative check, once per ray.
+__device__ double tri_t64(const float *__restrict__ v, const RayD &r) {
+    const double v0x = v[0], v0y = v[1], v0z = v[2];
+    const double e1x = (double) v[3] - v0x, e1y = (double) v[4] - v0y, e1z = (double) v[5] - v0z;
+    const double e2x = (double) v[6] - v0x, e2y = (double) v[7] - v0y, e2z = (double) v[8] - v0z;
+    const double ox = r.ox, oy = r.oy, oz = r.oz, dx = r.dx, dy = r.dy, dz = r.dz;
+    const double tx = ox - v0x, ty = oy - v0y, tz = oz - v0z;
+    const double px = dy * e2z - dz * e2y, py = dz * e2x - dx * e2z, pz = dx * e2y - dy * e2x;
+    const double qx = ty * e1z - tz * e1y, qy = tz * e1x - tx * e1z, qz = tx * e1y - ty * e1x;
+    const double det = px * e1x + py * e1y + pz * e1z;
+    return (qx * e2x + qy * e2y + qz * e2z) / det;
+}
+
+struct MeshArgs {
+    const WNode *nodes;
+    const Tri *tris;
+    const float *verts;
+    uint32_t root;
+    const float *O, *D;
+    int64_t n;
+    int32_t *out_id;
+    float *out_t;
+    double *out_t64;
+    unsigned long long *counter;
+    int stack_stride;
+};
+
+__device__ __forceinline__ void mesh_closest_one(const MeshArgs &a, SmemStack &st, int64_t i) {
+    const RayD r = load_ray(a.O, a.D, i);
+    const RayPre p = precompute(r);
+    float t = kInf, u = 0.f, v = 0.f;
+    const int hit = blas_closest(a.nodes, a.tris, a.root, r, p, st, t, u, v);
+    a.out_id[i] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+    a.out_t[i] = t;
+    if (a.out_t64)
+        a.out_t64[i] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r) : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+__global__ void k_mesh_closest(MeshArgs a) {
+    extern __shared__ uint2 smem[];
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
+        mesh_closest_one(a, st, i);
+}
+
+// Persistent: each warp takes the next 32 rays from the counter until none
+// are left. The counter is zeroed on the stream before the launch.
+__global__ void k_mesh_closest_persistent(MeshArgs a) {
+    extern __shared__ uint2 smem[];
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0)
+            base = atomicAdd(a.counter, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((int64_t) base >= a.n)
+            break;
+        const int64_t i = (int64_t) base + lane;
+        if (i < a.n)
+            mesh_closest_one(a, st, i);
+    }
+}
+
+__global__ void k_mesh_occluded(const WNode *nodes, const Tri *tris, uint32_t root,
+                                DevObject obj, const float *O, const float *D,
+                                const float *__restrict__ tmax, int64_t n, uint8_t *out) {
+    extern __shared__ uint2 smem[];
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const RayD r = load_ray(O, D, i);
+        const RayPre p = precompute(r);
+        out[i] = blas_occluded(nodes, tris, root, obj.root_box, r, p, st, __ldg(tmax + i)) ? 1 : 0;
+    }
+}
+
+__global__ void k_scene_closest(DevScene S, const float *O, const float *D, int64_t n,
+                                int32_t *out_obj, int32_t *out_prim, float *out_t, float *geo,
+                                int tlas_cap) {
+    extern __shared__ uint2 smem[];
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const RayD r = load_ray(O, D, i);
+        const RayPre p = precompute(r);
+        const SceneHit h = scene_closest(S, r, p, tst, bst);
+        out_obj[i] = h.obj;
+        out_t[i] = h.t;
+        if (h.obj < 0) {
+            out_prim[i] = -1;
+            continue;
+        }
+        const DevObject &o = S.objects[h.obj];
+        // hit coords (Triangle.cpp:37 / Sphere.hpp:37): origin + direction * t
+        const float cx = r.ox + r.dx * h.t, cy = r.oy + r.dy * h.t, cz = r.oz + r.dz * h.t;
+        float nx, ny, nz;
+        if (o.kind == kObjMesh) {
+            out_prim[i] = __ldg(&S.tris[h.tri].id);
+            nx = S.normals[(size_t) h.tri * 3 + 0];
+            ny = S.normals[(size_t) h.tri * 3 + 1];
+            nz = S.normals[(size_t) h.tri * 3 + 2];
+        } else {
+            out_prim[i] = 0;
+            // normalize(coords - center) (Vector.hpp:103-111)
+            float x = cx - o.cx, y = cy - o.cy, z = cz - o.cz;
+            float m2 = x * x + y * y + z * z;
+            if (m2 > 0) {
+                float inv = 1 / sqrtf(m2);
+                x = x * inv;
+                y = y * inv;
+                z = z * inv;
+            }
+            nx = x;
+            ny = y;
+            nz = z;
+        }
+        if (geo) {
+            geo[i * 6 + 0] = cx;
+            geo[i * 6 + 1] = cy;
+            geo[i * 6 + 2] = cz;
+            geo[i * 6 + 3] = nx;
+            geo[i * 6 + 4] = ny;
+            geo[i * 6 + 5] = nz;
+        }
+    }
+}
+
+__global__ void k_scene_occluded(DevScene S, const float *O, const float *D,
+                                 const float *__restrict__ tmax, int64_t n, uint8_t *out,
+                                 int tlas_cap) {
+    extern __shared__ uint2 smem[];
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const RayD r = load_ray(O, D, i);
+        const RayPre p = precompute(r);
+        out[i] = scene_occluded(S, r, p, tst, bst, __ldg(tmax + i)) ? 1 : 0;
+    }
+}
+
+int stack_cap(int depth) {
+    // entries outstanding <= deepest leaf depth; keep one spare slot
+    return std::max(1, depth + 1);
+}
+
+int grid_for(int64_t n, int block) {
+    const int64_t g = (n + block - 1) / block;
+    const int64_t cap = (int64_t) device_sm_count() * 64;
+    return (int) std::max<int64_t>(1, std::min(g, cap));
+}
+
+int set_smem(const void *fn, size_t bytes) {
+    if (bytes > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int) bytes);
+        if (e != cudaSuccess)
+            return fail(PRR_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    }
+    return PRR_OK;
+}
+
+} // namespace
+
+int device_sm_count() {
+    static int sms = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        return v;
+    }();
+    return sms;
+}
+
+int launch_mesh_closest(const Scene &s, int object, const float *o, const float *d, int64_t n,
+                        int32_t *id, float *t, double *t64, unsigned *counter,
+                        const prr_trace_config *cfg, cudaStream_t st) {
+    if (n == 0)
+        return PRR_OK;
+    const HostObject &obj = s.objects[object];
+    const DevObject *dobj = nullptr;
+    (void) dobj;
+    MeshArgs a;
+    a.nodes = s.dev.nodes;
+    a.tris = s.dev.tris;
+    a.verts = s.dev.verts;
+    a.root = obj.root;
+    a.O = o;
+    a.D = d;
+    a.n = n;
+    a.out_id = id;
+    a.out_t = t;
+    a.out_t64 = t64;
+    a.counter = (unsigned long long *) counter;
+    const int block = (cfg && cfg->block_size > 0) ? cfg->block_size : 128;
+    if (block % 32 != 0 || block > 1024)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 <= 1024");
+    const int cap = stack_cap(obj.bvh.max_depth);
+    a.stack_stride = block;
+    const size_t smem = (size_t) cap * block * sizeof(uint2);
+    if (smem > 227 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
+    const bool persistent = cfg && cfg->persistent;
+    if (persistent) {
+        if (!counter)
+            return fail(PRR_ERR_INVALID_ARGUMENT, "persistent launch needs a counter");
+        if (int rc = set_smem((const void *) k_mesh_closest_persistent, smem))
+            return rc;
+        int bps = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 0;
+        if (bps == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_mesh_closest_persistent, block,
+                                                          smem);
+            bps = std::max(1, bps);
+        }
+        PRR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
+        k_mesh_closest_persistent<<<device_sm_count() * bps, block, smem, st>>>(a);
+    } else {
+        if (int rc = set_smem((const void *) k_mesh_closest, smem))
+            return rc;
+        k_mesh_closest<<<grid_for(n, block), block, smem, st>>>(a);
+    }
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int launch_mesh_occluded(const Scene &s, int object, const float *o, const float *d,
+                         const float *tmax, int64_t n, uint8_t *hit, cudaStream_t st) {
+    if (n == 0)
+        return PRR_OK;
+    const HostObject &obj = s.objects[object];
+    DevObject dobj{};
+    for (int k = 0; k < 6; k++)
+        dobj.root_box[k] = obj.bvh.bounds[k];
+    const int block = 128;
+    const size_t smem = (size_t) stack_cap(obj.bvh.max_depth) * block * sizeof(uint2);
+    if (smem > 227 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
+    if (int rc = set_smem((const void *) k_mesh_occluded, smem))
+        return rc;
+    k_mesh_occluded<<<grid_for(n, block), block, smem, st>>>(s.dev.nodes, s.dev.tris, obj.root,
+                                                             dobj, o, d, tmax, n, hit);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int launch_scene_closest(const Scene &s, const float *o, const float *d, int64_t n,
+                         int32_t *obj, int32_t *prim, float *t, float *geo, cudaStream_t st) {
+    if (n == 0)
+        return PRR_OK;
+    const int block = 128;
+    const int tcap = stack_cap(s.dev.tlas_depth), bcap = stack_cap(s.dev.blas_depth);
+    const size_t smem = (size_t) (tcap + bcap) * block * sizeof(uint2);
+    if (smem > 227 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
+    if (int rc = set_smem((const void *) k_scene_closest, smem))
+        return rc;
+    k_scene_closest<<<grid_for(n, block), block, smem, st>>>(s.dev, o, d, n, obj, prim, t, geo,
+                                                             tcap);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int launch_scene_occluded(const Scene &s, const float *o, const float *d, const float *tmax,
+                          int64_t n, uint8_t *hit, cudaStream_t st) {
+    if (n == 0)
+        return PRR_OK;
+    const int block = 128;
+    const int tcap = stack_cap(s.dev.tlas_depth), bcap = stack_cap(s.dev.blas_depth);
+    const size_t smem = (size_t) (tcap + bcap) * block * sizeof(uint2);
+    if (smem > 227 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
+    if (int rc = set_smem((const void *) k_scene_occluded, smem))
+        return rc;
+    k_scene_occluded<<<grid_for(n, block), block, smem, st>>>(s.dev, o, d, tmax, n, hit, tcap);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+} // namespace prr

@@ -1,0 +1,110 @@
+// Internal host-side state behind the C ABI (include/prr.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/prr.h"
+#include "bvh_build.h"
+#include "device_types.h"
+
+namespace prr {
+
+// ---- error reporting: every ABI call returns a status and leaves a message
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+#define PRR_CUDA_TRY(expr)                                                                        \
+    do {                                                                                         \
+        cudaError_t e__ = (expr);                                                                \
+        if (e__ != cudaSuccess)                                                                  \
+            return ::prr::fail(PRR_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+    } while (0)
+
+// Owning device allocation.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        if (n == 0)
+            return cudaSuccess;
+        cudaError_t e = cudaMalloc(&ptr, n);
+        if (e == cudaSuccess)
+            bytes = n;
+        return e;
+    }
+    cudaError_t ensure(size_t n) { return n <= bytes ? cudaSuccess : alloc(n); }
+    template <class T> T *as() const { return (T *) ptr; }
+};
+
+struct HostMaterial {
+    int kind;
+    float params[9]; // baseColor[3], roughness, metallic, ior, emission[3]
+};
+
+struct HostObject {
+    int kind;          // kObjMesh / kObjSphere
+    int material;
+    std::vector<float> verts; // mesh: n x 9 input triangles
+    float center[3] = {0, 0, 0};
+    float radius = 0.f;
+    // filled by build
+    FlatBVH bvh;
+    PrimBox bounds;
+    float area = 0.f;
+    int tri_base = 0;
+    uint32_t root = 0;
+};
+
+struct Scene {
+    std::mutex mu;
+    std::vector<HostMaterial> materials;
+    std::vector<HostObject> objects;
+    float background[3] = {0.235294f, 0.67451f, 0.843137f}; // Scene.hpp:17
+    std::vector<float> env_rgb;
+    int env_w = 0, env_h = 0;
+    prr_camera camera{};
+    int width = 0, height = 0;
+    bool camera_set = false;
+
+    bool built = false;
+    FlatBVH tlas;
+    DevScene dev{};   // device pointers + scalars, passed to kernels by value
+    int64_t n_tris = 0;
+    size_t device_bytes = 0;
+
+    DevBuf d_nodes, d_tris, d_verts, d_normals, d_objects, d_materials, d_emissives;
+    DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin;
+    DevBuf d_scratch;      // staging for host-buffer entry points
+    DevBuf d_counter;      // persistent-kernel work counters
+};
+
+// Kernel launchers (k_*.cu). All return a status; launch errors are checked.
+int launch_mesh_closest(const Scene &s, int object, const float *o, const float *d, int64_t n,
+                        int32_t *id, float *t, double *t64, unsigned *counter,
+                        const prr_trace_config *cfg, cudaStream_t st);
+int launch_mesh_occluded(const Scene &s, int object, const float *o, const float *d,
+                         const float *tmax, int64_t n, uint8_t *hit, cudaStream_t st);
+int launch_scene_closest(const Scene &s, const float *o, const float *d, int64_t n,
+                         int32_t *obj, int32_t *prim, float *t, float *geo, cudaStream_t st);
+int launch_scene_occluded(const Scene &s, const float *o, const float *d, const float *tmax,
+                          int64_t n, uint8_t *hit, cudaStream_t st);
+int launch_env_cdf(Scene &s, cudaStream_t st);
+
+int device_sm_count();
+
+} // namespace prr

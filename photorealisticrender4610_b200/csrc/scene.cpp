@@ -1,0 +1,697 @@
+// Scene assembly and the C ABI of scene construction and batch queries.
+//
+// prr_scene_build restates Scene::buildBVH (Scene.cpp:15-27): one SAH BVH per
+// mesh with maxPrimsInNode 4 (Triangle.hpp:173-179), then the scene BVH over
+// all objects with maxPrimsInNode 1, then the emitter list and its total area.
+// The trees are then packed into the device layout of device_types.h and
+// uploaded once; the scene stays resident until prr_scene_destroy.
+#include "prr_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <thread>
+
+namespace prr {
+
+namespace {
+
+constexpr float kPi = 3.141592653589793f; // global.hpp:10 (a float)
+
+PrimBox mesh_bounds(const std::vector<float> &v) {
+    // min/max over all vertices, as MeshTriangle's bounding box is formed
+    // (Triangle.cpp:12-30); identical to the union of the triangle bounds.
+    const float inf = std::numeric_limits<float>::infinity();
+    PrimBox b{{inf, inf, inf}, {-inf, -inf, -inf}};
+    for (size_t i = 0; i < v.size(); i += 3)
+        for (int k = 0; k < 3; k++) {
+            b.mn[k] = std::min(b.mn[k], v[i + k]);
+            b.mx[k] = std::max(b.mx[k], v[i + k]);
+        }
+    return b;
+}
+
+// Pack one reference-layout tree into child-pair nodes. Leaves become
+// references to their first primitive (meshes) or to their object (scene
+// BVH). Returns the root reference.
+int pack_tree(const FlatBVH &f, bool object_leaves, int tri_base, std::vector<WNode> &out,
+              std::vector<Tri> *tris, uint32_t &root_ref) {
+    const size_t n = f.size();
+    std::vector<uint32_t> wide(n, 0xFFFFFFFFu);
+    const uint32_t base = (uint32_t) out.size();
+    uint32_t k = 0;
+    for (size_t i = 0; i < n; i++)
+        if ((f.meta[i] & 0x00FFFFFFu) == 0)
+            wide[i] = base + k++;
+    auto ref = [&](size_t i) -> uint32_t {
+        const uint32_t cnt = f.meta[i] & 0x00FFFFFFu;
+        if (cnt == 0)
+            return wide[i];
+        if (object_leaves)
+            return kLeafBit | (uint32_t) f.ordered[f.first_child[i]];
+        return kLeafBit | (uint32_t) (tri_base + f.first_child[i]);
+    };
+    for (size_t i = 0; i < n; i++) {
+        const uint32_t cnt = f.meta[i] & 0x00FFFFFFu;
+        if (cnt > 0) {
+            if (object_leaves && cnt != 1)
+                return fail(PRR_ERR_INTERNAL, "scene BVH leaf with more than one object");
+            if (tris)
+                (*tris)[tri_base + f.first_child[i]].leaf_count = cnt;
+        }
+    }
+    out.resize(base + k);
+    for (size_t i = 0; i < n; i++) {
+        if ((f.meta[i] & 0x00FFFFFFu) != 0)
+            continue;
+        WNode &w = out[wide[i]];
+        const size_t l = i + 1, r = f.first_child[i];
+        for (int q = 0; q < 6; q++) {
+            w.lb[q] = f.bounds[l * 6 + q];
+            w.rb[q] = f.bounds[r * 6 + q];
+        }
+        w.left = ref(l);
+        w.right = ref(r);
+        w.axis = f.meta[i] >> 24;
+        w.left_area = f.area[l];
+    }
+    root_ref = ref(0);
+    return PRR_OK;
+}
+
+template <class T> int upload(DevBuf &b, const std::vector<T> &v) {
+    PRR_CUDA_TRY(b.alloc(std::max<size_t>(v.size() * sizeof(T), 16)));
+    if (!v.empty())
+        PRR_CUDA_TRY(cudaMemcpy(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return PRR_OK;
+}
+
+int check_scene(const prr_scene *s, bool need_built) {
+    if (!s)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene is NULL");
+    if (need_built && !reinterpret_cast<const Scene *>(s)->built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    return PRR_OK;
+}
+
+Scene *S(prr_scene *s) { return reinterpret_cast<Scene *>(s); }
+const Scene *S(const prr_scene *s) { return reinterpret_cast<const Scene *>(s); }
+
+} // namespace
+
+int build_scene(Scene &s, cudaStream_t st) {
+    // ---- per-mesh BVHs (independent; built concurrently) ----
+    std::vector<int> meshes;
+    for (size_t k = 0; k < s.objects.size(); k++)
+        if (s.objects[k].kind == kObjMesh)
+            meshes.push_back((int) k);
+    const int hw = (int) std::max(1u, std::thread::hardware_concurrency());
+    auto build_one = [&](int k, int threads) {
+        HostObject &o = s.objects[k];
+        std::vector<PrimBox> pb;
+        std::vector<float> pa;
+        const int64_t nt = (int64_t) o.verts.size() / 9;
+        triangle_prims(o.verts.data(), nt, pb, pa);
+        o.bvh = build_sah(pb, pa, 4, threads);
+        o.bounds = mesh_bounds(o.verts);
+        // MeshTriangle::area: sum in input order (Triangle.hpp:119-121)
+        float a = 0.f;
+        for (float x : pa)
+            a += x;
+        o.area = a;
+    };
+    {
+        // big meshes get the threads; small ones run side by side
+        std::vector<std::thread> pool;
+        std::vector<int> small;
+        for (int k : meshes) {
+            if (s.objects[k].verts.size() / 9 > 200000)
+                build_one(k, hw);
+            else
+                small.push_back(k);
+        }
+        std::atomic<size_t> next{0};
+        const int nthr = std::min<int>(hw, (int) small.size());
+        for (int t = 0; t < nthr; t++)
+            pool.emplace_back([&] {
+                for (size_t i; (i = next.fetch_add(1)) < small.size();)
+                    build_one(small[i], 1);
+            });
+        for (auto &th : pool)
+            th.join();
+    }
+    for (auto &o : s.objects) {
+        if (o.kind == kObjSphere) {
+            const float r = o.radius;
+            o.bounds = PrimBox{{o.center[0] - r, o.center[1] - r, o.center[2] - r},
+                               {o.center[0] + r, o.center[1] + r, o.center[2] + r}};
+            o.area = 4 * kPi * r * r; // Sphere.hpp:16
+        }
+    }
+
+    // ---- device triangle arrays in leaf order ----
+    std::vector<Tri> tris;
+    std::vector<float> verts, normals;
+    std::vector<WNode> nodes;
+    int64_t ntri = 0;
+    for (int k : meshes)
+        ntri += (int64_t) s.objects[k].verts.size() / 9;
+    if (ntri >= (int64_t) kLeafBit)
+        return fail(PRR_ERR_UNSUPPORTED, "too many triangles");
+    tris.resize(ntri);
+    verts.resize((size_t) ntri * 9);
+    normals.resize((size_t) ntri * 3);
+    int base = 0;
+    int blas_depth = 0;
+    for (int k : meshes) {
+        HostObject &o = s.objects[k];
+        o.tri_base = base;
+        const int64_t nt = (int64_t) o.verts.size() / 9;
+        for (int64_t j = 0; j < nt; j++) {
+            const int32_t id = o.bvh.ordered[j];
+            const float *p = &o.verts[(size_t) id * 9];
+            Tri &t = tris[base + j];
+            // Triangle(v0, v1, v2) (Triangle.hpp:27-32)
+            const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
+            const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
+            t.v0x = p[0];
+            t.v0y = p[1];
+            t.v0z = p[2];
+            t.e1x = e1x;
+            t.e1y = e1y;
+            t.e1z = e1z;
+            t.e2x = e2x;
+            t.e2y = e2y;
+            t.e2z = e2z;
+            t.id = id;
+            t.leaf_count = 0;
+            const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z,
+                        cz = e1x * e2y - e1y * e2x;
+            t.area = std::sqrt(cx * cx + cy * cy + cz * cz) * 0.5f;
+            // normalize(crossProduct(e1, e2)) (Vector.hpp:103-111)
+            const float m2 = cx * cx + cy * cy + cz * cz;
+            float nx = cx, ny = cy, nz = cz;
+            if (m2 > 0) {
+                const float inv = 1 / sqrtf(m2);
+                nx = cx * inv;
+                ny = cy * inv;
+                nz = cz * inv;
+            }
+            normals[(size_t) (base + j) * 3 + 0] = nx;
+            normals[(size_t) (base + j) * 3 + 1] = ny;
+            normals[(size_t) (base + j) * 3 + 2] = nz;
+            std::memcpy(&verts[(size_t) (base + j) * 9], p, 9 * sizeof(float));
+        }
+        if (int rc = pack_tree(o.bvh, false, base, nodes, &tris, o.root))
+            return rc;
+        blas_depth = std::max(blas_depth, o.bvh.max_depth);
+        base += (int) nt;
+    }
+
+    // ---- scene BVH over objects, maxPrimsInNode 1 (Scene.cpp:17) ----
+    std::vector<PrimBox> ob(s.objects.size());
+    std::vector<float> oa(s.objects.size());
+    for (size_t k = 0; k < s.objects.size(); k++) {
+        ob[k] = s.objects[k].bounds;
+        oa[k] = s.objects[k].area;
+    }
+    s.tlas = build_sah(ob, oa, 1, 1);
+    uint32_t tlas_root = 0;
+    if (!s.objects.empty())
+        if (int rc = pack_tree(s.tlas, true, 0, nodes, nullptr, tlas_root))
+            return rc;
+
+    // ---- objects, materials, emitters (Scene.cpp:19-26) ----
+    std::vector<DevObject> dobj(s.objects.size());
+    std::vector<int32_t> emissives;
+    float emit_area = 0.f;
+    for (size_t k = 0; k < s.objects.size(); k++) {
+        const HostObject &o = s.objects[k];
+        DevObject &d = dobj[k];
+        std::memset(&d, 0, sizeof(d));
+        d.kind = o.kind;
+        d.material = o.material;
+        d.area = o.area;
+        if (o.kind == kObjMesh) {
+            d.root = o.root;
+            d.tri_base = o.tri_base;
+            d.ntri = (int32_t) (o.verts.size() / 9);
+            for (int q = 0; q < 6; q++)
+                d.root_box[q] = o.bvh.bounds[q];
+            d.bvh_area = o.bvh.total_area;
+            d.depth = o.bvh.max_depth;
+        } else {
+            d.cx = o.center[0];
+            d.cy = o.center[1];
+            d.cz = o.center[2];
+            d.radius = o.radius;
+            d.radius2 = o.radius * o.radius;
+        }
+        const float *em = s.materials[o.material].params + 6;
+        // Material::hasEmission: m_emission.norm() > EPSILON (Material.hpp:106-108)
+        if (std::sqrt(em[0] * em[0] + em[1] * em[1] + em[2] * em[2]) > 1e-3f) {
+            emissives.push_back((int32_t) k);
+            emit_area += o.area;
+        }
+    }
+    std::vector<DevMaterial> dmat(s.materials.size());
+    for (size_t m = 0; m < s.materials.size(); m++) {
+        DevMaterial &d = dmat[m];
+        std::memset(&d, 0, sizeof(d));
+        const float *p = s.materials[m].params;
+        d.kind = s.materials[m].kind;
+        d.base[0] = p[0];
+        d.base[1] = p[1];
+        d.base[2] = p[2];
+        d.roughness = p[3];
+        d.metallic = p[4];
+        d.ior = p[5];
+        d.emission[0] = p[6];
+        d.emission[1] = p[7];
+        d.emission[2] = p[8];
+        d.has_emission = std::sqrt(p[6] * p[6] + p[7] * p[7] + p[8] * p[8]) > 1e-3f;
+    }
+
+    if (int rc = upload(s.d_nodes, nodes))
+        return rc;
+    if (int rc = upload(s.d_tris, tris))
+        return rc;
+    if (int rc = upload(s.d_verts, verts))
+        return rc;
+    if (int rc = upload(s.d_normals, normals))
+        return rc;
+    if (int rc = upload(s.d_objects, dobj))
+        return rc;
+    if (int rc = upload(s.d_materials, dmat))
+        return rc;
+    if (int rc = upload(s.d_emissives, emissives))
+        return rc;
+
+    DevScene &D = s.dev;
+    std::memset(&D, 0, sizeof(D));
+    D.nodes = s.d_nodes.as<WNode>();
+    D.tris = s.d_tris.as<Tri>();
+    D.verts = s.d_verts.as<float>();
+    D.normals = s.d_normals.as<float>();
+    D.objects = s.d_objects.as<DevObject>();
+    D.materials = s.d_materials.as<DevMaterial>();
+    D.emissives = s.d_emissives.as<int32_t>();
+    D.n_objects = (int32_t) s.objects.size();
+    D.n_materials = (int32_t) s.materials.size();
+    D.n_emissives = (int32_t) emissives.size();
+    D.total_emit_area = emit_area;
+    D.tlas_root = tlas_root;
+    if (!s.objects.empty())
+        for (int q = 0; q < 6; q++)
+            D.tlas_box[q] = s.tlas.bounds[q];
+    D.tlas_depth = s.tlas.max_depth;
+    D.blas_depth = blas_depth;
+    std::memcpy(D.background, s.background, sizeof(D.background));
+
+    // ---- camera (Camera::init, Camera.hpp:43-56, and the focal length of
+    //      generateRay, :76) ----
+    if (s.camera_set) {
+        const prr_camera &c = s.camera;
+        auto normalize3 = [](float v[3]) {
+            const float m2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            if (m2 > 0) {
+                const float inv = 1 / sqrtf(m2);
+                v[0] = v[0] * inv;
+                v[1] = v[1] * inv;
+                v[2] = v[2] * inv;
+            }
+        };
+        float f[3] = {c.target[0] - c.eye[0], c.target[1] - c.eye[1], c.target[2] - c.eye[2]};
+        normalize3(f);
+        float r[3] = {f[1] * c.up[2] - f[2] * c.up[1], f[2] * c.up[0] - f[0] * c.up[2],
+                      f[0] * c.up[1] - f[1] * c.up[0]};
+        normalize3(r);
+        float u[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2],
+                      r[0] * f[1] - r[1] * f[0]};
+        DevCamera &dc = D.camera;
+        std::memcpy(dc.eye, c.eye, sizeof(dc.eye));
+        std::memcpy(dc.forward, f, sizeof(f));
+        std::memcpy(dc.right, r, sizeof(r));
+        std::memcpy(dc.up, u, sizeof(u));
+        const float half_fov_h = c.fovh * kPi / 180.0f * 0.5f;
+        dc.focal_px = ((float) s.width * 0.5f) / std::tan(half_fov_h);
+        dc.aperture = c.aperture;
+        float focus = c.focus_distance;
+        if (focus < 0.0f) {
+            const float dx = c.target[0] - c.eye[0], dy = c.target[1] - c.eye[1],
+                        dz = c.target[2] - c.eye[2];
+            focus = std::sqrt(dx * dx + dy * dy + dz * dz);
+        }
+        dc.focus_distance = focus;
+        dc.width = s.width;
+        dc.height = s.height;
+    }
+
+    // ---- environment map: pixels + CDF built on the device ----
+    if (!s.env_rgb.empty()) {
+        const int w = s.env_w, h = s.env_h;
+        std::vector<float4> px((size_t) w * h);
+        for (size_t i = 0; i < px.size(); i++)
+            px[i] = make_float4(s.env_rgb[i * 3], s.env_rgb[i * 3 + 1], s.env_rgb[i * 3 + 2], 0.f);
+        if (int rc = upload(s.d_env_px, px))
+            return rc;
+        // sin(theta) of each row centre, evaluated with the host libm exactly
+        // as EnvMap::buildCDF does (EnvMap.hpp:196-197)
+        std::vector<float> rs(h);
+        for (int row = 0; row < h; row++) {
+            const float theta = (row + 0.5f) / (float) h * kPi;
+            rs[row] = std::sin(theta);
+        }
+        if (int rc = upload(s.d_env_rowsin, rs))
+            return rc;
+        PRR_CUDA_TRY(s.d_env_cdf.alloc((size_t) w * h * sizeof(float)));
+        PRR_CUDA_TRY(s.d_env_marginal.alloc((size_t) h * sizeof(float)));
+        D.env.pixels = s.d_env_px.as<float4>();
+        D.env.cdf = s.d_env_cdf.as<float>();
+        D.env.marginal = s.d_env_marginal.as<float>();
+        D.env.width = w;
+        D.env.height = h;
+        D.env.loaded = 1;
+        if (int rc = launch_env_cdf(s, st))
+            return rc;
+    }
+
+    PRR_CUDA_TRY(s.d_counter.alloc(64));
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    s.n_tris = ntri;
+    s.device_bytes = s.d_nodes.bytes + s.d_tris.bytes + s.d_verts.bytes + s.d_normals.bytes +
+                     s.d_objects.bytes + s.d_materials.bytes + s.d_emissives.bytes +
+                     s.d_env_px.bytes + s.d_env_cdf.bytes + s.d_env_marginal.bytes;
+    s.built = true;
+    return PRR_OK;
+}
+
+} // namespace prr
+
+using namespace prr;
+
+extern "C" {
+
+int prr_scene_create(prr_scene **out) {
+    if (!out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "out is NULL");
+    try {
+        *out = reinterpret_cast<prr_scene *>(new Scene());
+    } catch (...) {
+        return fail(PRR_ERR_OUT_OF_MEMORY, "scene allocation failed");
+    }
+    return PRR_OK;
+}
+
+int prr_scene_destroy(prr_scene *scene) {
+    if (!scene)
+        return PRR_OK;
+    delete S(scene);
+    return PRR_OK;
+}
+
+int prr_scene_add_material(prr_scene *scene, int kind, const float params[9], int *out_id) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    if (kind < PRR_MAT_DIFFUSE || kind > PRR_MAT_GLASS || !params)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad material kind or params");
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    HostMaterial m;
+    m.kind = kind;
+    std::memcpy(m.params, params, sizeof(m.params));
+    s->materials.push_back(m);
+    if (out_id)
+        *out_id = (int) s->materials.size() - 1;
+    return PRR_OK;
+}
+
+int prr_scene_add_mesh(prr_scene *scene, const float *verts, int64_t ntri, int material,
+                       int *out_object) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    if (!verts || ntri <= 0)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "mesh needs at least one triangle");
+    if (material < 0 || material >= (int) s->materials.size())
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown material");
+    HostObject o;
+    o.kind = kObjMesh;
+    o.material = material;
+    o.verts.assign(verts, verts + ntri * 9);
+    s->objects.push_back(std::move(o));
+    if (out_object)
+        *out_object = (int) s->objects.size() - 1;
+    return PRR_OK;
+}
+
+int prr_scene_add_sphere(prr_scene *scene, const float center[3], float radius, int material,
+                         int *out_object) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    if (!center || !(radius > 0.f))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "sphere needs a center and radius > 0");
+    if (material < 0 || material >= (int) s->materials.size())
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown material");
+    HostObject o;
+    o.kind = kObjSphere;
+    o.material = material;
+    std::memcpy(o.center, center, sizeof(o.center));
+    o.radius = radius;
+    s->objects.push_back(std::move(o));
+    if (out_object)
+        *out_object = (int) s->objects.size() - 1;
+    return PRR_OK;
+}
+
+int prr_scene_set_background(prr_scene *scene, const float rgb[3]) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    if (!rgb)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "rgb is NULL");
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    std::memcpy(s->background, rgb, sizeof(s->background));
+    s->dev.background[0] = rgb[0];
+    s->dev.background[1] = rgb[1];
+    s->dev.background[2] = rgb[2];
+    return PRR_OK;
+}
+
+int prr_scene_set_env(prr_scene *scene, const float *rgb, int width, int height) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    if (!rgb || width <= 0 || height <= 0)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad environment map");
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    s->env_rgb.assign(rgb, rgb + (size_t) width * height * 3);
+    s->env_w = width;
+    s->env_h = height;
+    return PRR_OK;
+}
+
+int prr_scene_set_camera(prr_scene *scene, const prr_camera *camera, int width, int height) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    if (!camera || width <= 0 || height <= 0)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad camera");
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    s->camera = *camera;
+    s->width = width;
+    s->height = height;
+    s->camera_set = true;
+    return PRR_OK;
+}
+
+int prr_scene_build(prr_scene *scene, void *stream) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    try {
+        return build_scene(*s, (cudaStream_t) stream);
+    } catch (const std::bad_alloc &) {
+        return fail(PRR_ERR_OUT_OF_MEMORY, "host allocation failed during build");
+    }
+}
+
+int prr_scene_stats_get(const prr_scene *scene, prr_scene_stats *out) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    if (!out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "out is NULL");
+    const Scene *s = S(scene);
+    out->n_objects = (int64_t) s->objects.size();
+    out->n_triangles = s->n_tris;
+    out->n_nodes = (int64_t) (s->d_nodes.bytes / sizeof(WNode));
+    out->tlas_depth = s->dev.tlas_depth;
+    out->blas_depth = s->dev.blas_depth;
+    out->device_bytes = (int64_t) s->device_bytes;
+    out->total_emit_area = s->dev.total_emit_area;
+    return PRR_OK;
+}
+
+int64_t prr_scene_export_nodes(const prr_scene *scene, int object, float *bounds,
+                               uint32_t *first_child, uint32_t *meta, float *areas,
+                               int32_t *ordered) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    const Scene *s = S(scene);
+    const FlatBVH *f;
+    if (object < 0)
+        f = &s->tlas;
+    else if (object < (int) s->objects.size() && s->objects[object].kind == kObjMesh)
+        f = &s->objects[object].bvh;
+    else
+        return fail(PRR_ERR_INVALID_ARGUMENT, "object is not a mesh");
+    const size_t n = f->size();
+    if (bounds)
+        std::memcpy(bounds, f->bounds.data(), n * 6 * sizeof(float));
+    if (first_child)
+        std::memcpy(first_child, f->first_child.data(), n * sizeof(uint32_t));
+    if (meta)
+        std::memcpy(meta, f->meta.data(), n * sizeof(uint32_t));
+    if (areas)
+        std::memcpy(areas, f->area.data(), n * sizeof(float));
+    if (ordered)
+        std::memcpy(ordered, f->ordered.data(), f->ordered.size() * sizeof(int32_t));
+    return (int64_t) n;
+}
+
+static int check_mesh(const prr_scene *scene, int object) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    const Scene *s = S(scene);
+    if (object < 0 || object >= (int) s->objects.size() || s->objects[object].kind != kObjMesh)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "object is not a mesh");
+    return PRR_OK;
+}
+
+int prr_mesh_intersect(const prr_scene *scene, int object, const float *o, const float *d,
+                       int64_t n, int32_t *out_id, float *out_t, double *out_t64,
+                       const prr_trace_config *cfg, void *stream) {
+    if (int rc = check_mesh(scene, object))
+        return rc;
+    if (n < 0 || (n > 0 && (!o || !d || !out_id || !out_t)))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad ray or output arrays");
+    const Scene *s = S(scene);
+    return launch_mesh_closest(*s, object, o, d, n, out_id, out_t, out_t64,
+                               (unsigned *) s->d_counter.ptr, cfg, (cudaStream_t) stream);
+}
+
+int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const float *d,
+                            int64_t n, int32_t *out_id, float *out_t, void *stream) {
+    if (int rc = check_mesh(scene, object))
+        return rc;
+    if (n < 0 || (n > 0 && (!o || !d || !out_id || !out_t)))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad ray or output arrays");
+    if (n == 0)
+        return PRR_OK;
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    cudaStream_t st = (cudaStream_t) stream;
+    // Chunked pipeline: copies of chunk k+1 overlap the trace of chunk k when
+    // the host buffers are pinned.
+    const int64_t chunk = std::min<int64_t>(n, 1 << 20);
+    const int nbuf = 2;
+    const size_t per = (size_t) chunk * (6 * sizeof(float) + sizeof(int32_t) + sizeof(float));
+    PRR_CUDA_TRY(s->d_scratch.ensure(per * nbuf));
+    cudaStream_t streams[nbuf];
+    cudaEvent_t start_ev, done[nbuf];
+    PRR_CUDA_TRY(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
+    PRR_CUDA_TRY(cudaEventRecord(start_ev, st));
+    for (int b = 0; b < nbuf; b++) {
+        PRR_CUDA_TRY(cudaStreamCreateWithFlags(&streams[b], cudaStreamNonBlocking));
+        PRR_CUDA_TRY(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming));
+        PRR_CUDA_TRY(cudaStreamWaitEvent(streams[b], start_ev, 0));
+    }
+    int rc = PRR_OK;
+    int64_t k = 0;
+    for (int64_t off = 0; off < n && rc == PRR_OK; off += chunk, k++) {
+        const int b = (int) (k % nbuf);
+        const int64_t m = std::min(chunk, n - off);
+        char *base = (char *) s->d_scratch.ptr + per * b;
+        float *dO = (float *) base;
+        float *dD = dO + chunk * 3;
+        int32_t *dI = (int32_t *) (dD + chunk * 3);
+        float *dT = (float *) (dI + chunk);
+        cudaStream_t cs = streams[b];
+        if (cudaMemcpyAsync(dO, o + off * 3, m * 3 * sizeof(float), cudaMemcpyHostToDevice, cs) ||
+            cudaMemcpyAsync(dD, d + off * 3, m * 3 * sizeof(float), cudaMemcpyHostToDevice, cs)) {
+            rc = fail(PRR_ERR_CUDA, "host-to-device copy failed");
+            break;
+        }
+        rc = launch_mesh_closest(*s, object, dO, dD, m, dI, dT, nullptr, nullptr, nullptr, cs);
+        if (rc)
+            break;
+        if (cudaMemcpyAsync(out_id + off, dI, m * sizeof(int32_t), cudaMemcpyDeviceToHost, cs) ||
+            cudaMemcpyAsync(out_t + off, dT, m * sizeof(float), cudaMemcpyDeviceToHost, cs)) {
+            rc = fail(PRR_ERR_CUDA, "device-to-host copy failed");
+            break;
+        }
+    }
+    for (int b = 0; b < nbuf; b++) {
+        cudaEventRecord(done[b], streams[b]);
+        cudaStreamWaitEvent(st, done[b], 0);
+    }
+    cudaError_t e = cudaStreamSynchronize(st);
+    for (int b = 0; b < nbuf; b++) {
+        cudaEventDestroy(done[b]);
+        cudaStreamDestroy(streams[b]);
+    }
+    cudaEventDestroy(start_ev);
+    if (rc == PRR_OK && e != cudaSuccess)
+        rc = fail(PRR_ERR_CUDA, std::string("trace: ") + cudaGetErrorString(e));
+    return rc;
+}
+
+int prr_mesh_occluded(const prr_scene *scene, int object, const float *o, const float *d,
+                      const float *tmax, int64_t n, uint8_t *out_hit, void *stream) {
+    if (int rc = check_mesh(scene, object))
+        return rc;
+    if (n < 0 || (n > 0 && (!o || !d || !tmax || !out_hit)))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad ray or output arrays");
+    return launch_mesh_occluded(*S(scene), object, o, d, tmax, n, out_hit,
+                                (cudaStream_t) stream);
+}
+
+int prr_scene_intersect(const prr_scene *scene, const float *o, const float *d, int64_t n,
+                        int32_t *out_obj, int32_t *out_prim, float *out_t, float *out_geo,
+                        void *stream) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    if (n < 0 || (n > 0 && (!o || !d || !out_obj || !out_prim || !out_t)))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad ray or output arrays");
+    return launch_scene_closest(*S(scene), o, d, n, out_obj, out_prim, out_t, out_geo,
+                                (cudaStream_t) stream);
+}
+
+int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
+                       const float *tmax, int64_t n, uint8_t *out_hit, void *stream) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    if (n < 0 || (n > 0 && (!o || !d || !tmax || !out_hit)))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad ray or output arrays");
+    return launch_scene_occluded(*S(scene), o, d, tmax, n, out_hit, (cudaStream_t) stream);
+}
+
+} // extern "C"

@@ -1,0 +1,436 @@
+// Device ray traversal: the reference's closest-hit and any-hit BVH walks
+// (BVH.cpp:311-473) with Möller-Trumbore (Triangle.hpp:46-92) and the
+// analytic sphere (Sphere.hpp:22-44), over the 64-byte child-pair nodes of
+// device_types.h.
+//
+// Bit-exactness. Everything here is compiled with --fmad=false and IEEE
+// division/sqrt, and every expression keeps the reference's operation order,
+// so each slab distance, determinant and t is the float the reference's
+// IEEE build computes. The traversal order (near child first on
+// tLeft <= tRight, cull on tBox < closestT at push and at pop) is the
+// reference's, so ties resolve to the same triangle.
+//
+// Stacks live in shared memory, one column per thread ([depth][block]
+// layout), so a warp's pushes and pops hit distinct banks.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+
+namespace prr {
+
+#define kInf (__int_as_float(0x7f800000))
+
+struct RayD {
+    float ox, oy, oz;
+    float dx, dy, dz;
+};
+
+// BVHAccel::precompute (BVH.cpp:290-299)
+struct RayPre {
+    float ox, oy, oz;
+    float ix, iy, iz;
+    bool nx, ny, nz; // octant: direction negative on that axis
+};
+
+__device__ __forceinline__ RayPre precompute(const RayD &r) {
+    RayPre p;
+    p.ox = r.ox;
+    p.oy = r.oy;
+    p.oz = r.oz;
+    p.ix = (r.dx != 0.f) ? (1.f / r.dx) : kInf;
+    p.iy = (r.dy != 0.f) ? (1.f / r.dy) : kInf;
+    p.iz = (r.dz != 0.f) ? (1.f / r.dz) : kInf;
+    p.nx = r.dx < 0.f;
+    p.ny = r.dy < 0.f;
+    p.nz = r.dz < 0.f;
+    return p;
+}
+
+// BVHAccel::nodeIntersect (BVH.hpp:115-124) on bounds
+// [minX,maxX,minY,maxY,minZ,maxZ]. fmaxf/fminf agree with std::max(tMin,t0)
+// and std::min(tMax,t1) for every input, NaN included (the running bound is
+// never NaN, and both return it when the new term is NaN).
+__device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, float z0, float z1,
+                                      const RayPre &p) {
+    float tmin = 0.f, tmax = kInf;
+    float t0 = ((p.nx ? x1 : x0) - p.ox) * p.ix;
+    float t1 = ((p.nx ? x0 : x1) - p.ox) * p.ix;
+    tmin = fmaxf(tmin, t0);
+    tmax = fminf(tmax, t1);
+    t0 = ((p.ny ? y1 : y0) - p.oy) * p.iy;
+    t1 = ((p.ny ? y0 : y1) - p.oy) * p.iy;
+    tmin = fmaxf(tmin, t0);
+    tmax = fminf(tmax, t1);
+    t0 = ((p.nz ? z1 : z0) - p.oz) * p.iz;
+    t1 = ((p.nz ? z0 : z1) - p.oz) * p.iz;
+    tmin = fmaxf(tmin, t0);
+    tmax = fminf(tmax, t1);
+    return tmin <= tmax ? tmin : kInf;
+}
+
+__device__ __forceinline__ float slab6(const float *b, const RayPre &p) {
+    return slab(b[0], b[1], b[2], b[3], b[4], b[5], p);
+}
+
+struct NodeV {
+    float4 a, b, c;
+    uint4 link;
+};
+
+__device__ __forceinline__ NodeV load_node(const WNode *nodes, uint32_t idx) {
+    const float4 *q = reinterpret_cast<const float4 *>(nodes + idx);
+    NodeV n;
+    n.a = __ldg(q);
+    n.b = __ldg(q + 1);
+    n.c = __ldg(q + 2);
+    n.link = __ldg(reinterpret_cast<const uint4 *>(q + 3));
+    return n;
+}
+
+struct TriV {
+    float4 p, q, r;
+};
+
+__device__ __forceinline__ TriV load_tri(const Tri *tris, uint32_t idx) {
+    const float4 *t = reinterpret_cast<const float4 *>(tris + idx);
+    TriV v;
+    v.p = __ldg(t);
+    v.q = __ldg(t + 1);
+    v.r = __ldg(t + 2);
+    return v;
+}
+
+// Triangle::hitTest (Triangle.hpp:46-64), evaluated without early exits. The
+// miss tests are kept in their negated form so NaNs fall through exactly as
+// the reference's `if (cond) return miss` chain lets them.
+__device__ __forceinline__ bool tri_hit(const TriV &T, const RayD &r, float &t, float &u,
+                                        float &v) {
+    const float v0x = T.p.x, v0y = T.p.y, v0z = T.p.z;
+    const float e1x = T.p.w, e1y = T.q.x, e1z = T.q.y;
+    const float e2x = T.q.z, e2y = T.q.w, e2z = T.r.x;
+    // P = d x e2
+    const float px = r.dy * e2z - r.dz * e2y;
+    const float py = r.dz * e2x - r.dx * e2z;
+    const float pz = r.dx * e2y - r.dy * e2x;
+    const float det = px * e1x + py * e1y + pz * e1z;
+    const float inv = 1.f / det;
+    const float tx = r.ox - v0x, ty = r.oy - v0y, tz = r.oz - v0z;
+    u = (px * tx + py * ty + pz * tz) * inv;
+    // Q = T x e1
+    const float qx = ty * e1z - tz * e1y;
+    const float qy = tz * e1x - tx * e1z;
+    const float qz = tx * e1y - ty * e1x;
+    v = (qx * r.dx + qy * r.dy + qz * r.dz) * inv;
+    t = (qx * e2x + qy * e2y + qz * e2z) * inv;
+    return !(fabsf(det) < 1e-6f) && !(u < 0.f) && !(v < 0.f || u + v > 1.f) && !(t <= 1e-3f);
+}
+
+// Triangle::intersectT (Triangle.hpp:75-92) followed by the caller's
+// `t >= 0 && t < tMax` check (BVH.cpp:395-398).
+__device__ __forceinline__ bool tri_occludes(const TriV &T, const RayD &r, float tmax) {
+    const float v0x = T.p.x, v0y = T.p.y, v0z = T.p.z;
+    const float e1x = T.p.w, e1y = T.q.x, e1z = T.q.y;
+    const float e2x = T.q.z, e2y = T.q.w, e2z = T.r.x;
+    const float px = r.dy * e2z - r.dz * e2y;
+    const float py = r.dz * e2x - r.dx * e2z;
+    const float pz = r.dx * e2y - r.dy * e2x;
+    const float det = px * e1x + py * e1y + pz * e1z;
+    const float inv = 1.f / det;
+    const float tx = r.ox - v0x, ty = r.oy - v0y, tz = r.oz - v0z;
+    const float u = (px * tx + py * ty + pz * tz) * inv;
+    const float qx = ty * e1z - tz * e1y;
+    const float qy = tz * e1x - tx * e1z;
+    const float qz = tx * e1y - ty * e1x;
+    const float v = (qx * r.dx + qy * r.dy + qz * r.dz) * inv;
+    const float t = (qx * e2x + qy * e2y + qz * e2z) * inv;
+    return !(fabsf(det) < 1e-6f) && !(u < 0.f || u > 1.f) && !(v < 0.f || u + v > 1.f) &&
+           (t > 1e-3f && t < tmax);
+}
+
+// Per-thread stack column in shared memory.
+struct SmemStack {
+    uint2 *base; // &smem[tid]; entry k at base[k * stride]
+    int stride;
+    int sp;
+    __device__ __forceinline__ void push(uint32_t ref, float t) {
+        base[sp * stride] = make_uint2(ref, __float_as_uint(t));
+        sp++;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        --sp;
+        return base[sp * stride];
+    }
+};
+
+// BVHAccel::Intersect, triangle fast path (BVH.cpp:311-415) on one mesh BVH.
+// best_t enters as +inf (every mesh-level search starts fresh, BVH.cpp:331).
+// Returns the winning triangle's global leaf-order index, or -1.
+__device__ __forceinline__ int blas_closest(const WNode *__restrict__ nodes,
+                                            const Tri *__restrict__ tris, uint32_t root,
+                                            const RayD &r, const RayPre &p, SmemStack &st,
+                                            float &best_t, float &best_u, float &best_v) {
+    const int sp0 = st.sp;
+    uint32_t ref = root;
+    int hit = -1;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            const NodeV n = load_node(nodes, ref);
+            const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+            const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+            if (tl <= tr) {
+                if (tl < best_t) {
+                    if (tr < best_t)
+                        st.push(n.link.y, tr);
+                    ref = n.link.x;
+                    continue;
+                }
+            } else {
+                if (tr < best_t) {
+                    if (tl < best_t)
+                        st.push(n.link.x, tl);
+                    ref = n.link.y;
+                    continue;
+                }
+            }
+        } else {
+            const uint32_t first = ref & ~kLeafBit;
+            const uint32_t cnt = __ldg(&tris[first].leaf_count);
+            for (uint32_t i = 0; i < cnt; i++) {
+                const TriV T = load_tri(tris, first + i);
+                float t, u, v;
+                if (tri_hit(T, r, t, u, v) && t < best_t) {
+                    best_t = t;
+                    best_u = u;
+                    best_v = v;
+                    hit = (int) (first + i);
+                }
+            }
+        }
+        // pop the next entry whose box is still nearer than the closest hit
+        for (;;) {
+            if (st.sp == sp0)
+                return hit;
+            const uint2 e = st.pop();
+            if (__uint_as_float(e.y) < best_t) {
+                ref = e.x;
+                break;
+            }
+        }
+    }
+}
+
+// BVHAccel::IntersectP (BVH.cpp:421-473) on one mesh BVH whose root box is
+// root_box: true when a triangle occludes within tmax. Child boxes are tested
+// where the reference tests them (far child at push, near child at the top of
+// the next iteration), so exactly the same subtrees are entered.
+__device__ __forceinline__ bool blas_occluded(const WNode *__restrict__ nodes,
+                                              const Tri *__restrict__ tris, uint32_t root,
+                                              const float *root_box, const RayD &r,
+                                              const RayPre &p, SmemStack &st, float tmax) {
+    if (!(slab6(root_box, p) < tmax))
+        return false;
+    const int sp0 = st.sp;
+    uint32_t ref = root;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            const NodeV n = load_node(nodes, ref);
+            const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+            const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+            const uint32_t axis = n.link.z;
+            const bool neg = axis == 0 ? p.nx : (axis == 1 ? p.ny : p.nz);
+            // octant 0 -> near = left
+            const uint32_t near_ref = neg ? n.link.y : n.link.x;
+            const uint32_t far_ref = neg ? n.link.x : n.link.y;
+            const float tnear = neg ? tr : tl;
+            const float tfar = neg ? tl : tr;
+            if (tfar < tmax)
+                st.push(far_ref, 0.f);
+            if (tnear < tmax) {
+                ref = near_ref;
+                continue;
+            }
+        } else {
+            const uint32_t first = ref & ~kLeafBit;
+            const uint32_t cnt = __ldg(&tris[first].leaf_count);
+            for (uint32_t i = 0; i < cnt; i++) {
+                const TriV T = load_tri(tris, first + i);
+                if (tri_occludes(T, r, tmax)) {
+                    st.sp = sp0;
+                    return true;
+                }
+            }
+        }
+        if (st.sp == sp0)
+            return false;
+        ref = st.pop().x;
+    }
+}
+
+// Sphere::getIntersection (Sphere.hpp:22-44) with solveQuadratic
+// (global.hpp:19-33). The reference calls the double sqrt there and mixes
+// -0.5 (a double) into both roots, so those steps run in double and round to
+// float exactly where the reference's assignments do.
+__device__ __forceinline__ bool sphere_hit(const DevObject &s, const RayD &r, float &t_out) {
+    const float Lx = r.ox - s.cx, Ly = r.oy - s.cy, Lz = r.oz - s.cz;
+    const float a = r.dx * r.dx + r.dy * r.dy + r.dz * r.dz;
+    const float b = 2 * (r.dx * Lx + r.dy * Ly + r.dz * Lz);
+    const float c = (Lx * Lx + Ly * Ly + Lz * Lz) - s.radius2;
+    const float discr = b * b - 4 * a * c;
+    float x0, x1;
+    if (discr < 0)
+        return false;
+    else if (discr == 0) {
+        x0 = x1 = (float) (-0.5 * (double) b / (double) a);
+    } else {
+        const double sq = sqrt((double) discr);
+        const float q = (b > 0) ? (float) (-0.5 * ((double) b + sq))
+                                : (float) (-0.5 * ((double) b - sq));
+        x0 = q / a;
+        x1 = c / q;
+    }
+    if (x0 > x1) {
+        float tmp = x0;
+        x0 = x1;
+        x1 = tmp;
+    }
+    float t0 = x0;
+    if (t0 < 0)
+        t0 = x1;
+    if (t0 < 0)
+        return false;
+    t_out = t0;
+    return true;
+}
+
+struct SceneHit {
+    int obj;      // object index, -1 on a miss
+    int tri;      // global leaf-order triangle index (meshes), -1 for spheres
+    float t, u, v;
+};
+
+// Scene::intersect -> BVHAccel::Intersect, general path (BVH.cpp:359-369):
+// every scene-BVH leaf object is intersected on its own (meshes start their
+// own search at +inf) and replaces the winner when tnear < closestT.
+__device__ __forceinline__ SceneHit scene_closest(const DevScene &S, const RayD &r,
+                                                  const RayPre &p, SmemStack &tst,
+                                                  SmemStack &bst) {
+    SceneHit h;
+    h.obj = -1;
+    h.tri = -1;
+    h.t = kInf;
+    h.u = h.v = 0.f;
+    if (S.n_objects == 0)
+        return h;
+    float closest = kInf;
+    const int sp0 = tst.sp;
+    uint32_t ref = S.tlas_root;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            const NodeV n = load_node(S.nodes, ref);
+            const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+            const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+            if (tl <= tr) {
+                if (tl < closest) {
+                    if (tr < closest)
+                        tst.push(n.link.y, tr);
+                    ref = n.link.x;
+                    continue;
+                }
+            } else {
+                if (tr < closest) {
+                    if (tl < closest)
+                        tst.push(n.link.x, tl);
+                    ref = n.link.y;
+                    continue;
+                }
+            }
+        } else {
+            const int k = (int) (ref & ~kLeafBit);
+            const DevObject &o = S.objects[k];
+            if (o.kind == kObjMesh) {
+                float t = kInf, u = 0.f, v = 0.f;
+                const int tri = blas_closest(S.nodes, S.tris, o.root, r, p, bst, t, u, v);
+                if (tri >= 0 && t < closest) {
+                    closest = t;
+                    h.obj = k;
+                    h.tri = tri;
+                    h.t = t;
+                    h.u = u;
+                    h.v = v;
+                }
+            } else {
+                float t;
+                if (sphere_hit(o, r, t) && t < closest) {
+                    closest = t;
+                    h.obj = k;
+                    h.tri = -1;
+                    h.t = t;
+                }
+            }
+        }
+        for (;;) {
+            if (tst.sp == sp0)
+                return h;
+            const uint2 e = tst.pop();
+            if (__uint_as_float(e.y) < closest) {
+                ref = e.x;
+                break;
+            }
+        }
+    }
+}
+
+// Scene::intersectP -> BVHAccel::IntersectP over objects (BVH.cpp:421-473):
+// MeshTriangle::intersectT answers 1e-3 when its own IntersectP finds an
+// occluder (Triangle.hpp:141-147) and Sphere falls back to
+// Object::intersectT (Object.hpp:24-29); the caller then requires
+// t >= 0 && t < tMax.
+__device__ __forceinline__ bool scene_occluded(const DevScene &S, const RayD &r,
+                                               const RayPre &p, SmemStack &tst, SmemStack &bst,
+                                               float tmax) {
+    if (S.n_objects == 0)
+        return false;
+    if (!(slab6(S.tlas_box, p) < tmax))
+        return false;
+    const int sp0 = tst.sp;
+    uint32_t ref = S.tlas_root;
+    for (;;) {
+        if (!(ref & kLeafBit)) {
+            const NodeV n = load_node(S.nodes, ref);
+            const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+            const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+            const uint32_t axis = n.link.z;
+            const bool neg = axis == 0 ? p.nx : (axis == 1 ? p.ny : p.nz);
+            const uint32_t near_ref = neg ? n.link.y : n.link.x;
+            const uint32_t far_ref = neg ? n.link.x : n.link.y;
+            const float tnear = neg ? tr : tl;
+            const float tfar = neg ? tl : tr;
+            if (tfar < tmax)
+                tst.push(far_ref, 0.f);
+            if (tnear < tmax) {
+                ref = near_ref;
+                continue;
+            }
+        } else {
+            const DevObject &o = S.objects[ref & ~kLeafBit];
+            bool occ;
+            if (o.kind == kObjMesh) {
+                occ = blas_occluded(S.nodes, S.tris, o.root, o.root_box, r, p, bst, tmax) &&
+                      (1e-3f < tmax);
+            } else {
+                float t;
+                occ = sphere_hit(o, r, t) && t < tmax && t >= 0.f;
+            }
+            if (occ) {
+                tst.sp = sp0;
+                return true;
+            }
+        }
+        if (tst.sp == sp0)
+            return false;
+        ref = tst.pop().x;
+    }
+}
+
+} // namespace prr
