@@ -61,9 +61,12 @@ typedef struct prr_camera {
 /* Traversal launch shape (chosen by the autotuner; zero fields = defaults). */
 typedef struct prr_trace_config {
     int block_size;   /* threads per block (multiple of 32) */
-    int persistent;   /* 1: grid of SMs x blocks_per_sm pulling ray batches */
-    int blocks_per_sm;
-    int batch;        /* rays fetched per warp per atomic when persistent */
+    int persistent;   /* 0: one ray per thread; 1: persistent grid, each warp
+                         takes 32 rays at a time; 2: persistent grid, lanes whose
+                         ray finished take new rays as soon as `batch` lanes of the
+                         warp are idle */
+    int blocks_per_sm;/* persistent grids: resident blocks per SM (0 = occupancy) */
+    int batch;        /* mode 2 refill threshold in idle lanes (0 = 8) */
 } prr_trace_config;
 
 typedef struct prr_scene_stats {

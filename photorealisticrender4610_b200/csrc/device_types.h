@@ -7,7 +7,7 @@
 // CHILD boxes, so one interior step is one aligned 64-byte fetch (two 32-byte
 // sectors) instead of two scattered 32-byte ones. Leaves need no record: a
 // child reference with the top bit set points straight at the leaf's first
-// triangle, and that triangle carries the leaf's primitive count.
+// triangle and carries the leaf's primitive count.
 //
 // The slab test reads the same float bounds and does the same operations in
 // the same order as BVHAccel::nodeIntersect (BVH.hpp:115-124), so entry
@@ -25,13 +25,24 @@ namespace prr {
 
 constexpr uint32_t kLeafBit = 0x80000000u;
 
+// Mesh-BVH leaf references carry their primitive count: a mesh BVH is built
+// with maxPrimsInNode 4 (Triangle.hpp:173-179), so count-1 fits in the low two
+// bits and the first triangle in the 29 above. Scene-BVH leaves hold exactly
+// one object (maxPrimsInNode 1, Scene.cpp:17) and store its index directly.
+constexpr int64_t kMaxTriangles = int64_t(1) << 29;
+PRR_HD inline uint32_t mesh_leaf_ref(uint32_t first, uint32_t count) {
+    return kLeafBit | (first << 2) | (count - 1u);
+}
+PRR_HD inline uint32_t leaf_first(uint32_t ref) { return (ref & ~kLeafBit) >> 2; }
+PRR_HD inline uint32_t leaf_count(uint32_t ref) { return (ref & 3u) + 1u; }
+
 // One interior node: boxes of its left (reference idx+1) and right
 // (reference first_child) children, interleaved [minX,maxX,minY,maxY,minZ,maxZ]
 // like BVHNode::bounds, plus the child references.
 struct alignas(64) WNode {
     float lb[6];        // left child bounds
     float rb[6];        // right child bounds
-    uint32_t left;      // interior: WNode index; leaf: kLeafBit | first triangle
+    uint32_t left;      // interior: WNode index; leaf: mesh_leaf_ref / kLeafBit | object
     uint32_t right;
     uint32_t axis;      // split axis of this node (IntersectP near-child choice, BVH.cpp:384-391)
     float left_area;    // nodeAreas[idx+1] (light-sampling descent, BVH.cpp:488-496)
@@ -45,7 +56,7 @@ struct alignas(16) Tri {
     float e1y, e1z, e2x, e2y;
     float e2z;
     int32_t id;         // index of the triangle in its mesh's input order
-    uint32_t leaf_count;// primitive count of the leaf this triangle starts (0 inside a leaf)
+    uint32_t reserved;
     float area;         // Triangle::area (Triangle.hpp:31)
 };
 static_assert(sizeof(Tri) == 48, "Tri must be 48 bytes");

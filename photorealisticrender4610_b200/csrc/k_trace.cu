@@ -97,6 +97,141 @@ __global__ void k_mesh_closest_persistent(MeshArgs a) {
     }
 }
 
+// Persistent with per-lane refill. Each loop iteration performs ONE step of
+// the lane's ray: one interior node (two child slab tests, BVH.cpp:368-397),
+// or one triangle of the current leaf (BVH.cpp:343-357), followed when needed
+// by the pop of BVH.cpp:400-407. A lane whose ray is done stays idle until
+// `refill` lanes of its warp are idle; then the warp takes that many new rays
+// with one atomic and the idle lanes start them. Rays finishing at different
+// depths therefore no longer hold their warp hostage, and every ray still
+// visits exactly the nodes and triangles, in exactly the order, of the
+// reference walk.
+__global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
+    extern __shared__ uint2 smem[];
+    uint2 *col = smem + threadIdx.x;
+    const int stride = blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    int64_t idx = -1;
+    RayD r{};
+    RayPre p{};
+    float best = kInf;
+    int hit = -1;
+    uint32_t ref = 0, tri = 0, ntri = 0;
+    int sp = 0;
+    bool more = true; // warp-uniform: the ray counter is not exhausted
+    for (;;) {
+        const bool idle = idx < 0;
+        const unsigned im = __ballot_sync(full, idle);
+        if (!more && im == full)
+            break;
+        if (more && __popc(im) >= refill) {
+            const int cnt = __popc(im);
+            unsigned long long base = 0;
+            if (lane == 0)
+                base = atomicAdd(a.counter, (unsigned long long) cnt);
+            base = __shfl_sync(full, base, 0);
+            if ((int64_t) (base + cnt) >= a.n)
+                more = false;
+            if (idle) {
+                const int64_t ni = (int64_t) base + __popc(im & ((1u << lane) - 1u));
+                if (ni < a.n) {
+                    idx = ni;
+                    r = load_ray(a.O, a.D, ni);
+                    p = precompute(r);
+                    best = kInf;
+                    hit = -1;
+                    sp = 0;
+                    if (a.root & kLeafBit) {
+                        tri = leaf_first(a.root);
+                        ntri = leaf_count(a.root);
+                    } else {
+                        ref = a.root;
+                        ntri = 0;
+                    }
+                }
+            }
+        }
+        if (idx < 0)
+            continue;
+        bool pop = false;
+        if (ntri > 0) {
+            const TriV T = load_tri(a.tris, tri);
+            float t, u, v;
+            if (tri_hit(T, r, t, u, v) && t < best) {
+                best = t;
+                hit = (int) tri;
+            }
+            tri++;
+            ntri--;
+            pop = ntri == 0;
+        } else {
+            const NodeV n = load_node(a.nodes, ref);
+            const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+            const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+            uint32_t next = 0;
+            bool down = false;
+            if (tl <= tr) {
+                if (tl < best) {
+                    if (tr < best) {
+                        col[sp * stride] = make_uint2(n.link.y, __float_as_uint(tr));
+                        sp++;
+                    }
+                    next = n.link.x;
+                    down = true;
+                }
+            } else {
+                if (tr < best) {
+                    if (tl < best) {
+                        col[sp * stride] = make_uint2(n.link.x, __float_as_uint(tl));
+                        sp++;
+                    }
+                    next = n.link.y;
+                    down = true;
+                }
+            }
+            if (down) {
+                if (next & kLeafBit) {
+                    tri = leaf_first(next);
+                    ntri = leaf_count(next);
+                } else {
+                    ref = next;
+                }
+            } else {
+                pop = true;
+            }
+        }
+        if (pop) {
+            bool found = false;
+            uint32_t next = 0;
+            while (sp > 0) {
+                --sp;
+                const uint2 e = col[sp * stride];
+                if (__uint_as_float(e.y) < best) {
+                    next = e.x;
+                    found = true;
+                    break;
+                }
+            }
+            if (found) {
+                if (next & kLeafBit) {
+                    tri = leaf_first(next);
+                    ntri = leaf_count(next);
+                } else {
+                    ref = next;
+                }
+            } else {
+                a.out_id[idx] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+                a.out_t[idx] = best;
+                if (a.out_t64)
+                    a.out_t64[idx] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r)
+                                              : __longlong_as_double(0x7ff8000000000000LL);
+                idx = -1;
+            }
+        }
+    }
+}
+
 __global__ void k_mesh_occluded(const WNode *nodes, const Tri *tris, uint32_t root,
                                 DevObject obj, const float *O, const float *D,
                                 const float *__restrict__ tmax, int64_t n, uint8_t *out) {
@@ -238,20 +373,28 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     const size_t smem = (size_t) cap * block * sizeof(uint2);
     if (smem > 227 * 1024)
         return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
-    const bool persistent = cfg && cfg->persistent;
-    if (persistent) {
+    const int mode = cfg ? cfg->persistent : 0;
+    if (mode < 0 || mode > 2)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1 or 2");
+    if (mode > 0) {
         if (!counter)
             return fail(PRR_ERR_INVALID_ARGUMENT, "persistent launch needs a counter");
-        if (int rc = set_smem((const void *) k_mesh_closest_persistent, smem))
+        const void *fn = mode == 1 ? (const void *) k_mesh_closest_persistent
+                                   : (const void *) k_mesh_closest_refill;
+        if (int rc = set_smem(fn, smem))
             return rc;
         int bps = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 0;
         if (bps == 0) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_mesh_closest_persistent, block,
-                                                          smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, fn, block, smem);
             bps = std::max(1, bps);
         }
         PRR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
-        k_mesh_closest_persistent<<<device_sm_count() * bps, block, smem, st>>>(a);
+        if (mode == 1) {
+            k_mesh_closest_persistent<<<device_sm_count() * bps, block, smem, st>>>(a);
+        } else {
+            const int refill = cfg->batch > 0 ? std::min(cfg->batch, 32) : 8;
+            k_mesh_closest_refill<<<device_sm_count() * bps, block, smem, st>>>(a, refill);
+        }
     } else {
         if (int rc = set_smem((const void *) k_mesh_closest, smem))
             return rc;

@@ -37,7 +37,7 @@ PrimBox mesh_bounds(const std::vector<float> &v) {
 // references to their first primitive (meshes) or to their object (scene
 // BVH). Returns the root reference.
 int pack_tree(const FlatBVH &f, bool object_leaves, int tri_base, std::vector<WNode> &out,
-              std::vector<Tri> *tris, uint32_t &root_ref) {
+              uint32_t &root_ref) {
     const size_t n = f.size();
     std::vector<uint32_t> wide(n, 0xFFFFFFFFu);
     const uint32_t base = (uint32_t) out.size();
@@ -51,15 +51,15 @@ int pack_tree(const FlatBVH &f, bool object_leaves, int tri_base, std::vector<WN
             return wide[i];
         if (object_leaves)
             return kLeafBit | (uint32_t) f.ordered[f.first_child[i]];
-        return kLeafBit | (uint32_t) (tri_base + f.first_child[i]);
+        return mesh_leaf_ref((uint32_t) (tri_base + f.first_child[i]), cnt);
     };
     for (size_t i = 0; i < n; i++) {
         const uint32_t cnt = f.meta[i] & 0x00FFFFFFu;
         if (cnt > 0) {
             if (object_leaves && cnt != 1)
                 return fail(PRR_ERR_INTERNAL, "scene BVH leaf with more than one object");
-            if (tris)
-                (*tris)[tri_base + f.first_child[i]].leaf_count = cnt;
+            if (!object_leaves && cnt > 4)
+                return fail(PRR_ERR_INTERNAL, "mesh BVH leaf with more than four triangles");
         }
     }
     out.resize(base + k);
@@ -158,8 +158,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     int64_t ntri = 0;
     for (int k : meshes)
         ntri += (int64_t) s.objects[k].verts.size() / 9;
-    if (ntri >= (int64_t) kLeafBit)
-        return fail(PRR_ERR_UNSUPPORTED, "too many triangles");
+    if (ntri >= kMaxTriangles)
+        return fail(PRR_ERR_UNSUPPORTED, "too many triangles (limit 2^29 per scene)");
     tris.resize(ntri);
     verts.resize((size_t) ntri * 9);
     normals.resize((size_t) ntri * 3);
@@ -186,7 +186,7 @@ int build_scene(Scene &s, cudaStream_t st) {
             t.e2y = e2y;
             t.e2z = e2z;
             t.id = id;
-            t.leaf_count = 0;
+            t.reserved = 0;
             const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z,
                         cz = e1x * e2y - e1y * e2x;
             t.area = std::sqrt(cx * cx + cy * cy + cz * cz) * 0.5f;
@@ -204,7 +204,7 @@ int build_scene(Scene &s, cudaStream_t st) {
             normals[(size_t) (base + j) * 3 + 2] = nz;
             std::memcpy(&verts[(size_t) (base + j) * 9], p, 9 * sizeof(float));
         }
-        if (int rc = pack_tree(o.bvh, false, base, nodes, &tris, o.root))
+        if (int rc = pack_tree(o.bvh, false, base, nodes, o.root))
             return rc;
         blas_depth = std::max(blas_depth, o.bvh.max_depth);
         base += (int) nt;
@@ -220,7 +220,7 @@ int build_scene(Scene &s, cudaStream_t st) {
     s.tlas = build_sah(ob, oa, 1, 1);
     uint32_t tlas_root = 0;
     if (!s.objects.empty())
-        if (int rc = pack_tree(s.tlas, true, 0, nodes, nullptr, tlas_root))
+        if (int rc = pack_tree(s.tlas, true, 0, nodes, tlas_root))
             return rc;
 
     // ---- objects, materials, emitters (Scene.cpp:19-26) ----

@@ -194,8 +194,8 @@ __device__ __forceinline__ int blas_closest(const WNode *__restrict__ nodes,
                 }
             }
         } else {
-            const uint32_t first = ref & ~kLeafBit;
-            const uint32_t cnt = __ldg(&tris[first].leaf_count);
+            const uint32_t first = leaf_first(ref);
+            const uint32_t cnt = leaf_count(ref);
             for (uint32_t i = 0; i < cnt; i++) {
                 const TriV T = load_tri(tris, first + i);
                 float t, u, v;
@@ -251,8 +251,8 @@ __device__ __forceinline__ bool blas_occluded(const WNode *__restrict__ nodes,
                 continue;
             }
         } else {
-            const uint32_t first = ref & ~kLeafBit;
-            const uint32_t cnt = __ldg(&tris[first].leaf_count);
+            const uint32_t first = leaf_first(ref);
+            const uint32_t cnt = leaf_count(ref);
             for (uint32_t i = 0; i < cnt; i++) {
                 const TriV T = load_tri(tris, first + i);
                 if (tri_occludes(T, r, tmax)) {

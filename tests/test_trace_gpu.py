@@ -19,7 +19,9 @@ def dev(a, cuda):
 
 
 @pytest.mark.parametrize("case", MESH_CASES)
-@pytest.mark.parametrize("config", [None, {"persistent": 1}, {"block_size": 64}])
+@pytest.mark.parametrize("config", [None, {"persistent": 1}, {"block_size": 64},
+                                    {"persistent": 2}, {"persistent": 2, "batch": 1},
+                                    {"persistent": 2, "batch": 32, "block_size": 64}])
 def test_mesh_intersect_bit_exact(golden, cuda, case, config):
     g = golden("mesh")
     p = f"mesh_{case}_"
@@ -70,9 +72,12 @@ def test_query_set_full_size_against_restatement(port, cuda):
     assert hit.mean() > 0.99
     assert np.array_equal(t64[hit], rt64[hit])
     assert np.isnan(t64[~hit]).all()
-    # persistent launch shape gives the same answer
-    hid2, t2 = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), config={"persistent": 1})
-    assert np.array_equal(hid2.cpu().numpy(), rh)
+    # the persistent launch shapes give the same answer
+    for cfg in ({"persistent": 1}, {"persistent": 2}, {"persistent": 2, "batch": 16}):
+        hid2, t2, t642 = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), t64=True, config=cfg)
+        assert np.array_equal(hid2.cpu().numpy(), rh)
+        assert np.array_equal(t2.cpu().numpy().view(np.uint32), rt.view(np.uint32))
+        assert np.array_equal(t642.cpu().numpy()[hit], rt64[hit])
     # any hit agrees with closest hit at tmax just beyond / before the hit
     tm = np.where(hit, rt * np.float32(1.0001), np.float32(10.0)).astype(np.float32)
     occ = s.mesh_occluded(0, dev(o, cuda), dev(d, cuda), dev(tm, cuda)).cpu().numpy()
