@@ -69,6 +69,24 @@ typedef struct prr_trace_config {
     int batch;        /* mode 2 refill threshold in idle lanes (0 = 8) */
 } prr_trace_config;
 
+#define PRR_RENDER_PLAIN 0     /* one megakernel thread per (pixel, sample range) */
+#define PRR_RENDER_WAVEFRONT 1 /* staged wavefront integrator */
+
+/* RenderSettings (Renderer.hpp:42-55) plus the integrator's knobs. */
+typedef struct prr_render_settings {
+    int width, height;        /* must equal the camera's (Camera::init) */
+    int min_spp, max_spp;     /* minSPP == maxSPP: fixed spp; else the Welford
+                                 confidence stop of Renderer.cpp:88-95 */
+    int max_depth;            /* Integrator maxDepth */
+    float variance_threshold; /* varianceThreshold */
+    float indirect_clamp;     /* Integrator::indirectClamp (10 in the reference) */
+    int mode;                 /* PRR_RENDER_PLAIN / PRR_RENDER_WAVEFRONT */
+    uint64_t seed;            /* sample n of pixel m = i + j*W draws stream (seed, m, n) */
+    int x0, y0, x1, y1;       /* pixel window [x0,x1) x [y0,y1); x1 or y1 <= 0: full frame */
+    int sample_offset;        /* index of the first sample (progressive passes, resume) */
+    int slices;               /* plain fixed-spp mode: threads per pixel (0 = automatic) */
+} prr_render_settings;
+
 typedef struct prr_scene_stats {
     int64_t n_objects, n_triangles, n_nodes;
     int32_t tlas_depth, blas_depth;
@@ -151,6 +169,41 @@ int prr_scene_intersect(const prr_scene *scene, const float *o, const float *d, 
  * Sphere intersectT). */
 int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
                        const float *tmax, int64_t n, uint8_t *out_hit, void *stream);
+
+/* ---- rendering --------------------------------------------------------- */
+/* Renderer::Render's sample loop (Renderer.cpp:63-99) around
+ * Integrator::castRay (Integrator.cpp:104-263) over the window:
+ * out_rgb = window pixels x 3 floats, the linear mean radiance per pixel
+ * (the framebuffer before exposure and tone mapping), row-major.
+ * out_spp (optional) = samples taken per pixel; out_rays (optional, 2 x
+ * uint64) = closest-hit and shadow rays traced. Device pointers. */
+int prr_render(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
+               int32_t *out_spp, uint64_t *out_rays, void *stream);
+
+/* Integrator::castRay for a batch of (pixel, sample) pairs: the radiance of
+ * each path, drawing from stream (seed, px + py*W, sample) exactly as a render
+ * of that sample would. out_rgb = n x 3. */
+int prr_cast_samples(const prr_scene *scene, const int32_t *px, const int32_t *py,
+                     const int32_t *sample, int64_t n, uint64_t seed, int max_depth,
+                     float indirect_clamp, float *out_rgb, void *stream);
+/* Camera::generateRay (Camera.hpp:75-95) for given pixel offsets (pinhole). */
+int prr_camera_rays(const prr_scene *scene, const int32_t *px, const int32_t *py,
+                    const float *xo, const float *yo, int64_t n, float *out_o, float *out_d,
+                    void *stream);
+/* Scene::sampleLight (Scene.cpp:37-58), sample k drawing from stream
+ * (seed, k, 0): points, normals and the area pdf 1/totalEmitArea. */
+int prr_scene_sample_light(const prr_scene *scene, uint64_t seed, int64_t n, float *out_pos,
+                           float *out_normal, float *out_pdf, void *stream);
+/* EnvMap::sample and EnvMap::importanceSamplePdf (EnvMap.hpp:97-133). */
+int prr_env_eval(const prr_scene *scene, const float *dirs, int64_t n, float *out_rgb,
+                 float *out_pdf, void *stream);
+/* EnvMap::importanceSample (EnvMap.hpp:145-169), sample k drawing from
+ * stream (seed, k, 0). */
+int prr_env_importance_sample(const prr_scene *scene, uint64_t seed, int64_t n, float *out_dirs,
+                              float *out_pdf, void *stream);
+/* Host copies of the device-built CDF tables (EnvMap::cdf, marginalCdf,
+ * totalLuminance). Any output may be NULL. */
+int prr_env_export(const prr_scene *scene, float *cdf, float *marginal, float *total);
 
 #ifdef __cplusplus
 }

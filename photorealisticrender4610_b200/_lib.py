@@ -47,9 +47,9 @@ class prr_scene_stats(C.Structure):
 class prr_render_settings(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("min_spp", C.c_int),
                 ("max_spp", C.c_int), ("max_depth", C.c_int), ("variance_threshold", C.c_float),
-                ("seed", C.c_uint64), ("mode", C.c_int), ("x0", C.c_int), ("y0", C.c_int),
-                ("x1", C.c_int), ("y1", C.c_int), ("sample_offset", C.c_int),
-                ("reserved", C.c_int * 3)]
+                ("indirect_clamp", C.c_float), ("mode", C.c_int), ("seed", C.c_uint64),
+                ("x0", C.c_int), ("y0", C.c_int), ("x1", C.c_int), ("y1", C.c_int),
+                ("sample_offset", C.c_int), ("slices", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -76,6 +76,14 @@ _SIGS = {
     "prr_mesh_occluded": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
+    "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
+    "prr_cast_samples": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_uint64, C.c_int, C.c_float,
+                                   _vp, _vp]),
+    "prr_camera_rays": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp, _vp]),
+    "prr_scene_sample_light": (C.c_int, [_vp, C.c_uint64, C.c_int64, _vp, _vp, _vp, _vp]),
+    "prr_env_eval": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp, _vp]),
+    "prr_env_importance_sample": (C.c_int, [_vp, C.c_uint64, C.c_int64, _vp, _vp, _vp]),
+    "prr_env_export": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_float)]),
 }
 
 _lib = None

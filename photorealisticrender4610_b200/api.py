@@ -15,7 +15,9 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import check, prr_camera, prr_scene_stats, prr_trace_config
+from ._lib import check, prr_camera, prr_render_settings, prr_scene_stats, prr_trace_config
+
+RENDER_MODES = {"plain": 0, "wavefront": 1}
 
 
 def _ptr(t):
@@ -211,3 +213,102 @@ class Scene:
         check(self.lib.prr_scene_occluded(self.h, _ptr(o), _ptr(d), _ptr(tmax), o.shape[0],
                                           _ptr(out), _stream(stream)))
         return out
+
+    # ---- rendering (Renderer::Render up to the linear framebuffer) ----
+    def render(self, spp: int, max_depth: int, seed: int = 1, min_spp: int | None = None,
+               threshold: float = 0.05, mode: str = "plain", window=None,
+               indirect_clamp: float = 10.0, sample_offset: int = 0, slices: int = 0,
+               count_rays: bool = False, stream=None):
+        """Mean radiance per pixel of the window: (h, w, 3) float32 CUDA tensor,
+        plus samples per pixel and, with count_rays, (closest, shadow) rays."""
+        import torch
+        if self.desc is None:
+            raise ValueError("render needs a scene created with Scene.from_desc")
+        W, H = self.desc.width, self.desc.height
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        rs = prr_render_settings()
+        rs.width, rs.height = W, H
+        rs.min_spp = spp if min_spp is None else min_spp
+        rs.max_spp = spp
+        rs.max_depth = max_depth
+        rs.variance_threshold = threshold
+        rs.indirect_clamp = indirect_clamp
+        rs.mode = RENDER_MODES[mode]
+        rs.seed = seed
+        rs.x0, rs.y0, rs.x1, rs.y1 = x0, y0, x1, y1
+        rs.sample_offset = sample_offset
+        rs.slices = slices
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
+        cnt = torch.empty(((y1 - y0), (x1 - x0)), dtype=torch.int32, device=dev)
+        rays = torch.zeros(2, dtype=torch.int64, device=dev) if count_rays else None
+        check(self.lib.prr_render(self.h, C.byref(rs), _ptr(out), _ptr(cnt), _ptr(rays),
+                                  _stream(stream)))
+        if count_rays:
+            return out, cnt, rays
+        return out, cnt
+
+    # ---- per-call reference methods, batched ----
+    def cast_samples(self, px, py, sample, max_depth: int, seed: int = 1,
+                     indirect_clamp: float = 10.0, stream=None):
+        """Integrator::castRay per (pixel, sample): (n, 3) radiance."""
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        px = torch.as_tensor(np.ascontiguousarray(px, np.int32)).to(dev)
+        py = torch.as_tensor(np.ascontiguousarray(py, np.int32)).to(dev)
+        sm = torch.as_tensor(np.ascontiguousarray(sample, np.int32)).to(dev)
+        out = torch.empty((px.shape[0], 3), dtype=torch.float32, device=dev)
+        check(self.lib.prr_cast_samples(self.h, _ptr(px), _ptr(py), _ptr(sm), px.shape[0], seed,
+                                        max_depth, indirect_clamp, _ptr(out), _stream(stream)))
+        return out
+
+    def camera_rays(self, px, py, xo, yo, stream=None):
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        t = [torch.as_tensor(np.ascontiguousarray(a, dt)).to(dev)
+             for a, dt in ((px, np.int32), (py, np.int32), (xo, np.float32), (yo, np.float32))]
+        n = t[0].shape[0]
+        o = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        d = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        check(self.lib.prr_camera_rays(self.h, *map(_ptr, t), n, _ptr(o), _ptr(d),
+                                       _stream(stream)))
+        return o, d
+
+    def sample_light(self, seed: int, n: int, stream=None):
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        pos = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        nrm = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        pdf = torch.empty(n, dtype=torch.float32, device=dev)
+        check(self.lib.prr_scene_sample_light(self.h, seed, n, _ptr(pos), _ptr(nrm), _ptr(pdf),
+                                              _stream(stream)))
+        return pos, nrm, pdf
+
+    def env_eval(self, dirs, stream=None):
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        d = torch.as_tensor(np.ascontiguousarray(dirs, np.float32)).to(dev)
+        rgb = torch.empty_like(d)
+        pdf = torch.empty(d.shape[0], dtype=torch.float32, device=dev)
+        check(self.lib.prr_env_eval(self.h, _ptr(d), d.shape[0], _ptr(rgb), _ptr(pdf),
+                                    _stream(stream)))
+        return rgb, pdf
+
+    def env_importance_sample(self, seed: int, n: int, stream=None):
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        d = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        pdf = torch.empty(n, dtype=torch.float32, device=dev)
+        check(self.lib.prr_env_importance_sample(self.h, seed, n, _ptr(d), _ptr(pdf),
+                                                 _stream(stream)))
+        return d, pdf
+
+    def env_export(self):
+        e = self.desc.env
+        h, w = e.shape[:2]
+        cdf = np.empty(h * w, np.float32)
+        marg = np.empty(h, np.float32)
+        tot = C.c_float()
+        check(self.lib.prr_env_export(self.h, C.c_void_p(cdf.ctypes.data),
+                                      C.c_void_p(marg.ctypes.data), C.byref(tot)))
+        return cdf, marg, tot.value

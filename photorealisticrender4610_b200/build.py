@@ -78,7 +78,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, jobs: int = 8) -> 
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(max_workers=jobs) as ex:
             list(ex.map(lambda c: _run(c, verbose), cmds))
-    if cmds or not LIB.exists():
+    if cmds or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs),
               "-Xcompiler", "-pthread"], verbose)

@@ -90,7 +90,15 @@ struct Scene {
     DevBuf d_nodes, d_tris, d_verts, d_normals, d_objects, d_materials, d_emissives;
     DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin;
     DevBuf d_scratch;      // staging for host-buffer entry points
+    DevBuf d_render, d_render_spp; // per-slice partial sums / adaptive spp
     DevBuf d_counter;      // persistent-kernel work counters
+    // Renders reuse the scratch above; each render waits for the previous
+    // one's event before touching it, whatever stream either ran on.
+    cudaEvent_t scratch_done = nullptr;
+    ~Scene() {
+        if (scratch_done)
+            cudaEventDestroy(scratch_done);
+    }
 };
 
 // Kernel launchers (k_*.cu). All return a status; launch errors are checked.
@@ -104,6 +112,10 @@ int launch_scene_closest(const Scene &s, const float *o, const float *d, int64_t
 int launch_scene_occluded(const Scene &s, const float *o, const float *d, const float *tmax,
                           int64_t n, uint8_t *hit, cudaStream_t st);
 int launch_env_cdf(Scene &s, cudaStream_t st);
+int render_plain(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
+                 unsigned long long *out_rays, cudaStream_t st);
+int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
+                     unsigned long long *out_rays, cudaStream_t st);
 
 int device_sm_count();
 
