@@ -361,6 +361,106 @@ def run_ours(args, rank, world, on):
     return 0
 
 
+RENDER_WORKLOADS = {
+    # name: (scene factory, spp, depth, description)
+    "museum": (lambda: __import__("photorealisticrender4610_b200.scenes", fromlist=["x"]).museum_like(),
+               64, 8, "museum-like: 6 displaced level-7 icospheres (1,966,082 triangles), "
+               "2048x1024 HDR sky, 1920x1080, 64 spp, depth 8"),
+    "cornell": (lambda: __import__("photorealisticrender4610_b200.scenes", fromlist=["x"]).cornell_box(),
+                16, 5, "Cornell box 256x256, 16 spp, depth 5"),
+}
+
+
+def run_render(args, rank, world, on):
+    """Samples/s of the plain megakernel and of the wavefront integrator on a
+    full frame (value = wavefront, the faster one; both reported)."""
+    import torch
+    import photorealisticrender4610_b200 as prr
+
+    factory, spp, depth, desc_text = RENDER_WORKLOADS[args.workload]
+    dev = torch.device("cuda", torch.cuda.current_device())
+    desc = factory()
+    scene = prr.Scene.from_desc(desc)
+    npix = desc.width * desc.height
+    tuned = scene.autotune(4, depth)
+
+    def timed(mode, steps):
+        ms = []
+        rays = None
+        for _ in range(steps):
+            torch.cuda._sleep(2_000_000)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            img, _, rays = scene.render(spp, depth, seed=1, mode=mode, slices=0, count_rays=True)
+            b.record()
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return ms, img, rays
+
+    timed("plain", 1)
+    timed("wavefront", args.warmup)
+    with ClockSampler(dev.index) as clk:
+        barrier(on)
+        wf_ms, wf_img, wf_rays = timed("wavefront", args.steps)
+        barrier(on)
+    pl_ms, pl_img, pl_rays = timed("plain", max(1, min(args.steps, 3)))
+    wf_step = max_over_ranks(float(np.mean(wf_ms)), on)
+    pl_step = max_over_ranks(float(np.mean(pl_ms)), on)
+    samples = npix * spp
+    value = samples * world / (wf_step * 1e-3) / 1e6
+    plain_value = samples * world / (pl_step * 1e-3) / 1e6
+    rays = wf_rays.cpu().numpy()
+    rel = float(((wf_img - pl_img) ** 2).sum() / (pl_img ** 2).sum())
+
+    # end to end: the C ABI call plus the copy of the image to pinned host memory
+    host = torch.empty((desc.height, desc.width, 3), dtype=torch.float32).pin_memory()
+    e2e = []
+    for _ in range(max(2, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        img, _ = scene.render(spp, depth, seed=1, mode="wavefront")
+        host.copy_(img)
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_value = samples * world / (float(np.median(e2e)) * 1e-3) / 1e6
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    cpu = None
+    from oracle import loader
+    if loader.reference_available(fast=True):
+        ref = loader.ReferenceOracle(fast=True)
+        rs = ref.scene(desc)
+        win = (desc.width // 2 - 32, desc.height // 2 - 32, desc.width // 2 + 32,
+               desc.height // 2 + 32)
+        cspp = 16
+        t0 = time.perf_counter()
+        rs.render(depth, cspp, 1, window=win, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": 64 * 64 * cspp / dt / 1e6, "unit": "Msamples/s", "cores": threads,
+               "kind": "reference", "sample": f"64x64 centre crop at {cspp} spp"}
+    line = {
+        "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wf_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": desc_text, "mode": "wavefront", "autotuned": tuned,
+                   "l2": "inputs (scene 2M tris + paths) exceed L2; not flushed"},
+        "plain_msamples_s": plain_value, "wavefront_vs_plain": value / plain_value,
+        "plain_vs_wavefront_rel_mse": rel,
+        "mrays_s": float(rays.sum()) / (wf_step * 1e-3) / 1e6,
+        "rays_per_frame": {"closest": int(rays[0]), "shadow": int(rays[1])},
+        "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": npix * 12},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,6 +468,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--launch", default="", help="fixed launch shape, e.g. block=128,persistent=0")
+    ap.add_argument("--workload", choices=["query", "museum", "cornell"], default="query")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the kernel only (no e2e, no CPU baseline): profiling runs")
     args = ap.parse_args()
@@ -379,6 +480,8 @@ def main():
         return run_reference(args, rank, world)
     on = init_dist(world, local)
     try:
+        if args.workload != "query":
+            return run_render(args, rank, world, on)
         return run_ours(args, rank, world, on)
     finally:
         if on:

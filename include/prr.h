@@ -87,6 +87,13 @@ typedef struct prr_render_settings {
     int slices;               /* plain fixed-spp mode: threads per pixel (0 = automatic) */
 } prr_render_settings;
 
+/* Wavefront launch shape (chosen by prr_autotune; zero fields = defaults). */
+typedef struct prr_wavefront_config {
+    int64_t paths_per_pass; /* paths in flight per pass (0: about 2M) */
+    int block_size;         /* threads per block of the traversal stages (0: 128) */
+    int use_graphs;         /* 1: replay each pass from one captured CUDA graph */
+} prr_wavefront_config;
+
 typedef struct prr_scene_stats {
     int64_t n_objects, n_triangles, n_nodes;
     int32_t tlas_depth, blas_depth;
@@ -179,6 +186,15 @@ int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
  * uint64) = closest-hit and shadow rays traced. Device pointers. */
 int prr_render(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
                int32_t *out_spp, uint64_t *out_rays, void *stream);
+
+/* Sets the wavefront launch shape used by prr_render in wavefront mode. */
+int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config);
+/* The autotuner: times the wavefront renderer on `settings` (the window and
+ * depth of the intended render, a few samples per pixel) over a grid of
+ * paths-per-pass and block sizes, keeps the fastest on the scene for later
+ * renders and writes it to out_best (optional). Synchronises `stream`. */
+int prr_autotune(prr_scene *scene, const prr_render_settings *settings,
+                 prr_wavefront_config *out_best, void *stream);
 
 /* Integrator::castRay for a batch of (pixel, sample) pairs: the radiance of
  * each path, drawing from stream (seed, px + py*W, sample) exactly as a render

@@ -38,6 +38,10 @@ class prr_trace_config(C.Structure):
                 ("batch", C.c_int)]
 
 
+class prr_wavefront_config(C.Structure):
+    _fields_ = [("paths_per_pass", C.c_int64), ("block_size", C.c_int), ("use_graphs", C.c_int)]
+
+
 class prr_scene_stats(C.Structure):
     _fields_ = [("n_objects", C.c_int64), ("n_triangles", C.c_int64), ("n_nodes", C.c_int64),
                 ("tlas_depth", C.c_int32), ("blas_depth", C.c_int32),
@@ -77,6 +81,9 @@ _SIGS = {
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
+    "prr_scene_set_wavefront": (C.c_int, [_vp, C.POINTER(prr_wavefront_config)]),
+    "prr_autotune": (C.c_int, [_vp, C.POINTER(prr_render_settings),
+                               C.POINTER(prr_wavefront_config), _vp]),
     "prr_cast_samples": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_uint64, C.c_int, C.c_float,
                                    _vp, _vp]),
     "prr_camera_rays": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp, _vp]),

@@ -15,7 +15,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import check, prr_camera, prr_render_settings, prr_scene_stats, prr_trace_config
+from ._lib import (check, prr_camera, prr_render_settings, prr_scene_stats, prr_trace_config,
+                   prr_wavefront_config)
 
 RENDER_MODES = {"plain": 0, "wavefront": 1}
 
@@ -215,6 +216,36 @@ class Scene:
         return out
 
     # ---- rendering (Renderer::Render up to the linear framebuffer) ----
+    def _settings(self, spp, max_depth, seed, min_spp, threshold, mode, window, indirect_clamp,
+                  sample_offset, slices):
+        if self.desc is None:
+            raise ValueError("render needs a scene created with Scene.from_desc")
+        W, H = self.desc.width, self.desc.height
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        rs = prr_render_settings()
+        rs.width, rs.height = W, H
+        rs.min_spp = spp if min_spp is None else min_spp
+        rs.max_spp = spp
+        rs.max_depth = max_depth
+        rs.variance_threshold = threshold
+        rs.indirect_clamp = indirect_clamp
+        rs.mode = RENDER_MODES[mode]
+        rs.seed = seed
+        rs.x0, rs.y0, rs.x1, rs.y1 = x0, y0, x1, y1
+        rs.sample_offset = sample_offset
+        rs.slices = slices
+        return rs
+
+    def set_wavefront(self, paths_per_pass: int = 0, block_size: int = 0, use_graphs: bool = True):
+        cfg = prr_wavefront_config(paths_per_pass, block_size, int(use_graphs))
+        check(self.lib.prr_scene_set_wavefront(self.h, C.byref(cfg)))
+
+    def autotune(self, spp: int, max_depth: int, window=None, seed: int = 1, stream=None) -> dict:
+        rs = self._settings(spp, max_depth, seed, None, 0.05, "wavefront", window, 10.0, 0, 0)
+        best = prr_wavefront_config()
+        check(self.lib.prr_autotune(self.h, C.byref(rs), C.byref(best), _stream(stream)))
+        return {k: getattr(best, k) for k, _ in best._fields_}
+
     def render(self, spp: int, max_depth: int, seed: int = 1, min_spp: int | None = None,
                threshold: float = 0.05, mode: str = "plain", window=None,
                indirect_clamp: float = 10.0, sample_offset: int = 0, slices: int = 0,

@@ -120,21 +120,24 @@ static __device__ V3 cast_ray(const DevScene &S, Ray3 ray, int max_depth, float 
             const float dist = sqrtf(dist2);
             const V3 wi = to / dist;
             const float cos_l = smax(0.f, dot(-wi, normalized(lp.n)));
+            // evalLightSample is formed before the visibility test (it has no
+            // side effects); a zero contribution needs no shadow ray because
+            // castRay would add exactly zero either way
             V3 c = v3(0.f);
             if (cos_l > 0.f) {
                 const float pdf_sa = pdf_area * dist2 / cos_l;
-                cnt.shadow++;
-                const bool vis = !occluded(S, hp + wi * PRR_EPS, wi, dist - 2.f * PRR_EPS, tst, bst);
-                if (vis) {
-                    V3 f;
-                    float bp;
-                    mat_eval_pdf(m, sd, wi, wo, &f, &bp);
-                    const float w = mis(pdf_sa, bp);
-                    const DevMaterial &lm = S.materials[lp.material];
-                    c = w * v3(lm.emission[0], lm.emission[1], lm.emission[2]) * f / pdf_sa;
+                V3 f;
+                float bp;
+                mat_eval_pdf(m, sd, wi, wo, &f, &bp);
+                const float w = mis(pdf_sa, bp);
+                const DevMaterial &lm = S.materials[lp.material];
+                c = beta * (w * v3(lm.emission[0], lm.emission[1], lm.emission[2]) * f / pdf_sa);
+                if (!(c.x == 0.f && c.y == 0.f && c.z == 0.f)) {
+                    cnt.shadow++;
+                    if (occluded(S, hp + wi * PRR_EPS, wi, dist - 2.f * PRR_EPS, tst, bst))
+                        c = v3(0.f);
                 }
             }
-            c = beta * c;
             L = L + (indirect ? clamp_indirect(c, clamp) : c);
         }
         // NEE towards the environment (sampleEnvironmentMap + evalEnvironmentSample)
@@ -143,17 +146,18 @@ static __device__ V3 cast_ray(const DevScene &S, Ray3 ray, int max_depth, float 
             const V3 dir = env_importance(env, rng, pdf);
             V3 c = v3(0.f);
             if (!(pdf < 1e-6f)) {
-                cnt.shadow++;
-                if (!occluded(S, hp + dir * PRR_EPS, dir, kInf, tst, bst)) {
-                    const V3 em = env_lookup(env, dir);
-                    V3 f;
-                    float bp;
-                    mat_eval_pdf(m, sd, dir, wo, &f, &bp);
-                    const float w = mis(pdf, bp);
-                    c = w * em * f / (pdf + 1e-6f);
+                const V3 em = env_lookup(env, dir);
+                V3 f;
+                float bp;
+                mat_eval_pdf(m, sd, dir, wo, &f, &bp);
+                const float w = mis(pdf, bp);
+                c = beta * (w * em * f / (pdf + 1e-6f));
+                if (!(c.x == 0.f && c.y == 0.f && c.z == 0.f)) {
+                    cnt.shadow++;
+                    if (occluded(S, hp + dir * PRR_EPS, dir, kInf, tst, bst))
+                        c = v3(0.f);
                 }
             }
-            c = beta * c;
             L = L + (indirect ? clamp_indirect(c, clamp) : c);
         }
         // BSDF sampling (Integrator.cpp:198-244)

@@ -1,11 +1,794 @@
-// Wavefront integrator (placeholder until the staged kernels land).
+// Wavefront integrator: Integrator::castRay (Integrator.cpp:104-263) cut into
+// stages that run over queues of paths instead of one path per thread.
+//
+// A pass traces samples [base, base + k) of every pixel of the window at once
+// (P = k * pixels paths). Per bounce:
+//   extend   closest hit of every queued ray; the path is appended to the
+//            miss, delta (mirror/glass) or surface (diffuse/emissive) queue of
+//            its hit -- the sort by material, made with warp-aggregated appends
+//   miss     background / env contributions, path ends
+//   delta    specular chain step (Integrator.cpp:143-169)
+//   surface  NEE towards emitters and the environment (shadow rays queued with
+//            their would-be contributions), BSDF sample, next ray queued
+//   shadow   any-hit of the queued shadow rays; visible contributions added
+// The pending part of a non-delta bounce -- the MIS terms for an env miss or
+// an emitter hit, beta *= f/pdf, Russian roulette (Integrator.cpp:205-256) --
+// runs at the start of the stage that sees the next hit, so every path makes
+// the same random draws and the same additions to L in the same order as
+// castRay. At the end of a pass each pixel adds its k results in sample order,
+// so the film is the plain renderer's, bit for bit.
+//
+// Every kernel reads its queue length from device memory, so a pass is one
+// fixed launch sequence; it is captured once in a CUDA graph and replayed.
+#include "integrator.cuh"
 #include "prr_internal.h"
+#include "trace_step.cuh"
+
+#include <algorithm>
+#include <cstring>
 
 namespace prr {
+namespace {
 
-int render_wavefront(Scene &, const prr_render_settings &, float *, int32_t *,
-                     unsigned long long *, cudaStream_t) {
-    return fail(PRR_ERR_UNSUPPORTED, "wavefront mode not available in this build");
+enum : int { kFlagSpecular = 1, kFlagPending = 2, kFlagEndAfterShadow = 4 };
+enum : int {
+    kCntRay0 = 0, kCntRay1 = 1, kCntMiss = 2, kCntDelta = 3, kCntSurf = 4, kCntShadow = 5,
+    kCntExtend = 6, kCntShadowJobs = 7, kCntRays = 8, kCntShadowRays = 10, kCntShadowFetch = 12,
+    kCntSlots = 16
+};
+
+struct Wf {
+    int P, npix, spp_pass;
+    int W, x0, y0, ww;
+    int max_depth;
+    float clamp;
+    uint64_t seed;
+    int tlas_cap, blas_cap;
+    // path state
+    uint64_t *rng;
+    float4 *ro, *rd;     // current ray
+    float4 *beta;        // xyz
+    float4 *L;           // xyz
+    int *bounce, *flags;
+    float4 *pend;        // pending BSDF: f/pdf xyz, pdf
+    float4 *prev;        // pending BSDF: hit point it left from
+    int4 *hit;           // obj, tri, t bits
+    float4 *slo, *sld, *slc; // light shadow ray: origin+tmax, dir+valid, contribution
+    float4 *seo, *sed, *sec; // env shadow ray
+    float4 *result;      // final L per path
+    float3 *film;        // per pixel running sum
+    // queues
+    int *qray[2], *qmiss, *qdelta, *qsurf, *qshadow, *qjob;
+    uint8_t *vis;        // per shadow job (2 per path): 1 when nothing occludes
+    unsigned *cnt;       // kCntSlots counters (64-bit ray totals at kCntRays, kCntShadowRays)
+    int *pass_base;      // first sample of the current pass (advanced by the film kernel)
+    int sample_offset;
+};
+
+__device__ __forceinline__ int warp_append(unsigned *counter, bool pred) {
+    const unsigned active = __activemask();
+    const unsigned mask = __ballot_sync(active, pred);
+    if (!mask)
+        return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned base = 0;
+    if (lane == leader)
+        base = atomicAdd(counter, (unsigned) __popc(mask));
+    base = __shfl_sync(active, base, leader);
+    return pred ? (int) (base + __popc(mask & ((1u << lane) - 1u))) : -1;
+}
+
+__device__ __forceinline__ V3 ld3(const float4 *a, int i) {
+    const float4 v = a[i];
+    return v3(v.x, v.y, v.z);
+}
+__device__ __forceinline__ void st3(float4 *a, int i, V3 v, float w = 0.f) {
+    a[i] = make_float4(v.x, v.y, v.z, w);
+}
+
+__device__ __forceinline__ void finish(const Wf &w, int p, V3 L) {
+    if (!finite3(L))
+        L = v3(0.f);
+    w.result[p] = make_float4(L.x, L.y, L.z, 0.f);
+}
+
+// ---- generate: camera rays for every (pixel, sample) of the pass
+__global__ void k_wf_generate(DevScene S, Wf w) {
+    const int base = *w.pass_base;
+    const int stride = gridDim.x * blockDim.x;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < w.P; p += stride) {
+        const int q = p % w.npix;
+        const int s = base + p / w.npix;
+        const int i = w.x0 + q % w.ww, j = w.y0 + q / w.ww;
+        const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) w.W;
+        Rng rng{path_state(w.seed, m, (uint32_t) (w.sample_offset + s))};
+        const float xo = rng.next();
+        const float yo = rng.next();
+        const Ray3 r = generate_ray(S.camera, i, j, xo, yo, rng);
+        w.rng[p] = rng.s;
+        st3(w.ro, p, r.o);
+        st3(w.rd, p, r.d);
+        st3(w.beta, p, v3(1.f));
+        st3(w.L, p, v3(0.f));
+        w.bounce[p] = 0;
+        w.flags[p] = 0;
+        w.qray[0][p] = p;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.cnt[kCntRay0] = (unsigned) w.P;
+        w.cnt[kCntRay1] = 0;
+    }
+}
+
+// ---- per bounce: rotate the ray queues, clear the stage queues
+__global__ void k_wf_begin(Wf w, int it) {
+    // bounce `it` reads ray queue it&1 (filled by the previous bounce, or by
+    // generate) and its shading stages append to queue (it+1)&1
+    const int in = it & 1;
+    if (threadIdx.x == 0) {
+        w.cnt[kCntRay0 + (in ^ 1)] = 0;
+        w.cnt[kCntMiss] = w.cnt[kCntDelta] = w.cnt[kCntSurf] = w.cnt[kCntShadow] = 0;
+        w.cnt[kCntExtend] = w.cnt[kCntShadowJobs] = w.cnt[kCntShadowFetch] = 0;
+        unsigned long long *tot = reinterpret_cast<unsigned long long *>(w.cnt + kCntRays);
+        *tot += w.cnt[kCntRay0 + in];
+    }
+}
+
+// ---- extend: closest hit of the queued rays, then sort by material class.
+// Persistent: a lane whose ray is finished takes the next queued ray once
+// `refill` lanes of its warp are idle (one atomic per refill).
+__global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
+    extern __shared__ uint2 smem[];
+    uint2 *tcol = smem + threadIdx.x;
+    uint2 *bcol = smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x;
+    const int stride = blockDim.x;
+    const int *qin = w.qray[it & 1];
+    const int n = (int) w.cnt[kCntRay0 + (it & 1)];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int p = -1;
+    ClosestWalk cw;
+    bool more = n > 0;
+    if (!more)
+        return;
+    for (;;) {
+        const bool idle = p < 0;
+        const unsigned im = __ballot_sync(full, idle);
+        if (!more && im == full)
+            break;
+        if (more && __popc(im) >= refill) {
+            const int cnt = __popc(im);
+            unsigned base = 0;
+            if (lane == 0)
+                base = atomicAdd(w.cnt + kCntExtend, (unsigned) cnt);
+            base = __shfl_sync(full, base, 0);
+            if ((int) (base + cnt) >= n)
+                more = false;
+            if (idle) {
+                const int k = (int) base + __popc(im & ((1u << lane) - 1u));
+                if (k < n) {
+                    p = qin[k];
+                    const float4 o = w.ro[p], d = w.rd[p];
+                    cw.start(S, RayD{o.x, o.y, o.z, d.x, d.y, d.z});
+                }
+            }
+        }
+        bool done = false;
+        if (p >= 0)
+            done = S.n_objects == 0 || cw.step(S, tcol, bcol, stride);
+        int cls = -1;
+        if (done) {
+            w.hit[p] = make_int4(cw.hit_obj, cw.hit_tri, __float_as_int(cw.closest), 0);
+            if (cw.hit_obj < 0) {
+                cls = 0;
+            } else {
+                const int kind = S.materials[S.objects[cw.hit_obj].material].kind;
+                cls = (kind == kMatMirror || kind == kMatGlass) ? 1 : 2;
+            }
+        }
+        const int a = warp_append(w.cnt + kCntMiss, cls == 0);
+        const int b = warp_append(w.cnt + kCntDelta, cls == 1);
+        const int c = warp_append(w.cnt + kCntSurf, cls == 2);
+        if (cls == 0)
+            w.qmiss[a] = p;
+        else if (cls == 1)
+            w.qdelta[b] = p;
+        else if (cls == 2)
+            w.qsurf[c] = p;
+        if (done)
+            p = -1;
+    }
+}
+
+// Hit record -> Inter (Triangle::finalize / Sphere::getIntersection fields).
+__device__ __forceinline__ Inter load_inter(const DevScene &S, const Wf &w, int p) {
+    const int4 h = w.hit[p];
+    Inter in;
+    in.hit = h.x >= 0;
+    if (!in.hit) {
+        in.mat = -1;
+        in.p = in.n = v3(0.f);
+        return in;
+    }
+    const float t = __int_as_float(h.z);
+    const V3 o = ld3(w.ro, p), d = ld3(w.rd, p);
+    const DevObject &ob = S.objects[h.x];
+    in.mat = ob.material;
+    if (ob.kind == kObjMesh) {
+        in.p = o + t * d;
+        in.n = v3(S.normals[(size_t) h.y * 3], S.normals[(size_t) h.y * 3 + 1],
+                  S.normals[(size_t) h.y * 3 + 2]);
+    } else {
+        in.p = o + d * t;
+        in.n = normalize(in.p - v3(ob.cx, ob.cy, ob.cz));
+    }
+    return in;
+}
+
+// The tail of a non-delta bounce (Integrator.cpp:205-256) for the hit of the
+// ray it spawned, then the head of the next loop iteration. Returns false
+// when the path has ended (its result is written). `it` and `specular` are
+// the loop variables of the iteration that now processes `in`.
+__device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, int p,
+                                                const Inter &in, Rng &rng, V3 &beta, V3 &L,
+                                                int &it, bool &specular) {
+    const int k = w.bounce[p];
+    const int fl = w.flags[p];
+    const V3 bg = v3(S.background[0], S.background[1], S.background[2]);
+    if (fl & kFlagPending) {
+        const float4 pe = w.pend[p];
+        const V3 scale = v3(pe.x, pe.y, pe.z);
+        const float bpdf = pe.w;
+        const V3 wi = ld3(w.rd, p);
+        const bool indirect = k > 0;
+        if (!in.hit) {
+            V3 c;
+            if (S.env.loaded) {
+                const V3 el = env_lookup(S.env, wi);
+                const float ep = env_pdf(S.env, wi);
+                c = beta * scale * mis(bpdf, ep) * el;
+            } else {
+                c = beta * scale * bg;
+            }
+            L = L + (indirect ? clamp_indirect(c, w.clamp) : c);
+            return false;
+        }
+        const DevMaterial &hm = S.materials[in.mat];
+        if (hm.kind == kMatEmissive) {
+            const V3 hp = ld3(w.prev, p);
+            const float cos_l = smax(0.f, dot(-wi, normalized(in.n)));
+            const V3 dd = in.p - hp;
+            const float hd2 = dot(dd, dd);
+            const float pdf_area = S.total_emit_area > 0.f ? 1.f / S.total_emit_area : 0.f;
+            const float pdf_sa = pdf_area * hd2 / smax(cos_l, 1e-4f);
+            const V3 c = beta * scale * mis(bpdf, pdf_sa) *
+                         v3(hm.emission[0], hm.emission[1], hm.emission[2]);
+            L = L + (indirect ? clamp_indirect(c, w.clamp) : c);
+            return false;
+        }
+        beta = beta * scale;
+        if (!finite3(beta))
+            return false;
+        if (k >= 3) {
+            const float mc = max3(beta);
+            const float q = smax(0.05f, 1.f - mc);
+            if (rng.next() < q)
+                return false;
+            beta = beta * (1.f / (1.f - q));
+        }
+        it = k + 1;
+        specular = false;
+    } else if (fl & kFlagSpecular) {
+        it = k + 1;
+        specular = true;
+    } else {
+        it = 0;
+        specular = false;
+    }
+    if (it >= w.max_depth)
+        return false;
+    if (it == 0 || specular) {
+        const V3 d = ld3(w.rd, p);
+        if (!in.hit) {
+            const V3 b = S.env.loaded ? env_lookup(S.env, d) : bg;
+            const V3 c = beta * b;
+            L = L + ((it > 0) ? clamp_indirect(c, w.clamp) : c);
+        } else if (S.materials[in.mat].kind == kMatEmissive) {
+            const DevMaterial &hm = S.materials[in.mat];
+            const V3 c = beta * v3(hm.emission[0], hm.emission[1], hm.emission[2]);
+            L = L + ((it > 0) ? clamp_indirect(c, w.clamp) : c);
+        }
+    }
+    return in.hit;
+}
+
+// ---- miss: the path leaves the scene
+__global__ void k_wf_miss(DevScene S, Wf w) {
+    const int n = (int) w.cnt[kCntMiss];
+    const int stride = gridDim.x * blockDim.x;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const int p = w.qmiss[k];
+        Rng rng{w.rng[p]};
+        V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
+        Inter in;
+        in.hit = false;
+        in.mat = -1;
+        int it;
+        bool spec;
+        enter_iteration(S, w, p, in, rng, beta, L, it, spec);
+        finish(w, p, L);
+    }
+}
+
+// ---- delta: one step of the specular chain
+__global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
+    const int n = (int) w.cnt[kCntDelta];
+    int *qout = w.qray[it_next & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int k = base + threadIdx.x;
+        bool cont = false;
+        int p = 0;
+        if (k < n) {
+            p = w.qdelta[k];
+            Rng rng{w.rng[p]};
+            V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
+            const Inter in = load_inter(S, w, p);
+            int it;
+            bool spec;
+            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec)) {
+                finish(w, p, L);
+            } else {
+                const DevMaterial &m = S.materials[in.mat];
+                const V3 cd = ld3(w.rd, p);
+                const Shading sd = build_shading(m, in.n);
+                const BSDFSample bs = delta_sample(m, sd, -cd, rng);
+                if (bs.pdf < 1e-6f) {
+                    finish(w, p, L);
+                } else {
+                    beta = beta * bs.f / bs.pdf;
+                    const bool trans = dot(bs.wi, in.n) < 0.f;
+                    const V3 off = trans ? -in.n : in.n;
+                    if (trans)
+                        beta = beta * sd.base;
+                    // the next ray is only looked at if the loop runs again
+                    if (it + 1 >= w.max_depth) {
+                        finish(w, p, L);
+                    } else {
+                        st3(w.ro, p, in.p + off * PRR_EPS);
+                        st3(w.rd, p, bs.wi);
+                        st3(w.beta, p, beta);
+                        st3(w.L, p, L);
+                        w.bounce[p] = it;
+                        w.flags[p] = kFlagSpecular;
+                        w.rng[p] = rng.s;
+                        cont = true;
+                    }
+                }
+            }
+        }
+        const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
+        if (cont)
+            qout[slot] = p;
+    }
+}
+
+// ---- surface: NEE + BSDF sampling of a non-delta bounce
+__global__ void k_wf_surface(DevScene S, Wf w, int it_next) {
+    const int n = (int) w.cnt[kCntSurf];
+    int *qout = w.qray[it_next & 1];
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int k = base + threadIdx.x;
+        bool cont = false, shadow = false;
+        int p = 0;
+        if (k < n) {
+            p = w.qsurf[k];
+            Rng rng{w.rng[p]};
+            V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
+            const Inter in = load_inter(S, w, p);
+            int it;
+            bool spec;
+            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec)) {
+                finish(w, p, L);
+            } else {
+                const DevMaterial &m = S.materials[in.mat];
+                const V3 cd = ld3(w.rd, p);
+                const V3 hp = in.p;
+                const V3 sn = dot(cd, in.n) < 0.f ? in.n : -in.n;
+                const Shading sd = build_shading(m, sn);
+                const V3 wo = -cd;
+                const bool indirect = it > 0;
+                // NEE towards emitters: the contribution is formed now and
+                // added by the shadow stage if the light is visible
+                float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), ld = lo, lc = lo;
+                if (S.total_emit_area > 0.f) {
+                    const LightPoint lp = sample_light(S, rng);
+                    const float pdf_area = 1.0f / S.total_emit_area;
+                    const V3 to = lp.p - hp;
+                    const float dist2 = dot(to, to);
+                    const float dist = sqrtf(dist2);
+                    const V3 wi = to / dist;
+                    const float cos_l = smax(0.f, dot(-wi, normalized(lp.n)));
+                    if (cos_l > 0.f) {
+                        const float pdf_sa = pdf_area * dist2 / cos_l;
+                        V3 f;
+                        float bp;
+                        mat_eval_pdf(m, sd, wi, wo, &f, &bp);
+                        const DevMaterial &lm = S.materials[lp.material];
+                        V3 c = mis(pdf_sa, bp) * v3(lm.emission[0], lm.emission[1], lm.emission[2]) *
+                               f / pdf_sa;
+                        c = beta * c;
+                        if (!(c.x == 0.f && c.y == 0.f && c.z == 0.f)) {
+                            const V3 o = hp + wi * PRR_EPS;
+                            lo = make_float4(o.x, o.y, o.z, dist - 2.f * PRR_EPS);
+                            ld = make_float4(wi.x, wi.y, wi.z, 1.f);
+                            lc = make_float4(c.x, c.y, c.z, indirect ? 1.f : 0.f);
+                            shadow = true;
+                        }
+                    }
+                }
+                float4 eo = make_float4(0.f, 0.f, 0.f, 0.f), ed = eo, ec = eo;
+                if (S.env.loaded) {
+                    float pdf;
+                    const V3 dir = env_importance(S.env, rng, pdf);
+                    if (!(pdf < 1e-6f)) {
+                        const V3 em = env_lookup(S.env, dir);
+                        V3 f;
+                        float bp;
+                        mat_eval_pdf(m, sd, dir, wo, &f, &bp);
+                        V3 c = mis(pdf, bp) * em * f / (pdf + 1e-6f);
+                        c = beta * c;
+                        if (!(c.x == 0.f && c.y == 0.f && c.z == 0.f)) {
+                            const V3 o = hp + dir * PRR_EPS;
+                            eo = make_float4(o.x, o.y, o.z, kInf);
+                            ed = make_float4(dir.x, dir.y, dir.z, 1.f);
+                            ec = make_float4(c.x, c.y, c.z, indirect ? 1.f : 0.f);
+                            shadow = true;
+                        }
+                    }
+                }
+                if (shadow) {
+                    w.slo[p] = lo;
+                    w.sld[p] = ld;
+                    w.slc[p] = lc;
+                    w.seo[p] = eo;
+                    w.sed[p] = ed;
+                    w.sec[p] = ec;
+                }
+                BSDFSample bs;
+                if (m.kind == kMatDiffuse)
+                    bs = diffuse_sample(m, sd, wo, rng);
+                else
+                    bs.pdf = 0.f;
+                if (bs.pdf < 1e-6f) {
+                    if (shadow) {
+                        st3(w.L, p, L);
+                        w.flags[p] = kFlagEndAfterShadow;
+                    } else {
+                        finish(w, p, L);
+                    }
+                } else {
+                    const V3 scale = bs.f / bs.pdf;
+                    const V3 off = dot(bs.wi, sd.f.N) >= 0.f ? sd.f.N : -sd.f.N;
+                    st3(w.ro, p, hp + off * PRR_EPS);
+                    st3(w.rd, p, bs.wi);
+                    st3(w.pend, p, scale, bs.pdf);
+                    st3(w.prev, p, hp);
+                    st3(w.beta, p, beta);
+                    st3(w.L, p, L);
+                    w.bounce[p] = it;
+                    w.flags[p] = kFlagPending;
+                    cont = true;
+                }
+                w.rng[p] = rng.s;
+            }
+        }
+        const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
+        if (cont)
+            qout[slot] = p;
+        const int sslot = warp_append(w.cnt + kCntShadow, shadow);
+        if (shadow)
+            w.qshadow[sslot] = p;
+        const bool jl = shadow && w.sld[p].w != 0.f;
+        const bool je = shadow && w.sed[p].w != 0.f;
+        const int j0 = warp_append(w.cnt + kCntShadowJobs, jl);
+        if (jl)
+            w.qjob[j0] = p * 2;
+        const int j1 = warp_append(w.cnt + kCntShadowJobs, je);
+        if (je)
+            w.qjob[j1] = p * 2 + 1;
+    }
+}
+
+// ---- shadow: visibility of every queued NEE ray (persistent, per-lane refill)
+__global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
+    extern __shared__ uint2 smem[];
+    uint2 *tcol = smem + threadIdx.x;
+    uint2 *bcol = smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x;
+    const int stride = blockDim.x;
+    const int n = (int) w.cnt[kCntShadowJobs];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int job = -1;
+    AnyWalk aw;
+    bool more = n > 0;
+    unsigned rays = 0;
+    for (;;) {
+        const bool idle = job < 0;
+        const unsigned im = __ballot_sync(full, idle);
+        if (!more && im == full)
+            break;
+        if (more && __popc(im) >= refill) {
+            const int cnt = __popc(im);
+            unsigned base = 0;
+            if (lane == 0)
+                base = atomicAdd(w.cnt + kCntShadowFetch, (unsigned) cnt);
+            base = __shfl_sync(full, base, 0);
+            if ((int) (base + cnt) >= n)
+                more = false;
+            if (idle) {
+                const int k = (int) base + __popc(im & ((1u << lane) - 1u));
+                if (k < n) {
+                    job = w.qjob[k];
+                    const int p = job >> 1;
+                    const float4 o = (job & 1) ? w.seo[p] : w.slo[p];
+                    const float4 d = (job & 1) ? w.sed[p] : w.sld[p];
+                    rays++;
+                    if (!aw.start(S, RayD{o.x, o.y, o.z, d.x, d.y, d.z}, o.w)) {
+                        w.vis[job] = 1;
+                        job = -1;
+                    }
+                }
+            }
+        }
+        if (job >= 0 && aw.step(S, tcol, bcol, stride)) {
+            w.vis[job] = aw.occluded ? 0 : 1;
+            job = -1;
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        rays += __shfl_down_sync(full, rays, off);
+    if (lane == 0 && rays)
+        atomicAdd(reinterpret_cast<unsigned long long *>(w.cnt + kCntShadowRays),
+                  (unsigned long long) rays);
+}
+
+// ---- add the visible NEE contributions, light first, then env, as castRay
+__global__ void k_wf_shadow_resolve(Wf w) {
+    const int n = (int) w.cnt[kCntShadow];
+    const int stride = gridDim.x * blockDim.x;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+        const int p = w.qshadow[k];
+        V3 L = ld3(w.L, p);
+        for (int r = 0; r < 2; r++) {
+            const float4 d = r == 0 ? w.sld[p] : w.sed[p];
+            if (d.w == 0.f || !w.vis[p * 2 + r])
+                continue;
+            const float4 c = r == 0 ? w.slc[p] : w.sec[p];
+            const V3 cv = v3(c.x, c.y, c.z);
+            L = L + (c.w != 0.f ? clamp_indirect(cv, w.clamp) : cv);
+        }
+        if (w.flags[p] & kFlagEndAfterShadow)
+            finish(w, p, L);
+        else
+            st3(w.L, p, L);
+    }
+}
+
+// ---- film: add the pass's samples per pixel in sample order
+__global__ void k_wf_film(Wf w) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < w.npix) {
+        float3 f = w.film[q];
+        for (int s = 0; s < w.spp_pass; s++) {
+            const float4 r = w.result[(size_t) s * w.npix + q];
+            // a NaN sample is zeroed before accumulation (Renderer.cpp:78-83)
+            if (!(isnan(r.x) || isnan(r.y) || isnan(r.z))) {
+                f.x += r.x;
+                f.y += r.y;
+                f.z += r.z;
+            }
+        }
+        w.film[q] = f;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *w.pass_base += w.spp_pass;
+}
+
+__global__ void k_wf_resolve(const float3 *film, int npix, int n, float *out, int32_t *spp) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npix)
+        return;
+    const float3 f = film[q];
+    out[(size_t) q * 3 + 0] = f.x / (float) n;
+    out[(size_t) q * 3 + 1] = f.y / (float) n;
+    out[(size_t) q * 3 + 2] = f.z / (float) n;
+    if (spp)
+        spp[q] = n;
+}
+
+__global__ void k_wf_rays_out(const unsigned *cnt, unsigned long long *out) {
+    out[0] = *reinterpret_cast<const unsigned long long *>(cnt + kCntRays);
+    out[1] = *reinterpret_cast<const unsigned long long *>(cnt + kCntShadowRays);
+}
+
+uint32_t float_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof(u));
+    return u;
+}
+
+template <class T> T *carve(char *&p, size_t n) {
+    T *r = reinterpret_cast<T *>(p);
+    p += (n * sizeof(T) + 255) & ~size_t(255);
+    return r;
+}
+
+} // namespace
+
+struct WavefrontPlan {
+    // one captured pass per (scene, window, spp_pass, depth, block shape)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t key = 0;
+    ~WavefrontPlan() {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+    }
+};
+
+int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
+                     unsigned long long *out_rays, cudaStream_t st) {
+    if (rs.min_spp < rs.max_spp) // the Welford stop needs all of a pixel's samples in order
+        return render_plain(s, rs, out_rgb, out_spp, out_rays, st);
+    const DevScene &S = s.dev;
+    Wf w{};
+    w.W = s.width;
+    w.x0 = rs.x0;
+    w.y0 = rs.y0;
+    w.ww = rs.x1 - rs.x0;
+    const int wh = rs.y1 - rs.y0;
+    w.npix = w.ww * wh;
+    w.max_depth = rs.max_depth;
+    w.clamp = rs.indirect_clamp;
+    w.seed = rs.seed;
+    w.sample_offset = rs.sample_offset;
+    w.tlas_cap = S.tlas_depth + 1;
+    w.blas_cap = S.blas_depth + 1;
+    // paths per pass: whole samples of the window, about 2M paths in flight
+    const int64_t target = s.wf_paths > 0 ? s.wf_paths : (int64_t) 1 << 21;
+    int spp_pass = (int) std::max<int64_t>(1, target / std::max(1, w.npix));
+    spp_pass = std::min(spp_pass, rs.max_spp);
+    while (rs.max_spp % spp_pass)
+        spp_pass--;
+    w.spp_pass = spp_pass;
+    w.P = spp_pass * w.npix;
+    const size_t P = (size_t) w.P;
+    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) + (size_t) w.npix * 16 + 4096;
+    PRR_CUDA_TRY(s.d_wavefront.ensure(bytes));
+    char *cur = (char *) s.d_wavefront.ptr;
+    w.rng = carve<uint64_t>(cur, P);
+    w.ro = carve<float4>(cur, P);
+    w.rd = carve<float4>(cur, P);
+    w.beta = carve<float4>(cur, P);
+    w.L = carve<float4>(cur, P);
+    w.pend = carve<float4>(cur, P);
+    w.prev = carve<float4>(cur, P);
+    w.hit = carve<int4>(cur, P);
+    w.slo = carve<float4>(cur, P);
+    w.sld = carve<float4>(cur, P);
+    w.slc = carve<float4>(cur, P);
+    w.seo = carve<float4>(cur, P);
+    w.sed = carve<float4>(cur, P);
+    w.sec = carve<float4>(cur, P);
+    w.result = carve<float4>(cur, P);
+    w.bounce = carve<int>(cur, P);
+    w.flags = carve<int>(cur, P);
+    w.qray[0] = carve<int>(cur, P);
+    w.qray[1] = carve<int>(cur, P);
+    w.qmiss = carve<int>(cur, P);
+    w.qdelta = carve<int>(cur, P);
+    w.qsurf = carve<int>(cur, P);
+    w.qshadow = carve<int>(cur, P);
+    w.qjob = carve<int>(cur, 2 * P);
+    w.vis = carve<uint8_t>(cur, 2 * P);
+    w.film = carve<float3>(cur, (size_t) w.npix);
+    w.cnt = carve<unsigned>(cur, kCntSlots);
+    w.pass_base = carve<int>(cur, 4);
+    if ((size_t) (cur - (char *) s.d_wavefront.ptr) > bytes)
+        return fail(PRR_ERR_INTERNAL, "wavefront buffer layout overflow");
+
+    const int sms = device_sm_count();
+    const int block = s.wf_block > 0 ? s.wf_block : 128;
+    const size_t smem = (size_t) (w.tlas_cap + w.blas_cap) * block * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    if (smem > 48 * 1024) {
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_extend, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    }
+    const int refill = s.wf_refill > 0 ? std::min(s.wf_refill, 32) : 8;
+    int occ_ext = 1, occ_sh = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_wf_extend, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_wf_shadow, block, smem);
+    const int g_ext = sms * std::max(1, occ_ext);
+    const int g_sh = sms * std::max(1, occ_sh);
+    const int g_shade = sms * 8;
+    const int g_gen = (int) std::min<int64_t>((P + 255) / 256, (int64_t) sms * 16);
+
+    PRR_CUDA_TRY(cudaMemsetAsync(w.film, 0, (size_t) w.npix * sizeof(float3), st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.pass_base, 0, sizeof(int), st));
+
+    // capture one pass
+    auto enqueue_pass = [&](cudaStream_t cs) -> int {
+        k_wf_generate<<<g_gen, 256, 0, cs>>>(S, w);
+        for (int it = 0; it <= w.max_depth; it++) {
+            k_wf_begin<<<1, 32, 0, cs>>>(w, it);
+            k_wf_extend<<<g_ext, block, smem, cs>>>(S, w, it, refill);
+            k_wf_miss<<<g_shade, 128, 0, cs>>>(S, w);
+            k_wf_delta<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
+            k_wf_surface<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
+            k_wf_shadow<<<g_sh, block, smem, cs>>>(S, w, refill);
+            k_wf_shadow_resolve<<<g_shade, 128, 0, cs>>>(w);
+        }
+        k_wf_film<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
+        PRR_CUDA_TRY(cudaGetLastError());
+        return PRR_OK;
+    };
+    const int passes = rs.max_spp / spp_pass;
+    uint64_t key = (uint64_t) (uintptr_t) s.d_wavefront.ptr;
+    key = mix64(key ^ ((uint64_t) w.P << 20) ^ ((uint64_t) w.max_depth << 8) ^ (uint64_t) block ^
+                ((uint64_t) refill << 50));
+    key = mix64(key ^ ((uint64_t) (uint32_t) w.x0 << 32 | (uint32_t) w.y0) ^
+                ((uint64_t) (uint32_t) w.ww << 16) ^ rs.seed ^ ((uint64_t) rs.sample_offset << 40) ^
+                (uint64_t) float_bits(w.clamp));
+    if (!s.wf_plan)
+        s.wf_plan = std::make_shared<WavefrontPlan>();
+    WavefrontPlan &plan = *s.wf_plan;
+    if (s.wf_graphs && passes > 1) {
+        if (plan.key != key || !plan.exec) {
+            if (plan.exec) {
+                cudaGraphExecDestroy(plan.exec);
+                plan.exec = nullptr;
+            }
+            if (plan.graph) {
+                cudaGraphDestroy(plan.graph);
+                plan.graph = nullptr;
+            }
+            cudaStream_t cap;
+            PRR_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+            PRR_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_pass(cap);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(cap, &g);
+            cudaStreamDestroy(cap);
+            if (rc)
+                return rc;
+            if (e != cudaSuccess)
+                return fail(PRR_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            plan.graph = g;
+            PRR_CUDA_TRY(cudaGraphInstantiate(&plan.exec, g, 0));
+            plan.key = key;
+        }
+        for (int k = 0; k < passes; k++)
+            PRR_CUDA_TRY(cudaGraphLaunch(plan.exec, st));
+    } else {
+        for (int k = 0; k < passes; k++)
+            if (int rc = enqueue_pass(st))
+                return rc;
+    }
+    k_wf_resolve<<<(w.npix + 255) / 256, 256, 0, st>>>(w.film, w.npix, rs.max_spp, out_rgb, out_spp);
+    PRR_CUDA_TRY(cudaGetLastError());
+    if (out_rays) {
+        k_wf_rays_out<<<1, 1, 0, st>>>(w.cnt, out_rays);
+        PRR_CUDA_TRY(cudaGetLastError());
+    }
+    return PRR_OK;
 }
 
 } // namespace prr

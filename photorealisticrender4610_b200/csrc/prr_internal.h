@@ -70,6 +70,8 @@ struct HostObject {
     uint32_t root = 0;
 };
 
+struct WavefrontPlan;
+
 struct Scene {
     std::mutex mu;
     std::vector<HostMaterial> materials;
@@ -92,6 +94,12 @@ struct Scene {
     DevBuf d_scratch;      // staging for host-buffer entry points
     DevBuf d_render, d_render_spp; // per-slice partial sums / adaptive spp
     DevBuf d_counter;      // persistent-kernel work counters
+    DevBuf d_wavefront;    // wavefront path state, queues and film
+    std::shared_ptr<WavefrontPlan> wf_plan; // captured pass graph
+    int64_t wf_paths = 0;  // paths in flight per pass (0 = automatic)
+    int wf_block = 0;      // extend / shadow block size (0 = 128)
+    int wf_refill = 0;     // idle lanes that trigger a refill (0 = 8)
+    bool wf_graphs = true; // replay passes from a captured CUDA graph
     // Renders reuse the scratch above; each render waits for the previous
     // one's event before touching it, whatever stream either ran on.
     cudaEvent_t scratch_done = nullptr;

@@ -1,6 +1,8 @@
 // C ABI of the renderer (Renderer::Render, Renderer.cpp:24-212, up to the
-// linear framebuffer) and its argument checks.
+// linear framebuffer), its argument checks, and the wavefront autotuner.
 #include "prr_internal.h"
+
+#include <algorithm>
 
 namespace prr {
 
@@ -57,4 +59,89 @@ extern "C" int prr_render(prr_scene *scene, const prr_render_settings *settings,
         rc = render_plain(s, rs, out_rgb, out_spp, (unsigned long long *) out_rays, st);
     PRR_CUDA_TRY(cudaEventRecord(s.scratch_done, st));
     return rc;
+}
+
+extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config) {
+    if (!scene || !config)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene and config are required");
+    if (config->paths_per_pass < 0 || config->block_size < 0 || config->block_size % 32 != 0 ||
+        config->block_size > 512)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad wavefront config");
+    Scene &s = *reinterpret_cast<Scene *>(scene);
+    std::lock_guard<std::mutex> g(s.mu);
+    s.wf_paths = config->paths_per_pass;
+    s.wf_block = config->block_size;
+    s.wf_graphs = config->use_graphs != 0;
+    return PRR_OK;
+}
+
+extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *settings,
+                            prr_wavefront_config *out_best, void *stream) {
+    if (!scene || !settings)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene and settings are required");
+    Scene &s = *reinterpret_cast<Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    prr_render_settings rs = *settings;
+    rs.mode = PRR_RENDER_WAVEFRONT;
+    rs.min_spp = rs.max_spp;
+    if (int rc = validate_render(s, rs))
+        return rc;
+    cudaStream_t st = (cudaStream_t) stream;
+    const int64_t npix = (int64_t) (rs.x1 - rs.x0) * (rs.y1 - rs.y0);
+    DevBuf out;
+    PRR_CUDA_TRY(out.alloc((size_t) npix * 3 * sizeof(float)));
+    cudaEvent_t a, b;
+    PRR_CUDA_TRY(cudaEventCreate(&a));
+    PRR_CUDA_TRY(cudaEventCreate(&b));
+    const int64_t paths[] = {int64_t(1) << 19, int64_t(1) << 20, int64_t(1) << 21,
+                             int64_t(1) << 22};
+    const int blocks[] = {64, 128, 256};
+    float best_ms = 1e30f;
+    prr_wavefront_config best{0, 0, 1};
+    int rc = PRR_OK;
+    std::lock_guard<std::mutex> g(s.mu);
+    int64_t last = -1;
+    for (int64_t cand : paths) {
+        // a pass never holds more than the whole render
+        const int64_t pp = std::min<int64_t>(cand, npix * rs.max_spp);
+        if (pp == last)
+            continue;
+        last = pp;
+        for (int bl : blocks) {
+            s.wf_paths = pp;
+            s.wf_block = bl;
+            s.wf_graphs = true;
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 2 && rc == PRR_OK; rep++) {
+                cudaEventRecord(a, st);
+                rc = render_wavefront(s, rs, out.as<float>(), nullptr, nullptr, st);
+                cudaEventRecord(b, st);
+                if (cudaEventSynchronize(b) != cudaSuccess && rc == PRR_OK)
+                    rc = fail(PRR_ERR_CUDA, "autotune render failed");
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, a, b);
+                if (rep > 0) // the first run captures the graph
+                    ms_min = std::min(ms_min, ms);
+            }
+            if (rc)
+                break;
+            if (ms_min < best_ms) {
+                best_ms = ms_min;
+                best = prr_wavefront_config{pp, bl, 1};
+            }
+        }
+        if (rc)
+            break;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc)
+        return rc;
+    s.wf_paths = best.paths_per_pass;
+    s.wf_block = best.block_size;
+    s.wf_graphs = true;
+    if (out_best)
+        *out_best = best;
+    return PRR_OK;
 }

@@ -1,0 +1,59 @@
+"""The wavefront integrator against the plain megakernel: the same paths, the
+same random draws and the same per-pixel sample order, so the films are equal
+bit for bit (the plain renderer with one thread per pixel is itself checked
+against the reference in test_render_gpu.py)."""
+import numpy as np
+import pytest
+
+import photorealisticrender4610_b200 as prr
+from photorealisticrender4610_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def render_both(desc, spp, depth, seed=1, **kw):
+    s = prr.Scene.from_desc(desc)
+    plain, _, pr = s.render(spp, depth, seed=seed, slices=1, count_rays=True)
+    wave, n, wr = s.render(spp, depth, seed=seed, mode="wavefront", count_rays=True, **kw)
+    return s, plain.cpu().numpy(), wave.cpu().numpy(), pr.cpu().numpy(), wr.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["cornell", "museum", "caustics"])
+def test_wavefront_equals_plain(cuda, name):
+    if name == "cornell":
+        desc, depth = scenes.cornell_box(64, 64), 5
+    elif name == "museum":
+        desc, depth = scenes.museum_like(96, 54, level=3, env_size=(256, 128)), 8
+    else:
+        desc, depth = scenes.caustics(64, 64, level=2), 6
+    s, plain, wave, pr, wr = render_both(desc, 16, depth)
+    assert np.array_equal(plain.view(np.uint32), wave.view(np.uint32))
+    # the wavefront skips only the ray a delta bounce leaves after the last
+    # iteration, which castRay traces and ignores
+    assert wr[0] <= pr[0] and wr[0] > 0.9 * pr[0]
+    assert wr[1] == pr[1]
+
+
+def test_wavefront_passes_and_graphs(cuda):
+    desc = scenes.museum_like(64, 48, level=3, env_size=(256, 128))
+    s = prr.Scene.from_desc(desc)
+    ref, _ = s.render(24, 8, seed=3, slices=1)
+    ref = ref.cpu().numpy()
+    for paths, graphs in [(64 * 48 * 2, True), (64 * 48 * 3, False), (64 * 48 * 24, True)]:
+        s.set_wavefront(paths_per_pass=paths, block_size=64, use_graphs=graphs)
+        out, _ = s.render(24, 8, seed=3, mode="wavefront")
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32)), paths
+    # a window and a sample offset address the same (pixel, sample) streams
+    a, _ = s.render(8, 8, seed=3, mode="wavefront", sample_offset=8, window=(10, 5, 42, 29))
+    b, _ = s.render(8, 8, seed=3, slices=1, sample_offset=8)
+    assert np.array_equal(a.cpu().numpy(), b.cpu().numpy()[5:29, 10:42])
+
+
+def test_autotune_picks_a_config(cuda):
+    desc = scenes.cornell_box(128, 128)
+    s = prr.Scene.from_desc(desc)
+    best = s.autotune(4, 5)
+    assert best["paths_per_pass"] > 0 and best["block_size"] in (64, 128, 256)
+    a, _ = s.render(8, 5, mode="wavefront")
+    b, _ = s.render(8, 5, slices=1)
+    assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
