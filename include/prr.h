@@ -187,6 +187,22 @@ int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
 int prr_render(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
                int32_t *out_spp, uint64_t *out_rays, void *stream);
 
+/* Allocation-free rendering. No counterpart in the reference: this entry
+ * point exists for callers that cannot call cudaMalloc while they render (a
+ * host whose device memory is owned by another allocator, or a frame loop that
+ * must not enter the CUDA allocator). It renders like prr_render in
+ * PRR_RENDER_PLAIN mode with fixed spp (min_spp == max_spp), and calls no
+ * cudaMalloc, cudaFree or allocating library routine: its scratch (the
+ * per-slice partial sums) is a fixed device array inside the library of
+ * 2,097,152 partial sums (24 MiB), held on every GPU that loads the library
+ * until the process exits. Windows of more than 2,097,152 pixels are rejected
+ * with PRR_ERR_INVALID_ARGUMENT. The first call on a device looks up that
+ * array's device address, so make it before any stream capture. All calls
+ * share the array and keep its last contents: calls that overlap on the GPU
+ * race, so order them (one stream, or events). out_rays is optional. */
+int prr_render_noalloc(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
+                       uint64_t *out_rays, void *stream);
+
 /* Sets the wavefront launch shape used by prr_render in wavefront mode. */
 int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config);
 /* The autotuner: times the wavefront renderer on `settings` (the window and

@@ -81,6 +81,7 @@ _SIGS = {
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
+    "prr_render_noalloc": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp]),
     "prr_scene_set_wavefront": (C.c_int, [_vp, C.POINTER(prr_wavefront_config)]),
     "prr_autotune": (C.c_int, [_vp, C.POINTER(prr_render_settings),
                                C.POINTER(prr_wavefront_config), _vp]),

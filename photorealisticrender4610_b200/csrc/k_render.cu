@@ -13,6 +13,8 @@
 #include "prr_internal.h"
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 namespace prr {
 namespace {
@@ -229,4 +231,126 @@ int render_plain(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_
     return PRR_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free rendering.
+//
+// Some callers of this library cannot call cudaMalloc while they render: a
+// host application whose device memory is owned and budgeted by another
+// allocator, or a caller that must not enter the CUDA allocator (or its
+// implicit device synchronisation) on its frame loop. prr_render_noalloc
+// serves them: it runs the same plain megakernel and resolve kernels as
+// prr_render in its fixed-spp mode, but the per-slice partial sums live in the
+// file-scope array below instead of memory obtained from cudaMalloc.
+//
+// The array holds kNoAllocPartials float3 partial sums (pixels x slices,
+// 24 MiB). Every GPU on which the library's render module is loaded keeps
+// this memory until the process exits. All calls on a device share the one
+// array: calls whose kernels overlap on the GPU race on it, so callers must
+// order them (one stream, or events between streams). Each call writes every
+// partial sum it later reads, so nothing needs clearing between calls.
+// ---------------------------------------------------------------------------
+constexpr int64_t kNoAllocPartials = int64_t(1) << 21;
+static __device__ __align__(256) float3 g_noalloc_partials[kNoAllocPartials];
+
+namespace {
+
+// The array's device address, looked up once per device with that device
+// current (in host code the array's name is only a host-side stand-in).
+int noalloc_partials(float3 **out) {
+    static std::mutex mu;
+    static float3 *addr[256] = {};
+    int dev = 0;
+    PRR_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256)
+        return fail(PRR_ERR_UNSUPPORTED, "device ordinal out of range");
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || !p)
+            return fail(PRR_ERR_CUDA, std::string("cudaGetSymbolAddress(partial sums): ") +
+                                          cudaGetErrorString(e));
+        addr[dev] = (float3 *) p;
+    }
+    *out = addr[dev];
+    return PRR_OK;
+}
+
+} // namespace
 } // namespace prr
+
+extern "C" int prr_render_noalloc(prr_scene *scene, const prr_render_settings *settings,
+                                  float *out_rgb, uint64_t *out_rays, void *stream) {
+    using namespace prr;
+    if (!scene || !settings || !out_rgb)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene, settings and out_rgb are required");
+    Scene &s = *reinterpret_cast<Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    prr_render_settings rs = *settings;
+    if (int rc = validate_render(s, rs))
+        return rc;
+    if (rs.mode != PRR_RENDER_PLAIN)
+        return fail(PRR_ERR_UNSUPPORTED, "prr_render_noalloc renders with the plain kernel only");
+    if (rs.min_spp < rs.max_spp)
+        return fail(PRR_ERR_UNSUPPORTED, "prr_render_noalloc supports fixed spp only "
+                                         "(min_spp == max_spp)");
+    const int ww = rs.x1 - rs.x0, wh = rs.y1 - rs.y0;
+    const int64_t npix = (int64_t) ww * wh;
+    if (npix > kNoAllocPartials)
+        return fail(PRR_ERR_INVALID_ARGUMENT,
+                    "window of " + std::to_string(npix) + " pixels exceeds the " +
+                        std::to_string(kNoAllocPartials) +
+                        " partial sums of the allocation-free renderer");
+    const DevScene &S = s.dev;
+    RenderArgs a{};
+    a.W = s.width;
+    a.H = s.height;
+    a.x0 = rs.x0;
+    a.y0 = rs.y0;
+    a.ww = ww;
+    a.wh = wh;
+    a.min_spp = rs.min_spp;
+    a.max_spp = rs.max_spp;
+    a.threshold = rs.variance_threshold;
+    a.max_depth = rs.max_depth;
+    a.clamp = rs.indirect_clamp;
+    a.seed = rs.seed;
+    a.spp_begin = rs.sample_offset;
+    a.spp_end = rs.sample_offset + rs.max_spp;
+    a.rays = (unsigned long long *) out_rays;
+    int slices = rs.slices > 0 ? rs.slices : 1;
+    if (rs.slices <= 0) {
+        const int64_t want = (int64_t) device_sm_count() * 1024 * 2;
+        while (npix * slices < want && slices * 2 <= rs.max_spp)
+            slices *= 2;
+    }
+    slices = std::max(1, std::min(slices, rs.max_spp));
+    slices = (int) std::min<int64_t>(slices, kNoAllocPartials / npix);
+    a.slices = slices;
+    a.tlas_cap = S.tlas_depth + 1;
+    const int bcap = S.blas_depth + 1;
+    const size_t smem = (size_t) (a.tlas_cap + bcap) * kTileW * kTileH * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    float3 *partial = nullptr;
+    if (int rc = noalloc_partials(&partial))
+        return rc;
+    a.partial = partial;
+    cudaStream_t st = (cudaStream_t) stream;
+    std::lock_guard<std::mutex> g(s.mu);
+    if (out_rays)
+        PRR_CUDA_TRY(cudaMemsetAsync(out_rays, 0, 2 * sizeof(uint64_t), st));
+    if (smem > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_render_plain,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    const int tiles = ((ww + kTileW - 1) / kTileW) * ((wh + kTileH - 1) / kTileH);
+    k_render_plain<<<dim3(tiles, slices), kTileW * kTileH, smem, st>>>(S, a);
+    PRR_CUDA_TRY(cudaGetLastError());
+    k_render_resolve<<<(int) ((npix + 255) / 256), 256, 0, st>>>(partial, (int) npix, slices,
+                                                                  nullptr, rs.max_spp, out_rgb,
+                                                                  nullptr);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+

@@ -122,6 +122,7 @@ int launch_scene_occluded(const Scene &s, const float *o, const float *d, const 
 int launch_env_cdf(Scene &s, cudaStream_t st);
 int render_plain(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                  unsigned long long *out_rays, cudaStream_t st);
+int validate_render(const Scene &s, prr_render_settings &rs);
 int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                      unsigned long long *out_rays, cudaStream_t st);
 
