@@ -49,6 +49,14 @@ extern "C" {
 #define PRR_MAT_GLASS 3
 
 typedef struct prr_scene prr_scene;
+typedef struct prr_photon_map prr_photon_map;
+
+/* Tone mappers: tonemap::ToneMapper (ToneMapping.hpp:32-37) plus ACES. */
+#define PRR_TONEMAP_RAW 0
+#define PRR_TONEMAP_STANDARD 1
+#define PRR_TONEMAP_AGX 2
+#define PRR_TONEMAP_PBR_NEUTRAL 3
+#define PRR_TONEMAP_ACES 4 /* new: K. Narkowicz's ACES filmic fit + sRGB OETF */
 
 /* Camera fields of Camera::create + aperture/focusDistance (Camera.hpp:10-31). */
 typedef struct prr_camera {
@@ -186,6 +194,45 @@ int prr_scene_occluded(const prr_scene *scene, const float *o, const float *d,
  * uint64) = closest-hit and shadow rays traced. Device pointers. */
 int prr_render(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
                int32_t *out_spp, uint64_t *out_rays, void *stream);
+
+/* Display transform of Renderer.cpp:149-171: linear radiance times exposure,
+ * non-finite and negative channels zeroed, tonemap::apply(mapper)
+ * (ToneMapping.hpp:267-279), and the 8-bit quantisation
+ * (unsigned char)(clamp(c,0,1)*255 + 0.5). rgb = n x 3 floats; out_rgb
+ * (optional) = the mapped floats, out_u8 (optional) = n x 3 bytes. */
+int prr_tonemap(int mapper, float exposure, const float *rgb, int64_t n, float *out_rgb,
+                uint8_t *out_u8, void *stream);
+
+/* ---- caustic photons (PhotonMap, Photon.hpp:32-45) ---------------------- */
+int prr_photon_map_create(prr_photon_map **out);
+int prr_photon_map_destroy(prr_photon_map *map);
+/* PhotonMap::emit + trace (Photon.cpp:96-188): num_photons photons leave the
+ * scene's area emitters (photon i draws from stream (seed, i, 0xFFFFFFFF)) and
+ * every diffuse hit after a specular bounce is stored. The stored records stay
+ * on the device in canonical order: by emitting photon, then by trace order. */
+int prr_photon_emit(prr_photon_map *map, const prr_scene *scene, int64_t num_photons,
+                    uint64_t seed, int max_depth, void *stream);
+/* Replaces the photon array with n records of 9 floats (position, direction,
+ * power), host or device memory. */
+int prr_photon_set(prr_photon_map *map, const float *records, int64_t n, void *stream);
+/* PhotonMap::build -> PhotonGrid::build(caustic_map, photon_radius)
+ * (Photon.cpp:24-53, :189). */
+int prr_photon_build(prr_photon_map *map, float radius, void *stream);
+int prr_photon_info(const prr_photon_map *map, int64_t *count, int32_t *grid_res);
+/* Copies the records (n x 9) and their emitting photon indices (n). */
+int prr_photon_export(const prr_photon_map *map, float *records, int32_t *owner, void *stream);
+/* PhotonMap::estimateIrradiance (Photon.cpp:82-94) at n points (n x 3):
+ * sum of the powers within the radius over pi r^2. k_nearest > 0 (<= 64) caps
+ * it: with more than k photons in the radius, the k nearest over the disc
+ * through the k-th (identical to the fixed radius otherwise). */
+int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n, int k_nearest,
+                      float *out_rgb, void *stream);
+/* Caustic image: for every (pixel, sample) the camera ray follows the specular
+ * chain (Integrator.cpp:143-169) to its first diffuse hit x, which returns
+ * beta * baseColor/pi * E(x) from the photon map. out_rgb = window x 3. */
+int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
+                        const prr_render_settings *settings, int k_nearest, float *out_rgb,
+                        void *stream);
 
 /* Allocation-free rendering. No counterpart in the reference: this entry
  * point exists for callers that cannot call cudaMalloc while they render (a

@@ -81,6 +81,17 @@ _SIGS = {
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
+    "prr_photon_map_create": (C.c_int, [C.POINTER(_vp)]),
+    "prr_photon_map_destroy": (C.c_int, [_vp]),
+    "prr_photon_emit": (C.c_int, [_vp, _vp, C.c_int64, C.c_uint64, C.c_int, _vp]),
+    "prr_photon_set": (C.c_int, [_vp, _vp, C.c_int64, _vp]),
+    "prr_photon_build": (C.c_int, [_vp, C.c_float, _vp]),
+    "prr_photon_info": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "prr_photon_export": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "prr_photon_gather": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp]),
+    "prr_render_caustics": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int, _vp,
+                                      _vp]),
+    "prr_tonemap": (C.c_int, [C.c_int, C.c_float, _vp, C.c_int64, _vp, _vp, _vp]),
     "prr_render_noalloc": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp]),
     "prr_scene_set_wavefront": (C.c_int, [_vp, C.POINTER(prr_wavefront_config)]),
     "prr_autotune": (C.c_int, [_vp, C.POINTER(prr_render_settings),

@@ -19,6 +19,21 @@ from ._lib import (check, prr_camera, prr_render_settings, prr_scene_stats, prr_
                    prr_wavefront_config)
 
 RENDER_MODES = {"plain": 0, "wavefront": 1}
+TONEMAPPERS = {"raw": 0, "standard": 1, "agx": 2, "pbrneutral": 3, "aces": 4}
+
+
+def tonemap(rgb, mapper="agx", exposure: float = 1.0, stream=None):
+    """Renderer's display transform on a CUDA tensor of linear RGB (..., 3):
+    returns (mapped float32, uint8) tensors of the same shape."""
+    import torch
+    lib = _lib.load()
+    x = rgb.to(torch.float32).contiguous()
+    n = x.numel() // 3
+    out = torch.empty_like(x)
+    u8 = torch.empty(x.shape, dtype=torch.uint8, device=x.device)
+    m = TONEMAPPERS[mapper] if isinstance(mapper, str) else int(mapper)
+    check(lib.prr_tonemap(m, exposure, _ptr(x), n, _ptr(out), _ptr(u8), _stream(stream)))
+    return out, u8
 
 
 def _ptr(t):
@@ -343,3 +358,70 @@ class Scene:
         check(self.lib.prr_env_export(self.h, C.c_void_p(cdf.ctypes.data),
                                       C.c_void_p(marg.ctypes.data), C.byref(tot)))
         return cdf, marg, tot.value
+
+
+class PhotonMap:
+    """PhotonMap (Photon.hpp:32-45) on the device: emit/trace, grid build,
+    irradiance gathers and the caustic image."""
+
+    def __init__(self):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.prr_photon_map_create(C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.prr_photon_map_destroy(h)
+            self.h = None
+
+    def emit(self, scene: Scene, num_photons: int, seed: int = 1, max_depth: int = 30,
+             stream=None):
+        check(self.lib.prr_photon_emit(self.h, scene.h, num_photons, seed, max_depth,
+                                       _stream(stream)))
+        return self
+
+    def set(self, records, stream=None):
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, 9)
+        check(self.lib.prr_photon_set(self.h, C.c_void_p(r.ctypes.data), len(r), _stream(stream)))
+        return self
+
+    def build(self, radius: float = 0.01, stream=None):
+        check(self.lib.prr_photon_build(self.h, radius, _stream(stream)))
+        return self
+
+    def info(self):
+        n = C.c_int64()
+        res = C.c_int32()
+        check(self.lib.prr_photon_info(self.h, C.byref(n), C.byref(res)))
+        return n.value, res.value
+
+    def export(self):
+        n, _ = self.info()
+        rec = np.empty((n, 9), np.float32)
+        owner = np.empty(n, np.int32)
+        check(self.lib.prr_photon_export(self.h, C.c_void_p(rec.ctypes.data),
+                                         C.c_void_p(owner.ctypes.data), _stream(None)))
+        return rec, owner
+
+    def gather(self, points, k_nearest: int = 0, stream=None):
+        import torch
+        dev = torch.device("cuda", torch.cuda.current_device())
+        q = torch.as_tensor(np.ascontiguousarray(points, np.float32)).to(dev).reshape(-1, 3)
+        out = torch.empty_like(q)
+        check(self.lib.prr_photon_gather(self.h, _ptr(q), q.shape[0], k_nearest, _ptr(out),
+                                         _stream(stream)))
+        return out
+
+    def render_caustics(self, scene: Scene, spp: int, max_depth: int = 8, seed: int = 1,
+                        k_nearest: int = 0, window=None, stream=None):
+        import torch
+        rs = scene._settings(spp, max_depth, seed, None, 0.05, "plain", window, 10.0, 0, 0)
+        W, H = scene.desc.width, scene.desc.height
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
+        check(self.lib.prr_render_caustics(scene.h, self.h, C.byref(rs), k_nearest, _ptr(out),
+                                           _stream(stream)))
+        return out

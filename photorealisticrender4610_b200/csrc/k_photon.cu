@@ -1,0 +1,719 @@
+// Caustic photons on the device: PhotonMap::emit / trace (Photon.cpp:96-188),
+// PhotonGrid::build (Photon.cpp:24-53) and the fixed-radius
+// PhotonMap::estimateIrradiance (Photon.cpp:55-94), plus a k-nearest-capped
+// gather and a caustic render of the first diffuse camera hit.
+//
+// Emission: photon i draws from stream (seed, i, 0xFFFFFFFF) and is traced by
+// one thread with the recursion of PhotonMap::trace unrolled into a loop.
+// Stored records are appended with a key (photon index, record number) and
+// then sorted, so the photon array is in the canonical order (by photon, then
+// by trace order) no matter how the appends interleaved.
+//
+// Grid: the reference bins photons into an unordered_map keyed by cell index
+// with per-cell vectors in insertion order, and a query walks the cell box in
+// x, y, z order. Here photons are sorted by (cell, position in the photon
+// array) -- unique keys, so the order is fully determined -- and a per-cell
+// start table replaces the hash map. A query therefore adds the same photons in
+// the same order as the reference and gets the same float sum.
+//
+// Sorting: an in-house bitonic sort over 64-bit keys (global passes for long
+// strides, shared-memory passes for strides below 1024).
+#include "integrator.cuh"
+#include "prr_internal.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace prr {
+
+struct PhotonMap {
+    DevBuf rec;      // n x 9 floats: position, direction, power (canonical order)
+    DevBuf owner;    // n int32: emitting photon
+    int64_t n = 0;
+    // grid
+    bool built = false;
+    float radius = 0.01f; // PhotonMap::photon_radius default (Photon.hpp:36)
+    int res = 0;
+    float bmin[3] = {0, 0, 0}, cs[3] = {1, 1, 1};
+    DevBuf order;    // n int32: photon index, sorted by (cell, index)
+    DevBuf cell_of;  // n int32: cell of order[i]
+    DevBuf start;    // res^3 int32: first position in `order` of each cell, -1 if empty
+    DevBuf params;   // device copy of the grid parameters
+    DevBuf scratch;
+};
+
+namespace {
+
+constexpr float kPhotonEps = 1e-3f; // EPSILON (global.hpp:12)
+
+struct PhotonRecord {
+    V3 pos, dir, power;
+};
+
+// ---------------------------------------------------------------- emission
+struct EmitArgs {
+    int64_t n_photons;
+    uint64_t seed;
+    int max_depth;
+    float *rec;                 // capacity x 9
+    unsigned long long *keys;   // capacity: (photon << 5 | record) << 32 | slot
+    unsigned *count;
+    int64_t capacity;
+    int tlas_cap;
+};
+
+// sampleCosineHemisphere (BRDFUtils.hpp:66-73)
+__device__ __forceinline__ V3 sample_cosine(V3 N, Rng &rng) {
+    const float r1 = rng.next();
+    const float r2 = rng.next();
+    const float r = sqrtf(r1);
+    const float phi = 2.f * PRR_PI * r2;
+    return to_world(build_tbn(N), v3(r * cosf(phi), r * sinf(phi), sqrtf(smax(0.f, 1.f - r1))));
+}
+
+__global__ void k_photon_emit(DevScene S, EmitArgs a) {
+    extern __shared__ uint2 smem[];
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_photons)
+        return;
+    Rng rng{path_state(a.seed, (uint32_t) i, 0xFFFFFFFFu)};
+    // PhotonMap::emit body (Photon.cpp:166-180)
+    const LightPoint lp = sample_light(S, rng);
+    const float light_pdf = 1.0f / S.total_emit_area;
+    const float area = 1.0f / light_pdf;
+    const V3 dir0 = sample_cosine(lp.n, rng);
+    const DevMaterial &lm = S.materials[lp.material];
+    V3 power = v3(lm.emission[0], lm.emission[1], lm.emission[2]) * area / (float) a.n_photons;
+    V3 pos = lp.p + lp.n * kPhotonEps;
+    V3 dir = dir0;
+    bool caustic = false;
+    int stored = 0;
+    // PhotonMap::trace (Photon.cpp:96-154), tail recursion as a loop
+    for (int depth = 0; depth <= a.max_depth; depth++) {
+        const Inter hit = intersect(S, Ray3{pos, dir}, tst, bst);
+        if (!hit.hit)
+            break;
+        const DevMaterial &m = S.materials[hit.mat];
+        if (m.kind == kMatEmissive)
+            break;
+        const V3 gn = dot(dir, hit.n) < 0.0f ? hit.n : -hit.n;
+        if (m.kind == kMatMirror || m.kind == kMatGlass) {
+            Shading sd;
+            sd.f.N = gn; // trace fills only Ng and N (Photon.cpp:108-110)
+            const BSDFSample bs = delta_sample(m, sd, -dir, rng);
+            caustic = true;
+            power = power * bs.f;
+            dir = bs.wi;
+            pos = hit.p + (dot(bs.wi, gn) > 0.0f ? gn : -gn) * kPhotonEps;
+            continue;
+        }
+        if (depth > 0 && caustic) {
+            const unsigned slot = atomicAdd(a.count, 1u);
+            if ((int64_t) slot < a.capacity) {
+                float *r = a.rec + (size_t) slot * 9;
+                r[0] = hit.p.x;
+                r[1] = hit.p.y;
+                r[2] = hit.p.z;
+                r[3] = dir.x;
+                r[4] = dir.y;
+                r[5] = dir.z;
+                r[6] = power.x;
+                r[7] = power.y;
+                r[8] = power.z;
+                a.keys[slot] = ((((unsigned long long) i << 5) | (unsigned) stored) << 32) | slot;
+            }
+            stored++;
+        }
+        const float survival = smin(1.0f, max3(power));
+        if (!(rng.next() < survival && depth < a.max_depth))
+            break;
+        const Shading sd = build_shading(m, gn);
+        const V3 wo = -dir;
+        const BSDFSample bs = diffuse_sample(m, sd, wo, rng);
+        if (bs.pdf < 1e-6f)
+            break;
+        const float cos_t = smax(0.0f, dot(bs.wi, gn));
+        const V3 weight = bs.f * cos_t / bs.pdf;
+        power = power * weight;
+        const float s2 = smin(1.0f, max3(power));
+        if (rng.next() > s2)
+            break;
+        power = power / s2;
+        pos = hit.p + gn * kPhotonEps;
+        dir = bs.wi;
+    }
+}
+
+// ---------------------------------------------------------------- sorting
+__global__ void k_fill_keys(unsigned long long *keys, int64_t from, int64_t to) {
+    const int64_t i = from + (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < to)
+        keys[i] = ~0ull;
+}
+
+__global__ void k_bitonic_global(unsigned long long *keys, int64_t j, int64_t k, int64_t n) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int64_t l = i ^ j;
+    if (l <= i)
+        return;
+    const bool up = (i & k) == 0;
+    const unsigned long long a = keys[i], b = keys[l];
+    if ((a > b) == up) {
+        keys[i] = b;
+        keys[l] = a;
+    }
+}
+
+// strides j0, j0/2, ..., 1 of stage k inside 2048-element tiles
+__global__ void k_bitonic_shared(unsigned long long *keys, int64_t k, int j0) {
+    __shared__ unsigned long long t[2048];
+    const int64_t base = (int64_t) blockIdx.x * 2048;
+    t[threadIdx.x] = keys[base + threadIdx.x];
+    t[threadIdx.x + 1024] = keys[base + threadIdx.x + 1024];
+    __syncthreads();
+    for (int j = j0; j > 0; j >>= 1) {
+        for (int h = 0; h < 2; h++) {
+            const int i = (int) threadIdx.x + h * 1024;
+            const int l = i ^ j;
+            if (l > i) {
+                const bool up = ((base + i) & k) == 0;
+                const unsigned long long a = t[i], b = t[l];
+                if ((a > b) == up) {
+                    t[i] = b;
+                    t[l] = a;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    keys[base + threadIdx.x] = t[threadIdx.x];
+    keys[base + threadIdx.x + 1024] = t[threadIdx.x + 1024];
+}
+
+// Sorts keys[0, n2) ascending; n2 is a power of two >= 2048.
+int bitonic_sort(unsigned long long *keys, int64_t n2, cudaStream_t st) {
+    const int tb = 256;
+    const unsigned grid = (unsigned) ((n2 + tb - 1) / tb);
+    for (int64_t k = 2; k <= n2; k <<= 1) {
+        int64_t j = k >> 1;
+        for (; j >= 1024; j >>= 1)
+            k_bitonic_global<<<grid, tb, 0, st>>>(keys, j, k, n2);
+        k_bitonic_shared<<<(unsigned) (n2 / 2048), 1024, 0, st>>>(keys, k, (int) j);
+    }
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int64_t pow2_at_least(int64_t n) {
+    int64_t p = 2048;
+    while (p < n)
+        p <<= 1;
+    return p;
+}
+
+__global__ void k_gather_records(const unsigned long long *keys, const float *src, int64_t n,
+                                 float *dst, int32_t *owner) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned long long k = keys[i];
+    const unsigned slot = (unsigned) (k & 0xffffffffu);
+    for (int q = 0; q < 9; q++)
+        dst[i * 9 + q] = src[(size_t) slot * 9 + q];
+    owner[i] = (int32_t) ((k >> 32) >> 5);
+}
+
+// ---------------------------------------------------------------- grid
+struct GridParams {
+    float bmin[3], bmax[3], cs[3];
+    int res;
+};
+
+__global__ void k_bounds(const float *rec, int64_t n, float *partial) {
+    // per block min/max of positions; exact in any order
+    __shared__ float s[6][256];
+    float mn[3] = {kInf, kInf, kInf}, mx[3] = {-kInf, -kInf, -kInf};
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t) gridDim.x * blockDim.x)
+        for (int k = 0; k < 3; k++) {
+            const float v = rec[i * 9 + k];
+            mn[k] = fminf(mn[k], v);
+            mx[k] = fmaxf(mx[k], v);
+        }
+    for (int k = 0; k < 3; k++) {
+        s[k][threadIdx.x] = mn[k];
+        s[3 + k][threadIdx.x] = mx[k];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int) threadIdx.x < w)
+            for (int k = 0; k < 3; k++) {
+                s[k][threadIdx.x] = fminf(s[k][threadIdx.x], s[k][threadIdx.x + w]);
+                s[3 + k][threadIdx.x] = fmaxf(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 6; k++)
+            partial[blockIdx.x * 6 + k] = s[k][0];
+}
+
+// PhotonGrid::build's parameters (Photon.cpp:27-46), one thread.
+__global__ void k_grid_params(const float *partial, int nb, float radius, GridParams *g) {
+    float mn[3] = {kInf, kInf, kInf}, mx[3] = {-kInf, -kInf, -kInf};
+    for (int b = 0; b < nb; b++)
+        for (int k = 0; k < 3; k++) {
+            mn[k] = fminf(mn[k], partial[b * 6 + k]);
+            mx[k] = fmaxf(mx[k], partial[b * 6 + 3 + k]);
+        }
+    for (int k = 0; k < 3; k++) {
+        g->bmin[k] = mn[k] - 0.01f;
+        g->bmax[k] = mx[k] + 0.01f;
+    }
+    const float ex = g->bmax[0] - g->bmin[0], ey = g->bmax[1] - g->bmin[1],
+                ez = g->bmax[2] - g->bmin[2];
+    int res = (int) (sqrtf(ex * ex + ey * ey + ez * ez) / radius);
+    res = max(10, min(200, res));
+    g->res = res;
+    g->cs[0] = ex / (float) res;
+    g->cs[1] = ey / (float) res;
+    g->cs[2] = ez / (float) res;
+}
+
+// cell of each photon through worldToCell / cellToIndex (Photon.cpp:8-22)
+__global__ void k_cell_keys(const float *rec, int64_t n, const GridParams *g,
+                            unsigned long long *keys) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int res = g->res;
+    const int cx = (int) (float) (int) ((rec[i * 9 + 0] - g->bmin[0]) / g->cs[0]);
+    const int cy = (int) (float) (int) ((rec[i * 9 + 1] - g->bmin[1]) / g->cs[1]);
+    const int cz = (int) (float) (int) ((rec[i * 9 + 2] - g->bmin[2]) / g->cs[2]);
+    const unsigned cell = (unsigned) (cx + cy * res + cz * res * res);
+    keys[i] = ((unsigned long long) cell << 32) | (unsigned long long) i;
+}
+
+__global__ void k_cell_table(const unsigned long long *keys, int64_t n, int32_t *order,
+                             int32_t *cell_of, int32_t *start) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned cell = (unsigned) (keys[i] >> 32);
+    order[i] = (int32_t) (keys[i] & 0xffffffffu);
+    cell_of[i] = (int32_t) cell;
+    if (i == 0 || (unsigned) (keys[i - 1] >> 32) != cell)
+        start[cell] = (int32_t) i;
+}
+
+// ---------------------------------------------------------------- gather
+struct GridView {
+    const float *rec;
+    const int32_t *order, *cell_of, *start;
+    const GridParams *g;
+    int64_t n;
+    float radius;
+};
+
+// PhotonGrid::query + PhotonMap::estimateIrradiance (Photon.cpp:55-94). With
+// k_nearest > 0 and more than k photons inside the radius, the estimate uses
+// the k nearest and the disc through the k-th one instead.
+__device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc) {
+    const GridParams &g = *v.g;
+    const float r = v.radius;
+    int x0 = (int) ((pos.x - r - g.bmin[0]) / g.cs[0]);
+    int y0 = (int) ((pos.y - r - g.bmin[1]) / g.cs[1]);
+    int z0 = (int) ((pos.z - r - g.bmin[2]) / g.cs[2]);
+    int x1 = (int) ((pos.x + r - g.bmin[0]) / g.cs[0]);
+    int y1 = (int) ((pos.y + r - g.bmin[1]) / g.cs[1]);
+    int z1 = (int) ((pos.z + r - g.bmin[2]) / g.cs[2]);
+    x0 = max(0, x0);
+    x1 = min(g.res - 1, x1);
+    y0 = max(0, y0);
+    y1 = min(g.res - 1, y1);
+    z0 = max(0, z0);
+    z1 = min(g.res - 1, z1);
+    V3 e = v3(0.f);
+    int found = 0;
+    for (int cx = x0; cx <= x1; cx++)
+        for (int cy = y0; cy <= y1; cy++)
+            for (int cz = z0; cz <= z1; cz++) {
+                const int cell = cx + cy * g.res + cz * g.res * g.res;
+                int s = v.start[cell];
+                if (s < 0)
+                    continue;
+                for (; s < v.n && v.cell_of[s] == cell; s++) {
+                    const float *p = v.rec + (size_t) v.order[s] * 9;
+                    const V3 d = v3(p[0], p[1], p[2]) - pos;
+                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+                    if (dist <= r) {
+                        e = e + v3(p[6], p[7], p[8]);
+                        if (kd && found < k_nearest) {
+                            kd[found] = dist;
+                            kc[found] = v.order[s];
+                        } else if (kd) {
+                            // keep the k smallest distances (replace the largest)
+                            int worst = 0;
+                            for (int q = 1; q < k_nearest; q++)
+                                if (kd[q] > kd[worst])
+                                    worst = q;
+                            if (dist < kd[worst]) {
+                                kd[worst] = dist;
+                                kc[worst] = v.order[s];
+                            }
+                        }
+                        found++;
+                    }
+                }
+            }
+    if (found == 0)
+        return v3(0.f);
+    if (kd && found > k_nearest) {
+        // Jensen's estimate over the k nearest: sum / (pi r_k^2); the k kept
+        // photons are added in photon-array order for a fixed result
+        float rk = 0.f;
+        for (int q = 0; q < k_nearest; q++)
+            rk = fmaxf(rk, kd[q]);
+        for (int a = 1; a < k_nearest; a++) {
+            const int key = kc[a];
+            int b = a - 1;
+            while (b >= 0 && kc[b] > key) {
+                kc[b + 1] = kc[b];
+                b--;
+            }
+            kc[b + 1] = key;
+        }
+        V3 ek = v3(0.f);
+        for (int q = 0; q < k_nearest; q++) {
+            const float *p = v.rec + (size_t) kc[q] * 9;
+            ek = ek + v3(p[6], p[7], p[8]);
+        }
+        const float area = PRR_PI * rk * rk;
+        return ek / area;
+    }
+    const float area = PRR_PI * r * r;
+    return e / area;
+}
+
+constexpr int kMaxK = 64;
+
+__global__ void k_photon_gather(GridView v, const float *q, int64_t n, int k_nearest, float *out) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float kd[kMaxK];
+    int kc[kMaxK];
+    const V3 e = irradiance(v, v3(q[i * 3], q[i * 3 + 1], q[i * 3 + 2]), k_nearest,
+                            k_nearest > 0 ? kd : nullptr, kc);
+    out[i * 3] = e.x;
+    out[i * 3 + 1] = e.y;
+    out[i * 3 + 2] = e.z;
+}
+
+// Caustic render: per (pixel, sample), follow the camera ray through the
+// specular chain as castRay does (Integrator.cpp:143-169) and, at the first
+// non-delta hit, estimate the caustic radiance baseColor/pi * E(x).
+struct CausticArgs {
+    int W, x0, y0, ww, wh, spp, max_depth, k_nearest, tlas_cap;
+    uint64_t seed;
+    int sample_offset;
+    float *out;
+};
+
+__global__ void k_render_caustics(DevScene S, GridView v, CausticArgs a) {
+    extern __shared__ uint2 smem[];
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= a.ww * a.wh)
+        return;
+    const int i = a.x0 + q % a.ww, j = a.y0 + q / a.ww;
+    const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) a.W;
+    float kd[kMaxK];
+    int kc[kMaxK];
+    V3 acc = v3(0.f);
+    for (int n = 0; n < a.spp; n++) {
+        Rng rng{path_state(a.seed, m, (uint32_t) (a.sample_offset + n))};
+        const float xo = rng.next();
+        const float yo = rng.next();
+        Ray3 ray = generate_ray(S.camera, i, j, xo, yo, rng);
+        V3 beta = v3(1.f);
+        for (int d = 0; d < a.max_depth; d++) {
+            const Inter in = intersect(S, ray, tst, bst);
+            if (!in.hit)
+                break;
+            const DevMaterial &mt = S.materials[in.mat];
+            if (mt.kind == kMatEmissive)
+                break;
+            if (mt.kind == kMatMirror || mt.kind == kMatGlass) {
+                const Shading sd = build_shading(mt, in.n);
+                const BSDFSample bs = delta_sample(mt, sd, -ray.d, rng);
+                beta = beta * bs.f / bs.pdf;
+                const bool trans = dot(bs.wi, in.n) < 0.f;
+                ray = Ray3{in.p + (trans ? -in.n : in.n) * PRR_EPS, bs.wi};
+                if (trans)
+                    beta = beta * sd.base;
+                continue;
+            }
+            const V3 e = irradiance(v, in.p, a.k_nearest, a.k_nearest > 0 ? kd : nullptr, kc);
+            acc = acc + beta * (v3(mt.base[0], mt.base[1], mt.base[2]) / PRR_PI) * e;
+            break;
+        }
+    }
+    a.out[(size_t) q * 3] = acc.x / (float) a.spp;
+    a.out[(size_t) q * 3 + 1] = acc.y / (float) a.spp;
+    a.out[(size_t) q * 3 + 2] = acc.z / (float) a.spp;
+}
+
+PhotonMap *PM(prr_photon_map *p) { return reinterpret_cast<PhotonMap *>(p); }
+const PhotonMap *PM(const prr_photon_map *p) { return reinterpret_cast<const PhotonMap *>(p); }
+
+GridView view(const PhotonMap &pm) {
+    GridView v;
+    v.rec = pm.rec.as<float>();
+    v.order = pm.order.as<int32_t>();
+    v.cell_of = pm.cell_of.as<int32_t>();
+    v.start = pm.start.as<int32_t>();
+    v.g = pm.params.as<GridParams>();
+    v.n = pm.n;
+    v.radius = pm.radius;
+    return v;
+}
+
+} // namespace
+} // namespace prr
+
+using namespace prr;
+
+extern "C" {
+
+int prr_photon_map_create(prr_photon_map **out) {
+    if (!out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = reinterpret_cast<prr_photon_map *>(new PhotonMap());
+    return PRR_OK;
+}
+
+int prr_photon_map_destroy(prr_photon_map *pm) {
+    delete PM(pm);
+    return PRR_OK;
+}
+
+int prr_photon_emit(prr_photon_map *pmap, const prr_scene *scene, int64_t num_photons,
+                    uint64_t seed, int max_depth, void *stream) {
+    if (!pmap || !scene)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "photon map and scene are required");
+    const Scene &s = *reinterpret_cast<const Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    if (s.dev.n_emissives == 0 || !(s.dev.total_emit_area > 0.f))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene has no area emitters");
+    if (num_photons <= 0 || num_photons >= (int64_t) 1 << 27 || max_depth < 0 || max_depth > 30)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "need 0 < num_photons < 2^27, 0 <= max_depth <= 30");
+    PhotonMap &pm = *PM(pmap);
+    cudaStream_t st = (cudaStream_t) stream;
+    const int block = 128;
+    const int tcap = s.dev.tlas_depth + 1, bcap = s.dev.blas_depth + 1;
+    const size_t smem = (size_t) (tcap + bcap) * block * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    if (smem > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_photon_emit,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int64_t capacity = std::max<int64_t>(num_photons, 1 << 16);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        const int64_t n2 = pow2_at_least(capacity);
+        PRR_CUDA_TRY(pm.scratch.ensure((size_t) capacity * 9 * sizeof(float) + n2 * 8 + 64));
+        float *rec = pm.scratch.as<float>();
+        unsigned long long *keys =
+            reinterpret_cast<unsigned long long *>((char *) pm.scratch.ptr + capacity * 9 * 4);
+        unsigned *count = reinterpret_cast<unsigned *>((char *) keys + n2 * 8);
+        PRR_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(unsigned), st));
+        EmitArgs a{num_photons, seed, max_depth, rec, keys, count, capacity, tcap};
+        k_photon_emit<<<(unsigned) ((num_photons + block - 1) / block), block, smem, st>>>(s.dev, a);
+        PRR_CUDA_TRY(cudaGetLastError());
+        unsigned stored = 0;
+        PRR_CUDA_TRY(cudaMemcpyAsync(&stored, count, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        PRR_CUDA_TRY(cudaStreamSynchronize(st));
+        if ((int64_t) stored > capacity) { // rerun with room for every record
+            capacity = (int64_t) stored + (stored >> 3) + 1024;
+            continue;
+        }
+        const int64_t n = stored;
+        const int64_t np2 = pow2_at_least(std::max<int64_t>(n, 1));
+        if (np2 > n)
+            k_fill_keys<<<(unsigned) ((np2 - n + 255) / 256), 256, 0, st>>>(keys, n, np2);
+        if (int rc = bitonic_sort(keys, np2, st))
+            return rc;
+        PRR_CUDA_TRY(pm.rec.ensure((size_t) std::max<int64_t>(n, 1) * 9 * sizeof(float)));
+        PRR_CUDA_TRY(pm.owner.ensure((size_t) std::max<int64_t>(n, 1) * sizeof(int32_t)));
+        if (n > 0)
+            k_gather_records<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
+                keys, rec, n, pm.rec.as<float>(), pm.owner.as<int32_t>());
+        PRR_CUDA_TRY(cudaGetLastError());
+        PRR_CUDA_TRY(cudaStreamSynchronize(st));
+        pm.n = n;
+        pm.built = false;
+        return PRR_OK;
+    }
+    return fail(PRR_ERR_INTERNAL, "photon record buffer overflow");
+}
+
+int prr_photon_set(prr_photon_map *pmap, const float *records, int64_t n, void *stream) {
+    if (!pmap || n < 0 || (n > 0 && !records))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad photon array");
+    PhotonMap &pm = *PM(pmap);
+    cudaStream_t st = (cudaStream_t) stream;
+    PRR_CUDA_TRY(pm.rec.ensure((size_t) std::max<int64_t>(n, 1) * 9 * sizeof(float)));
+    PRR_CUDA_TRY(pm.owner.ensure((size_t) std::max<int64_t>(n, 1) * sizeof(int32_t)));
+    if (n > 0) {
+        PRR_CUDA_TRY(cudaMemcpyAsync(pm.rec.ptr, records, (size_t) n * 9 * sizeof(float),
+                                     cudaMemcpyDefault, st));
+        PRR_CUDA_TRY(cudaMemsetAsync(pm.owner.ptr, 0xff, (size_t) n * sizeof(int32_t), st));
+    }
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    pm.n = n;
+    pm.built = false;
+    return PRR_OK;
+}
+
+int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
+    if (!pmap || !(radius > 0.f))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "need a photon map and radius > 0");
+    PhotonMap &pm = *PM(pmap);
+    cudaStream_t st = (cudaStream_t) stream;
+    pm.radius = radius;
+    PRR_CUDA_TRY(pm.params.ensure(sizeof(GridParams)));
+    if (pm.n == 0) {
+        pm.built = true;
+        pm.res = 0;
+        return PRR_OK;
+    }
+    const int64_t n = pm.n;
+    const int nb = (int) std::min<int64_t>(1024, (n + 255) / 256);
+    const int64_t n2 = pow2_at_least(n);
+    PRR_CUDA_TRY(pm.scratch.ensure((size_t) n2 * 8 + (size_t) nb * 6 * 4 + 64));
+    unsigned long long *keys = pm.scratch.as<unsigned long long>();
+    float *partial = reinterpret_cast<float *>((char *) pm.scratch.ptr + n2 * 8);
+    k_bounds<<<nb, 256, 0, st>>>(pm.rec.as<float>(), n, partial);
+    k_grid_params<<<1, 1, 0, st>>>(partial, nb, radius, pm.params.as<GridParams>());
+    k_cell_keys<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(pm.rec.as<float>(), n,
+                                                              pm.params.as<GridParams>(), keys);
+    if (n2 > n)
+        k_fill_keys<<<(unsigned) ((n2 - n + 255) / 256), 256, 0, st>>>(keys, n, n2);
+    PRR_CUDA_TRY(cudaGetLastError());
+    if (int rc = bitonic_sort(keys, n2, st))
+        return rc;
+    GridParams g;
+    PRR_CUDA_TRY(cudaMemcpyAsync(&g, pm.params.ptr, sizeof(g), cudaMemcpyDeviceToHost, st));
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    const size_t cells = (size_t) g.res * g.res * g.res;
+    PRR_CUDA_TRY(pm.order.ensure((size_t) n * sizeof(int32_t)));
+    PRR_CUDA_TRY(pm.cell_of.ensure((size_t) n * sizeof(int32_t)));
+    PRR_CUDA_TRY(pm.start.ensure(cells * sizeof(int32_t)));
+    PRR_CUDA_TRY(cudaMemsetAsync(pm.start.ptr, 0xff, cells * sizeof(int32_t), st));
+    k_cell_table<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
+        keys, n, pm.order.as<int32_t>(), pm.cell_of.as<int32_t>(), pm.start.as<int32_t>());
+    PRR_CUDA_TRY(cudaGetLastError());
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    pm.res = g.res;
+    std::memcpy(pm.bmin, g.bmin, sizeof(pm.bmin));
+    std::memcpy(pm.cs, g.cs, sizeof(pm.cs));
+    pm.built = true;
+    return PRR_OK;
+}
+
+int prr_photon_info(const prr_photon_map *pmap, int64_t *count, int32_t *grid_res) {
+    if (!pmap)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "photon map is NULL");
+    const PhotonMap &pm = *PM(pmap);
+    if (count)
+        *count = pm.n;
+    if (grid_res)
+        *grid_res = pm.res;
+    return PRR_OK;
+}
+
+int prr_photon_export(const prr_photon_map *pmap, float *records, int32_t *owner, void *stream) {
+    if (!pmap)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "photon map is NULL");
+    const PhotonMap &pm = *PM(pmap);
+    cudaStream_t st = (cudaStream_t) stream;
+    if (pm.n > 0 && records)
+        PRR_CUDA_TRY(cudaMemcpyAsync(records, pm.rec.ptr, (size_t) pm.n * 9 * sizeof(float),
+                                     cudaMemcpyDefault, st));
+    if (pm.n > 0 && owner)
+        PRR_CUDA_TRY(cudaMemcpyAsync(owner, pm.owner.ptr, (size_t) pm.n * sizeof(int32_t),
+                                     cudaMemcpyDefault, st));
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    return PRR_OK;
+}
+
+int prr_photon_gather(const prr_photon_map *pmap, const float *points, int64_t n, int k_nearest,
+                      float *out_rgb, void *stream) {
+    if (!pmap || n < 0 || (n > 0 && (!points || !out_rgb)) || k_nearest < 0 || k_nearest > kMaxK)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad gather arguments (k_nearest <= 64)");
+    const PhotonMap &pm = *PM(pmap);
+    if (!pm.built)
+        return fail(PRR_ERR_NOT_BUILT, "photon map not built (call prr_photon_build)");
+    cudaStream_t st = (cudaStream_t) stream;
+    if (n == 0)
+        return PRR_OK;
+    if (pm.n == 0) {
+        PRR_CUDA_TRY(cudaMemsetAsync(out_rgb, 0, (size_t) n * 3 * sizeof(float), st));
+        return PRR_OK;
+    }
+    k_photon_gather<<<(unsigned) ((n + 127) / 128), 128, 0, st>>>(view(pm), points, n, k_nearest,
+                                                                   out_rgb);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int prr_render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
+                        const prr_render_settings *settings, int k_nearest, float *out_rgb,
+                        void *stream) {
+    if (!scene || !pmap || !settings || !out_rgb || k_nearest < 0 || k_nearest > kMaxK)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad caustic render arguments");
+    const Scene &s = *reinterpret_cast<const Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    const PhotonMap &pm = *PM(pmap);
+    if (!pm.built || pm.n == 0)
+        return fail(PRR_ERR_NOT_BUILT, "photon map empty or not built");
+    prr_render_settings rs = *settings;
+    rs.mode = PRR_RENDER_PLAIN;
+    rs.min_spp = rs.max_spp;
+    if (int rc = validate_render(s, rs))
+        return rc;
+    CausticArgs a{};
+    a.W = s.width;
+    a.x0 = rs.x0;
+    a.y0 = rs.y0;
+    a.ww = rs.x1 - rs.x0;
+    a.wh = rs.y1 - rs.y0;
+    a.spp = rs.max_spp;
+    a.max_depth = rs.max_depth;
+    a.k_nearest = k_nearest;
+    a.seed = rs.seed;
+    a.sample_offset = rs.sample_offset;
+    a.out = out_rgb;
+    a.tlas_cap = s.dev.tlas_depth + 1;
+    const int block = 128;
+    const size_t smem = (size_t) (a.tlas_cap + s.dev.blas_depth + 1) * block * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    if (smem > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_render_caustics,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    const int npix = a.ww * a.wh;
+    k_render_caustics<<<(npix + block - 1) / block, block, smem, (cudaStream_t) stream>>>(
+        s.dev, view(pm), a);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+} // extern "C"
