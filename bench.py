@@ -165,7 +165,8 @@ def workload_arrays():
 
 
 def parse_launch(text):
-    """'block=128,persistent=1' -> launch config dict."""
+    """'block=128,persistent=1' (or 'paths=1048576,block=128' for the
+    wavefront) -> launch config dict."""
     out = {}
     for kv in filter(None, (text or "").split(",")):
         k, v = kv.split("=")
@@ -303,6 +304,7 @@ def run_ours(args, rank, world, on):
         barrier(on)
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms_step = max_over_ranks(float(np.mean(kernel_ms)), on)
+    ms_median = max_over_ranks(float(np.median(kernel_ms)), on)
     value = N_RAYS * world / (ms_step * 1e-3) / 1e6
 
     assert int((hid >= 0).sum().item()) > 0.99 * N_RAYS
@@ -345,7 +347,8 @@ def run_ours(args, rank, world, on):
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "rays_per_step": N_RAYS, "triangles": N_TRIS,
                    "seed": 1, "l2": "flushed (512 MB write) before every timed step",
-                   "launch": best, "parallelism": f"replica x{world}" if world > 1 else "1 GPU"},
+                   "launch": best, "parallelism": f"replica x{world}" if world > 1 else "1 GPU",
+                   "step_ms": [round(x, 3) for x in kernel_ms], "median_ms": ms_median},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 24,
                 "d2h_bytes_per_step": N_RAYS * 8},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -380,9 +383,20 @@ def run_render(args, rank, world, on):
     factory, spp, depth, desc_text = RENDER_WORKLOADS[args.workload]
     dev = torch.device("cuda", torch.cuda.current_device())
     desc = factory()
+    if args.size:
+        desc.width, desc.height = (int(v) for v in args.size.split("x"))
+        desc_text += f" (resized to {desc.width}x{desc.height})"
+    if args.spp:
+        spp = args.spp
+        desc_text += f" (spp {spp})"
     scene = prr.Scene.from_desc(desc)
     npix = desc.width * desc.height
-    tuned = scene.autotune(4, depth)
+    if args.launch:
+        cfg = parse_launch(args.launch)
+        scene.set_wavefront(cfg.get("paths", 0), cfg.get("block_size", 0), True)
+        tuned = cfg
+    else:
+        tuned = scene.autotune(4, depth)
 
     def timed(mode, steps):
         ms = []
@@ -397,12 +411,18 @@ def run_render(args, rank, world, on):
             ms.append(a.elapsed_time(b))
         return ms, img, rays
 
-    timed("plain", 1)
+    if not args.kernel_only:
+        timed("plain", 1)
     timed("wavefront", args.warmup)
     with ClockSampler(dev.index) as clk:
         barrier(on)
         wf_ms, wf_img, wf_rays = timed("wavefront", args.steps)
         barrier(on)
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"frame_ms": wf_ms, "msamples_s": npix * spp / np.mean(wf_ms) / 1e3,
+                              "launch": tuned}))
+        return 0
     pl_ms, pl_img, pl_rays = timed("plain", max(1, min(args.steps, 3)))
     wf_step = max_over_ranks(float(np.mean(wf_ms)), on)
     pl_step = max_over_ranks(float(np.mean(pl_ms)), on)
@@ -461,14 +481,129 @@ def run_render(args, rank, world, on):
     return 0
 
 
+def serving_pool():
+    """Eight procedural scenes from about 10k to 2M triangles, built like the
+    museum-like scene (displaced icospheres under the HDR sky) and the query
+    set (a 1M / 1.5M triangle soup under the same sky)."""
+    import math
+    from photorealisticrender4610_b200 import scenes as sc
+    pool = []
+    for level in (3, 4, 5, 6, 7):
+        pool.append(sc.museum_like(512, 512, level=level, env_size=(1024, 512)))
+    for n in (1_000_000, 1_500_000):
+        d = sc.SceneDesc(width=512, height=512, name=f"soup{n}")
+        m = d.add_material(sc.Material(sc.DIFFUSE, (0.7, 0.6, 0.5), 0.6, 0.0))
+        v, _, _ = sc.query_set(n, 1, seed=n)
+        d.objects.append(sc.MeshObject(v, m))
+        d.env = pool[0].env
+        d.camera = sc.Camera(eye=(2.2, 1.6, 2.4), target=(0.5, 0.5, 0.5), fovv=40, fovh=45)
+        pool.append(d)
+    pool.append(sc.caustics(512, 512, level=3))
+    return pool
+
+
+def run_serving(args, rank, world, on):
+    """Continuous-batching server under Poisson arrivals against the plain
+    renderer run one request at a time in arrival order."""
+    import math
+    import threading
+    import torch
+    import photorealisticrender4610_b200 as prr
+
+    if rank != 0:
+        return 0
+    rng = np.random.Generator(np.random.PCG64(7))
+    pool = serving_pool()
+    scenes_ = [prr.Scene.from_desc(d) for d in pool]
+    tris = [d.n_triangles() for d in pool]
+    sizes = [(256, 256), (512, 512), (1024, 1024), (1920, 1080)]
+    n = args.requests
+    gaps = rng.exponential(1.0 / args.rate, n)
+    arrive = np.cumsum(gaps) - gaps[0]
+    reqs = []
+    for k in range(n):
+        spp = int(round(math.exp(rng.uniform(math.log(4), math.log(args.max_spp)))))
+        reqs.append((int(rng.integers(0, len(pool))), sizes[int(rng.integers(0, 4))], spp))
+    depth = 8
+    total_samples = sum(w * h * spp for _, (w, h), spp in reqs)
+
+    host = [torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
+            for _, (w, h), _ in reqs]
+
+    def serve(max_active, samples_per_step):
+        """Replays the arrival schedule against a server; returns latencies,
+        the wall span and the server stats."""
+        srv = prr.Server(max_active=max_active, samples_per_step=samples_per_step)
+        for s_ in scenes_:
+            srv.add_scene(s_)
+        srv.wait(srv.submit(0, 2, depth, size=(64, 64)))  # warm-up
+        ids = [None] * n
+        t_start = time.perf_counter()
+
+        def submitter():
+            for k, (sc_, size, spp) in enumerate(reqs):
+                delay = arrive[k] - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                ids[k] = srv.submit(sc_, spp, depth, seed=k + 1, size=size, out=host[k])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        infos = [srv.wait(i) for i in ids]
+        st = srv.stats()
+        srv.close()
+        lat = np.array([i["done_s"] - i["submit_s"] for i in infos])
+        span = max(i["done_s"] for i in infos) - min(i["submit_s"] for i in infos)
+        return lat, span, st
+
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        lat, span, st = serve(args.max_active, 1 << 20)
+    served_rate = total_samples / span / 1e6
+    busy_rate = total_samples / st["busy_s"] / 1e6
+    # baseline: the same schedule, one request at a time in arrival order
+    one, one_span, one_st = serve(1, 1 << 24)
+    line = {
+        "metric": "served p50/p99 latency (s) and Msamples/s", "value": float(np.percentile(lat, 99)),
+        "unit": "s (p99 latency)", "n_gpus": world, "steps": n, "warmup": 1,
+        "ms_per_step": float(np.mean(lat)) * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving: Poisson arrivals over a pool of 8 procedural scenes "
+                               f"({min(tris)}-{max(tris)} triangles), resolution from "
+                               "{256^2, 512^2, 1024^2, 1920x1080}, spp log-uniform "
+                               f"[4, {args.max_spp}], depth {depth}",
+                   "requests": n, "rate_per_s": args.rate, "max_active": args.max_active,
+                   "offered_msamples_s": total_samples / (arrive[-1] + 1e-9) / 1e6,
+                   "total_samples": total_samples},
+        "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+        "served_msamples_s": served_rate, "served_busy_msamples_s": busy_rate,
+        "one_at_a_time": {"p50_s": float(np.percentile(one, 50)),
+                          "p99_s": float(np.percentile(one, 99)),
+                          "msamples_s": total_samples / one_span / 1e6},
+        "failed": int(st["failed"]),
+        "e2e": {"value": served_rate, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(np.mean([w * h * 12 for _, (w, h), _ in reqs]))},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--launch", default="", help="fixed launch shape, e.g. block=128,persistent=0")
-    ap.add_argument("--workload", choices=["query", "museum", "cornell"], default="query")
+    ap.add_argument("--workload", choices=["query", "museum", "cornell", "serving"],
+                    default="query")
+    ap.add_argument("--requests", type=int, default=120, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrivals per s")
+    ap.add_argument("--max-spp", type=int, default=256, help="serving: spp upper bound")
+    ap.add_argument("--max-active", type=int, default=64, help="serving: concurrent requests")
+    ap.add_argument("--size", default="", help="render workloads: WxH override")
+    ap.add_argument("--spp", type=int, default=0, help="render workloads: spp override")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the kernel only (no e2e, no CPU baseline): profiling runs")
     args = ap.parse_args()
@@ -480,6 +615,8 @@ def main():
         return run_reference(args, rank, world)
     on = init_dist(world, local)
     try:
+        if args.workload == "serving":
+            return run_serving(args, rank, world, on)
         if args.workload != "query":
             return run_render(args, rank, world, on)
         return run_ours(args, rank, world, on)

@@ -234,6 +234,62 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream);
 
+/* ---- render server: continuous batching ---------------------------------
+ * No counterpart in the reference (its Renderer renders one scene per
+ * process). Requests are admitted in arrival order while a slot is free and
+ * the device budget (resident scenes + admitted requests) holds; every step
+ * renders the next sample chunk of every running request in one launch, so
+ * new requests join running ones at the next step. */
+typedef struct prr_server prr_server;
+typedef struct prr_server_config {
+    int64_t device_budget_bytes; /* resident scenes + admitted requests (0: 120 GiB) */
+    int max_active;              /* requests rendered at once (0: 64) */
+    int64_t samples_per_step;    /* samples per request per step (0: 1,048,576) */
+    int fail_every_nth_admission;/* fault injection on the host for tests (0: off):
+                                    every n-th admission fails its allocation */
+} prr_server_config;
+typedef struct prr_request {
+    int scene;                    /* id from prr_server_add_scene */
+    prr_render_settings settings; /* fixed spp (min_spp == max_spp), window, seed; width and
+                                     height may differ from the scene's: the scene's camera
+                                     is re-initialised for them (Camera::init) */
+    float *out_rgb;               /* window x 3 floats, host or device memory */
+} prr_request;
+#define PRR_REQUEST_QUEUED 0
+#define PRR_REQUEST_RUNNING 1
+#define PRR_REQUEST_DONE 2
+#define PRR_REQUEST_FAILED 3
+#define PRR_REQUEST_CANCELLED 4
+typedef struct prr_request_info {
+    int status;                   /* PRR_REQUEST_* */
+    int error;                    /* PRR_ERR_* when FAILED */
+    double submit_s, admit_s, done_s; /* server steady clock, seconds */
+    int64_t samples;              /* samples rendered so far */
+    uint64_t rays;                /* rays traced so far */
+} prr_request_info;
+typedef struct prr_server_stats {
+    int64_t submitted, completed, failed, active, queued;
+    int64_t samples;
+    uint64_t rays;
+    int64_t steps;
+    double busy_s;                /* time inside GPU steps */
+    int64_t bytes_in_use;
+    double now_s;
+} prr_server_stats;
+int prr_server_create(const prr_server_config *config, prr_server **out);
+/* Cancels queued requests, finishes running ones, joins the worker. */
+int prr_server_destroy(prr_server *server);
+/* Registers a built scene (kept resident; the caller keeps it alive until the
+ * server is destroyed). All scenes are added before the first submit. */
+int prr_server_add_scene(prr_server *server, prr_scene *scene, int *out_id);
+int prr_server_submit(prr_server *server, const prr_request *request, uint64_t *out_id);
+int prr_server_cancel(prr_server *server, uint64_t id);
+int prr_server_poll(prr_server *server, uint64_t id, prr_request_info *info);
+/* Blocks until the request is done, failed or cancelled (timeout_s < 0: no
+ * limit); PRR_ERR_TIMEOUT otherwise. */
+int prr_server_wait(prr_server *server, uint64_t id, double timeout_s, prr_request_info *info);
+int prr_server_stats_get(prr_server *server, prr_server_stats *out);
+
 /* Allocation-free rendering. No counterpart in the reference: this entry
  * point exists for callers that cannot call cudaMalloc while they render (a
  * host whose device memory is owned by another allocator, or a frame loop that

@@ -42,6 +42,24 @@ class prr_wavefront_config(C.Structure):
     _fields_ = [("paths_per_pass", C.c_int64), ("block_size", C.c_int), ("use_graphs", C.c_int)]
 
 
+class prr_server_config(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_int64), ("max_active", C.c_int),
+                ("samples_per_step", C.c_int64), ("fail_every_nth_admission", C.c_int)]
+
+
+class prr_request_info(C.Structure):
+    _fields_ = [("status", C.c_int), ("error", C.c_int), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double), ("samples", C.c_int64),
+                ("rays", C.c_uint64)]
+
+
+class prr_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("active", C.c_int64), ("queued", C.c_int64), ("samples", C.c_int64),
+                ("rays", C.c_uint64), ("steps", C.c_int64), ("busy_s", C.c_double),
+                ("bytes_in_use", C.c_int64), ("now_s", C.c_double)]
+
+
 class prr_scene_stats(C.Structure):
     _fields_ = [("n_objects", C.c_int64), ("n_triangles", C.c_int64), ("n_nodes", C.c_int64),
                 ("tlas_depth", C.c_int32), ("blas_depth", C.c_int32),
@@ -54,6 +72,10 @@ class prr_render_settings(C.Structure):
                 ("indirect_clamp", C.c_float), ("mode", C.c_int), ("seed", C.c_uint64),
                 ("x0", C.c_int), ("y0", C.c_int), ("x1", C.c_int), ("y1", C.c_int),
                 ("sample_offset", C.c_int), ("slices", C.c_int)]
+
+
+class prr_request(C.Structure):
+    _fields_ = [("scene", C.c_int), ("settings", prr_render_settings), ("out_rgb", C.c_void_p)]
 
 
 _vp = C.c_void_p
@@ -91,6 +113,14 @@ _SIGS = {
     "prr_photon_gather": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp]),
     "prr_render_caustics": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int, _vp,
                                       _vp]),
+    "prr_server_create": (C.c_int, [C.POINTER(prr_server_config), C.POINTER(_vp)]),
+    "prr_server_destroy": (C.c_int, [_vp]),
+    "prr_server_add_scene": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),
+    "prr_server_submit": (C.c_int, [_vp, _vp, C.POINTER(C.c_uint64)]),
+    "prr_server_cancel": (C.c_int, [_vp, C.c_uint64]),
+    "prr_server_poll": (C.c_int, [_vp, C.c_uint64, C.POINTER(prr_request_info)]),
+    "prr_server_wait": (C.c_int, [_vp, C.c_uint64, C.c_double, C.POINTER(prr_request_info)]),
+    "prr_server_stats_get": (C.c_int, [_vp, C.POINTER(prr_server_stats)]),
     "prr_tonemap": (C.c_int, [C.c_int, C.c_float, _vp, C.c_int64, _vp, _vp, _vp]),
     "prr_render_noalloc": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp]),
     "prr_scene_set_wavefront": (C.c_int, [_vp, C.POINTER(prr_wavefront_config)]),

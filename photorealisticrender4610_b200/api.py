@@ -15,7 +15,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (check, prr_camera, prr_render_settings, prr_scene_stats, prr_trace_config,
+from ._lib import (check, prr_camera, prr_render_settings, prr_request, prr_request_info,
+                   prr_scene_stats, prr_server_config, prr_server_stats, prr_trace_config,
                    prr_wavefront_config)
 
 RENDER_MODES = {"plain": 0, "wavefront": 1}
@@ -425,3 +426,83 @@ class PhotonMap:
         check(self.lib.prr_render_caustics(scene.h, self.h, C.byref(rs), k_nearest, _ptr(out),
                                            _stream(stream)))
         return out
+
+
+REQUEST_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class Server:
+    """The render server (continuous batching over resident scenes)."""
+
+    def __init__(self, budget_bytes: int = 0, max_active: int = 0, samples_per_step: int = 0,
+                 fail_every_nth_admission: int = 0):
+        self.lib = _lib.load()
+        cfg = prr_server_config(budget_bytes, max_active, samples_per_step,
+                                fail_every_nth_admission)
+        h = C.c_void_p()
+        check(self.lib.prr_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.scenes = []
+        self._keep = {}
+
+    def close(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.lib.prr_server_destroy(h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def add_scene(self, scene: Scene) -> int:
+        out = C.c_int()
+        check(self.lib.prr_server_add_scene(self.h, scene.h, C.byref(out)))
+        self.scenes.append(scene)
+        return out.value
+
+    def submit(self, scene_id: int, spp: int, max_depth: int, seed: int = 1, window=None,
+               out=None, size=None) -> int:
+        """Queue a render; `out` is a (h, w, 3) float32 CUDA tensor or a numpy
+        array (pinned or pageable) that receives the image; `size` = (W, H)
+        renders the scene's camera at another resolution."""
+        sc = self.scenes[scene_id]
+        rs = sc._settings(spp, max_depth, seed, None, 0.05, "plain", window, 10.0, 0, 0)
+        W, H = size or (sc.desc.width, sc.desc.height)
+        rs.width, rs.height = W, H
+        if window is None:
+            rs.x0, rs.y0, rs.x1, rs.y1 = 0, 0, W, H
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        if out is None:
+            out = np.empty((y1 - y0, x1 - x0, 3), np.float32)
+        ptr = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        req = prr_request(scene_id, rs, C.c_void_p(ptr))
+        rid = C.c_uint64()
+        check(self.lib.prr_server_submit(self.h, C.byref(req), C.byref(rid)))
+        self._keep[rid.value] = out
+        return rid.value
+
+    def result(self, rid: int):
+        return self._keep[rid]
+
+    def _info(self, info):
+        d = {k: getattr(info, k) for k, _ in info._fields_}
+        d["status"] = REQUEST_STATUS[d["status"]]
+        return d
+
+    def wait(self, rid: int, timeout: float = -1.0) -> dict:
+        info = prr_request_info()
+        check(self.lib.prr_server_wait(self.h, rid, timeout, C.byref(info)))
+        return self._info(info)
+
+    def poll(self, rid: int) -> dict:
+        info = prr_request_info()
+        check(self.lib.prr_server_poll(self.h, rid, C.byref(info)))
+        return self._info(info)
+
+    def cancel(self, rid: int):
+        check(self.lib.prr_server_cancel(self.h, rid))
+
+    def stats(self) -> dict:
+        st = prr_server_stats()
+        check(self.lib.prr_server_stats_get(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}

@@ -323,6 +323,10 @@ int grid_for(int64_t n, int block) {
 }
 
 int set_smem(const void *fn, size_t bytes) {
+    // The stack columns live in shared memory: ask for the largest carveout so
+    // the resident-block count the occupancy query reports is what launches.
+    cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     if (bytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int) bytes);

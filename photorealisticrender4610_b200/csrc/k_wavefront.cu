@@ -711,6 +711,10 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
         PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_extend, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     }
+    cudaFuncSetAttribute(k_wf_extend, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
+    cudaFuncSetAttribute(k_wf_shadow, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     const int refill = s.wf_refill > 0 ? std::min(s.wf_refill, 32) : 8;
     int occ_ext = 1, occ_sh = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_wf_extend, block, smem);

@@ -127,5 +127,6 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
                      unsigned long long *out_rays, cudaStream_t st);
 
 int device_sm_count();
+DevCamera make_camera(const prr_camera &c, int width, int height);
 
 } // namespace prr

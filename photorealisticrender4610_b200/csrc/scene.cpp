@@ -101,6 +101,44 @@ const Scene *S(const prr_scene *s) { return reinterpret_cast<const Scene *>(s); 
 
 } // namespace
 
+// Camera::init (Camera.hpp:43-56) and the focal length of generateRay (:76)
+// for an image of width x height, with the reference's float arithmetic.
+DevCamera make_camera(const prr_camera &c, int width, int height) {
+    auto normalize3 = [](float v[3]) {
+        const float m2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (m2 > 0) {
+            const float inv = 1 / sqrtf(m2);
+            v[0] = v[0] * inv;
+            v[1] = v[1] * inv;
+            v[2] = v[2] * inv;
+        }
+    };
+    float f[3] = {c.target[0] - c.eye[0], c.target[1] - c.eye[1], c.target[2] - c.eye[2]};
+    normalize3(f);
+    float r[3] = {f[1] * c.up[2] - f[2] * c.up[1], f[2] * c.up[0] - f[0] * c.up[2],
+                  f[0] * c.up[1] - f[1] * c.up[0]};
+    normalize3(r);
+    float u[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2], r[0] * f[1] - r[1] * f[0]};
+    DevCamera dc;
+    std::memcpy(dc.eye, c.eye, sizeof(dc.eye));
+    std::memcpy(dc.forward, f, sizeof(f));
+    std::memcpy(dc.right, r, sizeof(r));
+    std::memcpy(dc.up, u, sizeof(u));
+    const float half_fov_h = c.fovh * kPi / 180.0f * 0.5f;
+    dc.focal_px = ((float) width * 0.5f) / std::tan(half_fov_h);
+    dc.aperture = c.aperture;
+    float focus = c.focus_distance;
+    if (focus < 0.0f) {
+        const float dx = c.target[0] - c.eye[0], dy = c.target[1] - c.eye[1],
+                    dz = c.target[2] - c.eye[2];
+        focus = std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    dc.focus_distance = focus;
+    dc.width = width;
+    dc.height = height;
+    return dc;
+}
+
 int build_scene(Scene &s, cudaStream_t st) {
     // ---- per-mesh BVHs (independent; built concurrently) ----
     std::vector<int> meshes;
@@ -310,44 +348,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     D.blas_depth = blas_depth;
     std::memcpy(D.background, s.background, sizeof(D.background));
 
-    // ---- camera (Camera::init, Camera.hpp:43-56, and the focal length of
-    //      generateRay, :76) ----
-    if (s.camera_set) {
-        const prr_camera &c = s.camera;
-        auto normalize3 = [](float v[3]) {
-            const float m2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            if (m2 > 0) {
-                const float inv = 1 / sqrtf(m2);
-                v[0] = v[0] * inv;
-                v[1] = v[1] * inv;
-                v[2] = v[2] * inv;
-            }
-        };
-        float f[3] = {c.target[0] - c.eye[0], c.target[1] - c.eye[1], c.target[2] - c.eye[2]};
-        normalize3(f);
-        float r[3] = {f[1] * c.up[2] - f[2] * c.up[1], f[2] * c.up[0] - f[0] * c.up[2],
-                      f[0] * c.up[1] - f[1] * c.up[0]};
-        normalize3(r);
-        float u[3] = {r[1] * f[2] - r[2] * f[1], r[2] * f[0] - r[0] * f[2],
-                      r[0] * f[1] - r[1] * f[0]};
-        DevCamera &dc = D.camera;
-        std::memcpy(dc.eye, c.eye, sizeof(dc.eye));
-        std::memcpy(dc.forward, f, sizeof(f));
-        std::memcpy(dc.right, r, sizeof(r));
-        std::memcpy(dc.up, u, sizeof(u));
-        const float half_fov_h = c.fovh * kPi / 180.0f * 0.5f;
-        dc.focal_px = ((float) s.width * 0.5f) / std::tan(half_fov_h);
-        dc.aperture = c.aperture;
-        float focus = c.focus_distance;
-        if (focus < 0.0f) {
-            const float dx = c.target[0] - c.eye[0], dy = c.target[1] - c.eye[1],
-                        dz = c.target[2] - c.eye[2];
-            focus = std::sqrt(dx * dx + dy * dy + dz * dz);
-        }
-        dc.focus_distance = focus;
-        dc.width = s.width;
-        dc.height = s.height;
-    }
+    if (s.camera_set)
+        D.camera = make_camera(s.camera, s.width, s.height);
 
     // ---- environment map: pixels + CDF built on the device ----
     if (!s.env_rgb.empty()) {

@@ -1,0 +1,102 @@
+"""The render server: continuous batching over resident scenes. Each
+request's image is the same alone as in a mix (bit for bit), matches the
+plain renderer within float-summation tolerance, and admission respects the
+device budget; injected allocation failures, cancellations and timeouts are
+made on the host and leave the server serving."""
+import numpy as np
+import pytest
+import torch
+
+import photorealisticrender4610_b200 as prr
+from photorealisticrender4610_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+JOBS = [  # (scene, spp, depth, seed, window)
+    (0, 16, 5, 1, None),
+    (1, 32, 8, 2, None),
+    (2, 8, 6, 3, (8, 8, 40, 40)),
+    (1, 5, 8, 4, (0, 0, 48, 30)),
+    (0, 64, 5, 5, None),
+    (2, 12, 6, 6, None),
+]
+
+
+@pytest.fixture(scope="module")
+def scene_set(cuda):
+    descs = [scenes.cornell_box(64, 64), scenes.museum_like(96, 54, level=3, env_size=(256, 128)),
+             scenes.caustics(64, 64, level=2)]
+    return [prr.Scene.from_desc(d) for d in descs]
+
+
+def make_server(scene_set, **kw):
+    srv = prr.Server(samples_per_step=kw.pop("samples_per_step", 8192), **kw)
+    for s in scene_set:
+        srv.add_scene(s)
+    return srv
+
+
+def test_same_alone_and_in_mix(scene_set):
+    alone = []
+    for sc, spp, depth, seed, win in JOBS:
+        srv = make_server(scene_set)
+        rid = srv.submit(sc, spp, depth, seed=seed, window=win)
+        info = srv.wait(rid)
+        assert info["status"] == "done"
+        alone.append(srv.result(rid).copy())
+        srv.close()
+    srv = make_server(scene_set)
+    rids = []
+    for k, (sc, spp, depth, seed, win) in enumerate(JOBS):
+        if k % 2 == 0:  # half of them into device memory
+            W, H = scene_set[sc].desc.width, scene_set[sc].desc.height
+            x0, y0, x1, y1 = win or (0, 0, W, H)
+            out = torch.empty((y1 - y0, x1 - x0, 3), dtype=torch.float32, device="cuda")
+            rids.append(srv.submit(sc, spp, depth, seed=seed, window=win, out=out))
+        else:
+            rids.append(srv.submit(sc, spp, depth, seed=seed, window=win))
+    infos = [srv.wait(r) for r in rids]
+    assert all(i["status"] == "done" for i in infos)
+    # requests overlapped on the device
+    assert max(i["admit_s"] for i in infos) < min(i["done_s"] for i in infos)
+    for k, rid in enumerate(rids):
+        got = srv.result(rid)
+        got = got.cpu().numpy() if hasattr(got, "cpu") else got
+        assert np.array_equal(got.view(np.uint32), alone[k].view(np.uint32)), k
+    st = srv.stats()
+    assert st["completed"] == len(JOBS) and st["failed"] == 0 and st["steps"] > 0
+    srv.close()
+    # and each equals the plain renderer up to how the sample sums are grouped
+    for k, (sc, spp, depth, seed, win) in enumerate(JOBS):
+        ref, _ = scene_set[sc].render(spp, depth, seed=seed, window=win, slices=1)
+        assert np.allclose(alone[k], ref.cpu().numpy(), rtol=1e-5, atol=1e-6), k
+
+
+def test_budget_faults_cancel_timeout(scene_set):
+    scene_bytes = sum(s.stats()["device_bytes"] for s in scene_set)
+    # room for one 64x64 request at a time (film + host staging = 24 bytes/pixel)
+    srv = make_server(scene_set, budget_bytes=scene_bytes + 64 * 64 * 24 + 100,
+                      fail_every_nth_admission=3)
+    rids = [srv.submit(0, 8, 5, seed=k) for k in range(6)]
+    infos = [srv.wait(r) for r in rids]
+    st = [i["status"] for i in infos]
+    assert st == ["done", "done", "failed", "done", "done", "failed"], st
+    assert infos[2]["error"] == -3  # PRR_ERR_OUT_OF_MEMORY, injected on the host
+    done = [i for i in infos if i["status"] == "done"]
+    for a, b in zip(done, done[1:]):  # the budget admits one at a time
+        assert b["admit_s"] >= a["done_s"]
+    with pytest.raises(prr.PrrError, match="BUDGET"):
+        srv.submit(1, 4, 8)  # 96x54 never fits
+    # cancel a queued request, time out on a long one
+    long_id = srv.submit(0, 4096, 5, seed=9)
+    queued = srv.submit(0, 8, 5, seed=10)
+    srv.cancel(queued)
+    assert srv.wait(queued)["status"] == "cancelled"
+    with pytest.raises(prr.PrrError, match="TIMEOUT"):
+        srv.wait(long_id, timeout=0.0)
+    srv.cancel(long_id)
+    assert srv.wait(long_id)["status"] == "cancelled"
+    ok = srv.submit(0, 8, 5, seed=0)
+    assert srv.wait(ok)["status"] == "done"
+    assert np.array_equal(srv.result(ok), srv.result(rids[0]))
+    srv.close()
