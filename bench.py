@@ -398,10 +398,13 @@ def run_render(args, rank, world, on):
     else:
         tuned = scene.autotune(4, depth)
 
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
     def timed(mode, steps):
         ms = []
         rays = None
         for _ in range(steps):
+            flush.zero_()
             torch.cuda._sleep(2_000_000)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
@@ -465,7 +468,7 @@ def run_render(args, rank, world, on):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": desc_text, "mode": "wavefront", "autotuned": tuned,
-                   "l2": "inputs (scene 2M tris + paths) exceed L2; not flushed"},
+                   "l2": "flushed (512 MB write) before every timed frame"},
         "plain_msamples_s": plain_value, "wavefront_vs_plain": value / plain_value,
         "plain_vs_wavefront_rel_mse": rel,
         "mrays_s": float(rays.sum()) / (wf_step * 1e-3) / 1e6,

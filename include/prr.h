@@ -321,6 +321,11 @@ int prr_autotune(prr_scene *scene, const prr_render_settings *settings,
 int prr_cast_samples(const prr_scene *scene, const int32_t *px, const int32_t *py,
                      const int32_t *sample, int64_t n, uint64_t seed, int max_depth,
                      float indirect_clamp, float *out_rgb, void *stream);
+/* Integrator::castRay (Integrator.cpp:104-263) for arbitrary rays (n x 3
+ * origins and directions): path k draws from stream (seed, k, 0). */
+int prr_cast_rays(const prr_scene *scene, const float *o, const float *d, int64_t n,
+                  uint64_t seed, int max_depth, float indirect_clamp, float *out_rgb,
+                  void *stream);
 /* Camera::generateRay (Camera.hpp:75-95) for given pixel offsets (pinhole). */
 int prr_camera_rays(const prr_scene *scene, const int32_t *px, const int32_t *py,
                     const float *xo, const float *yo, int64_t n, float *out_o, float *out_d,

@@ -1,0 +1,442 @@
+// prr_dropin.hpp -- C++ classes with the reference renderer's names and
+// method signatures, forwarding to libprr's C ABI (prr.h). A program written
+// against the reference's Scene / MeshTriangle / Sphere / Material / Camera /
+// Integrator / Renderer / tonemap switches by including this header instead
+// of the reference headers and linking libprr.so.
+//
+// Mirrored interfaces (reference file:line):
+//   Vector3f, Vector2f            Vector.hpp:12-97 (arithmetic subset)
+//   Ray(origin, direction)        Ray.hpp:8-28
+//   Material + Diffuse/Emissive/Mirror/GlassMaterial (public fields)
+//                                 Material.hpp:38-183
+//   Triangle(v0, v1, v2, m)       Triangle.hpp:27-32
+//   MeshTriangle(tris, bounds, m) Triangle.hpp:116-124
+//   Sphere(center, radius, m)     Sphere.hpp:14-16
+//   Camera::create / fromBlender / init
+//                                 Camera.hpp:23-56
+//   Scene::Add / buildBVH / intersect / intersectP, envMap, camera,
+//   backgroundColor               Scene.hpp:15-41
+//   Integrator(scene, maxDepth, rr), castRay
+//                                 Integrator.hpp:15-23
+//   RenderSettings, Renderer::Render
+//                                 Renderer.hpp:42-59
+//   tonemap::ToneMapper / apply   ToneMapping.hpp:32-37, :267-279
+//
+// The per-ray calls (Scene::intersect, Integrator::castRay) run a one-ray
+// batch and exist for compatibility; the batch entry points of prr.h are the
+// hot path. Renderer::Render renders on the GPU, keeps the linear framebuffer
+// (framebuffer()), and writes output.ppm / output_raw.ppm like the reference
+// (Renderer.cpp:165-192; PNG output is left to the caller).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "prr.h"
+
+namespace prr_detail {
+inline void check(int rc) {
+    if (rc < 0) {
+        char buf[512];
+        prr_last_error(buf, sizeof(buf));
+        throw std::runtime_error(std::string("libprr: ") + buf);
+    }
+}
+template <class T> struct DeviceArray {
+    T *p = nullptr;
+    size_t n = 0;
+    explicit DeviceArray(size_t count) : n(count) {
+        if (cudaMalloc(&p, sizeof(T) * (count ? count : 1)) != cudaSuccess)
+            throw std::runtime_error("cudaMalloc failed");
+    }
+    ~DeviceArray() { cudaFree(p); }
+    void put(const T *h) { cudaMemcpy(p, h, sizeof(T) * n, cudaMemcpyHostToDevice); }
+    void get(T *h) const { cudaMemcpy(h, p, sizeof(T) * n, cudaMemcpyDeviceToHost); }
+};
+} // namespace prr_detail
+
+struct Vector3f {
+    float x = 0, y = 0, z = 0;
+    Vector3f() = default;
+    Vector3f(float v) : x(v), y(v), z(v) {}
+    Vector3f(float a, float b, float c) : x(a), y(b), z(c) {}
+    Vector3f operator+(const Vector3f &v) const { return {x + v.x, y + v.y, z + v.z}; }
+    Vector3f operator-(const Vector3f &v) const { return {x - v.x, y - v.y, z - v.z}; }
+    Vector3f operator*(const Vector3f &v) const { return {x * v.x, y * v.y, z * v.z}; }
+    Vector3f operator*(float r) const { return {x * r, y * r, z * r}; }
+    Vector3f operator/(float r) const { return {x / r, y / r, z / r}; }
+    Vector3f operator-() const { return {-x, -y, -z}; }
+    float norm() const { return std::sqrt(x * x + y * y + z * z); }
+};
+inline Vector3f operator*(float r, const Vector3f &v) { return {v.x * r, v.y * r, v.z * r}; }
+
+struct Vector2f {
+    float x = 0, y = 0;
+};
+
+struct Ray {
+    Vector3f origin, direction;
+    Ray(const Vector3f &o, const Vector3f &d) : origin(o), direction(d) {}
+};
+
+struct Bounds3 {
+    Vector3f pMin, pMax;
+    Bounds3() = default;
+    Bounds3(const Vector3f &a, const Vector3f &b) : pMin(a), pMax(b) {}
+};
+
+class Material {
+  public:
+    Vector3f m_emission = Vector3f(0.0f);
+    Vector3f baseColor = Vector3f(0.8f, 0.8f, 0.8f);
+    float roughness = 0.5f;
+    float metallic = 0.0f;
+    float ior = 1.5f;
+    virtual ~Material() = default;
+    virtual int kind() const = 0;
+    virtual bool isDelta() const { return false; }
+    virtual bool isEmissive() const { return false; }
+};
+class DiffuseMaterial : public Material {
+  public:
+    int kind() const override { return PRR_MAT_DIFFUSE; }
+};
+class EmissiveMaterial : public Material {
+  public:
+    int kind() const override { return PRR_MAT_EMISSIVE; }
+    bool isEmissive() const override { return true; }
+};
+class MirrorMaterial : public Material {
+  public:
+    int kind() const override { return PRR_MAT_MIRROR; }
+    bool isDelta() const override { return true; }
+};
+class GlassMaterial : public Material {
+  public:
+    int kind() const override { return PRR_MAT_GLASS; }
+    bool isDelta() const override { return true; }
+};
+
+class Object {
+  public:
+    virtual ~Object() = default;
+    Material *m = nullptr;
+};
+
+class Triangle {
+  public:
+    Vector3f v0, v1, v2;
+    Material *m;
+    Triangle(Vector3f a, Vector3f b, Vector3f c, Material *mat = nullptr)
+        : v0(a), v1(b), v2(c), m(mat) {}
+};
+
+class MeshTriangle : public Object {
+  public:
+    std::vector<Triangle> triangles;
+    Bounds3 bounding_box;
+    MeshTriangle(std::vector<Triangle> tris, Bounds3 bounds, Material *mt)
+        : triangles(std::move(tris)), bounding_box(bounds) {
+        m = mt;
+    }
+};
+
+class Sphere : public Object {
+  public:
+    Vector3f center;
+    float radius;
+    Sphere(const Vector3f &c, const float &r, Material *mt) : center(c), radius(r) { m = mt; }
+};
+
+struct Camera {
+    Vector3f eye = Vector3f(0, 0, -1), target = Vector3f(0, 0, 0), up = Vector3f(0, 1, 0);
+    float fovv = 40.0f, fovh = 40.0f, aperture = 0.0f, focusDistance = -1.0f;
+    int width = 0, height = 0;
+    static Camera create(Vector3f eye_, Vector3f target_, Vector3f up_, float fovv_, float fovh_) {
+        Camera c;
+        c.eye = eye_;
+        c.target = target_;
+        c.up = up_;
+        c.fovv = fovv_;
+        c.fovh = fovh_;
+        return c;
+    }
+    static Camera fromBlender(Vector3f eye_, Vector3f target_, Vector3f up_, float fovh_,
+                              float fovv_, float focusDist_) { // Camera.hpp:31-41
+        Camera c;
+        c.eye = Vector3f(eye_.x, eye_.z, -eye_.y);
+        c.target = Vector3f(target_.x, target_.z, -target_.y);
+        Vector3f u(up_.x, up_.z, -up_.y);
+        const float m2 = u.x * u.x + u.y * u.y + u.z * u.z;
+        if (m2 > 0) {
+            const float inv = 1 / sqrtf(m2);
+            u = Vector3f(u.x * inv, u.y * inv, u.z * inv);
+        }
+        c.up = u;
+        c.fovv = fovv_;
+        c.fovh = fovh_;
+        c.focusDistance = focusDist_;
+        return c;
+    }
+    void init(int w, int h) {
+        width = w;
+        height = h;
+    }
+};
+
+struct EnvMap {
+    std::vector<float> rgb; // decoded pixels, row-major RGB
+    int width = 0, height = 0;
+    bool empty() const { return rgb.empty(); }
+    void set(const float *pixels, int w, int h) {
+        rgb.assign(pixels, pixels + (size_t) w * h * 3);
+        width = w;
+        height = h;
+    }
+};
+
+struct Intersection {
+    bool happened = false;
+    Vector3f coords, normal;
+    double tnear = std::numeric_limits<double>::max();
+    int object = -1;    // index in Scene::objects
+    int primitive = -1; // triangle index within the mesh
+};
+
+class Scene {
+  public:
+    Vector3f backgroundColor = Vector3f(0.235294f, 0.67451f, 0.843137f);
+    std::vector<Object *> objects;
+    EnvMap envMap;
+    Camera camera;
+
+    Scene() { prr_detail::check(prr_scene_create(&h_)); }
+    ~Scene() { prr_scene_destroy(h_); }
+    Scene(const Scene &) = delete;
+    Scene &operator=(const Scene &) = delete;
+
+    void Add(Object *object) { objects.push_back(object); }
+
+    // Scene::buildBVH (Scene.cpp:15-27): uploads everything and builds on the GPU.
+    void buildBVH() {
+        std::vector<Material *> mats;
+        auto mat_id = [&](Material *m) {
+            for (size_t k = 0; k < mats.size(); k++)
+                if (mats[k] == m)
+                    return (int) k;
+            const float p[9] = {m->baseColor.x, m->baseColor.y, m->baseColor.z, m->roughness,
+                                m->metallic,    m->ior,         m->m_emission.x, m->m_emission.y,
+                                m->m_emission.z};
+            int id = -1;
+            prr_detail::check(prr_scene_add_material(h_, m->kind(), p, &id));
+            mats.push_back(m);
+            return id;
+        };
+        for (Object *o : objects) {
+            const int mid = mat_id(o->m);
+            if (auto *mesh = dynamic_cast<MeshTriangle *>(o)) {
+                std::vector<float> v;
+                v.reserve(mesh->triangles.size() * 9);
+                for (const Triangle &t : mesh->triangles)
+                    for (const Vector3f &p : {t.v0, t.v1, t.v2}) {
+                        v.push_back(p.x);
+                        v.push_back(p.y);
+                        v.push_back(p.z);
+                    }
+                prr_detail::check(
+                    prr_scene_add_mesh(h_, v.data(), (int64_t) mesh->triangles.size(), mid, nullptr));
+            } else if (auto *s = dynamic_cast<Sphere *>(o)) {
+                const float c[3] = {s->center.x, s->center.y, s->center.z};
+                prr_detail::check(prr_scene_add_sphere(h_, c, s->radius, mid, nullptr));
+            } else {
+                throw std::runtime_error("unsupported object type");
+            }
+        }
+        const float bg[3] = {backgroundColor.x, backgroundColor.y, backgroundColor.z};
+        prr_detail::check(prr_scene_set_background(h_, bg));
+        if (!envMap.empty())
+            prr_detail::check(prr_scene_set_env(h_, envMap.rgb.data(), envMap.width, envMap.height));
+        prr_camera c{};
+        const Vector3f *vs[3] = {&camera.eye, &camera.target, &camera.up};
+        float *ds[3] = {c.eye, c.target, c.up};
+        for (int k = 0; k < 3; k++) {
+            ds[k][0] = vs[k]->x;
+            ds[k][1] = vs[k]->y;
+            ds[k][2] = vs[k]->z;
+        }
+        c.fovv = camera.fovv;
+        c.fovh = camera.fovh;
+        c.aperture = camera.aperture;
+        c.focus_distance = camera.focusDistance;
+        if (camera.width > 0)
+            prr_detail::check(prr_scene_set_camera(h_, &c, camera.width, camera.height));
+        prr_detail::check(prr_scene_build(h_, nullptr));
+    }
+
+    // Scene::intersect (one-ray batch)
+    Intersection intersect(const Ray &ray) const {
+        const float o[3] = {ray.origin.x, ray.origin.y, ray.origin.z};
+        const float d[3] = {ray.direction.x, ray.direction.y, ray.direction.z};
+        prr_detail::DeviceArray<float> dO(3), dD(3), dT(1), dG(6);
+        prr_detail::DeviceArray<int32_t> dObj(1), dPrim(1);
+        dO.put(o);
+        dD.put(d);
+        prr_detail::check(prr_scene_intersect(h_, dO.p, dD.p, 1, dObj.p, dPrim.p, dT.p, dG.p, nullptr));
+        int32_t obj, prim;
+        float t, g[6];
+        dObj.get(&obj);
+        dPrim.get(&prim);
+        dT.get(&t);
+        dG.get(g);
+        Intersection in;
+        in.happened = obj >= 0;
+        if (in.happened) {
+            in.object = obj;
+            in.primitive = prim;
+            in.tnear = t;
+            in.coords = Vector3f(g[0], g[1], g[2]);
+            in.normal = Vector3f(g[3], g[4], g[5]);
+        }
+        return in;
+    }
+
+    // Scene::intersectP (one-ray batch)
+    bool intersectP(const Ray &ray, float tMax = std::numeric_limits<float>::infinity()) const {
+        const float o[3] = {ray.origin.x, ray.origin.y, ray.origin.z};
+        const float d[3] = {ray.direction.x, ray.direction.y, ray.direction.z};
+        prr_detail::DeviceArray<float> dO(3), dD(3), dM(1);
+        prr_detail::DeviceArray<uint8_t> dH(1);
+        dO.put(o);
+        dD.put(d);
+        dM.put(&tMax);
+        prr_detail::check(prr_scene_occluded(h_, dO.p, dD.p, dM.p, 1, dH.p, nullptr));
+        uint8_t hit;
+        dH.get(&hit);
+        return hit != 0;
+    }
+
+    prr_scene *handle() const { return h_; }
+
+  private:
+    prr_scene *h_ = nullptr;
+};
+
+class Integrator {
+  public:
+    float directClamp = 0.f;
+    float indirectClamp = 10.0f;
+    Integrator(const Scene &scene_, int maxDepth_, float rrThreshold_)
+        : scene(scene_), maxDepth(maxDepth_), rrThreshold(rrThreshold_) {}
+
+    // Integrator::castRay (Integrator.cpp:104-263) for one ray; successive
+    // calls draw from streams (seed, 0, 0), (seed, 1, 0), ...
+    Vector3f castRay(const Ray &ray) const {
+        const float o[3] = {ray.origin.x, ray.origin.y, ray.origin.z};
+        const float d[3] = {ray.direction.x, ray.direction.y, ray.direction.z};
+        prr_detail::DeviceArray<float> dO(3), dD(3), out(3);
+        dO.put(o);
+        dD.put(d);
+        prr_detail::check(prr_cast_rays(scene.handle(), dO.p, dD.p, 1, seed_ + calls_++ * 0x9E3779B97F4A7C15ull,
+                                        maxDepth, indirectClamp, out.p, nullptr));
+        float r[3];
+        out.get(r);
+        return Vector3f(r[0], r[1], r[2]);
+    }
+
+    // castRay for camera sample `sample` of pixel (i, j): the path the
+    // renderer traces for it (the ray itself is generated from the scene's
+    // camera and the (seed, pixel, sample) stream).
+    Vector3f castSample(int i, int j, int sample, uint64_t seed = 1) const {
+        prr_detail::DeviceArray<int32_t> a(1), b(1), c(1);
+        prr_detail::DeviceArray<float> out(3);
+        a.put(&i);
+        b.put(&j);
+        c.put(&sample);
+        prr_detail::check(prr_cast_samples(scene.handle(), a.p, b.p, c.p, 1, seed, maxDepth,
+                                           indirectClamp, out.p, nullptr));
+        float r[3];
+        out.get(r);
+        return Vector3f(r[0], r[1], r[2]);
+    }
+    const Scene &scene;
+    int maxDepth;
+    float rrThreshold; // stored, unused: as in the reference (Integrator.cpp:250-256)
+
+  private:
+    uint64_t seed_ = 1;
+    mutable uint64_t calls_ = 0;
+};
+
+namespace tonemap {
+enum class ToneMapper { Raw = PRR_TONEMAP_RAW, Standard = PRR_TONEMAP_STANDARD,
+                        AgX = PRR_TONEMAP_AGX, PBRNeutral = PRR_TONEMAP_PBR_NEUTRAL,
+                        ACES = PRR_TONEMAP_ACES };
+} // namespace tonemap
+
+struct RenderSettings {
+    int width = 1280;
+    int height = 1720;
+    int minSPP = 64;
+    int maxSPP = 64;
+    float russianRoulette = 0.95f;
+    int maxDepth = 30;
+    float varianceThreshold = 0.05f;
+    float exposure = 0.18f;
+    tonemap::ToneMapper toneMapper = tonemap::ToneMapper::AgX;
+    // additions of this implementation
+    uint64_t seed = 1;
+    int mode = PRR_RENDER_WAVEFRONT;
+};
+
+class Renderer {
+  public:
+    // Renderer::Render (Renderer.cpp:24-212): render, tone map, write PPMs.
+    void Render(const Scene &scene, const Integrator &integrator, const RenderSettings &s) {
+        prr_render_settings rs{};
+        rs.width = s.width;
+        rs.height = s.height;
+        rs.min_spp = s.minSPP;
+        rs.max_spp = s.maxSPP;
+        rs.max_depth = integrator.maxDepth;
+        rs.variance_threshold = s.varianceThreshold;
+        rs.indirect_clamp = integrator.indirectClamp;
+        rs.mode = s.mode;
+        rs.seed = s.seed;
+        const size_t n = (size_t) s.width * s.height;
+        prr_detail::DeviceArray<float> rgb(n * 3);
+        prr_detail::DeviceArray<int32_t> spp(n);
+        prr_detail::check(prr_render(scene.handle(), &rs, rgb.p, spp.p, nullptr, nullptr));
+        framebuffer_.resize(n * 3);
+        rgb.get(framebuffer_.data());
+        sampleCount_.resize(n);
+        spp.get(sampleCount_.data());
+        write(rgb, s.exposure, (int) s.toneMapper, s.width, s.height, "output.ppm");
+        if (s.toneMapper != tonemap::ToneMapper::Raw)
+            write(rgb, s.exposure, PRR_TONEMAP_RAW, s.width, s.height, "output_raw.ppm");
+    }
+    const std::vector<float> &framebuffer() const { return framebuffer_; }
+    const std::vector<int32_t> &sampleCount() const { return sampleCount_; }
+
+  private:
+    static void write(const prr_detail::DeviceArray<float> &rgb, float exposure, int mapper, int w,
+                      int h, const char *name) {
+        const size_t n = (size_t) w * h;
+        prr_detail::DeviceArray<uint8_t> u8(n * 3);
+        prr_detail::check(prr_tonemap(mapper, exposure, rgb.p, (int64_t) n, nullptr, u8.p, nullptr));
+        std::vector<uint8_t> buf(n * 3);
+        u8.get(buf.data());
+        if (FILE *fp = std::fopen(name, "wb")) {
+            std::fprintf(fp, "P6\n%d %d\n255\n", w, h);
+            std::fwrite(buf.data(), 1, buf.size(), fp);
+            std::fclose(fp);
+        }
+    }
+    std::vector<float> framebuffer_;
+    std::vector<int32_t> sampleCount_;
+};

@@ -128,6 +128,8 @@ _SIGS = {
                                C.POINTER(prr_wavefront_config), _vp]),
     "prr_cast_samples": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, C.c_uint64, C.c_int, C.c_float,
                                    _vp, _vp]),
+    "prr_cast_rays": (C.c_int, [_vp, _vp, _vp, C.c_int64, C.c_uint64, C.c_int, C.c_float, _vp,
+                                _vp]),
     "prr_camera_rays": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, _vp, _vp, _vp]),
     "prr_scene_sample_light": (C.c_int, [_vp, C.c_uint64, C.c_int64, _vp, _vp, _vp, _vp]),
     "prr_env_eval": (C.c_int, [_vp, _vp, C.c_int64, _vp, _vp, _vp]),

@@ -36,6 +36,24 @@ __global__ void k_cast_samples(DevScene S, const int32_t *__restrict__ px,
     out[k * 3 + 2] = s.z;
 }
 
+__global__ void k_cast_rays(DevScene S, const float *__restrict__ O, const float *__restrict__ D,
+                            int64_t n, uint64_t seed, int max_depth, float clamp,
+                            float *__restrict__ out, int tlas_cap) {
+    extern __shared__ uint2 smem[];
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    Rng rng{path_state(seed, (uint32_t) k, 0u)};
+    const Ray3 ray{v3(O[k * 3], O[k * 3 + 1], O[k * 3 + 2]), v3(D[k * 3], D[k * 3 + 1], D[k * 3 + 2])};
+    PathCounters cnt{0, 0};
+    const V3 s = cast_ray(S, ray, max_depth, clamp, rng, tst, bst, cnt);
+    out[k * 3 + 0] = s.x;
+    out[k * 3 + 1] = s.y;
+    out[k * 3 + 2] = s.z;
+}
+
 __global__ void k_camera_rays(DevCamera cam, const int32_t *px, const int32_t *py, const float *xo,
                               const float *yo, int64_t n, float *o, float *d) {
     const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
@@ -136,6 +154,30 @@ int prr_cast_samples(const prr_scene *scene, const int32_t *px, const int32_t *p
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     k_cast_samples<<<blocks(n, block), block, smem, (cudaStream_t) stream>>>(
         s->dev, px, py, sample, n, seed, max_depth, indirect_clamp, out_rgb, tcap);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+int prr_cast_rays(const prr_scene *scene, const float *o, const float *d, int64_t n,
+                  uint64_t seed, int max_depth, float indirect_clamp, float *out_rgb,
+                  void *stream) {
+    const Scene *s = built(scene);
+    if (!s)
+        return PRR_ERR_INVALID_ARGUMENT;
+    if (n < 0 || (n > 0 && (!o || !d || !out_rgb)) || max_depth < 1)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (n == 0)
+        return PRR_OK;
+    const int block = 128;
+    const int tcap = s->dev.tlas_depth + 1, bcap = s->dev.blas_depth + 1;
+    const size_t smem = (size_t) (tcap + bcap) * block * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    if (smem > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_cast_rays, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) smem));
+    k_cast_rays<<<blocks(n, block), block, smem, (cudaStream_t) stream>>>(
+        s->dev, o, d, n, seed, max_depth, indirect_clamp, out_rgb, tcap);
     PRR_CUDA_TRY(cudaGetLastError());
     return PRR_OK;
 }
