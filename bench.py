@@ -165,8 +165,8 @@ def workload_arrays():
 
 
 def parse_launch(text):
-    """'block=128,persistent=1' (or 'paths=1048576,block=128' for the
-    wavefront) -> launch config dict."""
+    """'block=128,persistent=1' (or 'paths=1048576,block=128,stack=12,ordered=1'
+    for the wavefront) -> launch config dict."""
     out = {}
     for kv in filter(None, (text or "").split(",")):
         k, v = kv.split("=")
@@ -393,10 +393,13 @@ def run_render(args, rank, world, on):
     npix = desc.width * desc.height
     if args.launch:
         cfg = parse_launch(args.launch)
-        scene.set_wavefront(cfg.get("paths", 0), cfg.get("block_size", 0), True)
+        scene.set_wavefront(cfg.get("paths", 0), cfg.get("block_size", 0), True,
+                            cfg.get("stack", 0), cfg.get("ordered", 1))
         tuned = cfg
     else:
-        tuned = scene.autotune(4, depth)
+        # tune on a few samples per pixel, or on the whole frame when it is small
+        # enough that one pass could hold all of it
+        tuned = scene.autotune(spp if npix * spp <= 1 << 22 else 4, depth)
 
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
@@ -421,11 +424,13 @@ def run_render(args, rank, world, on):
         barrier(on)
         wf_ms, wf_img, wf_rays = timed("wavefront", args.steps)
         barrier(on)
+    wf_launches = scene.stats()["last_render_launches"] * args.steps
     if args.kernel_only:
         if rank == 0:
             print(json.dumps({"frame_ms": wf_ms, "msamples_s": npix * spp / np.mean(wf_ms) / 1e3,
                               "launch": tuned}))
         return 0
+    timed("plain", 1)
     pl_ms, pl_img, pl_rays = timed("plain", max(1, min(args.steps, 3)))
     wf_step = max_over_ranks(float(np.mean(wf_ms)), on)
     pl_step = max_over_ranks(float(np.mean(pl_ms)), on)
@@ -468,7 +473,9 @@ def run_render(args, rank, world, on):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": desc_text, "mode": "wavefront", "autotuned": tuned,
-                   "l2": "flushed (512 MB write) before every timed frame"},
+                   "l2": "flushed (512 MB write) before every timed frame",
+                   "frame_ms": [round(x, 3) for x in wf_ms],
+                   "plain_frame_ms": [round(x, 3) for x in pl_ms]},
         "plain_msamples_s": plain_value, "wavefront_vs_plain": value / plain_value,
         "plain_vs_wavefront_rel_mse": rel,
         "mrays_s": float(rays.sum()) / (wf_step * 1e-3) / 1e6,
@@ -478,7 +485,7 @@ def run_render(args, rank, world, on):
         "roofline": None,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": None,
+        "gpu_launches": wf_launches,
     }
     print(json.dumps(line), flush=True)
     return 0

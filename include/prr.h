@@ -100,6 +100,10 @@ typedef struct prr_wavefront_config {
     int64_t paths_per_pass; /* paths in flight per pass (0: about 2M) */
     int block_size;         /* threads per block of the traversal stages (0: 128) */
     int use_graphs;         /* 1: replay each pass from one captured CUDA graph */
+    int stack_smem;         /* mesh-BVH stack entries per thread kept in shared memory;
+                               deeper entries spill to a global buffer (0: the whole stack) */
+    int ordered;            /* 1: rebuild the stage queues in path order (stable partition,
+                               next rays grouped by direction octant); 0: append order */
 } prr_wavefront_config;
 
 typedef struct prr_scene_stats {
@@ -107,6 +111,7 @@ typedef struct prr_scene_stats {
     int32_t tlas_depth, blas_depth;
     int64_t device_bytes;
     float total_emit_area;
+    int64_t last_render_launches; /* kernels launched by the last prr_render on this scene */
 } prr_scene_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -310,8 +315,10 @@ int prr_render_noalloc(prr_scene *scene, const prr_render_settings *settings, fl
 int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config);
 /* The autotuner: times the wavefront renderer on `settings` (the window and
  * depth of the intended render, a few samples per pixel) over a grid of
- * paths-per-pass and block sizes, keeps the fastest on the scene for later
- * renders and writes it to out_best (optional). Synchronises `stream`. */
+ * paths-per-pass and block sizes with ordered queues, then, at the best of
+ * those, append-order queues and shallower shared-memory stacks; keeps the
+ * fastest on the scene for later renders and writes it to out_best
+ * (optional). Synchronises `stream`. */
 int prr_autotune(prr_scene *scene, const prr_render_settings *settings,
                  prr_wavefront_config *out_best, void *stream);
 

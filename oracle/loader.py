@@ -44,16 +44,26 @@ def build_port() -> Path:
 
 def build_reference(ref_root: str | None = None) -> bool:
     """Compile the reference sources in place into oracle/_ref/ (needs the
-    reference tree, which exists only on the build host)."""
+    reference tree, which exists only on the build host). The bridge library
+    also needs the package's libprr.so, so it is built only when that exists."""
     root = ref_root or os.environ.get("PRR_REFERENCE_ROOT", "/root/reference")
     if not Path(root, "BVH.cpp").exists():
         return False
-    subprocess.run(["make", "-s", "-j8", "-C", str(HERE), "ref", f"REF={root}"], check=True)
+    targets = ["ref"]
+    if (HERE.parent / "photorealisticrender4610_b200" / "libprr.so").exists():
+        targets.append("bridge")
+    subprocess.run(["make", "-s", "-j8", "-C", str(HERE), *targets, f"REF={root}"], check=True)
     return True
 
 
-def reference_available(fast: bool = False) -> bool:
-    return (REF_DIR / ("libprr_ref_fast.so" if fast else "libprr_ref.so")).exists()
+def _ref_lib(fast: bool = False, bridge: bool = False) -> Path:
+    if bridge:
+        return REF_DIR / "libprr_ref_bridge.so"
+    return REF_DIR / ("libprr_ref_fast.so" if fast else "libprr_ref.so")
+
+
+def reference_available(fast: bool = False, bridge: bool = False) -> bool:
+    return _ref_lib(fast, bridge).exists()
 
 
 class PortOracle:
@@ -169,10 +179,13 @@ class PortMesh:
 
 
 class ReferenceOracle:
-    """The reference's own code (oracle/_ref/libprr_ref*.so via harness.cpp)."""
+    """The reference's own code (oracle/_ref/libprr_ref*.so via harness.cpp).
+    bridge=True loads the parity build that also carries the prr_bridge.hpp
+    test entry point (RefScene.bridge_render)."""
 
-    def __init__(self, fast: bool = False):
-        path = REF_DIR / ("libprr_ref_fast.so" if fast else "libprr_ref.so")
+    def __init__(self, fast: bool = False, bridge: bool = False):
+        path = _ref_lib(fast, bridge)
+        self.bridge = bridge
         if not path.exists():
             raise FileNotFoundError(f"{path} not built (oracle/Makefile ref)")
         L = C.CDLL(str(path))
@@ -228,6 +241,11 @@ class ReferenceOracle:
         L.prr_ref_photon_export.restype = C.c_int64
         L.prr_ref_photon_export.argtypes = [vp, vp, vp]
         L.prr_ref_photon_free.argtypes = [vp]
+        if bridge:
+            L.prr_ref_bridge_render.restype = C.c_int
+            L.prr_ref_bridge_render.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_float,
+                                                C.c_uint64, C.c_int, C.c_int, C.c_float, _f32p,
+                                                _i32p, _u8p, vp]
         L.prr_ref_photon_estimate.argtypes = [_f32p, C.c_int64, C.c_float, _f32p, C.c_int64,
                                               _f32p, C.POINTER(C.c_int32), C.c_int]
         self.L = L
@@ -354,6 +372,30 @@ class RefScene:
         if getattr(self, "h", None):
             self.ref.L.prr_ref_scene_free(self.h)
             self.h = None
+
+    def bridge_render(self, max_depth, min_spp, max_spp, threshold=0.05, seed=1, mode=1,
+                      mapper=2, exposure=0.18):
+        """This reference scene rendered by libprr through include/prr_bridge.hpp
+        (needs ReferenceOracle(bridge=True) and a GPU). Returns (linear rgb,
+        spp, 8-bit rgb, report dict)."""
+        if not self.ref.bridge:
+            raise RuntimeError("load ReferenceOracle(bridge=True) for the bridge entry point")
+        W, H = self.desc.width, self.desc.height
+        n = W * H
+        rgb = np.empty(n * 3, np.float32)
+        spp = np.empty(n, np.int32)
+        u8 = np.empty(n * 3, np.uint8)
+        rep = np.zeros(7, np.int64)
+        rc = self.ref.L.prr_ref_bridge_render(self.h, max_depth, min_spp, max_spp, threshold,
+                                              seed, mode, mapper, exposure, rgb, spp, u8,
+                                              rep.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("prr_ref_bridge_render failed (see stderr)")
+        keys = ("meshes", "spheres", "triangles", "materials", "textured_materials",
+                "smooth_normal_triangles", "skipped_objects")
+        shape = (H, W, 3)
+        return (rgb.reshape(shape), spp.reshape(H, W), u8.reshape(shape),
+                dict(zip(keys, rep.tolist())))
 
     def env_export(self):
         e = self.desc.env

@@ -408,6 +408,15 @@ void prr_ref_scene_build(void *h) {
     rs->scene.buildBVH();
 }
 
+// The reference Scene object itself, for code that consumes reference scenes
+// (the libprr bridge test in bridge.cpp).
+void *prr_ref_scene_object(void *h, int *width, int *height) {
+    RefScene *rs = (RefScene *) h;
+    *width = rs->width;
+    *height = rs->height;
+    return &rs->scene;
+}
+
 int64_t prr_ref_scene_tlas_nodes(void *h, float *bounds, uint32_t *first_child, uint32_t *meta,
                                  float *areas, int32_t *ordered) {
     RefScene *rs = (RefScene *) h;

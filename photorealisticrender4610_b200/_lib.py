@@ -39,7 +39,8 @@ class prr_trace_config(C.Structure):
 
 
 class prr_wavefront_config(C.Structure):
-    _fields_ = [("paths_per_pass", C.c_int64), ("block_size", C.c_int), ("use_graphs", C.c_int)]
+    _fields_ = [("paths_per_pass", C.c_int64), ("block_size", C.c_int), ("use_graphs", C.c_int),
+                ("stack_smem", C.c_int), ("ordered", C.c_int)]
 
 
 class prr_server_config(C.Structure):
@@ -63,7 +64,8 @@ class prr_server_stats(C.Structure):
 class prr_scene_stats(C.Structure):
     _fields_ = [("n_objects", C.c_int64), ("n_triangles", C.c_int64), ("n_nodes", C.c_int64),
                 ("tlas_depth", C.c_int32), ("blas_depth", C.c_int32),
-                ("device_bytes", C.c_int64), ("total_emit_area", C.c_float)]
+                ("device_bytes", C.c_int64), ("total_emit_area", C.c_float),
+                ("last_render_launches", C.c_int64)]
 
 
 class prr_render_settings(C.Structure):

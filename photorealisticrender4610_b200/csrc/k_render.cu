@@ -228,6 +228,7 @@ int render_plain(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_
     if (adaptive && out_spp)
         PRR_CUDA_TRY(cudaMemcpyAsync(out_spp, a.spp_out, (size_t) npix * sizeof(int32_t),
                                      cudaMemcpyDeviceToDevice, st));
+    s.last_launches = 2;
     return PRR_OK;
 }
 

@@ -43,7 +43,9 @@ struct Wf {
     int max_depth;
     float clamp;
     uint64_t seed;
-    int tlas_cap, blas_cap;
+    int tlas_cap, blas_cap; // stack entries a walk may need (tree depth + 1)
+    int blas_sm;            // mesh-stack entries kept in shared memory
+    void *spill;            // global part of the mesh stacks ([entry][grid thread])
     // path state
     uint64_t *rng;
     float4 *ro, *rd;     // current ray
@@ -63,7 +65,16 @@ struct Wf {
     unsigned *cnt;       // kCntSlots counters (64-bit ray totals at kCntRays, kCntShadowRays)
     int *pass_base;      // first sample of the current pass (advanced by the film kernel)
     int sample_offset;
+    // ordered queues: stages tag paths instead of appending them, and a stable
+    // partition builds the next queues in path (= pixel) order
+    int ordered;
+    uint8_t *tag;        // per path: bucket of the pending partition, 0xFF none
+    unsigned *tile;      // per partition tile: 8 bucket counts, then offsets
 };
+
+__device__ __forceinline__ uint8_t dir_octant(V3 d) {
+    return (uint8_t) ((d.x < 0.f) | ((d.y < 0.f) << 1) | ((d.z < 0.f) << 2));
+}
 
 __device__ __forceinline__ int warp_append(unsigned *counter, bool pred) {
     const unsigned active = __activemask();
@@ -114,6 +125,7 @@ __global__ void k_wf_generate(DevScene S, Wf w) {
         w.bounce[p] = 0;
         w.flags[p] = 0;
         w.qray[0][p] = p;
+        w.tag[p] = 0xFF;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.cnt[kCntRay0] = (unsigned) w.P;
@@ -138,11 +150,20 @@ __global__ void k_wf_begin(Wf w, int it) {
 // ---- extend: closest hit of the queued rays, then sort by material class.
 // Persistent: a lane whose ray is finished takes the next queued ray once
 // `refill` lanes of its warp are idle (one atomic per refill).
-__global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
+// The scene-level stack of this thread (all in shared memory) and its mesh-level
+// stack (blas_sm entries in shared memory, the rest in the spill buffer).
+template <class E>
+__device__ __forceinline__ void make_stacks(const Wf &w, E *smem, StackCol<E> &tc,
+                                            StackCol<E> &bc) {
+    tc = StackCol<E>{smem + threadIdx.x, nullptr, w.tlas_cap};
+    bc = StackCol<E>{smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x, (E *) w.spill,
+                     w.blas_sm};
+}
+
+__device__ __forceinline__ void wf_extend(const DevScene &S, const Wf &w, int it, int refill) {
     extern __shared__ uint2 smem[];
-    uint2 *tcol = smem + threadIdx.x;
-    uint2 *bcol = smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x;
-    const int stride = blockDim.x;
+    StackCol<uint2> tc, bc;
+    make_stacks(w, smem, tc, bc);
     const int *qin = w.qray[it & 1];
     const int n = (int) w.cnt[kCntRay0 + (it & 1)];
     const unsigned full = 0xffffffffu;
@@ -176,7 +197,7 @@ __global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
         }
         bool done = false;
         if (p >= 0)
-            done = S.n_objects == 0 || cw.step(S, tcol, bcol, stride);
+            done = S.n_objects == 0 || cw.step(S, tc, bc);
         int cls = -1;
         if (done) {
             w.hit[p] = make_int4(cw.hit_obj, cw.hit_tri, __float_as_int(cw.closest), 0);
@@ -187,15 +208,20 @@ __global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
                 cls = (kind == kMatMirror || kind == kMatGlass) ? 1 : 2;
             }
         }
-        const int a = warp_append(w.cnt + kCntMiss, cls == 0);
-        const int b = warp_append(w.cnt + kCntDelta, cls == 1);
-        const int c = warp_append(w.cnt + kCntSurf, cls == 2);
-        if (cls == 0)
-            w.qmiss[a] = p;
-        else if (cls == 1)
-            w.qdelta[b] = p;
-        else if (cls == 2)
-            w.qsurf[c] = p;
+        if (w.ordered) {
+            if (cls >= 0)
+                w.tag[p] = (uint8_t) cls;
+        } else {
+            const int a = warp_append(w.cnt + kCntMiss, cls == 0);
+            const int b = warp_append(w.cnt + kCntDelta, cls == 1);
+            const int c = warp_append(w.cnt + kCntSurf, cls == 2);
+            if (cls == 0)
+                w.qmiss[a] = p;
+            else if (cls == 1)
+                w.qdelta[b] = p;
+            else if (cls == 2)
+                w.qsurf[c] = p;
+        }
         if (done)
             p = -1;
     }
@@ -368,9 +394,14 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
                 }
             }
         }
-        const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
-        if (cont)
-            qout[slot] = p;
+        if (w.ordered) {
+            if (cont)
+                w.tag[p] = dir_octant(ld3(w.rd, p));
+        } else {
+            const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
+            if (cont)
+                qout[slot] = p;
+        }
     }
 }
 
@@ -485,9 +516,14 @@ __global__ void k_wf_surface(DevScene S, Wf w, int it_next) {
                 w.rng[p] = rng.s;
             }
         }
-        const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
-        if (cont)
-            qout[slot] = p;
+        if (w.ordered) {
+            if (cont)
+                w.tag[p] = dir_octant(ld3(w.rd, p));
+        } else {
+            const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
+            if (cont)
+                qout[slot] = p;
+        }
         const int sslot = warp_append(w.cnt + kCntShadow, shadow);
         if (shadow)
             w.qshadow[sslot] = p;
@@ -503,11 +539,10 @@ __global__ void k_wf_surface(DevScene S, Wf w, int it_next) {
 }
 
 // ---- shadow: visibility of every queued NEE ray (persistent, per-lane refill)
-__global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
-    extern __shared__ uint2 smem[];
-    uint2 *tcol = smem + threadIdx.x;
-    uint2 *bcol = smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x;
-    const int stride = blockDim.x;
+__device__ __forceinline__ void wf_shadow(const DevScene &S, const Wf &w, int refill) {
+    extern __shared__ uint32_t smem32[];
+    StackCol<uint32_t> tc, bc;
+    make_stacks(w, smem32, tc, bc);
     const int n = (int) w.cnt[kCntShadowJobs];
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -543,7 +578,7 @@ __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
                 }
             }
         }
-        if (job >= 0 && aw.step(S, tcol, bcol, stride)) {
+        if (job >= 0 && aw.step(S, tc, bc)) {
             w.vis[job] = aw.occluded ? 0 : 1;
             job = -1;
         }
@@ -553,6 +588,13 @@ __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
     if (lane == 0 && rays)
         atomicAdd(reinterpret_cast<unsigned long long *>(w.cnt + kCntShadowRays),
                   (unsigned long long) rays);
+}
+
+__global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
+    wf_extend(S, w, it, refill);
+}
+__global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
+    wf_shadow(S, w, refill);
 }
 
 // ---- add the visible NEE contributions, light first, then env, as castRay
@@ -578,6 +620,132 @@ __global__ void k_wf_shadow_resolve(Wf w) {
 }
 
 // ---- film: add the pass's samples per pixel in sample order
+// ---- ordered queues: a stable partition of the per-path tags into bucket
+// queues, in path order within each bucket. Tiles of kPartTile paths are
+// counted, the tile counts scanned per bucket, then each tile writes its paths
+// to their buckets (and clears their tags for the next partition).
+constexpr int kPartThreads = 256;
+constexpr int kPartTile = kPartThreads * 8;
+
+struct PartSpec {
+    int *q[8];          // bucket b's queue; concatenated: all in q[0], bucket order
+    int nb;             // buckets (<= 8)
+    int concat;
+    int count_slot[8];  // counter slot receiving bucket b's size (-1: none)
+    int total_slot;     // counter slot receiving the total (-1: none)
+};
+
+__global__ void __launch_bounds__(kPartThreads) k_part_count(Wf w, int nb) {
+    __shared__ unsigned c[8];
+    if (threadIdx.x < 8)
+        c[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    unsigned mine[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < kPartTile; i += kPartThreads) {
+        const int k = blockIdx.x * kPartTile + i;
+        const int t = k < w.P ? w.tag[k] : 0xFF;
+#pragma unroll
+        for (int b = 0; b < 8; b++)
+            if (b < nb)
+                mine[b] += __popc(__ballot_sync(0xffffffffu, t == b));
+    }
+    if (lane == 0)
+        for (int b = 0; b < nb; b++)
+            if (mine[b])
+                atomicAdd(&c[b], mine[b]);
+    __syncthreads();
+    if (threadIdx.x < 8)
+        w.tile[blockIdx.x * 8 + threadIdx.x] = c[threadIdx.x];
+}
+
+// One block of 1024: 128 threads per bucket, each scanning a run of tiles.
+__global__ void __launch_bounds__(1024) k_part_scan(Wf w, int ntiles, PartSpec ps) {
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned total[8];
+    const int b = threadIdx.x >> 7, j = threadIdx.x & 127, lane = threadIdx.x & 31;
+    const int per = (ntiles + 127) / 128;
+    const int t0 = j * per, t1 = min(ntiles, t0 + per);
+    unsigned sum = 0;
+    if (b < ps.nb)
+        for (int t = t0; t < t1; t++)
+            sum += w.tile[t * 8 + b];
+    // inclusive scan of the 128 run sums of this bucket
+    unsigned x = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        wsum[threadIdx.x >> 5] = x;
+    __syncthreads();
+    const int wb = b * 4; // this bucket's 4 warps
+    unsigned before = 0;
+    for (int k = wb; k < (threadIdx.x >> 5); k++)
+        before += wsum[k];
+    if (j == 127)
+        total[b] = before + x;
+    __syncthreads();
+    unsigned base = 0;
+    if (ps.concat)
+        for (int k = 0; k < b; k++)
+            base += total[k];
+    unsigned run = base + before + x - sum;
+    if (b < ps.nb)
+        for (int t = t0; t < t1; t++) {
+            const unsigned v = w.tile[t * 8 + b];
+            w.tile[t * 8 + b] = run;
+            run += v;
+        }
+    if (threadIdx.x < ps.nb && ps.count_slot[threadIdx.x] >= 0)
+        w.cnt[ps.count_slot[threadIdx.x]] = total[threadIdx.x];
+    if (threadIdx.x == 0 && ps.total_slot >= 0) {
+        unsigned all = 0;
+        for (int k = 0; k < ps.nb; k++)
+            all += total[k];
+        w.cnt[ps.total_slot] = all;
+    }
+}
+
+__global__ void __launch_bounds__(kPartThreads) k_part_scatter(Wf w, PartSpec ps) {
+    __shared__ unsigned run[8];
+    __shared__ unsigned wcnt[kPartThreads / 32][8];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < 8)
+        run[threadIdx.x] = threadIdx.x < ps.nb ? w.tile[blockIdx.x * 8 + threadIdx.x] : 0u;
+    for (int c = 0; c < kPartTile; c += kPartThreads) {
+        const int k = blockIdx.x * kPartTile + c + threadIdx.x;
+        const int t = k < w.P ? w.tag[k] : 0xFF;
+        int rank = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++) {
+            const unsigned m = __ballot_sync(0xffffffffu, t == b);
+            if (lane == 0)
+                wcnt[wid][b] = __popc(m);
+            if (t == b)
+                rank = __popc(m & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        if (t < ps.nb) {
+            unsigned off = run[t] + rank;
+            for (int v = 0; v < wid; v++)
+                off += wcnt[v][t];
+            int *q = ps.concat ? ps.q[0] : ps.q[t];
+            q[off] = k;
+            w.tag[k] = 0xFF;
+        }
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            unsigned add = 0;
+            for (int v = 0; v < kPartThreads / 32; v++)
+                add += wcnt[v][threadIdx.x];
+            run[threadIdx.x] += add;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_wf_film(Wf w) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q < w.npix) {
@@ -668,7 +836,9 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.spp_pass = spp_pass;
     w.P = spp_pass * w.npix;
     const size_t P = (size_t) w.P;
-    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) + (size_t) w.npix * 16 + 4096;
+    const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
+    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2 + 1) +
+                         (size_t) w.npix * 16 + (size_t) ntiles * 32 + 4096;
     PRR_CUDA_TRY(s.d_wavefront.ensure(bytes));
     char *cur = (char *) s.d_wavefront.ptr;
     w.rng = carve<uint64_t>(cur, P);
@@ -699,28 +869,53 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.film = carve<float3>(cur, (size_t) w.npix);
     w.cnt = carve<unsigned>(cur, kCntSlots);
     w.pass_base = carve<int>(cur, 4);
+    w.tag = carve<uint8_t>(cur, P);
+    w.tile = carve<unsigned>(cur, (size_t) ntiles * 8);
+    w.ordered = s.wf_ordered ? 1 : 0;
     if ((size_t) (cur - (char *) s.d_wavefront.ptr) > bytes)
         return fail(PRR_ERR_INTERNAL, "wavefront buffer layout overflow");
 
     const int sms = device_sm_count();
     const int block = s.wf_block > 0 ? s.wf_block : 128;
-    const size_t smem = (size_t) (w.tlas_cap + w.blas_cap) * block * sizeof(uint2);
-    if (smem > 200 * 1024)
-        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
-    if (smem > 48 * 1024) {
-        PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_extend, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        PRR_CUDA_TRY(cudaFuncSetAttribute(k_wf_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    }
-    cudaFuncSetAttribute(k_wf_extend, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
-    cudaFuncSetAttribute(k_wf_shadow, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         cudaSharedmemCarveoutMaxShared);
+    // Stacks: the scene-level one wholly in shared memory, the mesh one up to
+    // wf_stack entries (0: all of it) within 96 KB per block; its deeper
+    // entries go to the global spill buffer.
+    const int max_sm_entries = (96 * 1024) / (block * (int) sizeof(uint2));
+    if (w.tlas_cap + 1 > max_sm_entries)
+        return fail(PRR_ERR_UNSUPPORTED, "scene BVH too deep for the shared-memory stack");
+    w.blas_sm = s.wf_stack > 0 ? std::min(s.wf_stack, w.blas_cap) : w.blas_cap;
+    w.blas_sm = std::max(1, std::min(w.blas_sm, max_sm_entries - w.tlas_cap));
+    const size_t smem_ext = (size_t) (w.tlas_cap + w.blas_sm) * block * sizeof(uint2);
+    const size_t smem_sh = (size_t) (w.tlas_cap + w.blas_sm) * block * sizeof(uint32_t);
+    auto *k_ext = k_wf_extend;
+    auto *k_sh = k_wf_shadow;
+    if (smem_ext > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) k_ext,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_ext));
+    if (smem_sh > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) k_sh,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_sh));
+    // Deep stacks want the largest shared-memory split; shallow ones keep the
+    // default, since every change of split between consecutive kernels drains
+    // the SM (which dominates frames made of many short launches).
+    const int carve = smem_ext > 16 * 1024 ? (int) cudaSharedmemCarveoutMaxShared
+                                           : (int) cudaSharedmemCarveoutDefault;
+    cudaFuncSetAttribute((const void *) k_ext, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         carve);
+    cudaFuncSetAttribute((const void *) k_sh, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         carve);
     const int refill = s.wf_refill > 0 ? std::min(s.wf_refill, 32) : 8;
     int occ_ext = 1, occ_sh = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_wf_extend, block, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_wf_shadow, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, (const void *) k_ext, block, smem_ext);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, (const void *) k_sh, block, smem_sh);
     const int g_ext = sms * std::max(1, occ_ext);
     const int g_sh = sms * std::max(1, occ_sh);
+    const size_t spill_entries = (size_t) (w.blas_cap - w.blas_sm);
+    const size_t spill_bytes =
+        spill_entries * std::max((size_t) g_ext * block * sizeof(uint2),
+                                 (size_t) g_sh * block * sizeof(uint32_t));
+    PRR_CUDA_TRY(s.d_wf_spill.ensure(spill_bytes));
+    w.spill = s.d_wf_spill.ptr;
     const int g_shade = sms * 8;
     const int g_gen = (int) std::min<int64_t>((P + 255) / 256, (int64_t) sms * 16);
 
@@ -728,17 +923,49 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.pass_base, 0, sizeof(int), st));
 
+    // ordered queues: hit classes -> miss / delta / surface queues; next rays
+    // -> the ray queue, direction octant major
+    PartSpec part_cls{};
+    part_cls.q[0] = w.qmiss;
+    part_cls.q[1] = w.qdelta;
+    part_cls.q[2] = w.qsurf;
+    part_cls.nb = 3;
+    part_cls.concat = 0;
+    part_cls.count_slot[0] = kCntMiss;
+    part_cls.count_slot[1] = kCntDelta;
+    part_cls.count_slot[2] = kCntSurf;
+    part_cls.total_slot = -1;
+    PartSpec part_ray[2];
+    for (int r = 0; r < 2; r++) {
+        part_ray[r] = PartSpec{};
+        part_ray[r].q[0] = w.qray[r];
+        part_ray[r].nb = 8;
+        part_ray[r].concat = 1;
+        for (int b = 0; b < 8; b++)
+            part_ray[r].count_slot[b] = -1;
+        part_ray[r].total_slot = kCntRay0 + r;
+    }
+    auto partition = [&](const PartSpec &ps, cudaStream_t cs) {
+        k_part_count<<<ntiles, kPartThreads, 0, cs>>>(w, ps.nb);
+        k_part_scan<<<1, 1024, 0, cs>>>(w, ntiles, ps);
+        k_part_scatter<<<ntiles, kPartThreads, 0, cs>>>(w, ps);
+    };
+
     // capture one pass
     auto enqueue_pass = [&](cudaStream_t cs) -> int {
         k_wf_generate<<<g_gen, 256, 0, cs>>>(S, w);
         for (int it = 0; it <= w.max_depth; it++) {
             k_wf_begin<<<1, 32, 0, cs>>>(w, it);
-            k_wf_extend<<<g_ext, block, smem, cs>>>(S, w, it, refill);
+            k_ext<<<g_ext, block, smem_ext, cs>>>(S, w, it, refill);
+            if (w.ordered)
+                partition(part_cls, cs);
             k_wf_miss<<<g_shade, 128, 0, cs>>>(S, w);
             k_wf_delta<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
             k_wf_surface<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
-            k_wf_shadow<<<g_sh, block, smem, cs>>>(S, w, refill);
+            k_sh<<<g_sh, block, smem_sh, cs>>>(S, w, refill);
             k_wf_shadow_resolve<<<g_shade, 128, 0, cs>>>(w);
+            if (w.ordered)
+                partition(part_ray[(it + 1) & 1], cs);
         }
         k_wf_film<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
         PRR_CUDA_TRY(cudaGetLastError());
@@ -748,6 +975,8 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     uint64_t key = (uint64_t) (uintptr_t) s.d_wavefront.ptr;
     key = mix64(key ^ ((uint64_t) w.P << 20) ^ ((uint64_t) w.max_depth << 8) ^ (uint64_t) block ^
                 ((uint64_t) refill << 50));
+    key = mix64(key ^ (uint64_t) (uintptr_t) w.spill ^ ((uint64_t) w.blas_sm << 32) ^
+                ((uint64_t) w.ordered << 60));
     key = mix64(key ^ ((uint64_t) (uint32_t) w.x0 << 32 | (uint32_t) w.y0) ^
                 ((uint64_t) (uint32_t) w.ww << 16) ^ rs.seed ^ ((uint64_t) rs.sample_offset << 40) ^
                 (uint64_t) float_bits(w.clamp));
@@ -792,6 +1021,10 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
         k_wf_rays_out<<<1, 1, 0, st>>>(w.cnt, out_rays);
         PRR_CUDA_TRY(cudaGetLastError());
     }
+    // generate + per bounce (begin, extend, miss, delta, surface, shadow,
+    // shadow_resolve, and two 3-kernel partitions when ordered) + film
+    const int64_t per_pass = 2 + (int64_t) (w.max_depth + 1) * (7 + (w.ordered ? 6 : 0));
+    s.last_launches = per_pass * passes + 1 + (out_rays ? 1 : 0);
     return PRR_OK;
 }
 

@@ -100,6 +100,10 @@ struct Scene {
     int wf_block = 0;      // extend / shadow block size (0 = 128)
     int wf_refill = 0;     // idle lanes that trigger a refill (0 = 8)
     bool wf_graphs = true; // replay passes from a captured CUDA graph
+    int wf_stack = 0;      // mesh-stack entries per thread in shared memory (0 = whole stack)
+    bool wf_ordered = false; // queues rebuilt in path order by a stable partition
+    DevBuf d_wf_spill;     // global part of the traversal stacks
+    int64_t last_launches = 0; // kernels the last prr_render launched
     // Renders reuse the scratch above; each render waits for the previous
     // one's event before touching it, whatever stream either ran on.
     cudaEvent_t scratch_done = nullptr;

@@ -65,13 +65,15 @@ extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_con
     if (!scene || !config)
         return fail(PRR_ERR_INVALID_ARGUMENT, "scene and config are required");
     if (config->paths_per_pass < 0 || config->block_size < 0 || config->block_size % 32 != 0 ||
-        config->block_size > 512)
+        config->block_size > 512 || config->stack_smem < 0)
         return fail(PRR_ERR_INVALID_ARGUMENT, "bad wavefront config");
     Scene &s = *reinterpret_cast<Scene *>(scene);
     std::lock_guard<std::mutex> g(s.mu);
     s.wf_paths = config->paths_per_pass;
     s.wf_block = config->block_size;
     s.wf_graphs = config->use_graphs != 0;
+    s.wf_stack = config->stack_smem;
+    s.wf_ordered = config->ordered != 0;
     return PRR_OK;
 }
 
@@ -98,9 +100,34 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
                              int64_t(1) << 22};
     const int blocks[] = {64, 128, 256};
     float best_ms = 1e30f;
-    prr_wavefront_config best{0, 0, 1};
+    prr_wavefront_config best{0, 0, 1, 0, 1};
     int rc = PRR_OK;
     std::lock_guard<std::mutex> g(s.mu);
+    auto trial = [&](const prr_wavefront_config &c) {
+        s.wf_paths = c.paths_per_pass;
+        s.wf_block = c.block_size;
+        s.wf_graphs = true;
+        s.wf_stack = c.stack_smem;
+        s.wf_ordered = c.ordered != 0;
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 2 && rc == PRR_OK; rep++) {
+            cudaEventRecord(a, st);
+            rc = render_wavefront(s, rs, out.as<float>(), nullptr, nullptr, st);
+            cudaEventRecord(b, st);
+            if (cudaEventSynchronize(b) != cudaSuccess && rc == PRR_OK)
+                rc = fail(PRR_ERR_CUDA, "autotune render failed");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (rep > 0) // the first run captures the graph
+                ms_min = std::min(ms_min, ms);
+        }
+        if (rc == PRR_OK && ms_min < best_ms) {
+            best_ms = ms_min;
+            best = c;
+        }
+    };
+    // stage 1: paths per pass x block size, ordered queues, whole stacks in
+    // shared memory
     int64_t last = -1;
     for (int64_t cand : paths) {
         // a pass never holds more than the whole render
@@ -108,32 +135,19 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
         if (pp == last)
             continue;
         last = pp;
-        for (int bl : blocks) {
-            s.wf_paths = pp;
-            s.wf_block = bl;
-            s.wf_graphs = true;
-            float ms_min = 1e30f;
-            for (int rep = 0; rep < 2 && rc == PRR_OK; rep++) {
-                cudaEventRecord(a, st);
-                rc = render_wavefront(s, rs, out.as<float>(), nullptr, nullptr, st);
-                cudaEventRecord(b, st);
-                if (cudaEventSynchronize(b) != cudaSuccess && rc == PRR_OK)
-                    rc = fail(PRR_ERR_CUDA, "autotune render failed");
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, a, b);
-                if (rep > 0) // the first run captures the graph
-                    ms_min = std::min(ms_min, ms);
-            }
-            if (rc)
-                break;
-            if (ms_min < best_ms) {
-                best_ms = ms_min;
-                best = prr_wavefront_config{pp, bl, 1};
-            }
-        }
-        if (rc)
-            break;
+        for (int bl : blocks)
+            if (rc == PRR_OK)
+                trial(prr_wavefront_config{pp, bl, 1, 0, 1});
     }
+    // stage 2: at that shape, append-order queues, then shallower shared stacks
+    const prr_wavefront_config shape = best;
+    if (rc == PRR_OK)
+        trial(prr_wavefront_config{shape.paths_per_pass, shape.block_size, 1, 0, 0});
+    const prr_wavefront_config shape2 = best;
+    for (int sk : {16, 8})
+        if (rc == PRR_OK && sk < s.dev.blas_depth + 1)
+            trial(prr_wavefront_config{shape2.paths_per_pass, shape2.block_size, 1, sk,
+                                       shape2.ordered});
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (rc)
@@ -141,6 +155,8 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
     s.wf_paths = best.paths_per_pass;
     s.wf_block = best.block_size;
     s.wf_graphs = true;
+    s.wf_stack = best.stack_smem;
+    s.wf_ordered = best.ordered != 0;
     if (out_best)
         *out_best = best;
     return PRR_OK;

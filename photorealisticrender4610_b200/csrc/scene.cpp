@@ -549,6 +549,7 @@ int prr_scene_stats_get(const prr_scene *scene, prr_scene_stats *out) {
     out->blas_depth = s->dev.blas_depth;
     out->device_bytes = (int64_t) s->device_bytes;
     out->total_emit_area = s->dev.total_emit_area;
+    out->last_render_launches = s->last_launches;
     return PRR_OK;
 }
 

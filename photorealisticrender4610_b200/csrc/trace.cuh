@@ -148,6 +148,34 @@ __device__ __forceinline__ bool tri_occludes(const TriV &T, const RayD &r, float
            (t > 1e-3f && t < tmax);
 }
 
+// Per-thread stack with a bounded shared-memory part: entries [0, cap) in the
+// thread's shared-memory column (entry k at sm[k * blockDim.x]), deeper
+// entries in a global buffer laid out [entry - cap][grid thread], so a warp's
+// spills are coalesced. A walk pushes at most once per tree level, so tree
+// depth + 1 entries in the two parts together always suffice; the global part
+// is only reached deep in unbalanced subtrees and stays in L1/L2. Its address
+// is formed only on that cold path, so the stack costs two registers. `cap`
+// is a launch parameter: fewer shared entries leave more of the SM's L1 for
+// node and triangle fetches and let more blocks be resident.
+template <class E> struct StackCol {
+    E *sm;
+    E *gl;
+    int cap;
+    __device__ __forceinline__ E *spill_at(int k) const {
+        return gl + (size_t) (k - cap) * (gridDim.x * blockDim.x) + blockIdx.x * blockDim.x +
+               threadIdx.x;
+    }
+    __device__ __forceinline__ void put(int k, E v) const {
+        if (k < cap)
+            sm[k * blockDim.x] = v;
+        else
+            *spill_at(k) = v;
+    }
+    __device__ __forceinline__ E get(int k) const {
+        return k < cap ? sm[k * blockDim.x] : *spill_at(k);
+    }
+};
+
 // Per-thread stack column in shared memory.
 struct SmemStack {
     uint2 *base; // &smem[tid]; entry k at base[k * stride]

@@ -38,10 +38,10 @@ struct ClosestWalk {
     }
 
     // pops the scene-level stack; true when the walk is over
-    __device__ __forceinline__ bool scene_pop(uint2 *tcol, int stride) {
+    __device__ __forceinline__ bool scene_pop(const StackCol<uint2> &tc) {
         while (tsp > 0) {
             --tsp;
-            const uint2 e = tcol[tsp * stride];
+            const uint2 e = tc.get(tsp);
             if (__uint_as_float(e.y) < closest) {
                 tref = e.x;
                 return false;
@@ -60,7 +60,8 @@ struct ClosestWalk {
         }
     }
 
-    __device__ __forceinline__ bool step(const DevScene &S, uint2 *tcol, uint2 *bcol, int stride) {
+    __device__ __forceinline__ bool step(const DevScene &S, const StackCol<uint2> &tc,
+                                         const StackCol<uint2> &bc) {
         if (in_mesh) {
             bool pop = false;
             if (ntri > 0) {
@@ -80,14 +81,14 @@ struct ClosestWalk {
                 if (tl <= tr) {
                     if (tl < bbest) {
                         if (tr < bbest)
-                            bcol[(bsp++) * stride] = make_uint2(n.link.y, __float_as_uint(tr));
+                            bc.put(bsp++, make_uint2(n.link.y, __float_as_uint(tr)));
                         set_mesh_ref(n.link.x);
                         return false;
                     }
                 } else {
                     if (tr < bbest) {
                         if (tl < bbest)
-                            bcol[(bsp++) * stride] = make_uint2(n.link.x, __float_as_uint(tl));
+                            bc.put(bsp++, make_uint2(n.link.x, __float_as_uint(tl)));
                         set_mesh_ref(n.link.y);
                         return false;
                     }
@@ -98,7 +99,7 @@ struct ClosestWalk {
                 return false;
             while (bsp > 0) {
                 --bsp;
-                const uint2 e = bcol[bsp * stride];
+                const uint2 e = bc.get(bsp);
                 if (__uint_as_float(e.y) < bbest) {
                     set_mesh_ref(e.x);
                     return false;
@@ -111,7 +112,7 @@ struct ClosestWalk {
                 hit_tri = bhit;
             }
             in_mesh = false;
-            return scene_pop(tcol, stride);
+            return scene_pop(tc);
         }
         if (!(tref & kLeafBit)) {
             const NodeV n = load_node(S.nodes, tref);
@@ -120,19 +121,19 @@ struct ClosestWalk {
             if (tl <= tr) {
                 if (tl < closest) {
                     if (tr < closest)
-                        tcol[(tsp++) * stride] = make_uint2(n.link.y, __float_as_uint(tr));
+                        tc.put(tsp++, make_uint2(n.link.y, __float_as_uint(tr)));
                     tref = n.link.x;
                     return false;
                 }
             } else {
                 if (tr < closest) {
                     if (tl < closest)
-                        tcol[(tsp++) * stride] = make_uint2(n.link.x, __float_as_uint(tl));
+                        tc.put(tsp++, make_uint2(n.link.x, __float_as_uint(tl)));
                     tref = n.link.y;
                     return false;
                 }
             }
-            return scene_pop(tcol, stride);
+            return scene_pop(tc);
         }
         const int k = (int) (tref & ~kLeafBit);
         const DevObject &o = S.objects[k];
@@ -151,7 +152,7 @@ struct ClosestWalk {
             hit_obj = k;
             hit_tri = -1;
         }
-        return scene_pop(tcol, stride);
+        return scene_pop(tc);
     }
 };
 
@@ -191,16 +192,17 @@ struct AnyWalk {
         }
     }
 
-    __device__ __forceinline__ bool scene_pop(uint2 *tcol, int stride) {
+    __device__ __forceinline__ bool scene_pop(const StackCol<uint32_t> &tc) {
         if (tsp == 0)
             return true;
         --tsp;
-        tref = tcol[tsp * stride].x;
+        tref = tc.get(tsp);
         return false;
     }
 
     // one unit of work; true when the walk is over (result in `occluded`)
-    __device__ __forceinline__ bool step(const DevScene &S, uint2 *tcol, uint2 *bcol, int stride) {
+    __device__ __forceinline__ bool step(const DevScene &S, const StackCol<uint32_t> &tc,
+                                         const StackCol<uint32_t> &bc) {
         if (in_mesh) {
             if (ntri > 0) {
                 const TriV T = load_tri(S.tris, tri);
@@ -212,7 +214,7 @@ struct AnyWalk {
                         occluded = true;
                         return true;
                     }
-                    return scene_pop(tcol, stride);
+                    return scene_pop(tc);
                 }
                 tri++;
                 ntri--;
@@ -229,7 +231,7 @@ struct AnyWalk {
                 const float tnear = neg ? tr : tl;
                 const float tfar = neg ? tl : tr;
                 if (tfar < tmax)
-                    bcol[(bsp++) * stride] = make_uint2(far_ref, 0u);
+                    bc.put(bsp++, far_ref);
                 if (tnear < tmax) {
                     set_mesh_ref(near_ref);
                     return false;
@@ -237,11 +239,11 @@ struct AnyWalk {
             }
             if (bsp > 0) {
                 --bsp;
-                set_mesh_ref(bcol[bsp * stride].x);
+                set_mesh_ref(bc.get(bsp));
                 return false;
             }
             in_mesh = false;
-            return scene_pop(tcol, stride);
+            return scene_pop(tc);
         }
         if (!(tref & kLeafBit)) {
             const NodeV n = load_node(S.nodes, tref);
@@ -254,12 +256,12 @@ struct AnyWalk {
             const float tnear = neg ? tr : tl;
             const float tfar = neg ? tl : tr;
             if (tfar < tmax)
-                tcol[(tsp++) * stride] = make_uint2(far_ref, 0u);
+                tc.put(tsp++, far_ref);
             if (tnear < tmax) {
                 tref = near_ref;
                 return false;
             }
-            return scene_pop(tcol, stride);
+            return scene_pop(tc);
         }
         const DevObject &o = S.objects[tref & ~kLeafBit];
         if (o.kind == kObjMesh) {
@@ -270,14 +272,14 @@ struct AnyWalk {
                 set_mesh_ref(o.root);
                 return false;
             }
-            return scene_pop(tcol, stride);
+            return scene_pop(tc);
         }
         float t;
         if (sphere_hit(o, r, t) && t < tmax && t >= 0.f) {
             occluded = true;
             return true;
         }
-        return scene_pop(tcol, stride);
+        return scene_pop(tc);
     }
 };
 

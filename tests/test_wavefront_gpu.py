@@ -57,3 +57,47 @@ def test_autotune_picks_a_config(cuda):
     a, _ = s.render(8, 5, mode="wavefront")
     b, _ = s.render(8, 5, slices=1)
     assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+@pytest.mark.parametrize("stack,ordered", [(1, False), (3, True), (8, False), (12, True)])
+def test_wavefront_stack_spill(cuda, stack, ordered):
+    # mesh stacks mostly in the global spill buffer (stack=1) up to a few
+    # levels short of the tree depth: the same film as the plain renderer
+    desc = scenes.museum_like(80, 48, level=4, env_size=(256, 128))
+    s = prr.Scene.from_desc(desc)
+    assert s.stats()["blas_depth"] + 1 > 12
+    ref, _ = s.render(8, 8, seed=5, slices=1)
+    s.set_wavefront(paths_per_pass=80 * 48 * 4, block_size=128, stack_smem=stack, ordered=ordered)
+    out, _ = s.render(8, 8, seed=5, mode="wavefront")
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
+
+
+def test_autotune_tries_queue_order_and_stack_depth(cuda):
+    desc = scenes.museum_like(96, 64, level=3, env_size=(256, 128))
+    s = prr.Scene.from_desc(desc)
+    best = s.autotune(2, 8)
+    assert best["ordered"] in (0, 1) and best["stack_smem"] in (0, 16, 8)
+    a, _ = s.render(4, 8, mode="wavefront")
+    b, _ = s.render(4, 8, slices=1)
+    assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
+
+
+@pytest.mark.parametrize("name", ["cornell", "museum", "caustics"])
+def test_wavefront_ordered_queues_equal_plain(cuda, name):
+    # queues rebuilt in path order by the stable partition (ragged last tile,
+    # several passes): the same film, and the same ray counts as append order
+    if name == "cornell":
+        desc, depth = scenes.cornell_box(72, 40), 5
+    elif name == "museum":
+        desc, depth = scenes.museum_like(96, 54, level=3, env_size=(256, 128)), 8
+    else:
+        desc, depth = scenes.caustics(64, 48, level=2), 6
+    s = prr.Scene.from_desc(desc)
+    plain, _ = s.render(12, depth, seed=4, slices=1)
+    npix = desc.width * desc.height
+    s.set_wavefront(paths_per_pass=npix * 3, block_size=128, ordered=False)
+    _, _, r_app = s.render(12, depth, seed=4, mode="wavefront", count_rays=True)
+    s.set_wavefront(paths_per_pass=npix * 3, block_size=128, ordered=True)
+    wave, _, r_ord = s.render(12, depth, seed=4, mode="wavefront", count_rays=True)
+    assert np.array_equal(wave.cpu().numpy().view(np.uint32), plain.cpu().numpy().view(np.uint32))
+    assert np.array_equal(r_app.cpu().numpy(), r_ord.cpu().numpy())
