@@ -72,9 +72,12 @@ typedef struct prr_trace_config {
     int persistent;   /* 0: one ray per thread; 1: persistent grid, each warp
                          takes 32 rays at a time; 2: persistent grid, lanes whose
                          ray finished take new rays as soon as `batch` lanes of the
-                         warp are idle */
+                         warp are idle; 3: as 2, with postponed leaves (node and
+                         triangle steps in separate warp-wide phases) */
     int blocks_per_sm;/* persistent grids: resident blocks per SM (0 = occupancy) */
-    int batch;        /* mode 2 refill threshold in idle lanes (0 = 8) */
+    int batch;        /* modes 2-3: refill threshold in idle lanes (0 = 8) */
+    int leaf_batch;   /* mode 3: a triangle phase runs when this many lanes hold a
+                         parked leaf (0 = 16) */
 } prr_trace_config;
 
 #define PRR_RENDER_PLAIN 0     /* one megakernel thread per (pixel, sample range) */
@@ -171,9 +174,12 @@ int64_t prr_scene_export_nodes(const prr_scene *scene, int object, float *bounds
 int prr_mesh_intersect(const prr_scene *scene, int object, const float *o, const float *d,
                        int64_t n, int32_t *out_id, float *out_t, double *out_t64,
                        const prr_trace_config *cfg, void *stream);
-/* The same with host buffers: copies in, traces, copies out, synchronises. */
+/* The same with host buffers (pinned for the copies to overlap the traversal):
+ * copies in, traces, copies out in chunks over the library's own streams,
+ * ordered after `stream`; synchronises. cfg as for prr_mesh_intersect. */
 int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const float *d,
-                            int64_t n, int32_t *out_id, float *out_t, void *stream);
+                            int64_t n, int32_t *out_id, float *out_t,
+                            const prr_trace_config *cfg, void *stream);
 /* BVHAccel::IntersectP on one mesh (BVH.cpp:421-473, Triangle.hpp:75-92):
  * out_hit[i] = 1 if an occluder lies within tmax[i]. */
 int prr_mesh_occluded(const prr_scene *scene, int object, const float *o, const float *d,

@@ -35,7 +35,7 @@ class prr_camera(C.Structure):
 
 class prr_trace_config(C.Structure):
     _fields_ = [("block_size", C.c_int), ("persistent", C.c_int), ("blocks_per_sm", C.c_int),
-                ("batch", C.c_int)]
+                ("batch", C.c_int), ("leaf_batch", C.c_int)]
 
 
 class prr_wavefront_config(C.Structure):
@@ -100,7 +100,8 @@ _SIGS = {
     "prr_scene_export_nodes": (C.c_int64, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp]),
     "prr_mesh_intersect": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int64, _vp, _vp, _vp,
                                      C.POINTER(prr_trace_config), _vp]),
-    "prr_mesh_intersect_host": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int64, _vp, _vp, _vp]),
+    "prr_mesh_intersect_host": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int64, _vp, _vp, _vp,
+                                          _vp]),
     "prr_mesh_occluded": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),

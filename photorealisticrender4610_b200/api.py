@@ -37,6 +37,14 @@ def tonemap(rgb, mapper="agx", exposure: float = 1.0, stream=None):
     return out, u8
 
 
+def _trace_config(config: dict | None):
+    if not config:
+        return None
+    return prr_trace_config(config.get("block_size", 0), config.get("persistent", 0),
+                            config.get("blocks_per_sm", 0), config.get("batch", 0),
+                            config.get("leaf_batch", 0))
+
+
 def _ptr(t):
     return C.c_void_p(0 if t is None else t.data_ptr())
 
@@ -180,23 +188,26 @@ class Scene:
         tt = torch.empty(n, dtype=torch.float64, device=o.device) if t64 else None
         cfg = None
         if config:
-            cfg = prr_trace_config(config.get("block_size", 0), config.get("persistent", 0),
-                                   config.get("blocks_per_sm", 0), config.get("batch", 0))
+            cfg = _trace_config(config)
         check(self.lib.prr_mesh_intersect(self.h, obj, _ptr(o), _ptr(d), n, _ptr(hid), _ptr(t),
                                           _ptr(tt), C.byref(cfg) if cfg else None,
                                           _stream(stream)))
         return (hid, t, tt) if t64 else (hid, t)
 
-    def mesh_intersect_host(self, obj: int, o, d, out_id=None, out_t=None, stream=None):
+    def mesh_intersect_host(self, obj: int, o, d, out_id=None, out_t=None,
+                            config: dict | None = None, stream=None):
         o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
         d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
         n = len(o)
         hid = out_id if out_id is not None else np.empty(n, np.int32)
         t = out_t if out_t is not None else np.empty(n, np.float32)
+        cfg = _trace_config(config)
         check(self.lib.prr_mesh_intersect_host(self.h, obj, C.c_void_p(o.ctypes.data),
                                                C.c_void_p(d.ctypes.data), n,
                                                C.c_void_p(hid.ctypes.data),
-                                               C.c_void_p(t.ctypes.data), _stream(stream)))
+                                               C.c_void_p(t.ctypes.data),
+                                               C.byref(cfg) if cfg is not None else None,
+                                               _stream(stream)))
         return hid, t
 
     def mesh_occluded(self, obj: int, o, d, tmax, stream=None):

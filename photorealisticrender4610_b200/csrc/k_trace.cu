@@ -232,6 +232,143 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
     }
 }
 
+// Persistent closest hit with postponed leaves (phased): a lane that reaches a
+// leaf parks it and keeps walking interior nodes until it reaches a second
+// leaf; each warp step is then either a node step for every lane that can
+// walk or a triangle step for every lane holding a parked leaf (chosen when
+// at least `tri_min` lanes hold one), so the two kinds of work no longer
+// split a warp. Exactness: leaves are still taken in the reference's DFS
+// order, and a parked leaf is re-tested against the closest hit at the time
+// its triangles are tested (the box entry < closest test the reference makes
+// when it reaches that leaf); the interior nodes walked meanwhile with an
+// older closest hit only add leaves that this re-test then drops, since a
+// box contains the boxes below it and the slab entry distance is monotone in
+// the box.
+constexpr uint32_t kNoRef = 0xFFFFFFFFu;
+
+__global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
+    extern __shared__ uint2 smem[];
+    uint2 *col = smem + threadIdx.x;
+    const int stride = blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const unsigned full = 0xffffffffu;
+    int64_t idx = -1;
+    RayD r{};
+    RayPre p{};
+    float best = kInf;
+    int hit = -1;
+    uint32_t ref = kNoRef; // walk position: interior node, leaf waiting for the slot, or none
+    float ref_t = 0.f;     // box entry distance of ref
+    uint32_t ptri = 0;     // parked leaf: next triangle, triangles left, box entry
+    int pcnt = 0;
+    float pt = 0.f;
+    int sp = 0;
+    bool more = true; // warp-uniform: the ray counter is not exhausted
+    for (;;) {
+        const bool idle = idx < 0;
+        const unsigned im = __ballot_sync(full, idle);
+        if (!more && im == full)
+            break;
+        if (more && __popc(im) >= refill) {
+            const int cnt = __popc(im);
+            unsigned long long base = 0;
+            if (lane == 0)
+                base = atomicAdd(a.counter, (unsigned long long) cnt);
+            base = __shfl_sync(full, base, 0);
+            if ((int64_t) (base + cnt) >= a.n)
+                more = false;
+            if (idle) {
+                const int64_t ni = (int64_t) base + __popc(im & ((1u << lane) - 1u));
+                if (ni < a.n) {
+                    idx = ni;
+                    r = load_ray(a.O, a.D, ni);
+                    p = precompute(r);
+                    best = kInf;
+                    hit = -1;
+                    sp = 0;
+                    ref = a.root;
+                    ref_t = -kInf; // the root is entered without a box test
+                    pcnt = 0;
+                }
+            }
+        }
+        const bool act = idx >= 0;
+        const bool leaf_wait = ref != kNoRef && (ref & kLeafBit);
+        const bool tw = act && pcnt > 0;
+        const bool nw = act && !(leaf_wait && pcnt > 0) && !(ref == kNoRef && sp == 0);
+        const unsigned tm = __ballot_sync(full, tw);
+        const unsigned nm = __ballot_sync(full, nw);
+        if (tm != 0 && (nm == 0 || __popc(tm) >= tri_min)) {
+            if (tw) {
+                if (pt < best) {
+                    pt = -kInf; // the leaf passed; its other triangles follow unconditionally
+                    const TriV T = load_tri(a.tris, ptri);
+                    float t, u, v;
+                    if (tri_hit(T, r, t, u, v) && t < best) {
+                        best = t;
+                        hit = (int) ptri;
+                    }
+                    ptri++;
+                    pcnt--;
+                } else {
+                    pcnt = 0;
+                }
+            }
+        } else if (nw) {
+            if (ref != kNoRef && !(ref & kLeafBit)) {
+                const NodeV n = load_node(a.nodes, ref);
+                const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
+                const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
+                uint32_t next = kNoRef;
+                float next_t = 0.f;
+                if (tl <= tr) {
+                    if (tl < best) {
+                        if (tr < best) {
+                            col[sp * stride] = make_uint2(n.link.y, __float_as_uint(tr));
+                            sp++;
+                        }
+                        next = n.link.x;
+                        next_t = tl;
+                    }
+                } else {
+                    if (tr < best) {
+                        if (tl < best) {
+                            col[sp * stride] = make_uint2(n.link.x, __float_as_uint(tl));
+                            sp++;
+                        }
+                        next = n.link.y;
+                        next_t = tr;
+                    }
+                }
+                ref = next;
+                ref_t = next_t;
+            }
+            if (ref != kNoRef && (ref & kLeafBit) && pcnt == 0) {
+                ptri = leaf_first(ref);
+                pcnt = (int) leaf_count(ref);
+                pt = ref_t;
+                ref = kNoRef;
+            }
+            while (ref == kNoRef && sp > 0) {
+                --sp;
+                const uint2 e = col[sp * stride];
+                if (__uint_as_float(e.y) < best) {
+                    ref = e.x;
+                    ref_t = __uint_as_float(e.y);
+                }
+            }
+        }
+        if (act && ref == kNoRef && sp == 0 && pcnt == 0) {
+            a.out_id[idx] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+            a.out_t[idx] = best;
+            if (a.out_t64)
+                a.out_t64[idx] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r)
+                                          : __longlong_as_double(0x7ff8000000000000LL);
+            idx = -1;
+        }
+    }
+}
+
 __global__ void k_mesh_occluded(const WNode *nodes, const Tri *tris, uint32_t root,
                                 DevObject obj, const float *O, const float *D,
                                 const float *__restrict__ tmax, int64_t n, uint8_t *out) {
@@ -378,13 +515,14 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     if (smem > 227 * 1024)
         return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
     const int mode = cfg ? cfg->persistent : 0;
-    if (mode < 0 || mode > 2)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1 or 2");
+    if (mode < 0 || mode > 3)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1, 2 or 3");
     if (mode > 0) {
         if (!counter)
             return fail(PRR_ERR_INVALID_ARGUMENT, "persistent launch needs a counter");
-        const void *fn = mode == 1 ? (const void *) k_mesh_closest_persistent
-                                   : (const void *) k_mesh_closest_refill;
+        const void *fn = mode == 1   ? (const void *) k_mesh_closest_persistent
+                         : mode == 2 ? (const void *) k_mesh_closest_refill
+                                     : (const void *) k_mesh_closest_phased;
         if (int rc = set_smem(fn, smem))
             return rc;
         int bps = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 0;
@@ -395,9 +533,14 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
         PRR_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st));
         if (mode == 1) {
             k_mesh_closest_persistent<<<device_sm_count() * bps, block, smem, st>>>(a);
-        } else {
+        } else if (mode == 2) {
             const int refill = cfg->batch > 0 ? std::min(cfg->batch, 32) : 8;
             k_mesh_closest_refill<<<device_sm_count() * bps, block, smem, st>>>(a, refill);
+        } else {
+            const int refill = cfg->batch > 0 ? std::min(cfg->batch, 32) : 8;
+            const int tri_min = cfg->leaf_batch > 0 ? std::min(cfg->leaf_batch, 32) : 16;
+            k_mesh_closest_phased<<<device_sm_count() * bps, block, smem, st>>>(a, refill,
+                                                                              tri_min);
         }
     } else {
         if (int rc = set_smem((const void *) k_mesh_closest, smem))

@@ -621,11 +621,13 @@ __global__ void k_wf_shadow_resolve(Wf w) {
 
 // ---- film: add the pass's samples per pixel in sample order
 // ---- ordered queues: a stable partition of the per-path tags into bucket
-// queues, in path order within each bucket. Tiles of kPartTile paths are
-// counted, the tile counts scanned per bucket, then each tile writes its paths
-// to their buckets (and clears their tags for the next partition).
+// queues, in path order within each bucket. A tile is 4096 paths: 256
+// threads x 16 tags read as one 16-byte vector. Tiles are counted, the tile
+// counts scanned per bucket, then each tile writes its paths to their buckets
+// in order and clears their tags for the next partition. The tag array is
+// padded with 0xFF to whole tiles.
 constexpr int kPartThreads = 256;
-constexpr int kPartTile = kPartThreads * 8;
+constexpr int kPartTile = kPartThreads * 16;
 
 struct PartSpec {
     int *q[8];          // bucket b's queue; concatenated: all in q[0], bucket order
@@ -635,115 +637,166 @@ struct PartSpec {
     int total_slot;     // counter slot receiving the total (-1: none)
 };
 
+// How many of the 16 tag bytes in v equal b.
+__device__ __forceinline__ unsigned count_tag(const uint4 &v, unsigned b) {
+    const unsigned bb = b * 0x01010101u;
+    return (__popc(__vcmpeq4(v.x, bb)) + __popc(__vcmpeq4(v.y, bb)) +
+            __popc(__vcmpeq4(v.z, bb)) + __popc(__vcmpeq4(v.w, bb))) >> 3;
+}
+
 __global__ void __launch_bounds__(kPartThreads) k_part_count(Wf w, int nb) {
     __shared__ unsigned c[8];
     if (threadIdx.x < 8)
         c[threadIdx.x] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    unsigned mine[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < kPartTile; i += kPartThreads) {
-        const int k = blockIdx.x * kPartTile + i;
-        const int t = k < w.P ? w.tag[k] : 0xFF;
+    const uint4 v = reinterpret_cast<const uint4 *>(w.tag)[blockIdx.x * kPartThreads + threadIdx.x];
 #pragma unroll
-        for (int b = 0; b < 8; b++)
-            if (b < nb)
-                mine[b] += __popc(__ballot_sync(0xffffffffu, t == b));
-    }
-    if (lane == 0)
-        for (int b = 0; b < nb; b++)
-            if (mine[b])
-                atomicAdd(&c[b], mine[b]);
+    for (int b = 0; b < 8; b++)
+        if (b < nb) {
+            const unsigned r = __reduce_add_sync(0xffffffffu, count_tag(v, b));
+            if ((threadIdx.x & 31) == 0 && r)
+                atomicAdd(&c[b], r);
+        }
     __syncthreads();
     if (threadIdx.x < 8)
         w.tile[blockIdx.x * 8 + threadIdx.x] = c[threadIdx.x];
 }
 
-// One block of 1024: 128 threads per bucket, each scanning a run of tiles.
+// Exclusive scan over the tiles, all buckets at once: one block, one tile per
+// thread per round. Tile counts become the tiles' first output slots.
 __global__ void __launch_bounds__(1024) k_part_scan(Wf w, int ntiles, PartSpec ps) {
-    __shared__ unsigned wsum[32];
+    __shared__ unsigned wsum[32][8];
+    __shared__ unsigned carry[8];
     __shared__ unsigned total[8];
-    const int b = threadIdx.x >> 7, j = threadIdx.x & 127, lane = threadIdx.x & 31;
-    const int per = (ntiles + 127) / 128;
-    const int t0 = j * per, t1 = min(ntiles, t0 + per);
-    unsigned sum = 0;
-    if (b < ps.nb)
-        for (int t = t0; t < t1; t++)
-            sum += w.tile[t * 8 + b];
-    // inclusive scan of the 128 run sums of this bucket
-    unsigned x = sum;
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o)
-            x += y;
-    }
-    if (lane == 31)
-        wsum[threadIdx.x >> 5] = x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < 8)
+        carry[threadIdx.x] = 0;
     __syncthreads();
-    const int wb = b * 4; // this bucket's 4 warps
-    unsigned before = 0;
-    for (int k = wb; k < (threadIdx.x >> 5); k++)
-        before += wsum[k];
-    if (j == 127)
-        total[b] = before + x;
-    __syncthreads();
-    unsigned base = 0;
-    if (ps.concat)
-        for (int k = 0; k < b; k++)
-            base += total[k];
-    unsigned run = base + before + x - sum;
-    if (b < ps.nb)
-        for (int t = t0; t < t1; t++) {
-            const unsigned v = w.tile[t * 8 + b];
-            w.tile[t * 8 + b] = run;
-            run += v;
+    for (int r0 = 0; r0 < ntiles; r0 += 1024) {
+        const int t = r0 + threadIdx.x;
+        unsigned v[8];
+        if (t < ntiles) {
+            const uint4 a = reinterpret_cast<const uint4 *>(w.tile)[t * 2];
+            const uint4 b = reinterpret_cast<const uint4 *>(w.tile)[t * 2 + 1];
+            v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+            v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                v[k] = 0;
         }
-    if (threadIdx.x < ps.nb && ps.count_slot[threadIdx.x] >= 0)
-        w.cnt[ps.count_slot[threadIdx.x]] = total[threadIdx.x];
-    if (threadIdx.x == 0 && ps.total_slot >= 0) {
-        unsigned all = 0;
-        for (int k = 0; k < ps.nb; k++)
-            all += total[k];
-        w.cnt[ps.total_slot] = all;
+        unsigned x[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            x[k] = v[k];
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, x[k], o);
+                if (lane >= o)
+                    x[k] += y;
+            }
+            if (lane == 31)
+                wsum[wid][k] = x[k];
+        }
+        __syncthreads();
+        // warp 0 scans the 32 warp sums of each bucket
+        if (wid == 0) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const unsigned s0 = wsum[lane][k];
+                unsigned z = s0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned y = __shfl_up_sync(0xffffffffu, z, o);
+                    if (lane >= o)
+                        z += y;
+                }
+                wsum[lane][k] = z - s0; // exclusive
+                if (lane == 31) {
+                    // round total folded into the running carry after use
+                    total[k] = z;
+                }
+            }
+        }
+        __syncthreads();
+        if (t < ntiles) {
+            unsigned o[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                o[k] = carry[k] + wsum[wid][k] + x[k] - v[k];
+            reinterpret_cast<uint4 *>(w.tile)[t * 2] = make_uint4(o[0], o[1], o[2], o[3]);
+            reinterpret_cast<uint4 *>(w.tile)[t * 2 + 1] = make_uint4(o[4], o[5], o[6], o[7]);
+        }
+        __syncthreads();
+        if (threadIdx.x < 8)
+            carry[threadIdx.x] += total[threadIdx.x];
+        __syncthreads();
     }
+    // bucket bases (concatenated queues) and counts
+    if (threadIdx.x == 0) {
+        unsigned base = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (k < ps.nb) {
+                total[k] = base; // reuse: first slot of bucket k
+                if (ps.count_slot[k] >= 0)
+                    w.cnt[ps.count_slot[k]] = carry[k];
+                base += carry[k];
+            }
+        if (ps.total_slot >= 0)
+            w.cnt[ps.total_slot] = base;
+    }
+    __syncthreads();
+    if (ps.concat)
+        for (int i = threadIdx.x; i < ntiles * 8; i += 1024) {
+            const int k = i & 7;
+            if (k < ps.nb)
+                w.tile[i] += total[k];
+        }
 }
 
 __global__ void __launch_bounds__(kPartThreads) k_part_scatter(Wf w, PartSpec ps) {
-    __shared__ unsigned run[8];
-    __shared__ unsigned wcnt[kPartThreads / 32][8];
+    __shared__ unsigned wsum[kPartThreads / 32][8];
+    __shared__ unsigned base[8][kPartThreads];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (threadIdx.x < 8)
-        run[threadIdx.x] = threadIdx.x < ps.nb ? w.tile[blockIdx.x * 8 + threadIdx.x] : 0u;
-    for (int c = 0; c < kPartTile; c += kPartThreads) {
-        const int k = blockIdx.x * kPartTile + c + threadIdx.x;
-        const int t = k < w.P ? w.tag[k] : 0xFF;
-        int rank = 0;
+    uint4 *tv = reinterpret_cast<uint4 *>(w.tag) + blockIdx.x * kPartThreads + threadIdx.x;
+    const uint4 v = *tv;
+    unsigned c[8], x[8];
 #pragma unroll
-        for (int b = 0; b < 8; b++) {
-            const unsigned m = __ballot_sync(0xffffffffu, t == b);
-            if (lane == 0)
-                wcnt[wid][b] = __popc(m);
-            if (t == b)
-                rank = __popc(m & ((1u << lane) - 1u));
+    for (int k = 0; k < 8; k++) {
+        c[k] = k < ps.nb ? count_tag(v, k) : 0u;
+        x[k] = c[k];
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, x[k], o);
+            if (lane >= o)
+                x[k] += y;
         }
-        __syncthreads();
-        if (t < ps.nb) {
-            unsigned off = run[t] + rank;
-            for (int v = 0; v < wid; v++)
-                off += wcnt[v][t];
-            int *q = ps.concat ? ps.q[0] : ps.q[t];
-            q[off] = k;
-            w.tag[k] = 0xFF;
-        }
-        __syncthreads();
-        if (threadIdx.x < 8) {
-            unsigned add = 0;
-            for (int v = 0; v < kPartThreads / 32; v++)
-                add += wcnt[v][threadIdx.x];
-            run[threadIdx.x] += add;
-        }
-        __syncthreads();
+        if (lane == 31)
+            wsum[wid][k] = x[k];
     }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        unsigned before = 0;
+        for (int u = 0; u < wid; u++)
+            before += wsum[u][k];
+        base[k][threadIdx.x] = (k < ps.nb ? w.tile[blockIdx.x * 8 + k] : 0u) + before + x[k] - c[k];
+    }
+    const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+    const int first = (blockIdx.x * kPartThreads + threadIdx.x) * 16;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const unsigned t = (words[i >> 2] >> ((i & 3) * 8)) & 0xFFu;
+        if (t < (unsigned) ps.nb) {
+            int *q = ps.q[0];
+            if (!ps.concat) {
+#pragma unroll
+                for (int k = 1; k < 8; k++)
+                    if (t == (unsigned) k)
+                        q = ps.q[k];
+            }
+            q[base[t][threadIdx.x]++] = first + i;
+        }
+    }
+    *tv = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
 }
 
 __global__ void k_wf_film(Wf w) {
@@ -837,8 +890,9 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.P = spp_pass * w.npix;
     const size_t P = (size_t) w.P;
     const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
-    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2 + 1) +
-                         (size_t) w.npix * 16 + (size_t) ntiles * 32 + 4096;
+    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) +
+                         (size_t) ntiles * kPartTile + (size_t) w.npix * 16 +
+                         (size_t) ntiles * 32 + 4096;
     PRR_CUDA_TRY(s.d_wavefront.ensure(bytes));
     char *cur = (char *) s.d_wavefront.ptr;
     w.rng = carve<uint64_t>(cur, P);
@@ -869,7 +923,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.film = carve<float3>(cur, (size_t) w.npix);
     w.cnt = carve<unsigned>(cur, kCntSlots);
     w.pass_base = carve<int>(cur, 4);
-    w.tag = carve<uint8_t>(cur, P);
+    w.tag = carve<uint8_t>(cur, (size_t) ntiles * kPartTile);
     w.tile = carve<unsigned>(cur, (size_t) ntiles * 8);
     w.ordered = s.wf_ordered ? 1 : 0;
     if ((size_t) (cur - (char *) s.d_wavefront.ptr) > bytes)
@@ -920,6 +974,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     const int g_gen = (int) std::min<int64_t>((P + 255) / 256, (int64_t) sms * 16);
 
     PRR_CUDA_TRY(cudaMemsetAsync(w.film, 0, (size_t) w.npix * sizeof(float3), st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) ntiles * kPartTile, st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.pass_base, 0, sizeof(int), st));
 

@@ -107,9 +107,20 @@ struct Scene {
     // Renders reuse the scratch above; each render waits for the previous
     // one's event before touching it, whatever stream either ran on.
     cudaEvent_t scratch_done = nullptr;
+    // host-buffer pipeline of prr_mesh_intersect_host: streams and events
+    // created on first use
+    static constexpr int kHostBufs = 3;
+    cudaStream_t host_streams[kHostBufs] = {};
+    cudaEvent_t host_events[kHostBufs + 1] = {};
     ~Scene() {
         if (scratch_done)
             cudaEventDestroy(scratch_done);
+        for (cudaEvent_t e : host_events)
+            if (e)
+                cudaEventDestroy(e);
+        for (cudaStream_t h : host_streams)
+            if (h)
+                cudaStreamDestroy(h);
     }
 };
 

@@ -126,8 +126,9 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
             best = c;
         }
     };
-    // stage 1: paths per pass x block size, ordered queues, whole stacks in
-    // shared memory
+    // stage 1: paths per pass x block size, ordered queues, 8 shared stack
+    // entries (the rest of the L1 caches nodes and triangles)
+    const int stack1 = std::min(8, s.dev.blas_depth + 1);
     int64_t last = -1;
     for (int64_t cand : paths) {
         // a pass never holds more than the whole render
@@ -137,17 +138,18 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
         last = pp;
         for (int bl : blocks)
             if (rc == PRR_OK)
-                trial(prr_wavefront_config{pp, bl, 1, 0, 1});
+                trial(prr_wavefront_config{pp, bl, 1, stack1, 1});
     }
-    // stage 2: at that shape, append-order queues, then shallower shared stacks
+    // stage 2: at that shape, other shared stack depths (0: the whole stack)
     const prr_wavefront_config shape = best;
-    if (rc == PRR_OK)
-        trial(prr_wavefront_config{shape.paths_per_pass, shape.block_size, 1, 0, 0});
+    for (int sk : {0, 16, 4, 2})
+        if (rc == PRR_OK && sk < s.dev.blas_depth + 1 && sk != stack1)
+            trial(prr_wavefront_config{shape.paths_per_pass, shape.block_size, 1, sk, 1});
+    // stage 3: append-order queues
     const prr_wavefront_config shape2 = best;
-    for (int sk : {16, 8})
-        if (rc == PRR_OK && sk < s.dev.blas_depth + 1)
-            trial(prr_wavefront_config{shape2.paths_per_pass, shape2.block_size, 1, sk,
-                                       shape2.ordered});
+    if (rc == PRR_OK)
+        trial(prr_wavefront_config{shape2.paths_per_pass, shape2.block_size, 1,
+                                   shape2.stack_smem, 0});
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (rc)

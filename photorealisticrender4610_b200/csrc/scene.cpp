@@ -602,7 +602,8 @@ int prr_mesh_intersect(const prr_scene *scene, int object, const float *o, const
 }
 
 int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const float *d,
-                            int64_t n, int32_t *out_id, float *out_t, void *stream) {
+                            int64_t n, int32_t *out_id, float *out_t,
+                            const prr_trace_config *cfg, void *stream) {
     if (int rc = check_mesh(scene, object))
         return rc;
     if (n < 0 || (n > 0 && (!o || !d || !out_id || !out_t)))
@@ -612,21 +613,26 @@ int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const 
     Scene *s = S(scene);
     std::lock_guard<std::mutex> g(s->mu);
     cudaStream_t st = (cudaStream_t) stream;
-    // Chunked pipeline: copies of chunk k+1 overlap the trace of chunk k when
-    // the host buffers are pinned.
-    const int64_t chunk = std::min<int64_t>(n, 1 << 20);
-    const int nbuf = 2;
-    const size_t per = (size_t) chunk * (6 * sizeof(float) + sizeof(int32_t) + sizeof(float));
-    PRR_CUDA_TRY(s->d_scratch.ensure(per * nbuf));
-    cudaStream_t streams[nbuf];
-    cudaEvent_t start_ev, done[nbuf];
-    PRR_CUDA_TRY(cudaEventCreateWithFlags(&start_ev, cudaEventDisableTiming));
-    PRR_CUDA_TRY(cudaEventRecord(start_ev, st));
+    // Chunked pipeline over kHostBufs streams: the copies in of chunk k+1 and
+    // the copies out of chunk k-1 overlap the trace of chunk k (the host
+    // buffers must be pinned for the copies to be asynchronous). Each buffer
+    // has its own work counter, so persistent launch shapes are safe here.
+    constexpr int nbuf = Scene::kHostBufs;
+    const int64_t chunk = std::min<int64_t>(n, 1 << 19);
+    const size_t rays_b = (size_t) chunk * (6 * sizeof(float) + sizeof(int32_t) + sizeof(float));
+    const size_t per = (rays_b + 255) & ~size_t(255);
+    PRR_CUDA_TRY(s->d_scratch.ensure(per * nbuf + 256 * nbuf));
     for (int b = 0; b < nbuf; b++) {
-        PRR_CUDA_TRY(cudaStreamCreateWithFlags(&streams[b], cudaStreamNonBlocking));
-        PRR_CUDA_TRY(cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming));
-        PRR_CUDA_TRY(cudaStreamWaitEvent(streams[b], start_ev, 0));
+        if (!s->host_streams[b])
+            PRR_CUDA_TRY(cudaStreamCreateWithFlags(&s->host_streams[b], cudaStreamNonBlocking));
     }
+    for (cudaEvent_t &e : s->host_events)
+        if (!e)
+            PRR_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaEvent_t start_ev = s->host_events[nbuf];
+    PRR_CUDA_TRY(cudaEventRecord(start_ev, st));
+    for (int b = 0; b < nbuf; b++)
+        PRR_CUDA_TRY(cudaStreamWaitEvent(s->host_streams[b], start_ev, 0));
     int rc = PRR_OK;
     int64_t k = 0;
     for (int64_t off = 0; off < n && rc == PRR_OK; off += chunk, k++) {
@@ -637,13 +643,14 @@ int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const 
         float *dD = dO + chunk * 3;
         int32_t *dI = (int32_t *) (dD + chunk * 3);
         float *dT = (float *) (dI + chunk);
-        cudaStream_t cs = streams[b];
+        unsigned *counter = (unsigned *) ((char *) s->d_scratch.ptr + per * nbuf + 256 * b);
+        cudaStream_t cs = s->host_streams[b];
         if (cudaMemcpyAsync(dO, o + off * 3, m * 3 * sizeof(float), cudaMemcpyHostToDevice, cs) ||
             cudaMemcpyAsync(dD, d + off * 3, m * 3 * sizeof(float), cudaMemcpyHostToDevice, cs)) {
             rc = fail(PRR_ERR_CUDA, "host-to-device copy failed");
             break;
         }
-        rc = launch_mesh_closest(*s, object, dO, dD, m, dI, dT, nullptr, nullptr, nullptr, cs);
+        rc = launch_mesh_closest(*s, object, dO, dD, m, dI, dT, nullptr, counter, cfg, cs);
         if (rc)
             break;
         if (cudaMemcpyAsync(out_id + off, dI, m * sizeof(int32_t), cudaMemcpyDeviceToHost, cs) ||
@@ -653,15 +660,10 @@ int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const 
         }
     }
     for (int b = 0; b < nbuf; b++) {
-        cudaEventRecord(done[b], streams[b]);
-        cudaStreamWaitEvent(st, done[b], 0);
+        cudaEventRecord(s->host_events[b], s->host_streams[b]);
+        cudaStreamWaitEvent(st, s->host_events[b], 0);
     }
     cudaError_t e = cudaStreamSynchronize(st);
-    for (int b = 0; b < nbuf; b++) {
-        cudaEventDestroy(done[b]);
-        cudaStreamDestroy(streams[b]);
-    }
-    cudaEventDestroy(start_ev);
     if (rc == PRR_OK && e != cudaSuccess)
         rc = fail(PRR_ERR_CUDA, std::string("trace: ") + cudaGetErrorString(e));
     return rc;

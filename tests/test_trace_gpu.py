@@ -21,7 +21,10 @@ def dev(a, cuda):
 @pytest.mark.parametrize("case", MESH_CASES)
 @pytest.mark.parametrize("config", [None, {"persistent": 1}, {"block_size": 64},
                                     {"persistent": 2}, {"persistent": 2, "batch": 1},
-                                    {"persistent": 2, "batch": 32, "block_size": 64}])
+                                    {"persistent": 2, "batch": 32, "block_size": 64},
+                                    {"persistent": 3}, {"persistent": 3, "leaf_batch": 1},
+                                    {"persistent": 3, "leaf_batch": 32, "batch": 4},
+                                    {"persistent": 3, "leaf_batch": 8, "block_size": 256}])
 def test_mesh_intersect_bit_exact(golden, cuda, case, config):
     g = golden("mesh")
     p = f"mesh_{case}_"
@@ -45,13 +48,25 @@ def test_mesh_occluded_bit_exact(golden, cuda, case):
     assert np.array_equal(occ.cpu().numpy(), g[p + "occ"])
 
 
-def test_mesh_intersect_host_buffers(golden, cuda):
+@pytest.mark.parametrize("config", [None, {"persistent": 2}, {"persistent": 3}])
+def test_mesh_intersect_host_buffers(golden, cuda, config):
     g = golden("mesh")
     p = "mesh_q3000_"
     s = prr.Scene.single_mesh(g[p + "verts"])
-    hid, t = s.mesh_intersect_host(0, g[p + "o"], g[p + "d"])
+    hid, t = s.mesh_intersect_host(0, g[p + "o"], g[p + "d"], config=config)
     assert np.array_equal(hid, g[p + "id"])
     assert np.array_equal(t.view(np.uint32), g[p + "t"].view(np.uint32))
+    # many chunks over the pipeline's streams (1,200,000 rays: 3 chunks, the
+    # last one ragged), pinned buffers, against the device-array call
+    v, o, d = scenes.query_set(20_000, 1_200_000, seed=5)
+    s2 = prr.Scene.single_mesh(v)
+    import torch
+    ho = torch.from_numpy(o).pin_memory().numpy()
+    hd = torch.from_numpy(d).pin_memory().numpy()
+    hid2, t2 = s2.mesh_intersect_host(0, ho, hd, config=config)
+    did, dt = s2.mesh_intersect(0, dev(o, cuda), dev(d, cuda))
+    assert np.array_equal(hid2, did.cpu().numpy())
+    assert np.array_equal(t2.view(np.uint32), dt.cpu().numpy().view(np.uint32))
 
 
 def test_query_set_full_size_against_restatement(port, cuda):
@@ -73,7 +88,8 @@ def test_query_set_full_size_against_restatement(port, cuda):
     assert np.array_equal(t64[hit], rt64[hit])
     assert np.isnan(t64[~hit]).all()
     # the persistent launch shapes give the same answer
-    for cfg in ({"persistent": 1}, {"persistent": 2}, {"persistent": 2, "batch": 16}):
+    for cfg in ({"persistent": 1}, {"persistent": 2}, {"persistent": 2, "batch": 16},
+                {"persistent": 3}, {"persistent": 3, "leaf_batch": 24}):
         hid2, t2, t642 = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), t64=True, config=cfg)
         assert np.array_equal(hid2.cpu().numpy(), rh)
         assert np.array_equal(t2.cpu().numpy().view(np.uint32), rt.view(np.uint32))
@@ -132,3 +148,40 @@ def test_scene_intersect_many_objects_against_reference(ref, cuda):
     assert np.array_equal(st.cpu().numpy().view(np.uint32), rt.view(np.uint32))
     socc = s.intersectP(dev(o, cuda), dev(d, cuda), dev(tm, cuda))
     assert np.array_equal(socc.cpu().numpy(), rocc)
+
+
+def test_edge_and_vertex_ties_all_launch_shapes(port, cuda):
+    # rays aimed at the shared edges and vertices of a tessellated grid and of
+    # an icosphere: many hits at equal (or one-ulp apart) distances in
+    # neighbouring leaves, where only the reference's leaf order and culling
+    # decide the winner
+    n = 48
+    g = np.linspace(-1.0, 1.0, n + 1, dtype=np.float32)
+    tris = []
+    for i in range(n):
+        for j in range(n):
+            a = (g[i], g[j], 0.5)
+            b = (g[i + 1], g[j], 0.5)
+            c = (g[i + 1], g[j + 1], 0.5)
+            d = (g[i], g[j + 1], 0.5)
+            tris += [a + b + c, a + c + d]
+    grid = np.array(tris, np.float32)
+    ico = scenes.icosphere(4) * np.float32(0.4)
+    v = np.vstack([grid, ico.reshape(-1, 9)]).astype(np.float32)
+    rng = np.random.default_rng(9)
+    tv = grid.reshape(-1, 3)
+    targets = np.vstack([tv, (grid[:, 0:3] + grid[:, 3:6]) * np.float32(0.5),
+                         ico.reshape(-1, 3)]).astype(np.float32)
+    targets = targets[rng.permutation(len(targets))[:60000]]
+    o = np.column_stack([rng.uniform(-1.5, 1.5, len(targets)), rng.uniform(-1.5, 1.5, len(targets)),
+                         rng.uniform(1.5, 3.0, len(targets))]).astype(np.float32)
+    d = (targets - o).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True).astype(np.float32)
+    d = d.astype(np.float32)
+    s = prr.Scene.single_mesh(v)
+    rh, rt, _ = port.mesh(v).intersect(o, d)
+    for cfg in (None, {"persistent": 2}, {"persistent": 3}, {"persistent": 3, "leaf_batch": 1},
+                {"persistent": 3, "leaf_batch": 32}):
+        hid, t = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), config=cfg)
+        assert np.array_equal(hid.cpu().numpy(), rh), cfg
+        assert np.array_equal(t.cpu().numpy().view(np.uint32), rt.view(np.uint32)), cfg

@@ -76,7 +76,7 @@ def test_autotune_tries_queue_order_and_stack_depth(cuda):
     desc = scenes.museum_like(96, 64, level=3, env_size=(256, 128))
     s = prr.Scene.from_desc(desc)
     best = s.autotune(2, 8)
-    assert best["ordered"] in (0, 1) and best["stack_smem"] in (0, 16, 8)
+    assert best["ordered"] in (0, 1) and best["stack_smem"] in (0, 16, 8, 4, 2)
     a, _ = s.render(4, 8, mode="wavefront")
     b, _ = s.render(4, 8, slices=1)
     assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
