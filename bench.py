@@ -493,6 +493,95 @@ def run_render(args, rank, world, on):
     return 0
 
 
+CAUSTICS = ("caustics: glass sphere (r=1, IOR 1.5) over a diffuse plane, light of intensity 100 "
+            "at (0,4,0); 2,000,000 photons traced, grid radius 0.02, 64-nearest gather at every "
+            "camera hit; 1024x1024, 32 spp, depth 8")
+
+
+def run_caustics(args, rank, world, on):
+    """One step = trace 2M photons + build the photon grid + render the frame
+    with the caustic gather. value = camera samples/s of the whole step."""
+    import torch
+    import photorealisticrender4610_b200 as prr
+    from photorealisticrender4610_b200 import scenes
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    desc = scenes.caustics()
+    scene = prr.Scene.from_desc(desc)
+    pm = prr.PhotonMap()
+    n_ph, radius, spp, k, depth = 2_000_000, 0.02, 32, 64, 8
+    npix = desc.width * desc.height
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        flush.zero_()
+        torch.cuda._sleep(2_000_000)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        pm.emit(scene, n_ph, seed=1, max_depth=depth)
+        ev[1].record()
+        pm.build(radius)
+        ev[2].record()
+        img = pm.render_caustics(scene, spp, max_depth=depth, seed=1, k_nearest=k)
+        ev[3].record()
+        torch.cuda.synchronize()
+        return [ev[i].elapsed_time(ev[i + 1]) for i in range(3)], img
+
+    for _ in range(args.warmup):
+        step()
+    with ClockSampler(dev.index) as clk:
+        barrier(on)
+        phases = [step()[0] for _ in range(args.steps)]
+        barrier(on)
+    ph = np.array(phases)
+    step_ms = max_over_ranks(float(ph.sum(1).mean()), on)
+    value = npix * spp * world / (step_ms * 1e-3) / 1e6
+    stored, grid_res = pm.info()
+    # end to end: the same step through the API plus the image copied to pinned host memory
+    host = torch.empty((desc.height, desc.width, 3), dtype=torch.float32).pin_memory()
+    e2e = []
+    for _ in range(max(2, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, img = step()
+        host.copy_(img)
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_value = npix * spp * world / (float(np.median(e2e)) * 1e-3) / 1e6
+    if rank != 0:
+        return 0
+    cpu = None
+    from oracle import loader
+    if loader.reference_available(fast=True):
+        threads = os.cpu_count() or 1
+        rs = loader.ReferenceOracle(fast=True).scene(desc)
+        n_cpu = 200_000
+        t0 = time.perf_counter()
+        rs.photon_emit(n_cpu, 1, max_depth=depth, threads=threads)
+        dt = time.perf_counter() - t0
+        cpu = {"value": n_cpu / dt / 1e6, "unit": "Mphotons/s", "cores": threads,
+               "kind": "reference", "sample": f"{n_cpu} photons traced by Photon.cpp's trace"}
+    line = {
+        "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": CAUSTICS, "photons_stored": stored, "grid_res": grid_res,
+                   "l2": "flushed (512 MB write) before every timed step",
+                   "phase_ms": {"emit": float(ph[:, 0].mean()), "grid": float(ph[:, 1].mean()),
+                                "render_gather": float(ph[:, 2].mean())}},
+        "mphotons_s": n_ph / (float(ph[:, 0].mean()) * 1e-3) / 1e6,
+        "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": npix * 12},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def serving_pool():
     """Eight procedural scenes from about 10k to 2M triangles, built like the
     museum-like scene (displaced icospheres under the HDR sky) and the query
@@ -608,7 +697,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--launch", default="", help="fixed launch shape, e.g. block=128,persistent=0")
-    ap.add_argument("--workload", choices=["query", "museum", "cornell", "serving"],
+    ap.add_argument("--workload", choices=["query", "museum", "cornell", "serving", "caustics"],
                     default="query")
     ap.add_argument("--requests", type=int, default=120, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrivals per s")
@@ -629,6 +718,8 @@ def main():
     try:
         if args.workload == "serving":
             return run_serving(args, rank, world, on)
+        if args.workload == "caustics":
+            return run_caustics(args, rank, world, on)
         if args.workload != "query":
             return run_render(args, rank, world, on)
         return run_ours(args, rank, world, on)

@@ -162,3 +162,32 @@ def test_museum_like_lockstep(ref, cuda):
     img, _ = s.render(64, 8, seed=4)
     rimg, _ = rs.render(8, 64, 4)
     assert rel_mse(img.cpu().numpy(), rimg) < 5e-3
+
+
+@pytest.mark.parametrize("mode", ["plain", "wavefront"])
+def test_museum_like_4096spp_against_reference(ref, cuda, mode):
+    """The rMSE gate on the full museum-like configuration (six displaced
+    level-7 icospheres, 1,966,082 triangles, 2048x1024 sky, 1920x1080, depth
+    8): a 32x32 crop at 4096 spp against the reference renderer on the same
+    RNG streams, and the crop's mean luminance within 3 sigma of an
+    independent reference seed."""
+    desc = scenes.museum_like()
+    win = (944, 524, 976, 556)
+    s = prr.Scene.from_desc(desc)
+    img, _ = s.render(4096, 8, seed=1, window=win, mode=mode)
+    img = img.cpu().numpy()
+    rs = ref.scene(desc)
+    rimg, _ = rs.render(8, 4096, 1, window=win)
+    err = rel_mse(img, rimg)
+    print(f"museum-like 4096 spp crop rMSE vs reference ({mode}): {err:.3e}")
+    assert err < REL_MSE_TOL
+    rimg2, _ = rs.render(8, 4096, 2, window=win)
+    lum = lambda x: x @ np.array([0.2126, 0.7152, 0.0722])  # noqa: E731
+    w = win[2] - win[0]
+    per_px = s.cast_samples(np.repeat(np.arange(win[0], win[2]), 16),
+                            np.repeat(np.arange(win[1], win[3]), 16)[:16 * w],
+                            np.tile(np.arange(16) * 250, w), 8, seed=7)
+    sigma_sample = float(lum(per_px.cpu().numpy()).std())
+    n = 4096 * w * (win[3] - win[1])
+    sigma = sigma_sample / np.sqrt(n) * np.sqrt(2)
+    assert abs(lum(img).mean() - lum(rimg2).mean()) < 3 * sigma + 1e-6
