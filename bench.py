@@ -399,9 +399,13 @@ def run_render(args, rank, world, on):
                             cfg.get("stack", 0), cfg.get("ordered", 1))
         tuned = cfg
     else:
-        # tune on a few samples per pixel, or on the whole frame when it is small
-        # enough that one pass could hold all of it
-        tuned = scene.autotune(spp if npix * spp <= 1 << 22 else 4, depth)
+        # tune on enough samples per pixel (a power of two, so the candidate
+        # pass sizes divide it) that the largest candidate pass (32M paths)
+        # fits in the tuning render, or on the whole frame
+        tune_spp = 4
+        while tune_spp < spp and npix * tune_spp < (1 << 25):
+            tune_spp *= 2
+        tuned = scene.autotune(min(tune_spp, spp), depth)
 
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 

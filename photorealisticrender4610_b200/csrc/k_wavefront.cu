@@ -406,7 +406,9 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
 }
 
 // ---- surface: NEE + BSDF sampling of a non-delta bounce
-__global__ void k_wf_surface(DevScene S, Wf w, int it_next) {
+// 64 registers (8 blocks of 128 per SM): this stage waits on scattered path
+// state and scene data, so resident warps matter more than a few spills.
+__global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S, Wf w, int it_next) {
     const int n = (int) w.cnt[kCntSurf];
     int *qout = w.qray[it_next & 1];
     const int stride = gridDim.x * blockDim.x;
@@ -880,8 +882,8 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.sample_offset = rs.sample_offset;
     w.tlas_cap = S.tlas_depth + 1;
     w.blas_cap = S.blas_depth + 1;
-    // paths per pass: whole samples of the window, about 2M paths in flight
-    const int64_t target = s.wf_paths > 0 ? s.wf_paths : (int64_t) 1 << 21;
+    // paths per pass: whole samples of the window, about 8M paths in flight
+    const int64_t target = s.wf_paths > 0 ? s.wf_paths : (int64_t) 1 << 23;
     int spp_pass = (int) std::max<int64_t>(1, target / std::max(1, w.npix));
     spp_pass = std::min(spp_pass, rs.max_spp);
     while (rs.max_spp % spp_pass)
