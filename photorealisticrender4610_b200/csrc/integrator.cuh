@@ -216,4 +216,23 @@ static __device__ V3 cast_ray(const DevScene &S, Ray3 ray, int max_depth, float 
     return L;
 }
 
+// Welford online mean / variance and the 95% confidence stop of the
+// adaptive sampler (Renderer.hpp:14-40), with the reference's float steps.
+struct Welford {
+    int n = 0;
+    float mean = 0.f, M2 = 0.f;
+    __device__ void update(float x) {
+        n++;
+        const float delta = x - mean;
+        mean += delta / (float) n;
+        M2 += delta * (x - mean);
+    }
+    __device__ float variance() const { return n < 2 ? 0.f : M2 / (float) (n - 1); }
+    __device__ float ci() const {
+        if (n < 2 || fabsf(mean) < 1e-6f)
+            return 1.f;
+        return 1.96f * sqrtf(variance() / (float) n) / fabsf(mean);
+    }
+};
+
 } // namespace prr

@@ -37,23 +37,6 @@ struct RenderArgs {
     unsigned long long *rays; // [2]: closest, shadow
 };
 
-struct Welford { // Renderer.hpp:14-40
-    int n = 0;
-    float mean = 0.f, M2 = 0.f;
-    __device__ void update(float x) {
-        n++;
-        const float delta = x - mean;
-        mean += delta / (float) n;
-        M2 += delta * (x - mean);
-    }
-    __device__ float variance() const { return n < 2 ? 0.f : M2 / (float) (n - 1); }
-    __device__ float ci() const {
-        if (n < 2 || fabsf(mean) < 1e-6f)
-            return 1.f;
-        return 1.96f * sqrtf(variance() / (float) n) / fabsf(mean);
-    }
-};
-
 __device__ __forceinline__ void count_rays(unsigned long long *rays, const PathCounters &c) {
     if (!rays)
         return;

@@ -34,7 +34,7 @@ enum : int { kFlagSpecular = 1, kFlagPending = 2, kFlagEndAfterShadow = 4 };
 enum : int {
     kCntRay0 = 0, kCntRay1 = 1, kCntMiss = 2, kCntDelta = 3, kCntSurf = 4, kCntShadow = 5,
     kCntExtend = 6, kCntShadowJobs = 7, kCntRays = 8, kCntShadowRays = 10, kCntShadowFetch = 12,
-    kCntSlots = 16
+    kCntActive = 13, kCntSlots = 16
 };
 
 struct Wf {
@@ -70,6 +70,14 @@ struct Wf {
     int ordered;
     uint8_t *tag;        // per path: bucket of the pending partition, 0xFF none
     unsigned *tile;      // per partition tile: 8 bucket counts, then offsets
+    // adaptive sampling (min_spp < max_spp): each pass traces the next
+    // spp_pass samples of the pixels still active; the film stage replays the
+    // reference's per-sample Welford stop (Renderer.cpp:74-95) on them
+    int adaptive, min_spp, max_spp;
+    float threshold;
+    int *act, *act_next; // active pixels (window-local indices), in pixel order
+    uint8_t *ptag;       // per active slot: 0 = stays active, 0xFF = done
+    float4 *wel0, *wel1; // per pixel: (n, mean r, g, b), (M2 r, g, b, -)
 };
 
 __device__ __forceinline__ uint8_t dir_octant(V3 d) {
@@ -108,9 +116,13 @@ __device__ __forceinline__ void finish(const Wf &w, int p, V3 L) {
 __global__ void k_wf_generate(DevScene S, Wf w) {
     const int base = *w.pass_base;
     const int stride = gridDim.x * blockDim.x;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < w.P; p += stride) {
-        const int q = p % w.npix;
-        const int s = base + p / w.npix;
+    // fixed spp: every pixel; adaptive: the active ones (their count is on
+    // the device, set by the previous pass)
+    const int nq = w.adaptive ? (int) w.cnt[kCntActive] : w.npix;
+    const int P = w.adaptive ? nq * w.spp_pass : w.P;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += stride) {
+        const int q = w.adaptive ? w.act[p % nq] : p % w.npix;
+        const int s = base + p / nq;
         const int i = w.x0 + q % w.ww, j = w.y0 + q / w.ww;
         const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) w.W;
         Rng rng{path_state(w.seed, m, (uint32_t) (w.sample_offset + s))};
@@ -128,7 +140,7 @@ __global__ void k_wf_generate(DevScene S, Wf w) {
         w.tag[p] = 0xFF;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        w.cnt[kCntRay0] = (unsigned) w.P;
+        w.cnt[kCntRay0] = (unsigned) P;
         w.cnt[kCntRay1] = 0;
     }
 }
@@ -632,6 +644,8 @@ constexpr int kPartThreads = 256;
 constexpr int kPartTile = kPartThreads * 16;
 
 struct PartSpec {
+    uint8_t *tag;       // the tags, padded with 0xFF to whole tiles
+    const int *map;     // item k is written as map[k] (nullptr: k itself)
     int *q[8];          // bucket b's queue; concatenated: all in q[0], bucket order
     int nb;             // buckets (<= 8)
     int concat;
@@ -646,12 +660,13 @@ __device__ __forceinline__ unsigned count_tag(const uint4 &v, unsigned b) {
             __popc(__vcmpeq4(v.z, bb)) + __popc(__vcmpeq4(v.w, bb))) >> 3;
 }
 
-__global__ void __launch_bounds__(kPartThreads) k_part_count(Wf w, int nb) {
+__global__ void __launch_bounds__(kPartThreads) k_part_count(Wf w, PartSpec ps) {
+    const int nb = ps.nb;
     __shared__ unsigned c[8];
     if (threadIdx.x < 8)
         c[threadIdx.x] = 0;
     __syncthreads();
-    const uint4 v = reinterpret_cast<const uint4 *>(w.tag)[blockIdx.x * kPartThreads + threadIdx.x];
+    const uint4 v = reinterpret_cast<const uint4 *>(ps.tag)[blockIdx.x * kPartThreads + threadIdx.x];
 #pragma unroll
     for (int b = 0; b < 8; b++)
         if (b < nb) {
@@ -759,7 +774,7 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(Wf w, PartSpec ps
     __shared__ unsigned wsum[kPartThreads / 32][8];
     __shared__ unsigned base[8][kPartThreads];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint4 *tv = reinterpret_cast<uint4 *>(w.tag) + blockIdx.x * kPartThreads + threadIdx.x;
+    uint4 *tv = reinterpret_cast<uint4 *>(ps.tag) + blockIdx.x * kPartThreads + threadIdx.x;
     const uint4 v = *tv;
     unsigned c[8], x[8];
 #pragma unroll
@@ -795,10 +810,78 @@ __global__ void __launch_bounds__(kPartThreads) k_part_scatter(Wf w, PartSpec ps
                     if (t == (unsigned) k)
                         q = ps.q[k];
             }
-            q[base[t][threadIdx.x]++] = first + i;
+            q[base[t][threadIdx.x]++] = ps.map ? ps.map[first + i] : first + i;
         }
     }
     *tv = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+}
+
+// ---- adaptive film: each active pixel takes this pass's samples in sample
+// order -- running sum, per-channel Welford update, and the stop test after
+// every sample once min_spp samples are in (Renderer.cpp:74-95). Samples
+// traced past a pixel's stop are dropped, as the reference never draws them.
+__global__ void k_wf_film_adaptive(Wf w) {
+    const int na = (int) w.cnt[kCntActive];
+    const int stride = gridDim.x * blockDim.x;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += stride) {
+        const int q = w.act[a];
+        const float4 s0 = w.wel0[q], s1 = w.wel1[q];
+        Welford wr{(int) s0.x, s0.y, s1.x}, wg{(int) s0.x, s0.z, s1.y}, wb{(int) s0.x, s0.w, s1.z};
+        float3 f = w.film[q];
+        bool done = false;
+        for (int k = 0; k < w.spp_pass && !done; k++) {
+            float4 r = w.result[(size_t) k * na + a];
+            if (isnan(r.x) || isnan(r.y) || isnan(r.z))
+                r = make_float4(0.f, 0.f, 0.f, 0.f);
+            f.x += r.x;
+            f.y += r.y;
+            f.z += r.z;
+            wr.update(r.x);
+            wg.update(r.y);
+            wb.update(r.z);
+            done = wr.n >= w.min_spp && wr.ci() < w.threshold && wg.ci() < w.threshold &&
+                   wb.ci() < w.threshold;
+        }
+        w.film[q] = f;
+        w.wel0[q] = make_float4((float) wr.n, wr.mean, wg.mean, wb.mean);
+        w.wel1[q] = make_float4(wr.M2, wg.M2, wb.M2, 0.f);
+        w.ptag[a] = (done || wr.n >= w.max_spp) ? 0xFF : 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        *w.pass_base += w.spp_pass;
+}
+
+__global__ void k_wf_copy_active(Wf w) {
+    const int na = (int) w.cnt[kCntActive];
+    const int stride = gridDim.x * blockDim.x;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < na; a += stride)
+        w.act[a] = w.act_next[a];
+}
+
+__global__ void k_wf_adaptive_init(Wf w) {
+    const int stride = gridDim.x * blockDim.x;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < w.npix; q += stride) {
+        w.act[q] = q;
+        w.wel0[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+        w.wel1[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        w.cnt[kCntActive] = (unsigned) w.npix;
+}
+
+// mean = sum / n per pixel (Renderer.cpp:98-99)
+__global__ void k_wf_resolve_adaptive(const float3 *film, const float4 *wel0, int npix, float *out,
+                                      int32_t *spp) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npix)
+        return;
+    const float3 f = film[q];
+    const int n = (int) wel0[q].x;
+    out[(size_t) q * 3 + 0] = f.x / (float) n;
+    out[(size_t) q * 3 + 1] = f.y / (float) n;
+    out[(size_t) q * 3 + 2] = f.z / (float) n;
+    if (spp)
+        spp[q] = n;
 }
 
 __global__ void k_wf_film(Wf w) {
@@ -866,8 +949,6 @@ struct WavefrontPlan {
 
 int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                      unsigned long long *out_rays, cudaStream_t st) {
-    if (rs.min_spp < rs.max_spp) // the Welford stop needs all of a pixel's samples in order
-        return render_plain(s, rs, out_rgb, out_spp, out_rays, st);
     const DevScene &S = s.dev;
     Wf w{};
     w.W = s.width;
@@ -892,9 +973,11 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.P = spp_pass * w.npix;
     const size_t P = (size_t) w.P;
     const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
-    const size_t bytes = 256 * 40 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) +
-                         (size_t) ntiles * kPartTile + (size_t) w.npix * 16 +
-                         (size_t) ntiles * 32 + 4096;
+    const int ptiles = (w.npix + kPartTile - 1) / kPartTile; // active-pixel partition
+    const size_t bytes = 256 * 48 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) +
+                         (size_t) ntiles * kPartTile + (size_t) w.npix * (16 + 8 + 32) +
+                         (size_t) ptiles * kPartTile + (size_t) std::max(ntiles, ptiles) * 32 +
+                         4096;
     PRR_CUDA_TRY(s.d_wavefront.ensure(bytes));
     char *cur = (char *) s.d_wavefront.ptr;
     w.rng = carve<uint64_t>(cur, P);
@@ -926,8 +1009,17 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.cnt = carve<unsigned>(cur, kCntSlots);
     w.pass_base = carve<int>(cur, 4);
     w.tag = carve<uint8_t>(cur, (size_t) ntiles * kPartTile);
-    w.tile = carve<unsigned>(cur, (size_t) ntiles * 8);
+    w.tile = carve<unsigned>(cur, (size_t) std::max(ntiles, ptiles) * 8);
     w.ordered = s.wf_ordered ? 1 : 0;
+    w.adaptive = rs.min_spp < rs.max_spp ? 1 : 0;
+    w.min_spp = rs.min_spp;
+    w.max_spp = rs.max_spp;
+    w.threshold = rs.variance_threshold;
+    w.act = carve<int>(cur, (size_t) w.npix);
+    w.act_next = carve<int>(cur, (size_t) w.npix);
+    w.ptag = carve<uint8_t>(cur, (size_t) ptiles * kPartTile);
+    w.wel0 = carve<float4>(cur, (size_t) w.npix);
+    w.wel1 = carve<float4>(cur, (size_t) w.npix);
     if ((size_t) (cur - (char *) s.d_wavefront.ptr) > bytes)
         return fail(PRR_ERR_INTERNAL, "wavefront buffer layout overflow");
 
@@ -979,10 +1071,15 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) ntiles * kPartTile, st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.pass_base, 0, sizeof(int), st));
+    if (w.adaptive) { // after the counters are cleared: it sets the active count
+        PRR_CUDA_TRY(cudaMemsetAsync(w.ptag, 0xFF, (size_t) ptiles * kPartTile, st));
+        k_wf_adaptive_init<<<(w.npix + 255) / 256, 256, 0, st>>>(w);
+    }
 
     // ordered queues: hit classes -> miss / delta / surface queues; next rays
     // -> the ray queue, direction octant major
     PartSpec part_cls{};
+    part_cls.tag = w.tag;
     part_cls.q[0] = w.qmiss;
     part_cls.q[1] = w.qdelta;
     part_cls.q[2] = w.qsurf;
@@ -995,6 +1092,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     PartSpec part_ray[2];
     for (int r = 0; r < 2; r++) {
         part_ray[r] = PartSpec{};
+        part_ray[r].tag = w.tag;
         part_ray[r].q[0] = w.qray[r];
         part_ray[r].nb = 8;
         part_ray[r].concat = 1;
@@ -1002,10 +1100,19 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
             part_ray[r].count_slot[b] = -1;
         part_ray[r].total_slot = kCntRay0 + r;
     }
-    auto partition = [&](const PartSpec &ps, cudaStream_t cs) {
-        k_part_count<<<ntiles, kPartThreads, 0, cs>>>(w, ps.nb);
-        k_part_scan<<<1, 1024, 0, cs>>>(w, ntiles, ps);
-        k_part_scatter<<<ntiles, kPartThreads, 0, cs>>>(w, ps);
+    // adaptive: the pixels still active -> the next pass's active list
+    PartSpec part_act{};
+    part_act.tag = w.ptag;
+    part_act.map = w.act;
+    part_act.q[0] = w.act_next;
+    part_act.nb = 1;
+    part_act.concat = 1;
+    part_act.count_slot[0] = -1;
+    part_act.total_slot = kCntActive;
+    auto partition = [&](const PartSpec &ps, int nt, cudaStream_t cs) {
+        k_part_count<<<nt, kPartThreads, 0, cs>>>(w, ps);
+        k_part_scan<<<1, 1024, 0, cs>>>(w, nt, ps);
+        k_part_scatter<<<nt, kPartThreads, 0, cs>>>(w, ps);
     };
 
     // capture one pass
@@ -1015,16 +1122,22 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
             k_wf_begin<<<1, 32, 0, cs>>>(w, it);
             k_ext<<<g_ext, block, smem_ext, cs>>>(S, w, it, refill);
             if (w.ordered)
-                partition(part_cls, cs);
+                partition(part_cls, ntiles, cs);
             k_wf_miss<<<g_shade, 128, 0, cs>>>(S, w);
             k_wf_delta<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
             k_wf_surface<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
             k_sh<<<g_sh, block, smem_sh, cs>>>(S, w, refill);
             k_wf_shadow_resolve<<<g_shade, 128, 0, cs>>>(w);
             if (w.ordered)
-                partition(part_ray[(it + 1) & 1], cs);
+                partition(part_ray[(it + 1) & 1], ntiles, cs);
         }
-        k_wf_film<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
+        if (w.adaptive) {
+            k_wf_film_adaptive<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
+            partition(part_act, ptiles, cs);
+            k_wf_copy_active<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
+        } else {
+            k_wf_film<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
+        }
         PRR_CUDA_TRY(cudaGetLastError());
         return PRR_OK;
     };
@@ -1034,6 +1147,8 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
                 ((uint64_t) refill << 50));
     key = mix64(key ^ (uint64_t) (uintptr_t) w.spill ^ ((uint64_t) w.blas_sm << 32) ^
                 ((uint64_t) w.ordered << 60));
+    key = mix64(key ^ ((uint64_t) w.adaptive << 7) ^ ((uint64_t) w.min_spp << 24) ^
+                ((uint64_t) float_bits(w.threshold) << 28) ^ (uint64_t) w.max_spp);
     key = mix64(key ^ ((uint64_t) (uint32_t) w.x0 << 32 | (uint32_t) w.y0) ^
                 ((uint64_t) (uint32_t) w.ww << 16) ^ rs.seed ^ ((uint64_t) rs.sample_offset << 40) ^
                 (uint64_t) float_bits(w.clamp));
@@ -1072,7 +1187,12 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
             if (int rc = enqueue_pass(st))
                 return rc;
     }
-    k_wf_resolve<<<(w.npix + 255) / 256, 256, 0, st>>>(w.film, w.npix, rs.max_spp, out_rgb, out_spp);
+    if (w.adaptive)
+        k_wf_resolve_adaptive<<<(w.npix + 255) / 256, 256, 0, st>>>(w.film, w.wel0, w.npix,
+                                                                    out_rgb, out_spp);
+    else
+        k_wf_resolve<<<(w.npix + 255) / 256, 256, 0, st>>>(w.film, w.npix, rs.max_spp, out_rgb,
+                                                            out_spp);
     PRR_CUDA_TRY(cudaGetLastError());
     if (out_rays) {
         k_wf_rays_out<<<1, 1, 0, st>>>(w.cnt, out_rays);
@@ -1080,8 +1200,9 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     }
     // generate + per bounce (begin, extend, miss, delta, surface, shadow,
     // shadow_resolve, and two 3-kernel partitions when ordered) + film
-    const int64_t per_pass = 2 + (int64_t) (w.max_depth + 1) * (7 + (w.ordered ? 6 : 0));
-    s.last_launches = per_pass * passes + 1 + (out_rays ? 1 : 0);
+    const int64_t per_pass = 2 + (int64_t) (w.max_depth + 1) * (7 + (w.ordered ? 6 : 0)) +
+                             (w.adaptive ? 4 : 0);
+    s.last_launches = per_pass * passes + 1 + (w.adaptive ? 1 : 0) + (out_rays ? 1 : 0);
     return PRR_OK;
 }
 

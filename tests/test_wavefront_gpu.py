@@ -101,3 +101,27 @@ def test_wavefront_ordered_queues_equal_plain(cuda, name):
     wave, _, r_ord = s.render(12, depth, seed=4, mode="wavefront", count_rays=True)
     assert np.array_equal(wave.cpu().numpy().view(np.uint32), plain.cpu().numpy().view(np.uint32))
     assert np.array_equal(r_app.cpu().numpy(), r_ord.cpu().numpy())
+
+
+@pytest.mark.parametrize("name,paths_spp,ordered", [("cornell", 8, True), ("cornell", 32, False),
+                                                    ("museum", 4, True)])
+def test_wavefront_adaptive_equals_plain(cuda, name, paths_spp, ordered):
+    # adaptive sampling (Renderer.cpp:74-99) in the wavefront: passes over the
+    # still-active pixels, the Welford stop replayed per sample in the film
+    # stage; same sample counts and the same image as the plain adaptive
+    # renderer (itself checked against the reference in test_render_gpu.py)
+    if name == "cornell":
+        desc, depth, lo, hi, thr = scenes.cornell_box(48, 40), 5, 8, 128, 0.1
+    else:
+        desc, depth, lo, hi, thr = scenes.museum_like(64, 36, level=3, env_size=(256, 128)), 8, 4, 64, 0.2
+    s = prr.Scene.from_desc(desc)
+    ref, rspp = s.render(hi, depth, seed=6, min_spp=lo, threshold=thr)
+    npix = desc.width * desc.height
+    s.set_wavefront(paths_per_pass=npix * paths_spp, block_size=128, ordered=ordered)
+    out, spp, rays = s.render(hi, depth, seed=6, min_spp=lo, threshold=thr, mode="wavefront",
+                              count_rays=True)
+    spp, rspp = spp.cpu().numpy(), rspp.cpu().numpy()
+    assert np.array_equal(spp, rspp)
+    assert spp.min() >= lo and spp.max() <= hi and spp.min() < spp.max()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
+    assert s.stats()["last_render_launches"] > 0
