@@ -360,13 +360,22 @@ def run_ours(args, rank, world, on):
     return 0
 
 
+def _scenes():
+    return __import__("photorealisticrender4610_b200.scenes", fromlist=["x"])
+
+
 RENDER_WORKLOADS = {
-    # name: (scene factory, spp, depth, description)
-    "museum": (lambda: __import__("photorealisticrender4610_b200.scenes", fromlist=["x"]).museum_like(),
+    # name: (scene factory, max spp, depth, description, adaptive (min spp, threshold) or None)
+    "museum": (lambda: _scenes().museum_like(),
                64, 8, "museum-like: 6 displaced level-7 icospheres (1,966,082 triangles), "
-               "2048x1024 HDR sky, 1920x1080, 64 spp, depth 8"),
-    "cornell": (lambda: __import__("photorealisticrender4610_b200.scenes", fromlist=["x"]).cornell_box(),
-                16, 5, "Cornell box 256x256, 16 spp, depth 5"),
+               "2048x1024 HDR sky, 1920x1080, 64 spp, depth 8", None),
+    "cornell": (lambda: _scenes().cornell_box(),
+                16, 5, "Cornell box 256x256, 16 spp, depth 5", None),
+    # the reference's own render settings (main.cpp:11-20) on the museum-like scene
+    "museum-adaptive": (lambda: _scenes().museum_like(960, 540),
+                        256, 12, "museum-like scene with the reference renderer's main.cpp "
+                        "settings: 960x540, adaptive 1..256 spp, Welford threshold 0.01, "
+                        "depth 12", (1, 0.01)),
 }
 
 
@@ -376,7 +385,8 @@ def run_render(args, rank, world, on):
     import torch
     import photorealisticrender4610_b200 as prr
 
-    factory, spp, depth, desc_text = RENDER_WORKLOADS[args.workload]
+    factory, spp, depth, desc_text, adaptive = RENDER_WORKLOADS[args.workload]
+    min_spp, thr = adaptive if adaptive else (None, 0.05)
     dev = torch.device("cuda", torch.cuda.current_device())
     desc = factory()
     if args.size:
@@ -411,10 +421,12 @@ def run_render(args, rank, world, on):
             torch.cuda._sleep(20_000_000)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            img, _, rays = scene.render(spp, depth, seed=1, mode=mode, slices=0, count_rays=True)
+            img, cnt, rays = scene.render(spp, depth, seed=1, mode=mode, slices=0,
+                                          count_rays=True, min_spp=min_spp, threshold=thr)
             b.record()
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
+        timed.samples = int(cnt.sum().item())  # samples actually taken (adaptive: the spp map)
         return ms, img, rays
 
     if not args.kernel_only:
@@ -427,16 +439,17 @@ def run_render(args, rank, world, on):
     wf_launches = scene.stats()["last_render_launches"] * args.steps
     if args.kernel_only:
         if rank == 0:
-            print(json.dumps({"frame_ms": wf_ms, "msamples_s": npix * spp / np.mean(wf_ms) / 1e3,
+            print(json.dumps({"frame_ms": wf_ms,
+                              "msamples_s": timed.samples / np.mean(wf_ms) / 1e3,
                               "launch": tuned}))
         return 0
+    samples = timed.samples
     timed("plain", 1)
     pl_ms, pl_img, pl_rays = timed("plain", max(1, min(args.steps, 3)))
     wf_step = max_over_ranks(float(np.mean(wf_ms)), on)
     # the plain renderer is the comparison, not the headline: its median frame,
     # so one host stall longer than the queued busy-wait does not set the ratio
     pl_step = max_over_ranks(float(np.median(pl_ms)), on)
-    samples = npix * spp
     value = samples * world / (wf_step * 1e-3) / 1e6
     plain_value = samples * world / (pl_step * 1e-3) / 1e6
     rays = wf_rays.cpu().numpy()
@@ -448,7 +461,8 @@ def run_render(args, rank, world, on):
     for _ in range(max(2, min(args.steps, 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        img, _ = scene.render(spp, depth, seed=1, mode="wavefront")
+        img, _ = scene.render(spp, depth, seed=1, mode="wavefront", min_spp=min_spp,
+                              threshold=thr)
         host.copy_(img)
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
@@ -463,12 +477,14 @@ def run_render(args, rank, world, on):
         rs = ref.scene(desc)
         win = (desc.width // 2 - 32, desc.height // 2 - 32, desc.width // 2 + 32,
                desc.height // 2 + 32)
-        cspp = 16
+        cspp = 16 if not adaptive else spp
         t0 = time.perf_counter()
-        rs.render(depth, cspp, 1, window=win, threads=threads)
+        _, rcnt = rs.render(depth, cspp, 1, window=win, threads=threads, min_spp=min_spp,
+                            threshold=thr)
         dt = time.perf_counter() - t0
-        cpu = {"value": 64 * 64 * cspp / dt / 1e6, "unit": "Msamples/s", "cores": threads,
-               "kind": "reference", "sample": f"64x64 centre crop at {cspp} spp"}
+        cpu = {"value": float(np.sum(rcnt)) / dt / 1e6, "unit": "Msamples/s", "cores": threads,
+               "kind": "reference",
+               "sample": f"64x64 centre crop at {cspp} spp" + (" (adaptive)" if adaptive else "")}
     line = {
         "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": wf_step,
@@ -705,7 +721,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--launch", default="", help="fixed launch shape, e.g. block=128,persistent=0")
-    ap.add_argument("--workload", choices=["query", "museum", "cornell", "serving", "caustics"],
+    ap.add_argument("--workload", choices=["query", "museum", "cornell", "museum-adaptive",
+                                           "serving", "caustics"],
                     default="query")
     ap.add_argument("--requests", type=int, default=120, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrivals per s")
