@@ -144,6 +144,25 @@ int prr_scene_add_material(prr_scene *scene, int kind, const float params[9], in
  * maxPrimsInNode 4 (Triangle.hpp:173-179). */
 int prr_scene_add_mesh(prr_scene *scene, const float *verts, int64_t ntri, int material,
                        int *out_object);
+/* MeshTriangle from triangles with per-corner data, as the glTF loader builds
+ * them (GLTFLoader.cpp:224-262, Triangle.hpp:17-23): normals = ntri x 9
+ * (n0, n1, n2; normalized here, and the face normal becomes
+ * normalize(n0 + n1 + n2)), uvs = ntri x 6 (t0, t1, t2), tangents = ntri x 12
+ * (xyz + handedness w per corner). Any of the three may be NULL. Hits on the
+ * mesh interpolate them as Triangle::finalize does (Triangle.cpp:34-59). */
+int prr_scene_add_mesh_attr(prr_scene *scene, const float *verts, const float *normals,
+                            const float *uvs, const float *tangents, int64_t ntri, int material,
+                            int *out_object);
+/* A material texture (Texture, TextureUtils.hpp:9-18): width x height texels
+ * of 3 or 4 8-bit channels, row-major, as decoded from the image file. */
+int prr_scene_add_texture(prr_scene *scene, const uint8_t *texels, int width, int height,
+                          int channels, int *out_texture);
+/* Material::baseColorTex / metallicRoughnessTex / normalTex / emissiveTex
+ * (Material.hpp:45-48): texture ids from prr_scene_add_texture, -1 for none.
+ * Sampled bilinearly with wrap-around (TextureUtils.hpp:22-136) when shading
+ * data is built (Material.cpp:3-26). */
+int prr_scene_set_material_textures(prr_scene *scene, int material, int base_color,
+                                    int metallic_roughness, int normal, int emissive);
 /* Sphere(center, radius, mat) (Sphere.hpp:14-16) + Scene::Add. */
 int prr_scene_add_sphere(prr_scene *scene, const float center[3], float radius, int material,
                          int *out_object);

@@ -208,6 +208,11 @@ class ReferenceOracle:
         L.prr_ref_scene_add_material.argtypes = [vp, C.c_int, _f32p]
         L.prr_ref_scene_add_mesh.restype = C.c_int
         L.prr_ref_scene_add_mesh.argtypes = [vp, _f32p, C.c_int64, C.c_int]
+        L.prr_ref_scene_add_mesh_attr.restype = C.c_int
+        L.prr_ref_scene_add_mesh_attr.argtypes = [vp, _f32p, vp, vp, vp, C.c_int64, C.c_int]
+        L.prr_ref_scene_set_texture.restype = C.c_int
+        L.prr_ref_scene_set_texture.argtypes = [vp, C.c_int, C.c_int, _u8p, C.c_int, C.c_int,
+                                                C.c_int]
         L.prr_ref_scene_add_sphere.restype = C.c_int
         L.prr_ref_scene_add_sphere.argtypes = [vp, _f32p, C.c_float, C.c_int]
         L.prr_ref_scene_set_background.argtypes = [vp, _f32p]
@@ -341,9 +346,26 @@ class RefScene:
         self.desc = desc
         self.h = L.prr_ref_scene_new()
         for m in desc.materials:
-            L.prr_ref_scene_add_material(self.h, int(m.kind), _c(m.params(), np.float32))
+            mid = L.prr_ref_scene_add_material(self.h, int(m.kind), _c(m.params(), np.float32))
+            for slot, t in enumerate(m.texture_list()):
+                if t is not None:
+                    t = _c(t, np.uint8)
+                    L.prr_ref_scene_set_texture(self.h, mid, slot, t.reshape(-1), t.shape[1],
+                                                t.shape[0], t.shape[2])
+        keep = []
         for obj in desc.objects:
-            if obj.kind == "mesh":
+            if obj.kind == "mesh" and obj.has_attributes():
+                v = _c(obj.verts, np.float32).reshape(-1, 9)
+                ptrs = []
+                for a, k in ((obj.normals, 9), (obj.uvs, 6), (obj.tangents, 12)):
+                    if a is None:
+                        ptrs.append(None)
+                    else:
+                        a = _c(a, np.float32).reshape(-1, k)
+                        keep.append(a)
+                        ptrs.append(a.ctypes.data)
+                L.prr_ref_scene_add_mesh_attr(self.h, v, *ptrs, len(v), obj.material)
+            elif obj.kind == "mesh":
                 v = _c(obj.verts, np.float32).reshape(-1, 9)
                 L.prr_ref_scene_add_mesh(self.h, v, len(v), obj.material)
             else:

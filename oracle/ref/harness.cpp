@@ -315,6 +315,68 @@ int prr_ref_scene_add_mesh(void *h, const float *verts, int64_t ntri, int mat) {
     return (int) rs->objects.size() - 1;
 }
 
+// A MeshTriangle whose triangles carry per-corner data set the way
+// GLTFLoader::load does (GLTFLoader.cpp:236-262): normalized corner normals
+// and face normal normalize(n0 + n1 + n2), uvs, tangents with handedness.
+int prr_ref_scene_add_mesh_attr(void *h, const float *verts, const float *nrm, const float *uv,
+                                const float *tan, int64_t ntri, int mat) {
+    RefScene *rs = (RefScene *) h;
+    Material *m = rs->materials.at(mat);
+    std::vector<Triangle> tris = make_tris(verts, ntri, m);
+    for (int64_t i = 0; i < ntri; i++) {
+        Triangle &tri = tris[i];
+        if (nrm) {
+            const float *n = nrm + i * 9;
+            tri.n0 = normalize(Vector3f(n[0], n[1], n[2]));
+            tri.n1 = normalize(Vector3f(n[3], n[4], n[5]));
+            tri.n2 = normalize(Vector3f(n[6], n[7], n[8]));
+            tri.hasSmoothNormals = true;
+            tri.normal = normalize(tri.n0 + tri.n1 + tri.n2);
+        }
+        if (uv) {
+            const float *t = uv + i * 6;
+            tri.t0 = Vector2f(t[0], t[1]);
+            tri.t1 = Vector2f(t[2], t[3]);
+            tri.t2 = Vector2f(t[4], t[5]);
+        }
+        if (tan) {
+            const float *t = tan + i * 12;
+            tri.tan0 = Vector3f(t[0], t[1], t[2]);
+            tri.tan1 = Vector3f(t[4], t[5], t[6]);
+            tri.tan2 = Vector3f(t[8], t[9], t[10]);
+            tri.tangentW0 = t[3];
+            tri.tangentW1 = t[7];
+            tri.tangentW2 = t[11];
+            tri.hasTangents = true;
+        }
+    }
+    MeshTriangle *mesh = new MeshTriangle(std::move(tris), vertex_bounds(verts, ntri), m);
+    rs->scene.Add(mesh);
+    rs->objects.push_back(mesh);
+    rs->object_kind.push_back(0);
+    return (int) rs->objects.size() - 1;
+}
+
+// Material textures (Material.hpp:45-48): slot 0 base colour, 1 metallic-
+// roughness, 2 normal, 3 emissive.
+int prr_ref_scene_set_texture(void *h, int mat, int slot, const uint8_t *texels, int w, int hgt,
+                              int channels) {
+    RefScene *rs = (RefScene *) h;
+    Material *m = rs->materials.at(mat);
+    Texture *t = slot == 0   ? &m->baseColorTex
+                 : slot == 1 ? &m->metallicRoughnessTex
+                 : slot == 2 ? &m->normalTex
+                 : slot == 3 ? &m->emissiveTex
+                             : nullptr;
+    if (!t)
+        return -1;
+    t->data.assign(texels, texels + (size_t) w * hgt * channels);
+    t->width = w;
+    t->height = hgt;
+    t->channels = channels;
+    return 0;
+}
+
 int prr_ref_scene_add_sphere(void *h, const float *c, float r, int mat) {
     RefScene *rs = (RefScene *) h;
     Sphere *s = new Sphere(Vector3f(c[0], c[1], c[2]), r, rs->materials.at(mat));

@@ -90,6 +90,12 @@ _SIGS = {
     "prr_scene_destroy": (C.c_int, [_vp]),
     "prr_scene_add_material": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "prr_scene_add_mesh": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, C.POINTER(C.c_int)]),
+    "prr_scene_add_mesh_attr": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int64, C.c_int,
+                                          C.POINTER(C.c_int)]),
+    "prr_scene_add_texture": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(C.c_int)]),
+    "prr_scene_set_material_textures": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                  C.c_int]),
     "prr_scene_add_sphere": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_float, C.c_int,
                                        C.POINTER(C.c_int)]),
     "prr_scene_set_background": (C.c_int, [_vp, C.POINTER(C.c_float)]),

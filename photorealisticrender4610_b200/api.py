@@ -100,6 +100,37 @@ class Scene:
         self.objects.append(("mesh", len(v)))
         return out.value
 
+    def add_mesh_attr(self, verts, material: int, normals=None, uvs=None, tangents=None) -> int:
+        """MeshTriangle with per-corner normals (n, 9), uvs (n, 6) and tangents
+        (n, 12: xyz + handedness per corner), any of them None."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 9)
+        arrs = []
+        for a, k in ((normals, 9), (uvs, 6), (tangents, 12)):
+            arrs.append(None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1, k))
+        for a in arrs:
+            if a is not None and len(a) != len(v):
+                raise ValueError("per-corner arrays need one row per triangle")
+        ptr = [C.c_void_p(a.ctypes.data) if a is not None else None for a in arrs]
+        out = C.c_int()
+        check(self.lib.prr_scene_add_mesh_attr(self.h, C.c_void_p(v.ctypes.data), ptr[0], ptr[1],
+                                               ptr[2], len(v), material, C.byref(out)))
+        self.objects.append(("mesh", len(v)))
+        return out.value
+
+    def add_texture(self, texels) -> int:
+        """An 8-bit texture, (h, w, 3 or 4) uint8."""
+        t = np.ascontiguousarray(texels, np.uint8)
+        h, w, c = t.shape
+        out = C.c_int()
+        check(self.lib.prr_scene_add_texture(self.h, C.c_void_p(t.ctypes.data), w, h, c,
+                                             C.byref(out)))
+        return out.value
+
+    def set_material_textures(self, material: int, base_color: int = -1,
+                              metallic_roughness: int = -1, normal: int = -1, emissive: int = -1):
+        check(self.lib.prr_scene_set_material_textures(self.h, material, base_color,
+                                                       metallic_roughness, normal, emissive))
+
     def add_sphere(self, center, radius: float, material: int) -> int:
         out = C.c_int()
         check(self.lib.prr_scene_add_sphere(self.h, _f3(center), float(radius), material,
@@ -135,9 +166,14 @@ class Scene:
         s = cls()
         s.desc = desc
         for m in desc.materials:
-            s.add_material(int(m.kind), m.params())
+            mid = s.add_material(int(m.kind), m.params())
+            tex = [s.add_texture(t) if t is not None else -1 for t in m.texture_list()]
+            if any(t >= 0 for t in tex):
+                s.set_material_textures(mid, *tex)
         for o in desc.objects:
-            if o.kind == "mesh":
+            if o.kind == "mesh" and o.has_attributes():
+                s.add_mesh_attr(o.verts, o.material, o.normals, o.uvs, o.tangents)
+            elif o.kind == "mesh":
                 s.add_mesh(o.verts, o.material)
             else:
                 s.add_sphere(o.center, o.radius, o.material)

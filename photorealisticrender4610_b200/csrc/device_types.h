@@ -76,7 +76,21 @@ struct alignas(16) DevObject {
     float cx, cy, cz, radius, radius2;
     int32_t ntri;
     int32_t depth;      // max leaf depth of the mesh BVH (stack bound)
-    int32_t pad;
+    int32_t attr;       // mesh: kAttr* bits of the per-corner data it carries
+    int32_t attr_base;  // mesh: its first record in DevScene::attr
+    int32_t pad[2];
+};
+
+// Per-corner mesh data of Triangle (Triangle.hpp:17-23), one record of
+// kAttrFloats floats per triangle of an attributed mesh, leaf order:
+// n0 n1 n2 (normalized), t0 t1 t2, tan0 tan1 tan2, w0 w1 w2, pad.
+enum : int32_t { kAttrNormals = 1, kAttrUV = 2, kAttrTangents = 4 };
+constexpr int kAttrFloats = 28;
+
+// A material texture (TextureUtils.hpp:9-18): 8-bit texels, row-major.
+struct DevTexture {
+    const uint8_t *data;
+    int32_t width, height, channels, pad;
 };
 
 struct alignas(16) DevMaterial {
@@ -85,7 +99,9 @@ struct alignas(16) DevMaterial {
     float roughness, metallic, ior;
     float emission[3];
     int32_t has_emission; // Material::hasEmission: |m_emission| > EPSILON
-    float pad[2];
+    // textures (index into DevScene::textures, -1 none): baseColorTex,
+    // metallicRoughnessTex, normalTex, emissiveTex (Material.hpp:45-48)
+    int32_t tex_base, tex_mr, tex_normal, tex_emissive;
 };
 
 struct DevCamera {
@@ -111,6 +127,9 @@ struct DevScene {
     const float *normals; // Triangle::normal per triangle, leaf order
     const DevObject *objects;
     const DevMaterial *materials;
+    const float *attr;            // per-corner records of attributed meshes
+    const DevTexture *textures;
+    int32_t n_textures;
     const int32_t *emissives; // Scene::emissives, in object order
     int32_t n_objects, n_materials, n_emissives;
     float total_emit_area;

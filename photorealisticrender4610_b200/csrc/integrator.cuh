@@ -12,7 +12,37 @@ struct Inter {
     bool hit;
     V3 p, n;
     int mat;
+    SurfAttr a;
 };
+
+// Triangle::finalize (Triangle.cpp:34-59) for meshes with per-corner data:
+// the hit's barycentrics (re-derived by the same Moller-Trumbore test the
+// traversal ran), w0 = 1 - u - v, interpolated uv, smooth normal and tangent
+// with its handedness.
+__device__ __forceinline__ void finalize_attr(const DevScene &S, const DevObject &o, int tri,
+                                              const RayD &r, V3 &n, SurfAttr &a) {
+    a = no_attr();
+    if (!o.attr)
+        return;
+    float t, u, v;
+    tri_hit(load_tri(S.tris, (uint32_t) tri), r, t, u, v);
+    const float w0 = 1.f - u - v;
+    const float *R = S.attr + (size_t) (o.attr_base + (tri - o.tri_base)) * kAttrFloats;
+    if (o.attr & kAttrUV) {
+        a.u = R[9] * w0 + R[11] * u + R[13] * v;
+        a.v = R[10] * w0 + R[12] * u + R[14] * v;
+    }
+    if (o.attr & kAttrNormals)
+        n = normalize(v3(R[0], R[1], R[2]) * w0 + v3(R[3], R[4], R[5]) * u +
+                      v3(R[6], R[7], R[8]) * v);
+    if (o.attr & kAttrTangents) {
+        a.tan = normalize(v3(R[15], R[16], R[17]) * w0 + v3(R[18], R[19], R[20]) * u +
+                          v3(R[21], R[22], R[23]) * v);
+        const float w = R[24] * w0 + R[25] * u + R[26] * v;
+        a.hand = w >= 0.f ? 1.f : -1.f;
+        a.has_tan = 1;
+    }
+}
 
 __device__ __forceinline__ Inter intersect(const DevScene &S, const Ray3 &ray, SmemStack &tst,
                                            SmemStack &bst) {
@@ -21,6 +51,7 @@ __device__ __forceinline__ Inter intersect(const DevScene &S, const Ray3 &ray, S
     const SceneHit h = scene_closest(S, r, p, tst, bst);
     Inter in;
     in.hit = h.obj >= 0;
+    in.a = no_attr();
     if (!in.hit) {
         in.p = in.n = v3(0.f);
         in.mat = -1;
@@ -33,6 +64,7 @@ __device__ __forceinline__ Inter intersect(const DevScene &S, const Ray3 &ray, S
         in.p = ray.o + h.t * ray.d;
         in.n = v3(S.normals[(size_t) h.tri * 3], S.normals[(size_t) h.tri * 3 + 1],
                   S.normals[(size_t) h.tri * 3 + 2]);
+        finalize_attr(S, o, h.tri, r, in.n, in.a);
     } else {
         // Sphere::getIntersection (Sphere.hpp:37-39)
         in.p = ray.o + ray.d * h.t;
@@ -90,7 +122,7 @@ static __device__ V3 cast_ray(const DevScene &S, Ray3 ray, int max_depth, float 
         const V3 gn = in.n;
         if (m.kind == kMatMirror || m.kind == kMatGlass) {
             // delta chain (Integrator.cpp:143-169)
-            const Shading sd = build_shading(m, gn);
+            const Shading sd = build_shading(S, m, gn, in.a);
             const BSDFSample bs = delta_sample(m, sd, -cur.d, rng);
             if (bs.pdf < 1e-6f)
                 break;
@@ -107,7 +139,7 @@ static __device__ V3 cast_ray(const DevScene &S, Ray3 ray, int max_depth, float 
         }
         specular = false;
         const V3 sn = dot(cur.d, gn) < 0.f ? gn : -gn;
-        const Shading sd = build_shading(m, sn);
+        const Shading sd = build_shading(S, m, sn, in.a);
         const V3 wo = -cur.d;
         const bool indirect = bounce > 0;
 

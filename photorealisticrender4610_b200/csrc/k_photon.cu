@@ -129,7 +129,7 @@ __global__ void k_photon_emit(DevScene S, EmitArgs a) {
         const float survival = smin(1.0f, max3(power));
         if (!(rng.next() < survival && depth < a.max_depth))
             break;
-        const Shading sd = build_shading(m, gn);
+        const Shading sd = build_shading(S, m, gn, hit.a);
         const V3 wo = -dir;
         const BSDFSample bs = diffuse_sample(m, sd, wo, rng);
         if (bs.pdf < 1e-6f)
@@ -450,7 +450,7 @@ __global__ void k_render_caustics(DevScene S, GridView v, CausticArgs a) {
             if (mt.kind == kMatEmissive)
                 break;
             if (mt.kind == kMatMirror || mt.kind == kMatGlass) {
-                const Shading sd = build_shading(mt, in.n);
+                const Shading sd = build_shading(S, mt, in.n, in.a);
                 const BSDFSample bs = delta_sample(mt, sd, -ray.d, rng);
                 beta = beta * bs.f / bs.pdf;
                 const bool trans = dot(bs.wi, in.n) < 0.f;
@@ -460,7 +460,10 @@ __global__ void k_render_caustics(DevScene S, GridView v, CausticArgs a) {
                 continue;
             }
             const V3 e = irradiance(v, in.p, a.k_nearest, a.k_nearest > 0 ? kd : nullptr, kc);
-            acc = acc + beta * (v3(mt.base[0], mt.base[1], mt.base[2]) / PRR_PI) * e;
+            const V3 albedo = mt.tex_base >= 0
+                                  ? sample_base_color(S.textures[mt.tex_base], in.a.u, in.a.v)
+                                  : v3(mt.base[0], mt.base[1], mt.base[2]);
+            acc = acc + beta * (albedo / PRR_PI) * e;
             break;
         }
     }

@@ -408,6 +408,26 @@ __global__ void k_scene_closest(DevScene S, const float *O, const float *D, int6
             nx = S.normals[(size_t) h.tri * 3 + 0];
             ny = S.normals[(size_t) h.tri * 3 + 1];
             nz = S.normals[(size_t) h.tri * 3 + 2];
+            if (o.attr & kAttrNormals) {
+                // Triangle::finalize (Triangle.cpp:44-47): normalize(n0*w0 + n1*u + n2*v)
+                float t, u, v;
+                tri_hit(load_tri(S.tris, (uint32_t) h.tri), r, t, u, v);
+                const float w0 = 1.f - u - v;
+                const float *R = S.attr + (size_t) (o.attr_base + (h.tri - o.tri_base)) * kAttrFloats;
+                float x = R[0] * w0 + R[3] * u + R[6] * v;
+                float y = R[1] * w0 + R[4] * u + R[7] * v;
+                float z = R[2] * w0 + R[5] * u + R[8] * v;
+                const float m2 = x * x + y * y + z * z;
+                if (m2 > 0) {
+                    const float inv = 1 / sqrtf(m2);
+                    x = x * inv;
+                    y = y * inv;
+                    z = z * inv;
+                }
+                nx = x;
+                ny = y;
+                nz = z;
+            }
         } else {
             out_prim[i] = 0;
             // normalize(coords - center) (Vector.hpp:103-111)

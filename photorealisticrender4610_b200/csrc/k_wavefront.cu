@@ -244,6 +244,7 @@ __device__ __forceinline__ Inter load_inter(const DevScene &S, const Wf &w, int 
     const int4 h = w.hit[p];
     Inter in;
     in.hit = h.x >= 0;
+    in.a = no_attr();
     if (!in.hit) {
         in.mat = -1;
         in.p = in.n = v3(0.f);
@@ -257,6 +258,7 @@ __device__ __forceinline__ Inter load_inter(const DevScene &S, const Wf &w, int 
         in.p = o + t * d;
         in.n = v3(S.normals[(size_t) h.y * 3], S.normals[(size_t) h.y * 3 + 1],
                   S.normals[(size_t) h.y * 3 + 2]);
+        finalize_attr(S, ob, h.y, RayD{o.x, o.y, o.z, d.x, d.y, d.z}, in.n, in.a);
     } else {
         in.p = o + d * t;
         in.n = normalize(in.p - v3(ob.cx, ob.cy, ob.cz));
@@ -352,6 +354,7 @@ __global__ void k_wf_miss(DevScene S, Wf w) {
         Inter in;
         in.hit = false;
         in.mat = -1;
+        in.a = no_attr();
         int it;
         bool spec;
         enter_iteration(S, w, p, in, rng, beta, L, it, spec);
@@ -380,7 +383,7 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
             } else {
                 const DevMaterial &m = S.materials[in.mat];
                 const V3 cd = ld3(w.rd, p);
-                const Shading sd = build_shading(m, in.n);
+                const Shading sd = build_shading(S, m, in.n, in.a);
                 const BSDFSample bs = delta_sample(m, sd, -cd, rng);
                 if (bs.pdf < 1e-6f) {
                     finish(w, p, L);
@@ -442,7 +445,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S, Wf w, int it_
                 const V3 cd = ld3(w.rd, p);
                 const V3 hp = in.p;
                 const V3 sn = dot(cd, in.n) < 0.f ? in.n : -in.n;
-                const Shading sd = build_shading(m, sn);
+                const Shading sd = build_shading(S, m, sn, in.a);
                 const V3 wo = -cd;
                 const bool indirect = it > 0;
                 // NEE towards emitters: the contribution is formed now and

@@ -54,12 +54,21 @@ struct DevBuf {
 struct HostMaterial {
     int kind;
     float params[9]; // baseColor[3], roughness, metallic, ior, emission[3]
+    int tex[4] = {-1, -1, -1, -1}; // base colour, metallic-roughness, normal, emissive
+};
+
+struct HostTexture {
+    int width = 0, height = 0, channels = 0;
+    std::vector<uint8_t> texels;
 };
 
 struct HostObject {
     int kind;          // kObjMesh / kObjSphere
     int material;
     std::vector<float> verts; // mesh: n x 9 input triangles
+    // mesh per-corner data (empty when absent): n x 9 normals, n x 6 uvs,
+    // n x 12 tangents (xyz + handedness w per corner)
+    std::vector<float> cnormals, cuvs, ctangents;
     float center[3] = {0, 0, 0};
     float radius = 0.f;
     // filled by build
@@ -90,6 +99,8 @@ struct Scene {
     size_t device_bytes = 0;
 
     DevBuf d_nodes, d_tris, d_verts, d_normals, d_objects, d_materials, d_emissives;
+    std::vector<HostTexture> textures;
+    DevBuf d_attr, d_texels, d_textures;
     DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin;
     DevBuf d_scratch;      // staging for host-buffer entry points
     DevBuf d_render, d_render_spp; // per-slice partial sums / adaptive spp

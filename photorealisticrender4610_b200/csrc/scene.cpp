@@ -139,6 +139,20 @@ DevCamera make_camera(const prr_camera &c, int width, int height) {
     return dc;
 }
 
+// normalize (Vector.hpp:103-111), float steps as the reference
+static void normalize3f(const float *v, float *out) {
+    const float m2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    out[0] = v[0];
+    out[1] = v[1];
+    out[2] = v[2];
+    if (m2 > 0) {
+        const float inv = 1 / sqrtf(m2);
+        out[0] = v[0] * inv;
+        out[1] = v[1] * inv;
+        out[2] = v[2] * inv;
+    }
+}
+
 int build_scene(Scene &s, cudaStream_t st) {
     // ---- per-mesh BVHs (independent; built concurrently) ----
     std::vector<int> meshes;
@@ -237,6 +251,20 @@ int build_scene(Scene &s, cudaStream_t st) {
                 ny = cy * inv;
                 nz = cz * inv;
             }
+            if (!o.cnormals.empty()) {
+                // GLTFLoader.cpp:236-241: corners normalized, the face normal
+                // replaced by normalize(n0 + n1 + n2)
+                float c[9], sum[3];
+                for (int q = 0; q < 3; q++)
+                    normalize3f(&o.cnormals[(size_t) id * 9 + q * 3], c + q * 3);
+                for (int a = 0; a < 3; a++)
+                    sum[a] = (c[a] + c[3 + a]) + c[6 + a];
+                float fn[3];
+                normalize3f(sum, fn);
+                nx = fn[0];
+                ny = fn[1];
+                nz = fn[2];
+            }
             normals[(size_t) (base + j) * 3 + 0] = nx;
             normals[(size_t) (base + j) * 3 + 1] = ny;
             normals[(size_t) (base + j) * 3 + 2] = nz;
@@ -246,6 +274,34 @@ int build_scene(Scene &s, cudaStream_t st) {
             return rc;
         blas_depth = std::max(blas_depth, o.bvh.max_depth);
         base += (int) nt;
+    }
+
+    // ---- per-corner records of attributed meshes, leaf order ----
+    std::vector<float> attr;
+    std::vector<int> attr_base(s.objects.size(), 0);
+    for (int k : meshes) {
+        const HostObject &o = s.objects[k];
+        if (o.cnormals.empty() && o.cuvs.empty() && o.ctangents.empty())
+            continue;
+        const int64_t nt = (int64_t) o.verts.size() / 9;
+        attr_base[k] = (int) (attr.size() / kAttrFloats);
+        const size_t at0 = attr.size();
+        attr.resize(at0 + (size_t) nt * kAttrFloats, 0.f);
+        for (int64_t j = 0; j < nt; j++) {
+            const int32_t id = o.bvh.ordered[j];
+            float *r = &attr[at0 + (size_t) j * kAttrFloats];
+            if (!o.cnormals.empty())
+                for (int q = 0; q < 3; q++)
+                    normalize3f(&o.cnormals[(size_t) id * 9 + q * 3], r + q * 3);
+            if (!o.cuvs.empty())
+                std::memcpy(r + 9, &o.cuvs[(size_t) id * 6], 6 * sizeof(float));
+            if (!o.ctangents.empty())
+                for (int q = 0; q < 3; q++) {
+                    std::memcpy(r + 15 + q * 3, &o.ctangents[(size_t) id * 12 + q * 4],
+                                3 * sizeof(float));
+                    r[24 + q] = o.ctangents[(size_t) id * 12 + q * 4 + 3];
+                }
+        }
     }
 
     // ---- scene BVH over objects, maxPrimsInNode 1 (Scene.cpp:17) ----
@@ -280,6 +336,9 @@ int build_scene(Scene &s, cudaStream_t st) {
                 d.root_box[q] = o.bvh.bounds[q];
             d.bvh_area = o.bvh.total_area;
             d.depth = o.bvh.max_depth;
+            d.attr = (o.cnormals.empty() ? 0 : kAttrNormals) | (o.cuvs.empty() ? 0 : kAttrUV) |
+                     (o.ctangents.empty() ? 0 : kAttrTangents);
+            d.attr_base = attr_base[k];
         } else {
             d.cx = o.center[0];
             d.cy = o.center[1];
@@ -310,7 +369,36 @@ int build_scene(Scene &s, cudaStream_t st) {
         d.emission[1] = p[7];
         d.emission[2] = p[8];
         d.has_emission = std::sqrt(p[6] * p[6] + p[7] * p[7] + p[8] * p[8]) > 1e-3f;
+        d.tex_base = s.materials[m].tex[0];
+        d.tex_mr = s.materials[m].tex[1];
+        d.tex_normal = s.materials[m].tex[2];
+        d.tex_emissive = s.materials[m].tex[3];
     }
+    // ---- textures: texels packed 16-byte aligned in one buffer ----
+    std::vector<size_t> tex_off(s.textures.size());
+    size_t tex_bytes = 0;
+    for (size_t t = 0; t < s.textures.size(); t++) {
+        tex_off[t] = tex_bytes;
+        tex_bytes += (s.textures[t].texels.size() + 15) & ~size_t(15);
+    }
+    std::vector<uint8_t> texels(tex_bytes);
+    for (size_t t = 0; t < s.textures.size(); t++)
+        std::memcpy(texels.data() + tex_off[t], s.textures[t].texels.data(),
+                    s.textures[t].texels.size());
+    if (int rc = upload(s.d_texels, texels))
+        return rc;
+    std::vector<DevTexture> dtex(s.textures.size());
+    for (size_t t = 0; t < s.textures.size(); t++) {
+        dtex[t].data = s.d_texels.as<uint8_t>() + tex_off[t];
+        dtex[t].width = s.textures[t].width;
+        dtex[t].height = s.textures[t].height;
+        dtex[t].channels = s.textures[t].channels;
+        dtex[t].pad = 0;
+    }
+    if (int rc = upload(s.d_textures, dtex))
+        return rc;
+    if (int rc = upload(s.d_attr, attr))
+        return rc;
 
     if (int rc = upload(s.d_nodes, nodes))
         return rc;
@@ -335,6 +423,9 @@ int build_scene(Scene &s, cudaStream_t st) {
     D.normals = s.d_normals.as<float>();
     D.objects = s.d_objects.as<DevObject>();
     D.materials = s.d_materials.as<DevMaterial>();
+    D.attr = s.d_attr.as<float>();
+    D.textures = s.d_textures.as<DevTexture>();
+    D.n_textures = (int32_t) s.textures.size();
     D.emissives = s.d_emissives.as<int32_t>();
     D.n_objects = (int32_t) s.objects.size();
     D.n_materials = (int32_t) s.materials.size();
@@ -383,7 +474,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     PRR_CUDA_TRY(s.d_counter.alloc(64));
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     s.n_tris = ntri;
-    s.device_bytes = s.d_nodes.bytes + s.d_tris.bytes + s.d_verts.bytes + s.d_normals.bytes +
+    s.device_bytes = s.d_attr.bytes + s.d_texels.bytes + s.d_textures.bytes +
+                     s.d_nodes.bytes + s.d_tris.bytes + s.d_verts.bytes + s.d_normals.bytes +
                      s.d_objects.bytes + s.d_materials.bytes + s.d_emissives.bytes +
                      s.d_env_px.bytes + s.d_env_cdf.bytes + s.d_env_marginal.bytes;
     s.built = true;
@@ -451,6 +543,74 @@ int prr_scene_add_mesh(prr_scene *scene, const float *verts, int64_t ntri, int m
     s->objects.push_back(std::move(o));
     if (out_object)
         *out_object = (int) s->objects.size() - 1;
+    return PRR_OK;
+}
+
+int prr_scene_add_mesh_attr(prr_scene *scene, const float *verts, const float *normals,
+                            const float *uvs, const float *tangents, int64_t ntri, int material,
+                            int *out_object) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    Scene *s = S(scene);
+    {
+        std::lock_guard<std::mutex> g(s->mu);
+        if (s->built)
+            return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    }
+    int obj = -1;
+    if (int rc = prr_scene_add_mesh(scene, verts, ntri, material, &obj))
+        return rc;
+    std::lock_guard<std::mutex> g(s->mu);
+    HostObject &o = s->objects[obj];
+    if (normals)
+        o.cnormals.assign(normals, normals + ntri * 9);
+    if (uvs)
+        o.cuvs.assign(uvs, uvs + ntri * 6);
+    if (tangents)
+        o.ctangents.assign(tangents, tangents + ntri * 12);
+    if (out_object)
+        *out_object = obj;
+    return PRR_OK;
+}
+
+int prr_scene_add_texture(prr_scene *scene, const uint8_t *texels, int width, int height,
+                          int channels, int *out_texture) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    if (!texels || width <= 0 || height <= 0 || channels < 3 || channels > 4 ||
+        (int64_t) width * height > (int64_t) 1 << 28)
+        return fail(PRR_ERR_INVALID_ARGUMENT,
+                    "texture needs texels, a positive size and 3 or 4 channels");
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    HostTexture t;
+    t.width = width;
+    t.height = height;
+    t.channels = channels;
+    t.texels.assign(texels, texels + (size_t) width * height * channels);
+    s->textures.push_back(std::move(t));
+    if (out_texture)
+        *out_texture = (int) s->textures.size() - 1;
+    return PRR_OK;
+}
+
+int prr_scene_set_material_textures(prr_scene *scene, int material, int base_color,
+                                    int metallic_roughness, int normal, int emissive) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->built)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene already built");
+    if (material < 0 || material >= (int) s->materials.size())
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown material");
+    const int ids[4] = {base_color, metallic_roughness, normal, emissive};
+    for (int t : ids)
+        if (t < -1 || t >= (int) s->textures.size())
+            return fail(PRR_ERR_INVALID_ARGUMENT, "unknown texture");
+    std::memcpy(s->materials[material].tex, ids, sizeof(ids));
     return PRR_OK;
 }
 

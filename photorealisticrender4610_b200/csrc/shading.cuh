@@ -227,20 +227,123 @@ __device__ __forceinline__ float fresnel(V3 I, V3 N, float ior) { // :247-260
     return (Rs * Rs + Rp * Rp) * 0.5f;
 }
 
+// ---------------------------------------------------------------- textures
+// TextureUtils.hpp:22-136: bilinear with wrap-around on 8-bit texels.
+__device__ __forceinline__ void uv_to_texel(float u, float v, int w, int h, int &x0, int &y0,
+                                            int &x1, int &y1, float &fx, float &fy) {
+    u = u - floorf(u);
+    v = v - floorf(v);
+    const float px = u * (float) w;
+    const float py = v * (float) h;
+    x0 = (int) px % w;
+    y0 = (int) py % h;
+    x1 = (x0 + 1) % w;
+    y1 = (y0 + 1) % h;
+    fx = px - floorf(px);
+    fy = py - floorf(py);
+}
+__device__ __forceinline__ float texel(const DevTexture &t, int x, int y, int c) {
+    return (float) t.data[(y * t.width + x) * t.channels + c] / 255.f;
+}
+__device__ __forceinline__ V3 fetch_rgb(const DevTexture &t, int x, int y) {
+    return v3(texel(t, x, y, 0), texel(t, x, y, 1), texel(t, x, y, 2));
+}
+__device__ __forceinline__ V3 bilerp(V3 c00, V3 c10, V3 c01, V3 c11, float fx, float fy) {
+    const V3 top = c00 + (c10 - c00) * fx;
+    const V3 bottom = c01 + (c11 - c01) * fx;
+    return top + (bottom - top) * fy;
+}
+__device__ __forceinline__ float srgb_to_linear(float x) {
+    x = smax(0.f, x);
+    return x <= 0.04045f ? x / 12.92f : powf((x + 0.055f) / 1.055f, 2.4f);
+}
+// sampleBaseColor (TextureUtils.hpp:76-88)
+__device__ __forceinline__ V3 sample_base_color(const DevTexture &t, float u, float v) {
+    int x0, y0, x1, y1;
+    float fx, fy;
+    uv_to_texel(u, v, t.width, t.height, x0, y0, x1, y1, fx, fy);
+    const V3 c = bilerp(fetch_rgb(t, x0, y0), fetch_rgb(t, x1, y0), fetch_rgb(t, x0, y1),
+                        fetch_rgb(t, x1, y1), fx, fy);
+    return v3(srgb_to_linear(c.x), srgb_to_linear(c.y), srgb_to_linear(c.z));
+}
+// sampleNormalMap (TextureUtils.hpp:90-106)
+__device__ __forceinline__ V3 sample_normal_map(const DevTexture &t, float u, float v) {
+    int x0, y0, x1, y1;
+    float fx, fy;
+    uv_to_texel(u, v, t.width, t.height, x0, y0, x1, y1, fx, fy);
+    auto fetch = [&](int x, int y) {
+        return v3(texel(t, x, y, 0) * 2.f - 1.f, texel(t, x, y, 1) * 2.f - 1.f,
+                  texel(t, x, y, 2) * 2.f - 1.f);
+    };
+    return normalize(bilerp(fetch(x0, y0), fetch(x1, y0), fetch(x0, y1), fetch(x1, y1), fx, fy));
+}
+// sampleMetallicRoughness (TextureUtils.hpp:108-126): (G = roughness, B = metallic)
+__device__ __forceinline__ void sample_mr(const DevTexture &t, float u, float v, float &rough,
+                                          float &metal) {
+    int x0, y0, x1, y1;
+    float fx, fy;
+    uv_to_texel(u, v, t.width, t.height, x0, y0, x1, y1, fx, fy);
+    auto lerp = [](float a, float b, float s) { return a + (b - a) * s; };
+    const float r0 = lerp(texel(t, x0, y0, 1), texel(t, x1, y0, 1), fx);
+    const float r1 = lerp(texel(t, x0, y1, 1), texel(t, x1, y1, 1), fx);
+    const float m0 = lerp(texel(t, x0, y0, 2), texel(t, x1, y0, 2), fx);
+    const float m1 = lerp(texel(t, x0, y1, 2), texel(t, x1, y1, 2), fx);
+    rough = lerp(r0, r1, fy);
+    metal = lerp(m0, m1, fy);
+}
+
 // ---------------------------------------------------------------- materials
-// ShadingData for untextured materials (Material.cpp:3-26 with every texture
-// lookup on its fallback): N = Ng, roughness floored at 0.08.
+// Interpolated surface data of a hit (Intersection::tcoords, tangent,
+// tangentHandedness, hasTangent; Intersection.hpp:26-30).
+struct SurfAttr {
+    float u, v;
+    V3 tan;
+    float hand;
+    int has_tan;
+};
+__device__ __forceinline__ SurfAttr no_attr() { return SurfAttr{0.f, 0.f, v3(0.f), 1.f, 0}; }
+
+// ShadingData (Material.cpp:3-26 and the glTF-tangent overload of
+// Material.hpp:57-70): the frame T, B from the hit's tangent (Gram-Schmidt
+// against Ng, B = cross(Ng, T) * handedness) or from buildTBN(Ng); base
+// colour and metallic / roughness from their textures or factors, roughness
+// floored at 0.08; N from the normal map in that frame, else Ng. The BSDF
+// frame is buildTBN(N), as toLocal / toWorld build it (BRDFUtils.hpp:35-49).
 struct Shading {
     Frame f;
     V3 base;
     float roughness, metallic;
 };
-__device__ __forceinline__ Shading build_shading(const DevMaterial &m, V3 Ng) {
+__device__ __forceinline__ Shading build_shading(const DevScene &S, const DevMaterial &m, V3 Ng,
+                                                 const SurfAttr &a) {
     Shading sd;
-    sd.f = build_tbn(Ng);
-    sd.base = v3(m.base[0], m.base[1], m.base[2]);
-    sd.roughness = smax(m.roughness, 0.08f);
-    sd.metallic = m.metallic;
+    sd.base = m.tex_base >= 0 ? sample_base_color(S.textures[m.tex_base], a.u, a.v)
+                              : v3(m.base[0], m.base[1], m.base[2]);
+    float rough = m.roughness, metal = m.metallic;
+    if (m.tex_mr >= 0)
+        sample_mr(S.textures[m.tex_mr], a.u, a.v, rough, metal);
+    sd.roughness = smax(rough, 0.08f);
+    sd.metallic = metal;
+    V3 N = Ng;
+    if (m.tex_normal >= 0) {
+        Frame tb;
+        bool basis = false;
+        if (a.has_tan) {
+            const V3 tg = normalize(a.tan);
+            const V3 T = tg - dot(Ng, tg) * Ng;
+            const float tlen = sqrtf(T.x * T.x + T.y * T.y + T.z * T.z);
+            if (!(tlen < 1e-6f)) {
+                tb.T = T / tlen;
+                tb.B = cross(Ng, tb.T) * a.hand;
+                basis = true;
+            }
+        }
+        if (!basis)
+            tb = build_tbn(Ng);
+        const V3 tn = sample_normal_map(S.textures[m.tex_normal], a.u, a.v);
+        N = normalize(tn.x * tb.T + tn.y * tb.B + tn.z * Ng);
+    }
+    sd.f = build_tbn(N);
     return sd;
 }
 

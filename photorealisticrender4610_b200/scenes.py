@@ -41,10 +41,19 @@ class Material:
     metallic: float = 0.0
     ior: float = 1.5
     emission: tuple = (0.0, 0.0, 0.0)
+    # textures, (h, w, 3 or 4) uint8 (Material.hpp:45-48)
+    base_color_tex: Optional[np.ndarray] = None
+    metallic_roughness_tex: Optional[np.ndarray] = None
+    normal_tex: Optional[np.ndarray] = None
+    emissive_tex: Optional[np.ndarray] = None
 
     def params(self) -> np.ndarray:
         return np.array([*self.base_color, self.roughness, self.metallic, self.ior,
                          *self.emission], np.float32)
+
+    def texture_list(self) -> list:
+        return [self.base_color_tex, self.metallic_roughness_tex, self.normal_tex,
+                self.emissive_tex]
 
 
 @dataclass
@@ -52,6 +61,13 @@ class MeshObject:
     verts: np.ndarray  # (n, 9) float32: v0, v1, v2 per triangle
     material: int
     kind: str = "mesh"
+    # per-corner data (Triangle.hpp:17-23), None when absent
+    normals: Optional[np.ndarray] = None   # (n, 9)
+    uvs: Optional[np.ndarray] = None       # (n, 6)
+    tangents: Optional[np.ndarray] = None  # (n, 12): xyz + handedness per corner
+
+    def has_attributes(self) -> bool:
+        return self.normals is not None or self.uvs is not None or self.tangents is not None
 
 
 @dataclass
@@ -278,6 +294,106 @@ def cornell_box(width: int = 256, height: int = 256) -> SceneDesc:
     s.objects.append(SphereObject((0.45, -0.7, 0.3), 0.3, white))
     s.camera = Camera(eye=(0.0, 0.0, 3.5), target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0),
                       fovv=40.0, fovh=40.0)
+    return s
+
+
+def checker_texture(n: int = 64, cells: int = 8, a=(220, 200, 160), b=(40, 60, 110),
+                    channels: int = 3) -> np.ndarray:
+    """An n x n sRGB checkerboard, (n, n, channels) uint8."""
+    i = np.arange(n)
+    mask = ((i[:, None] * cells // n + i[None, :] * cells // n) % 2).astype(bool)
+    img = np.where(mask[..., None], np.array(a, np.uint8), np.array(b, np.uint8))
+    if channels == 4:
+        img = np.concatenate([img, np.full((n, n, 1), 255, np.uint8)], -1)
+    return np.ascontiguousarray(img)
+
+
+def bump_normal_map(n: int = 64, waves: float = 4.0, amp: float = 0.35) -> np.ndarray:
+    """A tangent-space normal map of sine ripples, encoded (n*0.5+0.5)*255."""
+    x = (np.arange(n) + 0.5) / n * 2 * math.pi * waves
+    dx = amp * np.cos(x)[None, :].repeat(n, 0)
+    dy = amp * np.cos(x)[:, None].repeat(n, 1)
+    nrm = np.stack([-dx, -dy, np.ones_like(dx)], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    return np.clip(np.round((nrm * 0.5 + 0.5) * 255), 0, 255).astype(np.uint8)
+
+
+def metal_rough_map(n: int = 32) -> np.ndarray:
+    """glTF metallic-roughness texels: G = roughness ramp, B = metallic stripes."""
+    img = np.zeros((n, n, 4), np.uint8)
+    img[..., 1] = np.linspace(20, 240, n, dtype=np.float64)[None, :].round().astype(np.uint8)
+    img[..., 2] = np.where((np.arange(n) // 4) % 2 == 0, 230, 10)[:, None].astype(np.uint8)
+    img[..., 3] = 255
+    return img
+
+
+def uv_sphere_attrs(tri: np.ndarray):
+    """Per-corner normals, spherical uvs and tangents (d/dphi, w = +1) of a
+    unit-sphere triangle soup (n, 3, 3)."""
+    n = tri / np.linalg.norm(tri, axis=-1, keepdims=True)
+    phi = np.arctan2(n[..., 2], n[..., 0])
+    u = phi / (2 * math.pi) + 0.5
+    v = np.arccos(np.clip(n[..., 1], -1, 1)) / math.pi
+    # keep a triangle's u on one side of the seam
+    span = u.max(1, keepdims=True) - u.min(1, keepdims=True)
+    u = np.where((span > 0.5) & (u < 0.5), u + 1.0, u)
+    tan = np.stack([-np.sin(phi), np.zeros_like(phi), np.cos(phi)], -1)
+    tan = np.concatenate([tan, np.ones(phi.shape + (1,))], -1)
+    return (n.reshape(-1, 9).astype(np.float32), np.stack([u, v], -1).reshape(-1, 6).astype(
+        np.float32), tan.reshape(-1, 12).astype(np.float32))
+
+
+def textured_showcase(width: int = 320, height: int = 240, env_size=(256, 128)) -> SceneDesc:
+    """Per-corner data and textures on the path: a floor grid (uv tiling,
+    tangents, base-colour checker, metallic-roughness map, ripple normal map),
+    a smooth-shaded icosphere (interpolated normals, spherical uvs, tangents,
+    checker and normal map), a glass sphere over it, a quad light and a sky."""
+    s = SceneDesc(width=width, height=height, name="textured")
+    floor_m = s.add_material(Material(DIFFUSE, (1.0, 1.0, 1.0), 0.6, 0.0,
+                                      base_color_tex=checker_texture(64, 8),
+                                      metallic_roughness_tex=metal_rough_map(32),
+                                      normal_tex=bump_normal_map(64, 4.0)))
+    ball_m = s.add_material(Material(DIFFUSE, (1.0, 1.0, 1.0), 0.35, 0.3,
+                                     base_color_tex=checker_texture(
+                                         32, 6, (200, 60, 50), (240, 230, 200), channels=4),
+                                     normal_tex=bump_normal_map(32, 6.0, 0.25)))
+    glass = s.add_material(Material(GLASS, (0.95, 1.0, 0.97), 0.0, 0.0, 1.5))
+    le = 12.0
+    light = s.add_material(Material(EMISSIVE, (0.8, 0.8, 0.8), 0.5, 0.0, 1.5, (le, le, le)))
+    # floor: a 6 x 6 grid of quads on y = 0, uvs tiled 3x, tangent +x
+    g = np.linspace(-3.0, 3.0, 7)
+    tris, uvs = [], []
+    for i in range(6):
+        for j in range(6):
+            a = (g[i], 0.0, g[j + 1])
+            b = (g[i + 1], 0.0, g[j + 1])
+            c = (g[i + 1], 0.0, g[j])
+            d = (g[i], 0.0, g[j])
+            ua = [(x + 3) / 2.0 for x in (a[0], a[2])]
+            ub = [(x + 3) / 2.0 for x in (b[0], b[2])]
+            uc = [(x + 3) / 2.0 for x in (c[0], c[2])]
+            ud = [(x + 3) / 2.0 for x in (d[0], d[2])]
+            tris += [a + b + c, a + c + d]
+            uvs += [ua + ub + uc, ua + uc + ud]
+    fv = np.array(tris, np.float32)
+    nf = len(fv)
+    s.objects.append(MeshObject(fv, floor_m,
+                                normals=np.tile(np.array([0, 1, 0] * 3, np.float32), (nf, 1)),
+                                uvs=np.array(uvs, np.float32),
+                                tangents=np.tile(np.array([1, 0, 0, 1] * 3, np.float32),
+                                                 (nf, 1))))
+    ico = icosphere(3)
+    nrm, uv, tan = uv_sphere_attrs(ico)
+    center, r = np.array([-0.8, 0.9, 0.2]), 0.9
+    s.objects.append(MeshObject((ico * r + center).reshape(-1, 9).astype(np.float32), ball_m,
+                                normals=nrm, uvs=uv, tangents=tan))
+    s.objects.append(SphereObject((1.1, 0.7, 0.6), 0.7, glass))
+    y = 3.2
+    s.objects.append(MeshObject(quad((-0.6, y, -0.6), (0.6, y, -0.6), (0.6, y, 0.6),
+                                     (-0.6, y, 0.6)), light))
+    s.env = procedural_sky(*env_size)
+    s.camera = Camera(eye=(0.0, 2.2, 5.0), target=(0.0, 0.6, 0.0), up=(0.0, 1.0, 0.0),
+                      fovv=45.0, fovh=50.0)
     return s
 
 
