@@ -48,6 +48,12 @@ extern "C" {
 #define PRR_MAT_MIRROR 2
 #define PRR_MAT_GLASS 3
 
+/* MaterialType of GLTFLoader::load (GLTFLoader.hpp:10) */
+#define PRR_GLTF_DIFFUSE 0
+#define PRR_GLTF_GLASS 1
+#define PRR_GLTF_MIRROR 2
+#define PRR_GLTF_EMIT 3
+
 typedef struct prr_scene prr_scene;
 typedef struct prr_photon_map prr_photon_map;
 
@@ -163,6 +169,29 @@ int prr_scene_add_texture(prr_scene *scene, const uint8_t *texels, int width, in
  * data is built (Material.cpp:3-26). */
 int prr_scene_set_material_textures(prr_scene *scene, int material, int base_color,
                                     int metallic_roughness, int normal, int emissive);
+/* GLTFLoader::load(path, type, override) + Scene::Add of every mesh it returns
+ * (GLTFLoader.cpp:140-281): a .glb, or a .gltf with external or base64
+ * buffers; one mesh per triangle primitive with its per-corner normals, uvs and
+ * tangents; a new material per primitive from the glTF material recast to
+ * `material_type` (PRR_GLTF_*), or `override_material` (>= 0) for all; PNG
+ * textures decoded to 8-bit RGBA. Node transforms are not applied (the
+ * reference reads primitives in mesh space). out_first / out_count: the objects
+ * added; out_undecoded: images left out (JPEG, interlaced PNG). Primitives
+ * without triangles add nothing. */
+int prr_scene_add_gltf(prr_scene *scene, const char *path, int material_type,
+                       int override_material, int *out_first, int *out_count, int *out_undecoded);
+/* Host-side view of a mesh as added (before or after the build): ntri, the
+ * kinds of per-corner data it carries (1 normals, 2 uvs, 4 tangents), and, for
+ * non-NULL arrays, its triangles (ntri x 9), normalized corner normals (ntri x
+ * 9), uvs (ntri x 6) and tangents (ntri x 12), in input order. */
+int prr_scene_export_mesh(const prr_scene *scene, int object, int64_t *out_ntri, int *out_attr,
+                          float *verts, float *normals, float *uvs, float *tangents);
+/* A material as added: kind, params[9] and its four texture ids (-1 none). */
+int prr_scene_export_material(const prr_scene *scene, int material, int *out_kind,
+                              float params[9], int textures[4]);
+/* A texture as added: size, channels and (texels non-NULL) its texels. */
+int prr_scene_export_texture(const prr_scene *scene, int texture, int *out_width,
+                             int *out_height, int *out_channels, uint8_t *texels);
 /* Sphere(center, radius, mat) (Sphere.hpp:14-16) + Scene::Add. */
 int prr_scene_add_sphere(prr_scene *scene, const float center[3], float radius, int material,
                          int *out_object);

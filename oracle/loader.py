@@ -208,6 +208,14 @@ class ReferenceOracle:
         L.prr_ref_scene_add_material.argtypes = [vp, C.c_int, _f32p]
         L.prr_ref_scene_add_mesh.restype = C.c_int
         L.prr_ref_scene_add_mesh.argtypes = [vp, _f32p, C.c_int64, C.c_int]
+        L.prr_ref_scene_add_gltf.restype = C.c_int
+        L.prr_ref_scene_add_gltf.argtypes = [vp, C.c_char_p, C.c_int]
+        L.prr_ref_scene_export_mesh.restype = C.c_int64
+        L.prr_ref_scene_export_mesh.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
+        L.prr_ref_scene_export_material.restype = C.c_int
+        L.prr_ref_scene_export_material.argtypes = [vp, C.c_int, vp, vp, vp]
+        L.prr_ref_scene_export_texture.restype = C.c_int
+        L.prr_ref_scene_export_texture.argtypes = [vp, C.c_int, C.c_int, vp]
         L.prr_ref_scene_add_mesh_attr.restype = C.c_int
         L.prr_ref_scene_add_mesh_attr.argtypes = [vp, _f32p, vp, vp, vp, C.c_int64, C.c_int]
         L.prr_ref_scene_set_texture.restype = C.c_int
@@ -537,3 +545,51 @@ class RefScene:
         finally:
             L.prr_ref_photon_free(ph)
         return rec, owner
+
+
+class RefGltf:
+    """Meshes and materials as the reference's GLTFLoader::load builds them
+    (oracle build), for comparing ingest field by field."""
+
+    TYPES = {"diffuse": 0, "glass": 1, "mirror": 2, "emit": 3}
+
+    def __init__(self, ref: ReferenceOracle, path, material_type="diffuse"):
+        self.ref = ref
+        self.h = ref.L.prr_ref_scene_new()
+        self.count = ref.L.prr_ref_scene_add_gltf(self.h, str(path).encode(),
+                                                  self.TYPES[material_type])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.L.prr_ref_scene_free(self.h)
+            self.h = None
+
+    def mesh(self, k):
+        L = self.ref.L
+        attr = C.c_int()
+        n = L.prr_ref_scene_export_mesh(self.h, k, C.byref(attr), None, None, None, None)
+        out = {"verts": np.empty((n, 9), np.float32), "normals": np.empty((n, 9), np.float32),
+               "uvs": np.empty((n, 6), np.float32), "tangents": np.empty((n, 12), np.float32)}
+        L.prr_ref_scene_export_mesh(self.h, k, None, out["verts"].ctypes.data,
+                                    out["normals"].ctypes.data, out["uvs"].ctypes.data,
+                                    out["tangents"].ctypes.data)
+        out["attr"] = attr.value
+        return out
+
+    def material(self, k):
+        L = self.ref.L
+        kind = C.c_int()
+        p = np.empty(9, np.float32)
+        dims = np.zeros(16, np.int32)
+        L.prr_ref_scene_export_material(self.h, k, C.byref(kind), p.ctypes.data, dims.ctypes.data)
+        tex = []
+        for slot in range(4):
+            w, h, c, nbytes = (int(x) for x in dims[slot * 4: slot * 4 + 4])
+            if w == 0:
+                tex.append(None)
+                continue
+            t = np.empty(nbytes, np.uint8)
+            L.prr_ref_scene_export_texture(self.h, k, slot, t.ctypes.data)
+            tex.append(t.reshape(h, w, -1) if nbytes % (w * h) == 0 else t)
+        
+        return {"kind": kind.value, "params": p, "textures": tex}

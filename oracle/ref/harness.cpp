@@ -43,6 +43,8 @@
 #include <vector>
 #include <omp.h>
 
+#include "GLTFLoader.hpp"
+
 // Private members needed by the oracle: BVHAccel's flattened nodes (to diff
 // the device tree node for node) and PhotonMap::trace (to key each photon's RNG
 // stream by its index).
@@ -374,6 +376,108 @@ int prr_ref_scene_set_texture(void *h, int mat, int slot, const uint8_t *texels,
     t->width = w;
     t->height = hgt;
     t->channels = channels;
+    return 0;
+}
+
+// GLTFLoader::load(path, type) + Scene::Add of every mesh it returns (the
+// reference's own ingest, main scene files' usage).
+int prr_ref_scene_add_gltf(void *h, const char *path, int type) {
+    RefScene *rs = (RefScene *) h;
+    std::vector<MeshTriangle *> meshes = GLTFLoader::load(path, (MaterialType) type);
+    for (MeshTriangle *m : meshes) {
+        rs->scene.Add(m);
+        rs->objects.push_back(m);
+        rs->object_kind.push_back(0);
+        rs->materials.push_back(m->m);
+    }
+    return (int) meshes.size();
+}
+
+// A mesh object's triangles as the reference holds them: v0 v1 v2, n0 n1 n2,
+// t0 t1 t2, tan0..2 with handedness; attr bit 1 = smooth normals, 4 = tangents.
+int64_t prr_ref_scene_export_mesh(void *h, int obj, int *attr, float *verts, float *normals,
+                                  float *uvs, float *tangents) {
+    RefScene *rs = (RefScene *) h;
+    MeshTriangle *mt = dynamic_cast<MeshTriangle *>(rs->objects.at(obj));
+    if (!mt)
+        return -1;
+    int a = 0;
+    const int64_t n = (int64_t) mt->triangles.size();
+    for (int64_t i = 0; i < n; i++) {
+        const Triangle &t = mt->triangles[i];
+        a |= (t.hasSmoothNormals ? 1 : 0) | (t.hasTangents ? 4 : 0);
+        const Vector3f *p[3] = {&t.v0, &t.v1, &t.v2};
+        const Vector3f *nn[3] = {&t.n0, &t.n1, &t.n2};
+        const Vector2f *uv[3] = {&t.t0, &t.t1, &t.t2};
+        const Vector3f *tg[3] = {&t.tan0, &t.tan1, &t.tan2};
+        const float tw[3] = {t.tangentW0, t.tangentW1, t.tangentW2};
+        for (int q = 0; q < 3; q++) {
+            if (verts) {
+                verts[i * 9 + q * 3] = p[q]->x;
+                verts[i * 9 + q * 3 + 1] = p[q]->y;
+                verts[i * 9 + q * 3 + 2] = p[q]->z;
+            }
+            if (normals) {
+                normals[i * 9 + q * 3] = nn[q]->x;
+                normals[i * 9 + q * 3 + 1] = nn[q]->y;
+                normals[i * 9 + q * 3 + 2] = nn[q]->z;
+            }
+            if (uvs) {
+                uvs[i * 6 + q * 2] = uv[q]->x;
+                uvs[i * 6 + q * 2 + 1] = uv[q]->y;
+            }
+            if (tangents) {
+                tangents[i * 12 + q * 4] = tg[q]->x;
+                tangents[i * 12 + q * 4 + 1] = tg[q]->y;
+                tangents[i * 12 + q * 4 + 2] = tg[q]->z;
+                tangents[i * 12 + q * 4 + 3] = tw[q];
+            }
+        }
+    }
+    if (attr)
+        *attr = a;
+    return n;
+}
+
+// The material of a mesh object: kind (0 diffuse, 1 emissive, 2 mirror, 3
+// glass), params[9], and per texture slot (base colour, metallic-roughness,
+// normal, emissive) its width, height, channels and byte count (zeros when
+// empty; a 16-bit emissive image keeps 2 bytes per sample).
+int prr_ref_scene_export_material(void *h, int obj, int *kind, float *params, int *tex_dims) {
+    RefScene *rs = (RefScene *) h;
+    MeshTriangle *mt = dynamic_cast<MeshTriangle *>(rs->objects.at(obj));
+    if (!mt)
+        return -1;
+    const Material *m = mt->m;
+    *kind = dynamic_cast<const EmissiveMaterial *>(m) ? 1
+            : dynamic_cast<const MirrorMaterial *>(m) ? 2
+            : dynamic_cast<const GlassMaterial *>(m)  ? 3
+                                                      : 0;
+    const float p[9] = {m->baseColor.x, m->baseColor.y, m->baseColor.z, m->roughness,
+                        m->metallic,    m->ior,         m->m_emission.x, m->m_emission.y,
+                        m->m_emission.z};
+    std::memcpy(params, p, sizeof(p));
+    const Texture *t[4] = {&m->baseColorTex, &m->metallicRoughnessTex, &m->normalTex,
+                           &m->emissiveTex};
+    for (int k = 0; k < 4; k++) {
+        const bool e = t[k]->empty();
+        tex_dims[k * 4] = e ? 0 : t[k]->width;
+        tex_dims[k * 4 + 1] = e ? 0 : t[k]->height;
+        tex_dims[k * 4 + 2] = e ? 0 : t[k]->channels;
+        tex_dims[k * 4 + 3] = e ? 0 : (int) t[k]->data.size();
+    }
+    return 0;
+}
+
+int prr_ref_scene_export_texture(void *h, int obj, int slot, uint8_t *texels) {
+    RefScene *rs = (RefScene *) h;
+    MeshTriangle *mt = dynamic_cast<MeshTriangle *>(rs->objects.at(obj));
+    if (!mt || slot < 0 || slot > 3)
+        return -1;
+    const Material *m = mt->m;
+    const Texture *t[4] = {&m->baseColorTex, &m->metallicRoughnessTex, &m->normalTex,
+                           &m->emissiveTex};
+    std::memcpy(texels, t[slot]->data.data(), t[slot]->data.size());
     return 0;
 }
 

@@ -96,6 +96,13 @@ _SIGS = {
                                         C.POINTER(C.c_int)]),
     "prr_scene_set_material_textures": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int,
                                                   C.c_int]),
+    "prr_scene_add_gltf": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "prr_scene_export_mesh": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
+                                        _vp, _vp, _vp, _vp]),
+    "prr_scene_export_material": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), _vp, _vp]),
+    "prr_scene_export_texture": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int), _vp]),
     "prr_scene_add_sphere": (C.c_int, [_vp, C.POINTER(C.c_float), C.c_float, C.c_int,
                                        C.POINTER(C.c_int)]),
     "prr_scene_set_background": (C.c_int, [_vp, C.POINTER(C.c_float)]),

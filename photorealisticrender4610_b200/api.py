@@ -78,6 +78,7 @@ class Scene:
         self.h = h
         self.objects = []
         self.desc = None
+        self.size = None  # (width, height) of the camera, set by set_camera
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -131,6 +132,59 @@ class Scene:
         check(self.lib.prr_scene_set_material_textures(self.h, material, base_color,
                                                        metallic_roughness, normal, emissive))
 
+    GLTF_TYPES = {"diffuse": 0, "glass": 1, "mirror": 2, "emit": 3}
+
+    def add_gltf(self, path: str, material_type: str = "diffuse",
+                 override_material: int = -1) -> dict:
+        """GLTFLoader::load + Scene::Add for every primitive: returns the first
+        object added, how many, and how many images could not be decoded."""
+        first, count, und = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.prr_scene_add_gltf(self.h, str(path).encode(),
+                                          self.GLTF_TYPES[material_type], override_material,
+                                          C.byref(first), C.byref(count), C.byref(und)))
+        for k in range(count.value):
+            nt = C.c_int64()
+            check(self.lib.prr_scene_export_mesh(self.h, first.value + k, C.byref(nt), None,
+                                                 None, None, None, None))
+            self.objects.append(("mesh", nt.value))
+        return {"first": first.value, "count": count.value, "undecoded_images": und.value}
+
+    def export_mesh(self, obj: int) -> dict:
+        """The mesh as added (host side): triangles and per-corner data."""
+        nt, attr = C.c_int64(), C.c_int()
+        check(self.lib.prr_scene_export_mesh(self.h, obj, C.byref(nt), C.byref(attr), None, None,
+                                             None, None))
+        n = nt.value
+        out = {"verts": np.empty((n, 9), np.float32)}
+        if attr.value & 1:
+            out["normals"] = np.empty((n, 9), np.float32)
+        if attr.value & 2:
+            out["uvs"] = np.empty((n, 6), np.float32)
+        if attr.value & 4:
+            out["tangents"] = np.empty((n, 12), np.float32)
+        ptr = lambda k: C.c_void_p(out[k].ctypes.data) if k in out else None  # noqa: E731
+        check(self.lib.prr_scene_export_mesh(self.h, obj, None, None, ptr("verts"),
+                                             ptr("normals"), ptr("uvs"), ptr("tangents")))
+        return out
+
+    def export_material(self, material: int) -> dict:
+        kind = C.c_int()
+        p = np.empty(9, np.float32)
+        tex = np.empty(4, np.int32)
+        check(self.lib.prr_scene_export_material(self.h, material, C.byref(kind),
+                                                 C.c_void_p(p.ctypes.data),
+                                                 C.c_void_p(tex.ctypes.data)))
+        return {"kind": kind.value, "params": p, "textures": tex}
+
+    def export_texture(self, texture: int) -> np.ndarray:
+        w, h, c = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.prr_scene_export_texture(self.h, texture, C.byref(w), C.byref(h),
+                                                C.byref(c), None))
+        t = np.empty((h.value, w.value, c.value), np.uint8)
+        check(self.lib.prr_scene_export_texture(self.h, texture, None, None, None,
+                                                C.c_void_p(t.ctypes.data)))
+        return t
+
     def add_sphere(self, center, radius: float, material: int) -> int:
         out = C.c_int()
         check(self.lib.prr_scene_add_sphere(self.h, _f3(center), float(radius), material,
@@ -156,6 +210,7 @@ class Scene:
         c.aperture = cam.aperture
         c.focus_distance = cam.focus_distance
         check(self.lib.prr_scene_set_camera(self.h, C.byref(c), width, height))
+        self.size = (int(width), int(height))
 
     def buildBVH(self, stream=None):
         check(self.lib.prr_scene_build(self.h, _stream(stream)))
@@ -281,9 +336,9 @@ class Scene:
     # ---- rendering (Renderer::Render up to the linear framebuffer) ----
     def _settings(self, spp, max_depth, seed, min_spp, threshold, mode, window, indirect_clamp,
                   sample_offset, slices):
-        if self.desc is None:
-            raise ValueError("render needs a scene created with Scene.from_desc")
-        W, H = self.desc.width, self.desc.height
+        if self.size is None:
+            raise ValueError("render needs a camera (set_camera or Scene.from_desc)")
+        W, H = self.size
         x0, y0, x1, y1 = window or (0, 0, W, H)
         rs = prr_render_settings()
         rs.width, rs.height = W, H
@@ -318,9 +373,9 @@ class Scene:
         """Mean radiance per pixel of the window: (h, w, 3) float32 CUDA tensor,
         plus samples per pixel and, with count_rays, (closest, shadow) rays."""
         import torch
-        if self.desc is None:
-            raise ValueError("render needs a scene created with Scene.from_desc")
-        W, H = self.desc.width, self.desc.height
+        if self.size is None:
+            raise ValueError("render needs a camera (set_camera or Scene.from_desc)")
+        W, H = self.size
         x0, y0, x1, y1 = window or (0, 0, W, H)
         rs = prr_render_settings()
         rs.width, rs.height = W, H
@@ -468,7 +523,7 @@ class PhotonMap:
                         k_nearest: int = 0, window=None, stream=None):
         import torch
         rs = scene._settings(spp, max_depth, seed, None, 0.05, "plain", window, 10.0, 0, 0)
-        W, H = scene.desc.width, scene.desc.height
+        W, H = scene.size
         x0, y0, x1, y1 = window or (0, 0, W, H)
         dev = torch.device("cuda", torch.cuda.current_device())
         out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
@@ -516,7 +571,7 @@ class Server:
         renders the scene's camera at another resolution."""
         sc = self.scenes[scene_id]
         rs = sc._settings(spp, max_depth, seed, None, 0.05, "plain", window, 10.0, 0, 0)
-        W, H = size or (sc.desc.width, sc.desc.height)
+        W, H = size or sc.size
         rs.width, rs.height = W, H
         if window is None:
             rs.x0, rs.y0, rs.x1, rs.y1 = 0, 0, W, H

@@ -81,7 +81,7 @@ def build(verbose: bool = False, ptxas_verbose: bool = False, jobs: int = 8) -> 
     if cmds or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs),
-              "-Xcompiler", "-pthread"], verbose)
+              "-Xcompiler", "-pthread", "-lz"], verbose)
         shutil.move(str(tmp), str(LIB))
     return LIB
 

@@ -614,6 +614,71 @@ int prr_scene_set_material_textures(prr_scene *scene, int material, int base_col
     return PRR_OK;
 }
 
+int prr_scene_export_mesh(const prr_scene *scene, int object, int64_t *out_ntri, int *out_attr,
+                          float *verts, float *normals, float *uvs, float *tangents) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    const Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(const_cast<Scene *>(s)->mu);
+    if (object < 0 || object >= (int) s->objects.size() || s->objects[object].kind != kObjMesh)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "not a mesh object");
+    const HostObject &o = s->objects[object];
+    const int64_t nt = (int64_t) o.verts.size() / 9;
+    if (out_ntri)
+        *out_ntri = nt;
+    if (out_attr)
+        *out_attr = (o.cnormals.empty() ? 0 : kAttrNormals) | (o.cuvs.empty() ? 0 : kAttrUV) |
+                    (o.ctangents.empty() ? 0 : kAttrTangents);
+    if (verts)
+        std::memcpy(verts, o.verts.data(), o.verts.size() * sizeof(float));
+    if (normals && !o.cnormals.empty())
+        for (int64_t k = 0; k < nt * 3; k++)
+            normalize3f(&o.cnormals[(size_t) k * 3], normals + k * 3);
+    if (uvs && !o.cuvs.empty())
+        std::memcpy(uvs, o.cuvs.data(), o.cuvs.size() * sizeof(float));
+    if (tangents && !o.ctangents.empty())
+        std::memcpy(tangents, o.ctangents.data(), o.ctangents.size() * sizeof(float));
+    return PRR_OK;
+}
+
+int prr_scene_export_material(const prr_scene *scene, int material, int *out_kind,
+                              float params[9], int textures[4]) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    const Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(const_cast<Scene *>(s)->mu);
+    if (material < 0 || material >= (int) s->materials.size())
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown material");
+    const HostMaterial &m = s->materials[material];
+    if (out_kind)
+        *out_kind = m.kind;
+    if (params)
+        std::memcpy(params, m.params, sizeof(m.params));
+    if (textures)
+        std::memcpy(textures, m.tex, sizeof(m.tex));
+    return PRR_OK;
+}
+
+int prr_scene_export_texture(const prr_scene *scene, int texture, int *out_width,
+                             int *out_height, int *out_channels, uint8_t *texels) {
+    if (int rc = check_scene(scene, false))
+        return rc;
+    const Scene *s = S(scene);
+    std::lock_guard<std::mutex> g(const_cast<Scene *>(s)->mu);
+    if (texture < 0 || texture >= (int) s->textures.size())
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown texture");
+    const HostTexture &t = s->textures[texture];
+    if (out_width)
+        *out_width = t.width;
+    if (out_height)
+        *out_height = t.height;
+    if (out_channels)
+        *out_channels = t.channels;
+    if (texels)
+        std::memcpy(texels, t.texels.data(), t.texels.size());
+    return PRR_OK;
+}
+
 int prr_scene_add_sphere(prr_scene *scene, const float center[3], float radius, int material,
                          int *out_object) {
     if (int rc = check_scene(scene, false))
