@@ -150,12 +150,13 @@ int prr_scene_add_material(prr_scene *scene, int kind, const float params[9], in
  * maxPrimsInNode 4 (Triangle.hpp:173-179). */
 int prr_scene_add_mesh(prr_scene *scene, const float *verts, int64_t ntri, int material,
                        int *out_object);
-/* MeshTriangle from triangles with per-corner data, as the glTF loader builds
- * them (GLTFLoader.cpp:224-262, Triangle.hpp:17-23): normals = ntri x 9
- * (n0, n1, n2; normalized here, and the face normal becomes
- * normalize(n0 + n1 + n2)), uvs = ntri x 6 (t0, t1, t2), tangents = ntri x 12
- * (xyz + handedness w per corner). Any of the three may be NULL. Hits on the
- * mesh interpolate them as Triangle::finalize does (Triangle.cpp:34-59). */
+/* MeshTriangle from triangles with per-corner data (Triangle.hpp:17-23), the
+ * fields as a Triangle holds them: normals = ntri x 9 (n0, n1, n2, used as
+ * given -- the glTF loader normalizes them first, GLTFLoader.cpp:237-239 -- and
+ * the face normal becomes normalize(n0 + n1 + n2)), uvs = ntri x 6 (t0, t1,
+ * t2), tangents = ntri x 12 (xyz + handedness w per corner). Any of the three
+ * may be NULL. Hits on the mesh interpolate them as Triangle::finalize does
+ * (Triangle.cpp:34-59). */
 int prr_scene_add_mesh_attr(prr_scene *scene, const float *verts, const float *normals,
                             const float *uvs, const float *tangents, int64_t ntri, int material,
                             int *out_object);
@@ -182,8 +183,8 @@ int prr_scene_add_gltf(prr_scene *scene, const char *path, int material_type,
                        int override_material, int *out_first, int *out_count, int *out_undecoded);
 /* Host-side view of a mesh as added (before or after the build): ntri, the
  * kinds of per-corner data it carries (1 normals, 2 uvs, 4 tangents), and, for
- * non-NULL arrays, its triangles (ntri x 9), normalized corner normals (ntri x
- * 9), uvs (ntri x 6) and tangents (ntri x 12), in input order. */
+ * non-NULL arrays, its triangles (ntri x 9), corner normals (ntri x 9), uvs
+ * (ntri x 6) and tangents (ntri x 12), in input order. */
 int prr_scene_export_mesh(const prr_scene *scene, int object, int64_t *out_ntri, int *out_attr,
                           float *verts, float *normals, float *uvs, float *tangents);
 /* A material as added: kind, params[9] and its four texture ids (-1 none). */
@@ -261,6 +262,14 @@ int prr_render(prr_scene *scene, const prr_render_settings *settings, float *out
  * (optional) = the mapped floats, out_u8 (optional) = n x 3 bytes. */
 int prr_tonemap(int mapper, float exposure, const float *rgb, int64_t n, float *out_rgb,
                 uint8_t *out_u8, void *stream);
+
+/* The image files of Renderer::Render (Renderer.cpp:163-185): width x height
+ * 8-bit RGB written to `path` as PNG (".png") or binary PPM (".ppm"). Host
+ * memory. */
+int prr_write_image(const char *path, const uint8_t *rgb, int width, int height);
+/* The adaptive-sampling visualisation (Renderer.cpp:193-211): per pixel
+ * v = (uint8)(255 * spp / max_spp) as an RGB grey. Host memory. */
+int prr_sample_count_image(const int32_t *spp, int64_t n, int max_spp, uint8_t *out_rgb);
 
 /* ---- caustic photons (PhotonMap, Photon.hpp:32-45) ---------------------- */
 int prr_photon_map_create(prr_photon_map **out);

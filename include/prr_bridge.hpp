@@ -18,9 +18,15 @@
 //                                                      Camera.hpp:9-15
 //   RenderSettings                                     Renderer.hpp:42-55
 //
-// Not carried over (Report counts them so a caller can refuse the scene):
-// textures (Material::*Tex), per-vertex smooth normals and tangents, and any
-// Object subclass other than MeshTriangle and Sphere.
+//   Triangle::n0..n2, t0..t2, tan0..tan2, tangentW*, hasSmoothNormals,
+//   hasTangents                                        Triangle.hpp:17-23
+//   Material::baseColorTex, metallicRoughnessTex, normalTex, emissiveTex
+//                                                      Material.hpp:45-48
+//
+// Not carried over (Report counts them so a caller can refuse the scene): any
+// Object subclass other than MeshTriangle and Sphere, per-corner data on a
+// mesh where only some triangles have it, and texture data that is not
+// width x height x channels bytes.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -45,9 +51,10 @@ inline void check(int rc) {
 
 struct Report {
     int64_t meshes = 0, spheres = 0, triangles = 0, materials = 0;
-    int64_t textured_materials = 0;      // textures are not sampled by libprr
-    int64_t smooth_normal_triangles = 0; // shaded with the face normal instead
-    int64_t skipped_objects = 0;         // Object subclasses libprr does not know
+    int64_t textures = 0;          // textures carried over
+    int64_t attributed_meshes = 0; // meshes carried with per-corner data
+    int64_t skipped_objects = 0;   // Object subclasses libprr does not know
+    int64_t dropped = 0;           // per-corner data or textures left out (see above)
 };
 
 // Owns the libprr scene built from a reference Scene.
@@ -93,32 +100,75 @@ inline GpuScene upload(const Scene &scene, int width, int height, Report *report
         p[4] = m->metallic;
         p[5] = m->ior;
         put3(p + 6, m->m_emission);
-        if (!m->baseColorTex.empty() || !m->emissiveTex.empty() || !m->normalTex.empty() ||
-            !m->metallicRoughnessTex.empty())
-            rep.textured_materials++;
         int id = -1;
         check(prr_scene_add_material(h, material_kind(m), p, &id));
+        const Texture *tex[4] = {&m->baseColorTex, &m->metallicRoughnessTex, &m->normalTex,
+                                 &m->emissiveTex};
+        int tid[4] = {-1, -1, -1, -1};
+        for (int k = 0; k < 4; k++) {
+            const Texture &t = *tex[k];
+            if (t.empty())
+                continue;
+            if ((t.channels != 3 && t.channels != 4) ||
+                t.data.size() != (size_t) t.width * t.height * t.channels) {
+                rep.dropped++;
+                continue;
+            }
+            check(prr_scene_add_texture(h, t.data.data(), t.width, t.height, t.channels, &tid[k]));
+            rep.textures++;
+        }
+        if (tid[0] >= 0 || tid[1] >= 0 || tid[2] >= 0 || tid[3] >= 0)
+            check(prr_scene_set_material_textures(h, id, tid[0], tid[1], tid[2], tid[3]));
         ids.emplace(m, id);
         rep.materials++;
         return id;
     };
-    std::vector<float> verts;
+    std::vector<float> verts, nrm, uvs, tan;
     for (const Object *o : scene.objects) {
         int obj = -1;
         if (auto *mesh = dynamic_cast<const MeshTriangle *>(o)) {
-            verts.resize(mesh->triangles.size() * 9);
-            float *v = verts.data();
-            for (const Triangle &t : mesh->triangles) {
-                put3(v, t.v0);
-                put3(v + 3, t.v1);
-                put3(v + 6, t.v2);
-                v += 9;
-                if (t.hasSmoothNormals) rep.smooth_normal_triangles++;
+            const size_t n = mesh->triangles.size();
+            size_t with_n = 0, with_t = 0;
+            bool any_uv = false;
+            verts.resize(n * 9);
+            nrm.resize(n * 9);
+            uvs.resize(n * 6);
+            tan.resize(n * 12);
+            for (size_t i = 0; i < n; i++) {
+                const Triangle &t = mesh->triangles[i];
+                put3(&verts[i * 9], t.v0);
+                put3(&verts[i * 9 + 3], t.v1);
+                put3(&verts[i * 9 + 6], t.v2);
+                put3(&nrm[i * 9], t.n0);
+                put3(&nrm[i * 9 + 3], t.n1);
+                put3(&nrm[i * 9 + 6], t.n2);
+                const Vector2f *uv[3] = {&t.t0, &t.t1, &t.t2};
+                const Vector3f *tg[3] = {&t.tan0, &t.tan1, &t.tan2};
+                const float tw[3] = {t.tangentW0, t.tangentW1, t.tangentW2};
+                for (int q = 0; q < 3; q++) {
+                    uvs[i * 6 + q * 2] = uv[q]->x;
+                    uvs[i * 6 + q * 2 + 1] = uv[q]->y;
+                    any_uv = any_uv || uv[q]->x != 0.f || uv[q]->y != 0.f;
+                    put3(&tan[i * 12 + q * 4], *tg[q]);
+                    tan[i * 12 + q * 4 + 3] = tw[q];
+                }
+                with_n += t.hasSmoothNormals ? 1 : 0;
+                with_t += t.hasTangents ? 1 : 0;
             }
-            check(prr_scene_add_mesh(h, verts.data(), (int64_t) mesh->triangles.size(),
-                                     material(mesh->m), &obj));
+            const bool use_n = with_n == n && n > 0, use_t = with_t == n && n > 0;
+            if ((with_n && !use_n) || (with_t && !use_t))
+                rep.dropped++;
+            if (use_n || use_t || any_uv) {
+                check(prr_scene_add_mesh_attr(h, verts.data(), use_n ? nrm.data() : nullptr,
+                                              any_uv ? uvs.data() : nullptr,
+                                              use_t ? tan.data() : nullptr, (int64_t) n,
+                                              material(mesh->m), &obj));
+                rep.attributed_meshes++;
+            } else {
+                check(prr_scene_add_mesh(h, verts.data(), (int64_t) n, material(mesh->m), &obj));
+            }
             rep.meshes++;
-            rep.triangles += (int64_t) mesh->triangles.size();
+            rep.triangles += (int64_t) n;
         } else if (auto *sph = dynamic_cast<const Sphere *>(o)) {
             float c[3];
             put3(c, sph->center);

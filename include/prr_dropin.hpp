@@ -12,6 +12,11 @@
 //   Triangle(v0, v1, v2, m)       Triangle.hpp:27-32
 //   MeshTriangle(tris, bounds, m) Triangle.hpp:116-124
 //   Sphere(center, radius, m)     Sphere.hpp:14-16
+//   Texture; Triangle's per-corner data; Material textures
+//                                 TextureUtils.hpp:9-18, Triangle.hpp:17-23,
+//                                 Material.hpp:45-48
+//   GLTFLoader::load(file, MaterialType, override)
+//                                 GLTFLoader.hpp:10-26
 //   Camera::create / fromBlender / init
 //                                 Camera.hpp:23-56
 //   Scene::Add / buildBVH / intersect / intersectP, envMap, camera,
@@ -25,11 +30,12 @@
 // The per-ray calls (Scene::intersect, Integrator::castRay) run a one-ray
 // batch and exist for compatibility; the batch entry points of prr.h are the
 // hot path. Renderer::Render renders on the GPU, keeps the linear framebuffer
-// (framebuffer()), and writes output.ppm / output_raw.ppm like the reference
-// (Renderer.cpp:165-192; PNG output is left to the caller).
+// (framebuffer()), and writes output, output_raw and sample_count as .png and
+// .ppm like the reference (Renderer.cpp:163-211).
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -78,6 +84,8 @@ inline Vector3f operator*(float r, const Vector3f &v) { return {v.x * r, v.y * r
 
 struct Vector2f {
     float x = 0, y = 0;
+    Vector2f() = default;
+    Vector2f(float a, float b) : x(a), y(b) {}
 };
 
 struct Ray {
@@ -91,6 +99,15 @@ struct Bounds3 {
     Bounds3(const Vector3f &a, const Vector3f &b) : pMin(a), pMax(b) {}
 };
 
+// Texture (TextureUtils.hpp:9-18): 8-bit texels, row-major.
+struct Texture {
+    std::vector<unsigned char> data;
+    int width = 0;
+    int height = 0;
+    int channels = 4;
+    bool empty() const { return data.empty(); }
+};
+
 class Material {
   public:
     Vector3f m_emission = Vector3f(0.0f);
@@ -98,6 +115,10 @@ class Material {
     float roughness = 0.5f;
     float metallic = 0.0f;
     float ior = 1.5f;
+    Texture emissiveTex;
+    Texture baseColorTex;
+    Texture normalTex;
+    Texture metallicRoughnessTex;
     virtual ~Material() = default;
     virtual int kind() const = 0;
     virtual bool isDelta() const { return false; }
@@ -132,6 +153,12 @@ class Object {
 class Triangle {
   public:
     Vector3f v0, v1, v2;
+    Vector2f t0, t1, t2;       // per-corner texture coordinates
+    Vector3f tan0, tan1, tan2; // per-corner tangents
+    float tangentW0 = 1.f, tangentW1 = 1.f, tangentW2 = 1.f;
+    bool hasTangents = false;
+    Vector3f n0, n1, n2; // per-corner smooth normals
+    bool hasSmoothNormals = false;
     Material *m;
     Triangle(Vector3f a, Vector3f b, Vector3f c, Material *mat = nullptr)
         : v0(a), v1(b), v2(c), m(mat) {}
@@ -152,6 +179,117 @@ class Sphere : public Object {
     Vector3f center;
     float radius;
     Sphere(const Vector3f &c, const float &r, Material *mt) : center(c), radius(r) { m = mt; }
+};
+
+enum class MaterialType { Diffuse, Glass, Mirror, Emit }; // GLTFLoader.hpp:10
+
+// GLTFLoader::load (GLTFLoader.cpp:140-281): one heap-allocated MeshTriangle
+// per triangle primitive, with its per-corner data and a new material per
+// primitive (or overrideMat for all). Parsed by libprr's glTF reader.
+class GLTFLoader {
+  public:
+    static std::vector<MeshTriangle *> load(const std::string &filename, MaterialType matType,
+                                            Material *overrideMat = nullptr) {
+        prr_scene *tmp = nullptr;
+        prr_detail::check(prr_scene_create(&tmp));
+        std::vector<MeshTriangle *> out;
+        try {
+            int first = -1, count = 0, undecoded = 0;
+            int over = -1;
+            if (overrideMat) {
+                const float p[9] = {0.8f, 0.8f, 0.8f, 0.5f, 0.f, 1.5f, 0.f, 0.f, 0.f};
+                prr_detail::check(prr_scene_add_material(tmp, PRR_MAT_DIFFUSE, p, &over));
+            }
+            prr_detail::check(prr_scene_add_gltf(tmp, filename.c_str(), (int) matType, over,
+                                                 &first, &count, &undecoded));
+            for (int k = 0; k < count; k++) {
+                const int obj = first + k;
+                int64_t nt = 0;
+                int attr = 0;
+                prr_detail::check(prr_scene_export_mesh(tmp, obj, &nt, &attr, nullptr, nullptr,
+                                                        nullptr, nullptr));
+                std::vector<float> v(nt * 9), n(nt * 9), uv(nt * 6), tg(nt * 12);
+                prr_detail::check(prr_scene_export_mesh(tmp, obj, nullptr, nullptr, v.data(),
+                                                        n.data(), uv.data(), tg.data()));
+                Material *mat = overrideMat ? overrideMat : export_material(tmp, over < 0 ? k : -1);
+                std::vector<Triangle> tris;
+                Vector3f lo(std::numeric_limits<float>::infinity());
+                Vector3f hi(-std::numeric_limits<float>::infinity());
+                for (int64_t i = 0; i < nt; i++) {
+                    const float *p = &v[i * 9];
+                    Triangle t(Vector3f(p[0], p[1], p[2]), Vector3f(p[3], p[4], p[5]),
+                               Vector3f(p[6], p[7], p[8]), mat);
+                    for (int q = 0; q < 3; q++) {
+                        lo = Vector3f(std::min(lo.x, p[q * 3]), std::min(lo.y, p[q * 3 + 1]),
+                                      std::min(lo.z, p[q * 3 + 2]));
+                        hi = Vector3f(std::max(hi.x, p[q * 3]), std::max(hi.y, p[q * 3 + 1]),
+                                      std::max(hi.z, p[q * 3 + 2]));
+                    }
+                    if (attr & 1) {
+                        const float *c = &n[i * 9];
+                        t.n0 = Vector3f(c[0], c[1], c[2]);
+                        t.n1 = Vector3f(c[3], c[4], c[5]);
+                        t.n2 = Vector3f(c[6], c[7], c[8]);
+                        t.hasSmoothNormals = true;
+                    }
+                    if (attr & 2) {
+                        const float *c = &uv[i * 6];
+                        t.t0 = Vector2f(c[0], c[1]);
+                        t.t1 = Vector2f(c[2], c[3]);
+                        t.t2 = Vector2f(c[4], c[5]);
+                    }
+                    if (attr & 4) {
+                        const float *c = &tg[i * 12];
+                        t.tan0 = Vector3f(c[0], c[1], c[2]);
+                        t.tan1 = Vector3f(c[4], c[5], c[6]);
+                        t.tan2 = Vector3f(c[8], c[9], c[10]);
+                        t.tangentW0 = c[3];
+                        t.tangentW1 = c[7];
+                        t.tangentW2 = c[11];
+                        t.hasTangents = true;
+                    }
+                    tris.push_back(t);
+                }
+                out.push_back(new MeshTriangle(std::move(tris), Bounds3(lo, hi), mat));
+            }
+        } catch (...) {
+            prr_scene_destroy(tmp);
+            throw;
+        }
+        prr_scene_destroy(tmp);
+        return out;
+    }
+
+  private:
+    static Material *export_material(prr_scene *tmp, int id) {
+        int kind = 0, tex[4];
+        float p[9];
+        prr_detail::check(prr_scene_export_material(tmp, id, &kind, p, tex));
+        Material *m = kind == PRR_MAT_GLASS      ? (Material *) new GlassMaterial()
+                      : kind == PRR_MAT_MIRROR   ? (Material *) new MirrorMaterial()
+                      : kind == PRR_MAT_EMISSIVE ? (Material *) new EmissiveMaterial()
+                                                 : (Material *) new DiffuseMaterial();
+        m->baseColor = Vector3f(p[0], p[1], p[2]);
+        m->roughness = p[3];
+        m->metallic = p[4];
+        m->ior = p[5];
+        m->m_emission = Vector3f(p[6], p[7], p[8]);
+        Texture *slots[4] = {&m->baseColorTex, &m->metallicRoughnessTex, &m->normalTex,
+                             &m->emissiveTex};
+        for (int k = 0; k < 4; k++) {
+            if (tex[k] < 0)
+                continue;
+            int w = 0, h = 0, c = 0;
+            prr_detail::check(prr_scene_export_texture(tmp, tex[k], &w, &h, &c, nullptr));
+            slots[k]->data.resize((size_t) w * h * c);
+            slots[k]->width = w;
+            slots[k]->height = h;
+            slots[k]->channels = c;
+            prr_detail::check(
+                prr_scene_export_texture(tmp, tex[k], nullptr, nullptr, nullptr, slots[k]->data.data()));
+        }
+        return m;
+    }
 };
 
 struct Camera {
@@ -226,31 +364,61 @@ class Scene {
     // Scene::buildBVH (Scene.cpp:15-27): uploads everything and builds on the GPU.
     void buildBVH() {
         std::vector<Material *> mats;
+        std::vector<int> mat_ids;
         auto mat_id = [&](Material *m) {
             for (size_t k = 0; k < mats.size(); k++)
                 if (mats[k] == m)
-                    return (int) k;
+                    return mat_ids[k];
             const float p[9] = {m->baseColor.x, m->baseColor.y, m->baseColor.z, m->roughness,
                                 m->metallic,    m->ior,         m->m_emission.x, m->m_emission.y,
                                 m->m_emission.z};
             int id = -1;
             prr_detail::check(prr_scene_add_material(h_, m->kind(), p, &id));
+            const Texture *tex[4] = {&m->baseColorTex, &m->metallicRoughnessTex, &m->normalTex,
+                                     &m->emissiveTex};
+            int tid[4] = {-1, -1, -1, -1};
+            for (int k = 0; k < 4; k++)
+                if (!tex[k]->empty())
+                    prr_detail::check(prr_scene_add_texture(h_, tex[k]->data.data(),
+                                                            tex[k]->width, tex[k]->height,
+                                                            tex[k]->channels, &tid[k]));
+            if (tid[0] >= 0 || tid[1] >= 0 || tid[2] >= 0 || tid[3] >= 0)
+                prr_detail::check(
+                    prr_scene_set_material_textures(h_, id, tid[0], tid[1], tid[2], tid[3]));
             mats.push_back(m);
+            mat_ids.push_back(id);
             return id;
         };
         for (Object *o : objects) {
             const int mid = mat_id(o->m);
             if (auto *mesh = dynamic_cast<MeshTriangle *>(o)) {
-                std::vector<float> v;
-                v.reserve(mesh->triangles.size() * 9);
-                for (const Triangle &t : mesh->triangles)
-                    for (const Vector3f &p : {t.v0, t.v1, t.v2}) {
-                        v.push_back(p.x);
-                        v.push_back(p.y);
-                        v.push_back(p.z);
+                const size_t n = mesh->triangles.size();
+                std::vector<float> v, nrm, uv, tg;
+                bool has_n = n > 0, has_t = n > 0, has_uv = false;
+                for (const Triangle &t : mesh->triangles) {
+                    has_n = has_n && t.hasSmoothNormals;
+                    has_t = has_t && t.hasTangents;
+                    for (const Vector2f *q : {&t.t0, &t.t1, &t.t2})
+                        has_uv = has_uv || q->x != 0.f || q->y != 0.f;
+                }
+                for (const Triangle &t : mesh->triangles) {
+                    for (const Vector3f &p : {t.v0, t.v1, t.v2})
+                        v.insert(v.end(), {p.x, p.y, p.z});
+                    if (has_n)
+                        for (const Vector3f &p : {t.n0, t.n1, t.n2})
+                            nrm.insert(nrm.end(), {p.x, p.y, p.z});
+                    if (has_uv)
+                        for (const Vector2f &p : {t.t0, t.t1, t.t2})
+                            uv.insert(uv.end(), {p.x, p.y});
+                    if (has_t) {
+                        tg.insert(tg.end(), {t.tan0.x, t.tan0.y, t.tan0.z, t.tangentW0});
+                        tg.insert(tg.end(), {t.tan1.x, t.tan1.y, t.tan1.z, t.tangentW1});
+                        tg.insert(tg.end(), {t.tan2.x, t.tan2.y, t.tan2.z, t.tangentW2});
                     }
-                prr_detail::check(
-                    prr_scene_add_mesh(h_, v.data(), (int64_t) mesh->triangles.size(), mid, nullptr));
+                }
+                prr_detail::check(prr_scene_add_mesh_attr(
+                    h_, v.data(), has_n ? nrm.data() : nullptr, has_uv ? uv.data() : nullptr,
+                    has_t ? tg.data() : nullptr, (int64_t) n, mid, nullptr));
             } else if (auto *s = dynamic_cast<Sphere *>(o)) {
                 const float c[3] = {s->center.x, s->center.y, s->center.z};
                 prr_detail::check(prr_scene_add_sphere(h_, c, s->radius, mid, nullptr));
@@ -416,26 +584,30 @@ class Renderer {
         rgb.get(framebuffer_.data());
         sampleCount_.resize(n);
         spp.get(sampleCount_.data());
-        write(rgb, s.exposure, (int) s.toneMapper, s.width, s.height, "output.ppm");
+        write(rgb, s.exposure, (int) s.toneMapper, s.width, s.height, "output");
         if (s.toneMapper != tonemap::ToneMapper::Raw)
-            write(rgb, s.exposure, PRR_TONEMAP_RAW, s.width, s.height, "output_raw.ppm");
+            write(rgb, s.exposure, PRR_TONEMAP_RAW, s.width, s.height, "output_raw");
+        // adaptive-sampling visualisation (Renderer.cpp:193-211)
+        std::vector<uint8_t> vis(n * 3);
+        prr_detail::check(
+            prr_sample_count_image(sampleCount_.data(), (int64_t) n, s.maxSPP, vis.data()));
+        prr_detail::check(prr_write_image("sample_count.ppm", vis.data(), s.width, s.height));
+        prr_detail::check(prr_write_image("sample_count.png", vis.data(), s.width, s.height));
     }
     const std::vector<float> &framebuffer() const { return framebuffer_; }
     const std::vector<int32_t> &sampleCount() const { return sampleCount_; }
 
   private:
+    // Renderer.cpp:163-185: tone map, then <base>.ppm and <base>.png
     static void write(const prr_detail::DeviceArray<float> &rgb, float exposure, int mapper, int w,
-                      int h, const char *name) {
+                      int h, const char *base) {
         const size_t n = (size_t) w * h;
         prr_detail::DeviceArray<uint8_t> u8(n * 3);
         prr_detail::check(prr_tonemap(mapper, exposure, rgb.p, (int64_t) n, nullptr, u8.p, nullptr));
         std::vector<uint8_t> buf(n * 3);
         u8.get(buf.data());
-        if (FILE *fp = std::fopen(name, "wb")) {
-            std::fprintf(fp, "P6\n%d %d\n255\n", w, h);
-            std::fwrite(buf.data(), 1, buf.size(), fp);
-            std::fclose(fp);
-        }
+        prr_detail::check(prr_write_image((std::string(base) + ".ppm").c_str(), buf.data(), w, h));
+        prr_detail::check(prr_write_image((std::string(base) + ".png").c_str(), buf.data(), w, h));
     }
     std::vector<float> framebuffer_;
     std::vector<int32_t> sampleCount_;

@@ -415,14 +415,14 @@ class RefScene:
         rgb = np.empty(n * 3, np.float32)
         spp = np.empty(n, np.int32)
         u8 = np.empty(n * 3, np.uint8)
-        rep = np.zeros(7, np.int64)
+        rep = np.zeros(8, np.int64)
         rc = self.ref.L.prr_ref_bridge_render(self.h, max_depth, min_spp, max_spp, threshold,
                                               seed, mode, mapper, exposure, rgb, spp, u8,
                                               rep.ctypes.data)
         if rc != 0:
             raise RuntimeError("prr_ref_bridge_render failed (see stderr)")
-        keys = ("meshes", "spheres", "triangles", "materials", "textured_materials",
-                "smooth_normal_triangles", "skipped_objects")
+        keys = ("meshes", "spheres", "triangles", "materials", "textures",
+                "attributed_meshes", "skipped_objects", "dropped")
         shape = (H, W, 3)
         return (rgb.reshape(shape), spp.reshape(H, W), u8.reshape(shape),
                 dict(zip(keys, rep.tolist())))

@@ -16,7 +16,7 @@ extern "C" void *prr_ref_scene_object(void *h, int *width, int *height);
 extern "C" int prr_ref_bridge_render(void *h, int max_depth, int min_spp, int max_spp,
                                      float threshold, uint64_t seed, int mode, int mapper,
                                      float exposure, float *out_rgb, int32_t *out_spp,
-                                     uint8_t *out_u8, int64_t *report7) {
+                                     uint8_t *out_u8, int64_t *report8) {
     int w = 0, hh = 0;
     const Scene &scene = *(const Scene *) prr_ref_scene_object(h, &w, &hh);
     RenderSettings s;
@@ -38,13 +38,9 @@ extern "C" int prr_ref_bridge_render(void *h, int max_depth, int min_spp, int ma
         std::fprintf(stderr, "prr_ref_bridge_render: %s\n", e.what());
         return -1;
     }
-    const int64_t r[7] = {rep.meshes,
-                          rep.spheres,
-                          rep.triangles,
-                          rep.materials,
-                          rep.textured_materials,
-                          rep.smooth_normal_triangles,
-                          rep.skipped_objects};
-    std::copy(r, r + 7, report7);
+    const int64_t r[8] = {rep.meshes,   rep.spheres,           rep.triangles,
+                          rep.materials, rep.textures,          rep.attributed_meshes,
+                          rep.skipped_objects, rep.dropped};
+    std::copy(r, r + 8, report8);
     return 0;
 }

@@ -37,6 +37,35 @@ def tonemap(rgb, mapper="agx", exposure: float = 1.0, stream=None):
     return out, u8
 
 
+def write_image(path, rgb8) -> None:
+    """The 8-bit output files of Renderer::Render: (h, w, 3) uint8 (numpy or a
+    CUDA tensor) to a .png or .ppm file."""
+    a = rgb8.cpu().numpy() if hasattr(rgb8, "cpu") else rgb8
+    a = np.ascontiguousarray(a, np.uint8)
+    h, w = a.shape[:2]
+    check(_lib.load().prr_write_image(str(path).encode(), C.c_void_p(a.ctypes.data), w, h))
+
+
+def sample_count_image(spp, max_spp: int) -> np.ndarray:
+    """The adaptive-sampling visualisation (h, w, 3) uint8 of an spp map."""
+    a = spp.cpu().numpy() if hasattr(spp, "cpu") else spp
+    a = np.ascontiguousarray(a, np.int32)
+    out = np.empty(a.shape + (3,), np.uint8)
+    check(_lib.load().prr_sample_count_image(C.c_void_p(a.ctypes.data), a.size, max_spp,
+                                              C.c_void_p(out.ctypes.data)))
+    return out
+
+
+def _normalize_rows(v: np.ndarray) -> np.ndarray:
+    """normalize (Vector.hpp:103-111) row by row in float32: v * (1 / sqrt(|v|^2))."""
+    x, y, z = v[:, 0], v[:, 1], v[:, 2]
+    m2 = x * x + y * y + z * z
+    with np.errstate(divide="ignore"):
+        inv = np.float32(1) / np.sqrt(m2)
+    out = v * inv[:, None]
+    return np.where((m2 > 0)[:, None], out, v).astype(np.float32)
+
+
 def _trace_config(config: dict | None):
     if not config:
         return None
@@ -101,10 +130,15 @@ class Scene:
         self.objects.append(("mesh", len(v)))
         return out.value
 
-    def add_mesh_attr(self, verts, material: int, normals=None, uvs=None, tangents=None) -> int:
+    def add_mesh_attr(self, verts, material: int, normals=None, uvs=None, tangents=None,
+                      normalize: bool = True) -> int:
         """MeshTriangle with per-corner normals (n, 9), uvs (n, 6) and tangents
-        (n, 12: xyz + handedness per corner), any of them None."""
+        (n, 12: xyz + handedness per corner), any of them None. With
+        `normalize` the corner normals are normalized first, as the glTF
+        loader does (GLTFLoader.cpp:237-239), in the same float steps."""
         v = np.ascontiguousarray(verts, np.float32).reshape(-1, 9)
+        if normals is not None and normalize:
+            normals = _normalize_rows(np.ascontiguousarray(normals, np.float32).reshape(-1, 3))
         arrs = []
         for a, k in ((normals, 9), (uvs, 6), (tangents, 12)):
             arrs.append(None if a is None else np.ascontiguousarray(a, np.float32).reshape(-1, k))

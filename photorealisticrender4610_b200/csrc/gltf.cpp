@@ -789,8 +789,20 @@ extern "C" int prr_scene_add_gltf(prr_scene *scene, const char *path, int materi
                 for (int q = 0; q < 3; q++) {
                     const uint32_t k = idx[t * 3 + q];
                     std::memcpy(&v[t * 9 + q * 3], &pos[k * 3], 3 * sizeof(float));
-                    if (!cn.empty())
-                        std::memcpy(&cn[t * 9 + q * 3], &nrm[k * 3], 3 * sizeof(float));
+                    if (!cn.empty()) { // normalize (GLTFLoader.cpp:237-239, Vector.hpp:103-111)
+                        const float *r = &nrm[k * 3];
+                        float *o = &cn[t * 9 + q * 3];
+                        const float m2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                        o[0] = r[0];
+                        o[1] = r[1];
+                        o[2] = r[2];
+                        if (m2 > 0) {
+                            const float inv = 1 / sqrtf(m2);
+                            o[0] = r[0] * inv;
+                            o[1] = r[1] * inv;
+                            o[2] = r[2] * inv;
+                        }
+                    }
                     if (!cu.empty())
                         std::memcpy(&cu[t * 6 + q * 2], &uvs[k * 2], 2 * sizeof(float));
                     if (!ctan.empty())

@@ -252,11 +252,10 @@ int build_scene(Scene &s, cudaStream_t st) {
                 nz = cz * inv;
             }
             if (!o.cnormals.empty()) {
-                // GLTFLoader.cpp:236-241: corners normalized, the face normal
-                // replaced by normalize(n0 + n1 + n2)
-                float c[9], sum[3];
-                for (int q = 0; q < 3; q++)
-                    normalize3f(&o.cnormals[(size_t) id * 9 + q * 3], c + q * 3);
+                // the face normal of a smooth triangle is normalize(n0 + n1 + n2)
+                // (GLTFLoader.cpp:241)
+                const float *c = &o.cnormals[(size_t) id * 9];
+                float sum[3];
                 for (int a = 0; a < 3; a++)
                     sum[a] = (c[a] + c[3 + a]) + c[6 + a];
                 float fn[3];
@@ -291,8 +290,7 @@ int build_scene(Scene &s, cudaStream_t st) {
             const int32_t id = o.bvh.ordered[j];
             float *r = &attr[at0 + (size_t) j * kAttrFloats];
             if (!o.cnormals.empty())
-                for (int q = 0; q < 3; q++)
-                    normalize3f(&o.cnormals[(size_t) id * 9 + q * 3], r + q * 3);
+                std::memcpy(r, &o.cnormals[(size_t) id * 9], 9 * sizeof(float));
             if (!o.cuvs.empty())
                 std::memcpy(r + 9, &o.cuvs[(size_t) id * 6], 6 * sizeof(float));
             if (!o.ctangents.empty())
@@ -632,8 +630,7 @@ int prr_scene_export_mesh(const prr_scene *scene, int object, int64_t *out_ntri,
     if (verts)
         std::memcpy(verts, o.verts.data(), o.verts.size() * sizeof(float));
     if (normals && !o.cnormals.empty())
-        for (int64_t k = 0; k < nt * 3; k++)
-            normalize3f(&o.cnormals[(size_t) k * 3], normals + k * 3);
+        std::memcpy(normals, o.cnormals.data(), o.cnormals.size() * sizeof(float));
     if (uvs && !o.cuvs.empty())
         std::memcpy(uvs, o.cuvs.data(), o.cuvs.size() * sizeof(float));
     if (tangents && !o.ctangents.empty())

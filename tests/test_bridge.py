@@ -27,6 +27,7 @@ def _scenes():
     from photorealisticrender4610_b200 import scenes
     yield "cornell", scenes.cornell_box(64, 64), 5
     yield "museum", scenes.museum_like(96, 64, level=3, env_size=(256, 128)), 8
+    yield "textured", scenes.textured_showcase(96, 72), 8
 
 
 @pytest.mark.gpu
@@ -40,7 +41,11 @@ def test_bridge_render_matches_api(bridge_ref, cuda, mode):
                                              mapper=2, exposure=0.18)
         n_mesh = sum(o.kind == "mesh" for o in desc.objects)
         assert rep["meshes"] == n_mesh and rep["skipped_objects"] == 0, (name, rep)
-        assert rep["spheres"] == len(desc.objects) - n_mesh
+        assert rep["spheres"] == len(desc.objects) - n_mesh and rep["dropped"] == 0
+        assert rep["attributed_meshes"] == sum(o.kind == "mesh" and o.has_attributes()
+                                               for o in desc.objects)
+        assert rep["textures"] == sum(t is not None for m in desc.materials
+                                      for t in m.texture_list())
         s = prr.Scene.from_desc(desc)
         want, cnt = s.render(8, depth, seed=3, mode=mode)
         assert np.array_equal(rgb.view(np.uint32), want.cpu().numpy().view(np.uint32)), name

@@ -9,13 +9,14 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 SRC = ROOT / "tests" / "cpp" / "dropin_example.cpp"
+GLTF_SRC = ROOT / "tests" / "cpp" / "gltf_example.cpp"
 LIBDIR = ROOT / "photorealisticrender4610_b200"
 
 
-def build_example(tmp_path):
-    exe = tmp_path / "dropin_example"
+def build_example(tmp_path, src=SRC):
+    exe = tmp_path / src.stem
     cmd = ["/usr/bin/g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"),
-           "-I", "/usr/local/cuda/include", str(SRC), "-o", str(exe), "-L", str(LIBDIR), "-lprr",
+           "-I", "/usr/local/cuda/include", str(src), "-o", str(exe), "-L", str(LIBDIR), "-lprr",
            f"-Wl,-rpath,{LIBDIR}", "-L", "/usr/local/cuda/lib64", "-lcudart",
            "-Wl,-rpath,/usr/local/cuda/lib64"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
@@ -24,6 +25,7 @@ def build_example(tmp_path):
 
 def test_dropin_example_compiles(tmp_path, lib):
     assert build_example(tmp_path).exists()
+    assert build_example(tmp_path, GLTF_SRC).exists()
 
 
 @pytest.mark.gpu
@@ -39,5 +41,40 @@ def test_dropin_renders_like_the_python_api(tmp_path, cuda):
     s = prr.Scene.from_desc(scenes.cornell_box(64, 64))
     want, _ = s.render(16, 5, seed=1)
     assert np.array_equal(fb.view(np.uint32), want.cpu().numpy().view(np.uint32))
-    assert (tmp_path / "output.ppm").exists() and (tmp_path / "output_raw.ppm").exists()
+    for name in ("output", "output_raw", "sample_count"):
+        assert (tmp_path / f"{name}.ppm").exists() and (tmp_path / f"{name}.png").exists()
+    # output.png is the tone-mapped framebuffer (the drop-in's default AgX, exposure 1)
+    from PIL import Image
+    _, u8 = prr.tonemap(want, "agx", 1.0)
+    png = np.asarray(Image.open(tmp_path / "output.png").convert("RGB"))
+    assert np.array_equal(png, u8.cpu().numpy())
     assert "hit 1 obj 2" in r.stdout  # the back wall
+
+
+@pytest.mark.gpu
+def test_gltf_dropin_renders_like_the_python_api(tmp_path, cuda):
+    """GLTFLoader::load of the drop-in header on a file written by the test
+    writer, rendered by Renderer::Render, equals the Python API's add_gltf
+    scene rendered in the same mode and seed."""
+    import sys
+    sys.path.insert(0, str(ROOT / "tests"))
+    import gltf_writer
+    import photorealisticrender4610_b200 as prr
+    from photorealisticrender4610_b200 import scenes
+    path = tmp_path / "features.glb"
+    gltf_writer.feature_file(path)
+    exe = build_example(tmp_path, GLTF_SRC)
+    out = tmp_path / "fb.bin"
+    r = subprocess.run([str(exe), str(path), str(out)], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    fb = np.fromfile(out, np.float32).reshape(72, 96, 3)
+    s = prr.Scene()
+    s.add_gltf(path)
+    lm = s.add_material(1, [0.8, 0.8, 0.8, 0.5, 0.0, 1.5, 20.0, 20.0, 20.0])
+    s.add_sphere((0.3, 1.4, 0.2), 0.25, lm)
+    s.set_camera(scenes.Camera(eye=(0.0, 2.0, 2.6), target=(0, 0, 0), up=(0, 1, 0), fovv=50.0,
+                               fovh=60.0), 96, 72)
+    s.buildBVH()
+    want, _ = s.render(64, 6, seed=3, mode="wavefront")
+    assert np.array_equal(fb.view(np.uint32), want.cpu().numpy().view(np.uint32))
