@@ -620,8 +620,9 @@ def serving_pool():
 
 
 def run_serving(args, rank, world, on):
-    """Continuous-batching server under Poisson arrivals against the plain
-    renderer run one request at a time in arrival order."""
+    """Continuous-batching server (wavefront steps) under Poisson arrivals,
+    beside the same server on megakernel steps and the plain renderer run one
+    request at a time in arrival order."""
     import math
     import threading
     import torch
@@ -647,10 +648,11 @@ def run_serving(args, rank, world, on):
     host = [torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
             for _, (w, h), _ in reqs]
 
-    def serve(max_active, samples_per_step, arrive=arrive):
+    def serve(max_active, samples_per_step, arrive=arrive, integrator="wavefront"):
         """Replays the arrival schedule against a server; returns latencies,
         the wall span and the server stats."""
-        srv = prr.Server(max_active=max_active, samples_per_step=samples_per_step)
+        srv = prr.Server(max_active=max_active, samples_per_step=samples_per_step,
+                         integrator=integrator)
         for s_ in scenes_:
             srv.add_scene(s_)
         srv.wait(srv.submit(0, 2, depth, size=(64, 64)))  # warm-up
@@ -678,8 +680,11 @@ def run_serving(args, rank, world, on):
         lat, span, st = serve(args.max_active, 1 << 20)
     served_rate = total_samples / span / 1e6
     busy_rate = total_samples / st["busy_s"] / 1e6
-    # baseline: the same schedule, one request at a time in arrival order
-    one, one_span, one_st = serve(1, 1 << 24)
+    # the same schedule on megakernel steps (one launch over request tiles)
+    mk, mk_span, mk_st = serve(args.max_active, 1 << 20, integrator="megakernel")
+    # baseline: the same schedule, one request at a time in arrival order,
+    # each rendered by the plain megakernel
+    one, one_span, one_st = serve(1, 1 << 24, integrator="megakernel")
     # a sustainable load: the same requests arriving at 70% of the measured
     # busy throughput (mean work per request / capacity)
     sus_rate = 0.7 * busy_rate * 1e6 / (total_samples / n)
@@ -698,6 +703,11 @@ def run_serving(args, rank, world, on):
                    "total_samples": total_samples},
         "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
         "served_msamples_s": served_rate, "served_busy_msamples_s": busy_rate,
+        "steps": "wavefront (all running requests in one set of ordered ray queues)",
+        "megakernel_steps": {"p50_s": float(np.percentile(mk, 50)),
+                             "p99_s": float(np.percentile(mk, 99)),
+                             "msamples_s": total_samples / mk_span / 1e6,
+                             "busy_msamples_s": total_samples / mk_st["busy_s"] / 1e6},
         "one_at_a_time": {"p50_s": float(np.percentile(one, 50)),
                           "p99_s": float(np.percentile(one, 99)),
                           "msamples_s": total_samples / one_span / 1e6},

@@ -306,8 +306,8 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
  * No counterpart in the reference (its Renderer renders one scene per
  * process). Requests are admitted in arrival order while a slot is free and
  * the device budget (resident scenes + admitted requests) holds; every step
- * renders the next sample chunk of every running request in one launch, so
- * new requests join running ones at the next step. */
+ * renders the next sample chunk of every running request together, so new
+ * requests join running ones at the next step. */
 typedef struct prr_server prr_server;
 typedef struct prr_server_config {
     int64_t device_budget_bytes; /* resident scenes + admitted requests (0: 120 GiB) */
@@ -315,7 +315,14 @@ typedef struct prr_server_config {
     int64_t samples_per_step;    /* samples per request per step (0: 1,048,576) */
     int fail_every_nth_admission;/* fault injection on the host for tests (0: off):
                                     every n-th admission fails its allocation */
+    int integrator;              /* PRR_SERVER_WAVEFRONT (0) or PRR_SERVER_MEGAKERNEL */
+    int64_t paths_per_launch;    /* wavefront: paths per launch group (0: 16,777,216) */
 } prr_server_config;
+/* Wavefront steps: the paths of every running request share one set of
+ * ordered ray queues (one traversal launch per bounce for all of them).
+ * Megakernel steps: one launch over (request, 16x8 tile) items. */
+#define PRR_SERVER_WAVEFRONT 0
+#define PRR_SERVER_MEGAKERNEL 1
 typedef struct prr_request {
     int scene;                    /* id from prr_server_add_scene */
     prr_render_settings settings; /* fixed spp (min_spp == max_spp), window, seed; width and

@@ -45,7 +45,8 @@ class prr_wavefront_config(C.Structure):
 
 class prr_server_config(C.Structure):
     _fields_ = [("device_budget_bytes", C.c_int64), ("max_active", C.c_int),
-                ("samples_per_step", C.c_int64), ("fail_every_nth_admission", C.c_int)]
+                ("samples_per_step", C.c_int64), ("fail_every_nth_admission", C.c_int),
+                ("integrator", C.c_int), ("paths_per_launch", C.c_int64)]
 
 
 class prr_request_info(C.Structure):

@@ -573,10 +573,17 @@ class Server:
     """The render server (continuous batching over resident scenes)."""
 
     def __init__(self, budget_bytes: int = 0, max_active: int = 0, samples_per_step: int = 0,
-                 fail_every_nth_admission: int = 0):
+                 fail_every_nth_admission: int = 0, integrator: str = "wavefront",
+                 paths_per_launch: int = 0):
+        """`integrator`: "wavefront" (every running request's paths in one
+        set of ordered ray queues per step) or "megakernel" (one launch over
+        (request, tile) items per step)."""
         self.lib = _lib.load()
+        kinds = {"wavefront": 0, "megakernel": 1}
+        if integrator not in kinds:
+            raise ValueError(f"integrator must be one of {sorted(kinds)}")
         cfg = prr_server_config(budget_bytes, max_active, samples_per_step,
-                                fail_every_nth_admission)
+                                fail_every_nth_admission, kinds[integrator], paths_per_launch)
         h = C.c_void_p()
         check(self.lib.prr_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

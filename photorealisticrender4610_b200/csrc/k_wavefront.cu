@@ -37,6 +37,22 @@ enum : int {
     kCntActive = 13, kCntSlots = 16
 };
 
+// One request of a multi-request step (the render server): its scene, camera
+// and window, the samples this step traces, and where its paths and pixels
+// start in the step's arrays.
+struct WfReq {
+    const DevScene *scene;
+    DevCamera camera;
+    int W, x0, y0, ww, npix;     // image width, window, window pixels
+    int s0, nspp;                // samples [s0, s0 + nspp) of every window pixel
+    int max_depth;
+    float clamp;
+    uint64_t seed;
+    int64_t path_base, pix_base; // first path / first pixel of this request in the step
+    float3 *film;                // running per-pixel sums, window order
+    unsigned long long rays[2];  // closest, shadow rays traced (added by the kernels)
+};
+
 struct Wf {
     int P, npix, spp_pass;
     int W, x0, y0, ww;
@@ -78,7 +94,57 @@ struct Wf {
     int *act, *act_next; // active pixels (window-local indices), in pixel order
     uint8_t *ptag;       // per active slot: 0 = stays active, 0xFF = done
     float4 *wel0, *wel1; // per pixel: (n, mean r, g, b), (M2 r, g, b, -)
+    // multi-request steps: the request table and each path's request
+    WfReq *reqs;
+    int n_reqs;
+    int *req;
 };
+
+// Per-path scene, clamp and depth: the kernel's own for a render, the path's
+// request's for a server step.
+template <bool MULTI>
+__device__ __forceinline__ const DevScene &scene_of(const DevScene &S0, const Wf &w, int p) {
+    if constexpr (MULTI)
+        return *w.reqs[w.req[p]].scene;
+    else
+        return S0;
+}
+template <bool MULTI> __device__ __forceinline__ float clamp_of(const Wf &w, int p) {
+    if constexpr (MULTI)
+        return w.reqs[w.req[p]].clamp;
+    else
+        return w.clamp;
+}
+template <bool MULTI> __device__ __forceinline__ int depth_of(const Wf &w, int p) {
+    if constexpr (MULTI)
+        return w.reqs[w.req[p]].max_depth;
+    else
+        return w.max_depth;
+}
+// the request whose [base, base + count) range holds index x (bases ascending)
+__device__ __forceinline__ int find_req(const WfReq *reqs, int n, int64_t x, bool pixels) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int64_t b = pixels ? reqs[mid].pix_base : reqs[mid].path_base;
+        if (b <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+// Adds one to a per-request ray counter for every lane of `mask` whose
+// predicate holds, one atomic per request present in the warp.
+__device__ __forceinline__ void count_req_rays(const Wf &w, unsigned mask, bool pred, int r,
+                                               int which) {
+    const unsigned m = __ballot_sync(mask, pred);
+    if (!pred)
+        return;
+    const unsigned same = __match_any_sync(m, r);
+    if ((threadIdx.x & 31) == __ffs(same) - 1)
+        atomicAdd(&w.reqs[r].rays[which], (unsigned long long) __popc(same));
+}
 
 __device__ __forceinline__ uint8_t dir_octant(V3 d) {
     return (uint8_t) ((d.x < 0.f) | ((d.y < 0.f) << 1) | ((d.z < 0.f) << 2));
@@ -113,22 +179,44 @@ __device__ __forceinline__ void finish(const Wf &w, int p, V3 L) {
 }
 
 // ---- generate: camera rays for every (pixel, sample) of the pass
-__global__ void k_wf_generate(DevScene S, Wf w) {
-    const int base = *w.pass_base;
+template <bool MULTI> __global__ void k_wf_generate(DevScene S, Wf w) {
+    const int base = MULTI ? 0 : *w.pass_base;
     const int stride = gridDim.x * blockDim.x;
     // fixed spp: every pixel; adaptive: the active ones (their count is on
-    // the device, set by the previous pass)
+    // the device, set by the previous pass); server step: every request's
+    // window times its samples of this step, request after request
     const int nq = w.adaptive ? (int) w.cnt[kCntActive] : w.npix;
-    const int P = w.adaptive ? nq * w.spp_pass : w.P;
+    const int P = (w.adaptive && !MULTI) ? nq * w.spp_pass : w.P;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += stride) {
-        const int q = w.adaptive ? w.act[p % nq] : p % w.npix;
-        const int s = base + p / nq;
-        const int i = w.x0 + q % w.ww, j = w.y0 + q / w.ww;
-        const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) w.W;
-        Rng rng{path_state(w.seed, m, (uint32_t) (w.sample_offset + s))};
+        int i, j;
+        uint32_t m, sample;
+        uint64_t seed;
+        const DevCamera *cam;
+        if constexpr (MULTI) {
+            const int r = find_req(w.reqs, w.n_reqs, p, false);
+            const WfReq &R = w.reqs[r];
+            const int64_t o = p - R.path_base;
+            const int q = (int) (o % R.npix);
+            i = R.x0 + q % R.ww;
+            j = R.y0 + q / R.ww;
+            m = (uint32_t) i + (uint32_t) j * (uint32_t) R.W;
+            sample = (uint32_t) (R.s0 + o / R.npix);
+            seed = R.seed;
+            cam = &R.camera;
+            w.req[p] = r;
+        } else {
+            const int q = w.adaptive ? w.act[p % nq] : p % w.npix;
+            i = w.x0 + q % w.ww;
+            j = w.y0 + q / w.ww;
+            m = (uint32_t) i + (uint32_t) j * (uint32_t) w.W;
+            sample = (uint32_t) (w.sample_offset + base + p / nq);
+            seed = w.seed;
+            cam = &S.camera;
+        }
+        Rng rng{path_state(seed, m, sample)};
         const float xo = rng.next();
         const float yo = rng.next();
-        const Ray3 r = generate_ray(S.camera, i, j, xo, yo, rng);
+        const Ray3 r = generate_ray(*cam, i, j, xo, yo, rng);
         w.rng[p] = rng.s;
         st3(w.ro, p, r.o);
         st3(w.rd, p, r.d);
@@ -172,7 +260,16 @@ __device__ __forceinline__ void make_stacks(const Wf &w, E *smem, StackCol<E> &t
                      w.blas_sm};
 }
 
-__device__ __forceinline__ void wf_extend(const DevScene &S, const Wf &w, int it, int refill) {
+template <bool MULTI>
+__device__ __forceinline__ const DevScene &lane_scene(const DevScene &S0, const DevScene *ls) {
+    if constexpr (MULTI)
+        return *ls;
+    else
+        return S0;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int it, int refill) {
     extern __shared__ uint2 smem[];
     StackCol<uint2> tc, bc;
     make_stacks(w, smem, tc, bc);
@@ -181,6 +278,8 @@ __device__ __forceinline__ void wf_extend(const DevScene &S, const Wf &w, int it
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int p = -1;
+    // this lane's ray's scene (server steps; a valid scene before the first ray)
+    const DevScene *ls = MULTI ? w.reqs[0].scene : nullptr;
     ClosestWalk cw;
     bool more = n > 0;
     if (!more)
@@ -198,16 +297,23 @@ __device__ __forceinline__ void wf_extend(const DevScene &S, const Wf &w, int it
             base = __shfl_sync(full, base, 0);
             if ((int) (base + cnt) >= n)
                 more = false;
-            if (idle) {
-                const int k = (int) base + __popc(im & ((1u << lane) - 1u));
-                if (k < n) {
-                    p = qin[k];
-                    const float4 o = w.ro[p], d = w.rd[p];
-                    cw.start(S, RayD{o.x, o.y, o.z, d.x, d.y, d.z});
+            const int k = (int) base + __popc(im & ((1u << lane) - 1u));
+            const bool take = idle && k < n;
+            int r = 0;
+            if (take) {
+                p = qin[k];
+                if constexpr (MULTI) {
+                    r = w.req[p];
+                    ls = w.reqs[r].scene;
                 }
+                const float4 o = w.ro[p], d = w.rd[p];
+                cw.start(lane_scene<MULTI>(S0, ls), RayD{o.x, o.y, o.z, d.x, d.y, d.z});
             }
+            if constexpr (MULTI)
+                count_req_rays(w, full, take, r, 0);
         }
         bool done = false;
+        const DevScene &S = lane_scene<MULTI>(S0, ls);
         if (p >= 0)
             done = S.n_objects == 0 || cw.step(S, tc, bc);
         int cls = -1;
@@ -272,7 +378,8 @@ __device__ __forceinline__ Inter load_inter(const DevScene &S, const Wf &w, int 
 // the loop variables of the iteration that now processes `in`.
 __device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, int p,
                                                 const Inter &in, Rng &rng, V3 &beta, V3 &L,
-                                                int &it, bool &specular) {
+                                                int &it, bool &specular, float clamp,
+                                                int max_depth) {
     const int k = w.bounce[p];
     const int fl = w.flags[p];
     const V3 bg = v3(S.background[0], S.background[1], S.background[2]);
@@ -291,7 +398,7 @@ __device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, 
             } else {
                 c = beta * scale * bg;
             }
-            L = L + (indirect ? clamp_indirect(c, w.clamp) : c);
+            L = L + (indirect ? clamp_indirect(c, clamp) : c);
             return false;
         }
         const DevMaterial &hm = S.materials[in.mat];
@@ -304,7 +411,7 @@ __device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, 
             const float pdf_sa = pdf_area * hd2 / smax(cos_l, 1e-4f);
             const V3 c = beta * scale * mis(bpdf, pdf_sa) *
                          v3(hm.emission[0], hm.emission[1], hm.emission[2]);
-            L = L + (indirect ? clamp_indirect(c, w.clamp) : c);
+            L = L + (indirect ? clamp_indirect(c, clamp) : c);
             return false;
         }
         beta = beta * scale;
@@ -326,29 +433,30 @@ __device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, 
         it = 0;
         specular = false;
     }
-    if (it >= w.max_depth)
+    if (it >= max_depth)
         return false;
     if (it == 0 || specular) {
         const V3 d = ld3(w.rd, p);
         if (!in.hit) {
             const V3 b = S.env.loaded ? env_lookup(S.env, d) : bg;
             const V3 c = beta * b;
-            L = L + ((it > 0) ? clamp_indirect(c, w.clamp) : c);
+            L = L + ((it > 0) ? clamp_indirect(c, clamp) : c);
         } else if (S.materials[in.mat].kind == kMatEmissive) {
             const DevMaterial &hm = S.materials[in.mat];
             const V3 c = beta * v3(hm.emission[0], hm.emission[1], hm.emission[2]);
-            L = L + ((it > 0) ? clamp_indirect(c, w.clamp) : c);
+            L = L + ((it > 0) ? clamp_indirect(c, clamp) : c);
         }
     }
     return in.hit;
 }
 
 // ---- miss: the path leaves the scene
-__global__ void k_wf_miss(DevScene S, Wf w) {
+template <bool MULTI> __global__ void k_wf_miss(DevScene S0, Wf w) {
     const int n = (int) w.cnt[kCntMiss];
     const int stride = gridDim.x * blockDim.x;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const int p = w.qmiss[k];
+        const DevScene &S = scene_of<MULTI>(S0, w, p);
         Rng rng{w.rng[p]};
         V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
         Inter in;
@@ -357,13 +465,14 @@ __global__ void k_wf_miss(DevScene S, Wf w) {
         in.a = no_attr();
         int it;
         bool spec;
-        enter_iteration(S, w, p, in, rng, beta, L, it, spec);
+        enter_iteration(S, w, p, in, rng, beta, L, it, spec, clamp_of<MULTI>(w, p),
+                        depth_of<MULTI>(w, p));
         finish(w, p, L);
     }
 }
 
 // ---- delta: one step of the specular chain
-__global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
+template <bool MULTI> __global__ void k_wf_delta(DevScene S0, Wf w, int it_next) {
     const int n = (int) w.cnt[kCntDelta];
     int *qout = w.qray[it_next & 1];
     const int stride = gridDim.x * blockDim.x;
@@ -373,12 +482,15 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
         int p = 0;
         if (k < n) {
             p = w.qdelta[k];
+            const DevScene &S = scene_of<MULTI>(S0, w, p);
+            const int max_depth = depth_of<MULTI>(w, p);
             Rng rng{w.rng[p]};
             V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
             const Inter in = load_inter(S, w, p);
             int it;
             bool spec;
-            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec)) {
+            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec, clamp_of<MULTI>(w, p),
+                                 max_depth)) {
                 finish(w, p, L);
             } else {
                 const DevMaterial &m = S.materials[in.mat];
@@ -394,7 +506,7 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
                     if (trans)
                         beta = beta * sd.base;
                     // the next ray is only looked at if the loop runs again
-                    if (it + 1 >= w.max_depth) {
+                    if (it + 1 >= max_depth) {
                         finish(w, p, L);
                     } else {
                         st3(w.ro, p, in.p + off * PRR_EPS);
@@ -423,7 +535,8 @@ __global__ void k_wf_delta(DevScene S, Wf w, int it_next) {
 // ---- surface: NEE + BSDF sampling of a non-delta bounce
 // 64 registers (8 blocks of 128 per SM): this stage waits on scattered path
 // state and scene data, so resident warps matter more than a few spills.
-__global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S, Wf w, int it_next) {
+template <bool MULTI>
+__global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it_next) {
     const int n = (int) w.cnt[kCntSurf];
     int *qout = w.qray[it_next & 1];
     const int stride = gridDim.x * blockDim.x;
@@ -433,12 +546,14 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S, Wf w, int it_
         int p = 0;
         if (k < n) {
             p = w.qsurf[k];
+            const DevScene &S = scene_of<MULTI>(S0, w, p);
             Rng rng{w.rng[p]};
             V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
             const Inter in = load_inter(S, w, p);
             int it;
             bool spec;
-            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec)) {
+            if (!enter_iteration(S, w, p, in, rng, beta, L, it, spec, clamp_of<MULTI>(w, p),
+                                 depth_of<MULTI>(w, p))) {
                 finish(w, p, L);
             } else {
                 const DevMaterial &m = S.materials[in.mat];
@@ -556,7 +671,8 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S, Wf w, int it_
 }
 
 // ---- shadow: visibility of every queued NEE ray (persistent, per-lane refill)
-__device__ __forceinline__ void wf_shadow(const DevScene &S, const Wf &w, int refill) {
+template <bool MULTI>
+__device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int refill) {
     extern __shared__ uint32_t smem32[];
     StackCol<uint32_t> tc, bc;
     make_stacks(w, smem32, tc, bc);
@@ -564,6 +680,8 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S, const Wf &w, int re
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int job = -1;
+    // this lane's ray's scene (server steps; a valid scene before the first ray)
+    const DevScene *ls = MULTI ? w.reqs[0].scene : nullptr;
     AnyWalk aw;
     bool more = n > 0;
     unsigned rays = 0;
@@ -580,21 +698,28 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S, const Wf &w, int re
             base = __shfl_sync(full, base, 0);
             if ((int) (base + cnt) >= n)
                 more = false;
-            if (idle) {
-                const int k = (int) base + __popc(im & ((1u << lane) - 1u));
-                if (k < n) {
-                    job = w.qjob[k];
-                    const int p = job >> 1;
-                    const float4 o = (job & 1) ? w.seo[p] : w.slo[p];
-                    const float4 d = (job & 1) ? w.sed[p] : w.sld[p];
-                    rays++;
-                    if (!aw.start(S, RayD{o.x, o.y, o.z, d.x, d.y, d.z}, o.w)) {
-                        w.vis[job] = 1;
-                        job = -1;
-                    }
+            const int k = (int) base + __popc(im & ((1u << lane) - 1u));
+            const bool take = idle && k < n;
+            int r = 0;
+            if (take) {
+                job = w.qjob[k];
+                const int p = job >> 1;
+                if constexpr (MULTI) {
+                    r = w.req[p];
+                    ls = w.reqs[r].scene;
+                }
+                const float4 o = (job & 1) ? w.seo[p] : w.slo[p];
+                const float4 d = (job & 1) ? w.sed[p] : w.sld[p];
+                rays++;
+                if (!aw.start(lane_scene<MULTI>(S0, ls), RayD{o.x, o.y, o.z, d.x, d.y, d.z}, o.w)) {
+                    w.vis[job] = 1;
+                    job = -1;
                 }
             }
+            if constexpr (MULTI)
+                count_req_rays(w, full, take, r, 1);
         }
+        const DevScene &S = lane_scene<MULTI>(S0, ls);
         if (job >= 0 && aw.step(S, tc, bc)) {
             w.vis[job] = aw.occluded ? 0 : 1;
             job = -1;
@@ -607,15 +732,15 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S, const Wf &w, int re
                   (unsigned long long) rays);
 }
 
-__global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
-    wf_extend(S, w, it, refill);
+template <bool MULTI> __global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
+    wf_extend<MULTI>(S, w, it, refill);
 }
-__global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
-    wf_shadow(S, w, refill);
+template <bool MULTI> __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
+    wf_shadow<MULTI>(S, w, refill);
 }
 
 // ---- add the visible NEE contributions, light first, then env, as castRay
-__global__ void k_wf_shadow_resolve(Wf w) {
+template <bool MULTI> __global__ void k_wf_shadow_resolve(Wf w) {
     const int n = (int) w.cnt[kCntShadow];
     const int stride = gridDim.x * blockDim.x;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -627,7 +752,7 @@ __global__ void k_wf_shadow_resolve(Wf w) {
                 continue;
             const float4 c = r == 0 ? w.slc[p] : w.sec[p];
             const V3 cv = v3(c.x, c.y, c.z);
-            L = L + (c.w != 0.f ? clamp_indirect(cv, w.clamp) : cv);
+            L = L + (c.w != 0.f ? clamp_indirect(cv, clamp_of<MULTI>(w, p)) : cv);
         }
         if (w.flags[p] & kFlagEndAfterShadow)
             finish(w, p, L);
@@ -887,6 +1012,28 @@ __global__ void k_wf_resolve_adaptive(const float3 *film, const float4 *wel0, in
         spp[q] = n;
 }
 
+// ---- server step film: every request's window pixels take this step's
+// samples in sample order (the same sums as a render of the request alone)
+__global__ void k_wf_film_multi(Wf w, int64_t total_pixels) {
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < total_pixels;
+         t += stride) {
+        const int r = find_req(w.reqs, w.n_reqs, t, true);
+        const WfReq &R = w.reqs[r];
+        const int q = (int) (t - R.pix_base);
+        float3 f = R.film[q];
+        for (int s = 0; s < R.nspp; s++) {
+            const float4 v = w.result[R.path_base + (int64_t) s * R.npix + q];
+            if (!(isnan(v.x) || isnan(v.y) || isnan(v.z))) {
+                f.x += v.x;
+                f.y += v.y;
+                f.z += v.z;
+            }
+        }
+        R.film[q] = f;
+    }
+}
+
 __global__ void k_wf_film(Wf w) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q < w.npix) {
@@ -950,6 +1097,199 @@ struct WavefrontPlan {
     }
 };
 
+namespace {
+
+// Bytes of the path-state layout for P paths and npix film pixels.
+size_t wf_bytes(size_t P, int npix) {
+    const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
+    const int ptiles = (npix + kPartTile - 1) / kPartTile;
+    return 256 * 48 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2 + 4) + (size_t) ntiles * kPartTile +
+           (size_t) npix * (16 + 8 + 32) + (size_t) ptiles * kPartTile +
+           (size_t) std::max(ntiles, ptiles) * 32 + 4096;
+}
+
+// Carves the per-path arrays, queues, counters and partition buffers of P
+// paths and npix pixels out of `buf` (grown as needed).
+int wf_layout(DevBuf &buf, Wf &w, size_t P, int npix) {
+    const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
+    const int ptiles = (npix + kPartTile - 1) / kPartTile;
+    const size_t bytes = wf_bytes(P, npix);
+    PRR_CUDA_TRY(buf.ensure(bytes));
+    char *cur = (char *) buf.ptr;
+    w.rng = carve<uint64_t>(cur, P);
+    w.ro = carve<float4>(cur, P);
+    w.rd = carve<float4>(cur, P);
+    w.beta = carve<float4>(cur, P);
+    w.L = carve<float4>(cur, P);
+    w.pend = carve<float4>(cur, P);
+    w.prev = carve<float4>(cur, P);
+    w.hit = carve<int4>(cur, P);
+    w.slo = carve<float4>(cur, P);
+    w.sld = carve<float4>(cur, P);
+    w.slc = carve<float4>(cur, P);
+    w.seo = carve<float4>(cur, P);
+    w.sed = carve<float4>(cur, P);
+    w.sec = carve<float4>(cur, P);
+    w.result = carve<float4>(cur, P);
+    w.bounce = carve<int>(cur, P);
+    w.flags = carve<int>(cur, P);
+    w.req = carve<int>(cur, P);
+    w.qray[0] = carve<int>(cur, P);
+    w.qray[1] = carve<int>(cur, P);
+    w.qmiss = carve<int>(cur, P);
+    w.qdelta = carve<int>(cur, P);
+    w.qsurf = carve<int>(cur, P);
+    w.qshadow = carve<int>(cur, P);
+    w.qjob = carve<int>(cur, 2 * P);
+    w.vis = carve<uint8_t>(cur, 2 * P);
+    w.film = carve<float3>(cur, (size_t) npix);
+    w.cnt = carve<unsigned>(cur, kCntSlots);
+    w.pass_base = carve<int>(cur, 4);
+    w.tag = carve<uint8_t>(cur, (size_t) ntiles * kPartTile);
+    w.tile = carve<unsigned>(cur, (size_t) std::max(ntiles, ptiles) * 8);
+    w.act = carve<int>(cur, (size_t) npix);
+    w.act_next = carve<int>(cur, (size_t) npix);
+    w.ptag = carve<uint8_t>(cur, (size_t) ptiles * kPartTile);
+    w.wel0 = carve<float4>(cur, (size_t) npix);
+    w.wel1 = carve<float4>(cur, (size_t) npix);
+    if ((size_t) (cur - (char *) buf.ptr) > bytes)
+        return fail(PRR_ERR_INTERNAL, "wavefront buffer layout overflow");
+    return PRR_OK;
+}
+
+// Launch shape of one bounce: traversal grids, stack split, spill buffer.
+struct WfShape {
+    int block, refill, g_ext, g_sh, g_shade, g_gen, ntiles, ptiles;
+    size_t smem_ext, smem_sh;
+    void (*ext)(DevScene, Wf, int, int);
+    void (*sh)(DevScene, Wf, int);
+};
+
+template <bool MULTI>
+int wf_shape(Wf &w, DevBuf &spill, int block_req, int stack_req, int refill_req, WfShape &L) {
+    const int sms = device_sm_count();
+    L.block = block_req > 0 ? block_req : 128;
+    // Stacks: the scene-level one wholly in shared memory, the mesh one up to
+    // stack_req entries (0: all of it) within 96 KB per block; its deeper
+    // entries go to the global spill buffer.
+    const int max_sm_entries = (96 * 1024) / (L.block * (int) sizeof(uint2));
+    if (w.tlas_cap + 1 > max_sm_entries)
+        return fail(PRR_ERR_UNSUPPORTED, "scene BVH too deep for the shared-memory stack");
+    w.blas_sm = stack_req > 0 ? std::min(stack_req, w.blas_cap) : w.blas_cap;
+    w.blas_sm = std::max(1, std::min(w.blas_sm, max_sm_entries - w.tlas_cap));
+    L.smem_ext = (size_t) (w.tlas_cap + w.blas_sm) * L.block * sizeof(uint2);
+    L.smem_sh = (size_t) (w.tlas_cap + w.blas_sm) * L.block * sizeof(uint32_t);
+    L.ext = k_wf_extend<MULTI>;
+    L.sh = k_wf_shadow<MULTI>;
+    if (L.smem_ext > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) L.ext,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) L.smem_ext));
+    if (L.smem_sh > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) L.sh,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) L.smem_sh));
+    // Deep stacks want the largest shared-memory split; shallow ones keep the
+    // default, since every change of split between consecutive kernels drains
+    // the SM (which dominates frames made of many short launches).
+    const int carve_pref = L.smem_ext > 16 * 1024 ? (int) cudaSharedmemCarveoutMaxShared
+                                                  : (int) cudaSharedmemCarveoutDefault;
+    cudaFuncSetAttribute((const void *) L.ext, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         carve_pref);
+    cudaFuncSetAttribute((const void *) L.sh, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         carve_pref);
+    L.refill = refill_req > 0 ? std::min(refill_req, 32) : 8;
+    int occ_ext = 1, occ_sh = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, (const void *) L.ext, L.block,
+                                                  L.smem_ext);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, (const void *) L.sh, L.block,
+                                                  L.smem_sh);
+    L.g_ext = sms * std::max(1, occ_ext);
+    L.g_sh = sms * std::max(1, occ_sh);
+    const size_t spill_entries = (size_t) (w.blas_cap - w.blas_sm);
+    const size_t spill_bytes =
+        spill_entries * std::max((size_t) L.g_ext * L.block * sizeof(uint2),
+                                 (size_t) L.g_sh * L.block * sizeof(uint32_t));
+    PRR_CUDA_TRY(spill.ensure(spill_bytes));
+    w.spill = spill.ptr;
+    L.g_shade = sms * 8;
+    L.g_gen = (int) std::min<int64_t>(((int64_t) w.P + 255) / 256, (int64_t) sms * 16);
+    L.ntiles = (int) (((size_t) w.P + kPartTile - 1) / kPartTile);
+    L.ptiles = (w.npix + kPartTile - 1) / kPartTile;
+    return PRR_OK;
+}
+
+// The stable partitions of the ordered queues.
+struct WfParts {
+    PartSpec cls, ray[2], act;
+};
+WfParts wf_parts(const Wf &w) {
+    WfParts P;
+    // hit classes -> miss / delta / surface queues
+    P.cls = PartSpec{};
+    P.cls.tag = w.tag;
+    P.cls.q[0] = w.qmiss;
+    P.cls.q[1] = w.qdelta;
+    P.cls.q[2] = w.qsurf;
+    P.cls.nb = 3;
+    P.cls.concat = 0;
+    P.cls.count_slot[0] = kCntMiss;
+    P.cls.count_slot[1] = kCntDelta;
+    P.cls.count_slot[2] = kCntSurf;
+    P.cls.total_slot = -1;
+    // next rays -> the ray queue, direction octant major
+    for (int r = 0; r < 2; r++) {
+        P.ray[r] = PartSpec{};
+        P.ray[r].tag = w.tag;
+        P.ray[r].q[0] = w.qray[r];
+        P.ray[r].nb = 8;
+        P.ray[r].concat = 1;
+        for (int b = 0; b < 8; b++)
+            P.ray[r].count_slot[b] = -1;
+        P.ray[r].total_slot = kCntRay0 + r;
+    }
+    // adaptive: the pixels still active -> the next pass's active list
+    P.act = PartSpec{};
+    P.act.tag = w.ptag;
+    P.act.map = w.act;
+    P.act.q[0] = w.act_next;
+    P.act.nb = 1;
+    P.act.concat = 1;
+    P.act.count_slot[0] = -1;
+    P.act.total_slot = kCntActive;
+    return P;
+}
+
+void wf_partition(const Wf &w, const PartSpec &ps, int nt, cudaStream_t cs) {
+    k_part_count<<<nt, kPartThreads, 0, cs>>>(w, ps);
+    k_part_scan<<<1, 1024, 0, cs>>>(w, nt, ps);
+    k_part_scatter<<<nt, kPartThreads, 0, cs>>>(w, ps);
+}
+
+// generate + every bounce of one pass (no film stage)
+template <bool MULTI>
+int wf_enqueue_bounces(const DevScene &S, const Wf &w, const WfShape &L, const WfParts &parts,
+                       cudaStream_t cs) {
+    k_wf_generate<MULTI><<<L.g_gen, 256, 0, cs>>>(S, w);
+    for (int it = 0; it <= w.max_depth; it++) {
+        k_wf_begin<<<1, 32, 0, cs>>>(w, it);
+        L.ext<<<L.g_ext, L.block, L.smem_ext, cs>>>(S, w, it, L.refill);
+        if (w.ordered)
+            wf_partition(w, parts.cls, L.ntiles, cs);
+        k_wf_miss<MULTI><<<L.g_shade, 128, 0, cs>>>(S, w);
+        k_wf_delta<MULTI><<<L.g_shade, 128, 0, cs>>>(S, w, it + 1);
+        k_wf_surface<MULTI><<<L.g_shade, 128, 0, cs>>>(S, w, it + 1);
+        L.sh<<<L.g_sh, L.block, L.smem_sh, cs>>>(S, w, L.refill);
+        k_wf_shadow_resolve<MULTI><<<L.g_shade, 128, 0, cs>>>(w);
+        if (w.ordered)
+            wf_partition(w, parts.ray[(it + 1) & 1], L.ntiles, cs);
+    }
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
+} // namespace
+
 int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                      unsigned long long *out_rays, cudaStream_t st) {
     const DevScene &S = s.dev;
@@ -974,169 +1314,34 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
         spp_pass--;
     w.spp_pass = spp_pass;
     w.P = spp_pass * w.npix;
-    const size_t P = (size_t) w.P;
-    const int ntiles = (int) ((P + kPartTile - 1) / kPartTile);
-    const int ptiles = (w.npix + kPartTile - 1) / kPartTile; // active-pixel partition
-    const size_t bytes = 256 * 48 + P * (8 + 16 * 16 + 4 * 2 + 4 * 9 + 2) +
-                         (size_t) ntiles * kPartTile + (size_t) w.npix * (16 + 8 + 32) +
-                         (size_t) ptiles * kPartTile + (size_t) std::max(ntiles, ptiles) * 32 +
-                         4096;
-    PRR_CUDA_TRY(s.d_wavefront.ensure(bytes));
-    char *cur = (char *) s.d_wavefront.ptr;
-    w.rng = carve<uint64_t>(cur, P);
-    w.ro = carve<float4>(cur, P);
-    w.rd = carve<float4>(cur, P);
-    w.beta = carve<float4>(cur, P);
-    w.L = carve<float4>(cur, P);
-    w.pend = carve<float4>(cur, P);
-    w.prev = carve<float4>(cur, P);
-    w.hit = carve<int4>(cur, P);
-    w.slo = carve<float4>(cur, P);
-    w.sld = carve<float4>(cur, P);
-    w.slc = carve<float4>(cur, P);
-    w.seo = carve<float4>(cur, P);
-    w.sed = carve<float4>(cur, P);
-    w.sec = carve<float4>(cur, P);
-    w.result = carve<float4>(cur, P);
-    w.bounce = carve<int>(cur, P);
-    w.flags = carve<int>(cur, P);
-    w.qray[0] = carve<int>(cur, P);
-    w.qray[1] = carve<int>(cur, P);
-    w.qmiss = carve<int>(cur, P);
-    w.qdelta = carve<int>(cur, P);
-    w.qsurf = carve<int>(cur, P);
-    w.qshadow = carve<int>(cur, P);
-    w.qjob = carve<int>(cur, 2 * P);
-    w.vis = carve<uint8_t>(cur, 2 * P);
-    w.film = carve<float3>(cur, (size_t) w.npix);
-    w.cnt = carve<unsigned>(cur, kCntSlots);
-    w.pass_base = carve<int>(cur, 4);
-    w.tag = carve<uint8_t>(cur, (size_t) ntiles * kPartTile);
-    w.tile = carve<unsigned>(cur, (size_t) std::max(ntiles, ptiles) * 8);
+    if (int rc = wf_layout(s.d_wavefront, w, (size_t) w.P, w.npix))
+        return rc;
     w.ordered = s.wf_ordered ? 1 : 0;
     w.adaptive = rs.min_spp < rs.max_spp ? 1 : 0;
     w.min_spp = rs.min_spp;
     w.max_spp = rs.max_spp;
     w.threshold = rs.variance_threshold;
-    w.act = carve<int>(cur, (size_t) w.npix);
-    w.act_next = carve<int>(cur, (size_t) w.npix);
-    w.ptag = carve<uint8_t>(cur, (size_t) ptiles * kPartTile);
-    w.wel0 = carve<float4>(cur, (size_t) w.npix);
-    w.wel1 = carve<float4>(cur, (size_t) w.npix);
-    if ((size_t) (cur - (char *) s.d_wavefront.ptr) > bytes)
-        return fail(PRR_ERR_INTERNAL, "wavefront buffer layout overflow");
-
-    const int sms = device_sm_count();
-    const int block = s.wf_block > 0 ? s.wf_block : 128;
-    // Stacks: the scene-level one wholly in shared memory, the mesh one up to
-    // wf_stack entries (0: all of it) within 96 KB per block; its deeper
-    // entries go to the global spill buffer.
-    const int max_sm_entries = (96 * 1024) / (block * (int) sizeof(uint2));
-    if (w.tlas_cap + 1 > max_sm_entries)
-        return fail(PRR_ERR_UNSUPPORTED, "scene BVH too deep for the shared-memory stack");
-    w.blas_sm = s.wf_stack > 0 ? std::min(s.wf_stack, w.blas_cap) : w.blas_cap;
-    w.blas_sm = std::max(1, std::min(w.blas_sm, max_sm_entries - w.tlas_cap));
-    const size_t smem_ext = (size_t) (w.tlas_cap + w.blas_sm) * block * sizeof(uint2);
-    const size_t smem_sh = (size_t) (w.tlas_cap + w.blas_sm) * block * sizeof(uint32_t);
-    auto *k_ext = k_wf_extend;
-    auto *k_sh = k_wf_shadow;
-    if (smem_ext > 48 * 1024)
-        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) k_ext,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_ext));
-    if (smem_sh > 48 * 1024)
-        PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) k_sh,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_sh));
-    // Deep stacks want the largest shared-memory split; shallow ones keep the
-    // default, since every change of split between consecutive kernels drains
-    // the SM (which dominates frames made of many short launches).
-    const int carve = smem_ext > 16 * 1024 ? (int) cudaSharedmemCarveoutMaxShared
-                                           : (int) cudaSharedmemCarveoutDefault;
-    cudaFuncSetAttribute((const void *) k_ext, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         carve);
-    cudaFuncSetAttribute((const void *) k_sh, cudaFuncAttributePreferredSharedMemoryCarveout,
-                         carve);
-    const int refill = s.wf_refill > 0 ? std::min(s.wf_refill, 32) : 8;
-    int occ_ext = 1, occ_sh = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, (const void *) k_ext, block, smem_ext);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, (const void *) k_sh, block, smem_sh);
-    const int g_ext = sms * std::max(1, occ_ext);
-    const int g_sh = sms * std::max(1, occ_sh);
-    const size_t spill_entries = (size_t) (w.blas_cap - w.blas_sm);
-    const size_t spill_bytes =
-        spill_entries * std::max((size_t) g_ext * block * sizeof(uint2),
-                                 (size_t) g_sh * block * sizeof(uint32_t));
-    PRR_CUDA_TRY(s.d_wf_spill.ensure(spill_bytes));
-    w.spill = s.d_wf_spill.ptr;
-    const int g_shade = sms * 8;
-    const int g_gen = (int) std::min<int64_t>((P + 255) / 256, (int64_t) sms * 16);
+    WfShape L;
+    if (int rc = wf_shape<false>(w, s.d_wf_spill, s.wf_block, s.wf_stack, s.wf_refill, L))
+        return rc;
+    const WfParts parts = wf_parts(w);
 
     PRR_CUDA_TRY(cudaMemsetAsync(w.film, 0, (size_t) w.npix * sizeof(float3), st));
-    PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) ntiles * kPartTile, st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) L.ntiles * kPartTile, st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
     PRR_CUDA_TRY(cudaMemsetAsync(w.pass_base, 0, sizeof(int), st));
     if (w.adaptive) { // after the counters are cleared: it sets the active count
-        PRR_CUDA_TRY(cudaMemsetAsync(w.ptag, 0xFF, (size_t) ptiles * kPartTile, st));
+        PRR_CUDA_TRY(cudaMemsetAsync(w.ptag, 0xFF, (size_t) L.ptiles * kPartTile, st));
         k_wf_adaptive_init<<<(w.npix + 255) / 256, 256, 0, st>>>(w);
     }
 
-    // ordered queues: hit classes -> miss / delta / surface queues; next rays
-    // -> the ray queue, direction octant major
-    PartSpec part_cls{};
-    part_cls.tag = w.tag;
-    part_cls.q[0] = w.qmiss;
-    part_cls.q[1] = w.qdelta;
-    part_cls.q[2] = w.qsurf;
-    part_cls.nb = 3;
-    part_cls.concat = 0;
-    part_cls.count_slot[0] = kCntMiss;
-    part_cls.count_slot[1] = kCntDelta;
-    part_cls.count_slot[2] = kCntSurf;
-    part_cls.total_slot = -1;
-    PartSpec part_ray[2];
-    for (int r = 0; r < 2; r++) {
-        part_ray[r] = PartSpec{};
-        part_ray[r].tag = w.tag;
-        part_ray[r].q[0] = w.qray[r];
-        part_ray[r].nb = 8;
-        part_ray[r].concat = 1;
-        for (int b = 0; b < 8; b++)
-            part_ray[r].count_slot[b] = -1;
-        part_ray[r].total_slot = kCntRay0 + r;
-    }
-    // adaptive: the pixels still active -> the next pass's active list
-    PartSpec part_act{};
-    part_act.tag = w.ptag;
-    part_act.map = w.act;
-    part_act.q[0] = w.act_next;
-    part_act.nb = 1;
-    part_act.concat = 1;
-    part_act.count_slot[0] = -1;
-    part_act.total_slot = kCntActive;
-    auto partition = [&](const PartSpec &ps, int nt, cudaStream_t cs) {
-        k_part_count<<<nt, kPartThreads, 0, cs>>>(w, ps);
-        k_part_scan<<<1, 1024, 0, cs>>>(w, nt, ps);
-        k_part_scatter<<<nt, kPartThreads, 0, cs>>>(w, ps);
-    };
-
-    // capture one pass
+    // one pass: the bounces, then the film stage
     auto enqueue_pass = [&](cudaStream_t cs) -> int {
-        k_wf_generate<<<g_gen, 256, 0, cs>>>(S, w);
-        for (int it = 0; it <= w.max_depth; it++) {
-            k_wf_begin<<<1, 32, 0, cs>>>(w, it);
-            k_ext<<<g_ext, block, smem_ext, cs>>>(S, w, it, refill);
-            if (w.ordered)
-                partition(part_cls, ntiles, cs);
-            k_wf_miss<<<g_shade, 128, 0, cs>>>(S, w);
-            k_wf_delta<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
-            k_wf_surface<<<g_shade, 128, 0, cs>>>(S, w, it + 1);
-            k_sh<<<g_sh, block, smem_sh, cs>>>(S, w, refill);
-            k_wf_shadow_resolve<<<g_shade, 128, 0, cs>>>(w);
-            if (w.ordered)
-                partition(part_ray[(it + 1) & 1], ntiles, cs);
-        }
+        if (int rc = wf_enqueue_bounces<false>(S, w, L, parts, cs))
+            return rc;
         if (w.adaptive) {
             k_wf_film_adaptive<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
-            partition(part_act, ptiles, cs);
+            wf_partition(w, parts.act, L.ptiles, cs);
             k_wf_copy_active<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
         } else {
             k_wf_film<<<(w.npix + 255) / 256, 256, 0, cs>>>(w);
@@ -1146,8 +1351,8 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     };
     const int passes = rs.max_spp / spp_pass;
     uint64_t key = (uint64_t) (uintptr_t) s.d_wavefront.ptr;
-    key = mix64(key ^ ((uint64_t) w.P << 20) ^ ((uint64_t) w.max_depth << 8) ^ (uint64_t) block ^
-                ((uint64_t) refill << 50));
+    key = mix64(key ^ ((uint64_t) w.P << 20) ^ ((uint64_t) w.max_depth << 8) ^
+                (uint64_t) L.block ^ ((uint64_t) L.refill << 50));
     key = mix64(key ^ (uint64_t) (uintptr_t) w.spill ^ ((uint64_t) w.blas_sm << 32) ^
                 ((uint64_t) w.ordered << 60));
     key = mix64(key ^ ((uint64_t) w.adaptive << 7) ^ ((uint64_t) w.min_spp << 24) ^
@@ -1206,6 +1411,76 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     const int64_t per_pass = 2 + (int64_t) (w.max_depth + 1) * (7 + (w.ordered ? 6 : 0)) +
                              (w.adaptive ? 4 : 0);
     s.last_launches = per_pass * passes + 1 + (w.adaptive ? 1 : 0) + (out_rays ? 1 : 0);
+    return PRR_OK;
+}
+
+int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n, int tlas_cap,
+                         int blas_cap, unsigned long long *rays_host, cudaStream_t st,
+                         int64_t *launches) {
+    if (n <= 0)
+        return PRR_OK;
+    Wf w{};
+    int64_t P = 0, npix = 0;
+    int max_depth = 1;
+    std::vector<WfReq> table(n);
+    for (int k = 0; k < n; k++) {
+        const WfStepReq &q = reqs[k];
+        WfReq &t = table[k];
+        std::memset(&t, 0, sizeof(t));
+        t.scene = q.scene;
+        t.camera = q.camera;
+        t.W = q.camera.width;
+        t.x0 = q.x0;
+        t.y0 = q.y0;
+        t.ww = q.ww;
+        t.npix = q.ww * q.wh;
+        t.s0 = q.s0;
+        t.nspp = q.nspp;
+        t.max_depth = q.max_depth;
+        t.clamp = q.clamp;
+        t.seed = q.seed;
+        t.path_base = P;
+        t.pix_base = npix;
+        t.film = q.film;
+        P += (int64_t) t.npix * t.nspp;
+        npix += t.npix;
+        max_depth = std::max(max_depth, q.max_depth);
+    }
+    if (P >= ((int64_t) 1 << 31))
+        return fail(PRR_ERR_INVALID_ARGUMENT, "server step too large");
+    w.P = (int) P;
+    w.npix = 0; // no per-render film or active list in a server step
+    w.max_depth = max_depth;
+    w.ordered = 1;
+    w.n_reqs = n;
+    w.tlas_cap = tlas_cap;
+    w.blas_cap = blas_cap;
+    if (int rc = wf_layout(ms.state, w, (size_t) P, 1))
+        return rc;
+    PRR_CUDA_TRY(ms.reqs.ensure((size_t) n * sizeof(WfReq)));
+    w.reqs = ms.reqs.as<WfReq>();
+    WfShape L;
+    if (int rc = wf_shape<true>(w, ms.spill, 128, 8, 8, L))
+        return rc;
+    const WfParts parts = wf_parts(w);
+    PRR_CUDA_TRY(cudaMemcpyAsync(w.reqs, table.data(), (size_t) n * sizeof(WfReq),
+                                 cudaMemcpyHostToDevice, st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) L.ntiles * kPartTile, st));
+    PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
+    if (int rc = wf_enqueue_bounces<true>(DevScene{}, w, L, parts, st))
+        return rc;
+    k_wf_film_multi<<<(int) std::min<int64_t>((npix + 255) / 256, (int64_t) device_sm_count() * 16),
+                      256, 0, st>>>(w, npix);
+    PRR_CUDA_TRY(cudaGetLastError());
+    // the rays each request traced: one strided copy out of the table
+    if (rays_host)
+        PRR_CUDA_TRY(cudaMemcpy2DAsync(rays_host, 2 * sizeof(unsigned long long), &w.reqs[0].rays,
+                                       sizeof(WfReq), 2 * sizeof(unsigned long long), n,
+                                       cudaMemcpyDeviceToHost, st));
+    // generate + per bounce (begin, extend, 3-kernel partition, miss, delta,
+    // surface, shadow, shadow_resolve, 3-kernel partition) + film
+    if (launches)
+        *launches = 1 + (int64_t) (w.max_depth + 1) * 13 + 1;
     return PRR_OK;
 }
 

@@ -152,6 +152,29 @@ int validate_render(const Scene &s, prr_render_settings &rs);
 int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                      unsigned long long *out_rays, cudaStream_t st);
 
+// One request of a render-server step on the wavefront integrator: samples
+// [s0, s0 + nspp) of every pixel of its window, summed into `film`.
+struct WfStepReq {
+    const DevScene *scene; // the scene's resident descriptor (device memory)
+    DevCamera camera;      // the scene's camera at the request's resolution
+    int x0, y0, ww, wh;    // pixel window
+    int s0, nspp;
+    int max_depth;
+    float clamp;
+    uint64_t seed;
+    float3 *film; // ww*wh running sums (device)
+};
+// Device buffers a server keeps across its wavefront steps.
+struct WfMultiState {
+    DevBuf state, spill, reqs;
+};
+// Traces one step of n requests as one set of ordered ray queues. Per
+// request, rays_host[2k], rays_host[2k+1] receive the closest and shadow rays
+// it traced (valid once the stream has drained); `launches` the kernel count.
+int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n, int tlas_cap,
+                         int blas_cap, unsigned long long *rays_host, cudaStream_t st,
+                         int64_t *launches);
+
 int device_sm_count();
 DevCamera make_camera(const prr_camera &c, int width, int height);
 

@@ -4,14 +4,19 @@
 // prr_server_submit and admitted in arrival order by a worker thread as long
 // as (a) fewer than max_active requests are running and (b) the device bytes
 // of the resident scenes plus every admitted request stay within the budget.
-// Every step renders the next sample chunk of EVERY running request in one
-// launch (k_serve.cu), so requests that arrive while others are on the GPU
-// join at the next step and overlap with them; a request leaves as soon as
-// its last chunk is done, freeing its slot and memory for the queue.
+// Every step renders the next sample chunk of EVERY running request, so
+// requests that arrive while others are on the GPU join at the next step and
+// overlap with them; a request leaves as soon as its last chunk is done,
+// freeing its slot and memory for the queue. A step runs either on the
+// wavefront integrator (k_wavefront.cu: the paths of all running requests,
+// up to paths_per_launch per group, share one set of ordered ray queues, so
+// each bounce is one traversal launch for all of them) or as one megakernel
+// launch over (request, 16x8 tile) items (k_serve.cu).
 //
 // A request's chunk size depends only on the request (samples_per_step / its
-// pixel count), and its film adds chunk sums in chunk order, so its image is
-// the same alone as in any mix.
+// pixel count), and its film adds samples (wavefront: one by one, in sample
+// order, as a render of the request does) or chunk sums (megakernel) in
+// order, so its image is the same alone as in any mix.
 #include "prr_internal.h"
 #include "serve.h"
 
@@ -74,6 +79,11 @@ struct Server {
     ServeReq *p_reqs = nullptr;   // pinned
     size_t cap_items = 0, cap_reqs = 0;
     DevBuf d_items, d_reqs;
+    // wavefront steps
+    WfMultiState wf;
+    std::vector<WfStepReq> wf_reqs;
+    unsigned long long *p_rays = nullptr; // pinned, 2 per active request
+    size_t cap_rays = 0;
 
     // stats
     int64_t submitted = 0, completed = 0, failed = 0, samples = 0, steps = 0;
@@ -85,6 +95,8 @@ struct Server {
             cudaFreeHost(p_items);
         if (p_reqs)
             cudaFreeHost(p_reqs);
+        if (p_rays)
+            cudaFreeHost(p_rays);
         if (st)
             cudaStreamDestroy(st);
     }
@@ -150,8 +162,73 @@ int ensure_tables(Server &S, size_t items, size_t reqs) {
     return PRR_OK;
 }
 
+// One wavefront step over every running request: groups of requests (in
+// admission order) of at most paths_per_launch paths each, one after another
+// on the server's stream.
+int run_step_wavefront(Server &S) {
+    const DevScene *d_scenes = S.d_scenes.as<DevScene>();
+    const size_t n = S.active.size();
+    if (2 * n > S.cap_rays) {
+        if (S.p_rays)
+            cudaFreeHost(S.p_rays);
+        S.p_rays = nullptr;
+        S.cap_rays = std::max(2 * n, 2 * S.cap_rays);
+        PRR_CUDA_TRY(cudaMallocHost(&S.p_rays, S.cap_rays * sizeof(unsigned long long)));
+    }
+    S.wf_reqs.resize(n);
+    for (size_t q = 0; q < n; q++) {
+        const Req *r = S.active[q];
+        WfStepReq &d = S.wf_reqs[q];
+        d.scene = d_scenes + r->scene;
+        d.camera = r->camera;
+        d.x0 = r->rs.x0;
+        d.y0 = r->rs.y0;
+        d.ww = r->ww;
+        d.wh = r->wh;
+        d.s0 = r->rs.sample_offset + r->next;
+        d.nspp = std::min(r->next + r->chunk, r->rs.max_spp) - r->next;
+        d.max_depth = r->rs.max_depth;
+        d.clamp = r->rs.indirect_clamp;
+        d.seed = r->rs.seed;
+        d.film = r->film.as<float3>();
+    }
+    const int64_t cap = S.cfg.paths_per_launch;
+    const double t0 = now_s();
+    for (size_t a = 0; a < n;) {
+        size_t b = a;
+        int64_t paths = 0;
+        while (b < n) {
+            const int64_t p = (int64_t) S.wf_reqs[b].ww * S.wf_reqs[b].wh * S.wf_reqs[b].nspp;
+            if (b > a && paths + p > cap)
+                break;
+            paths += p;
+            b++;
+        }
+        int64_t launches = 0;
+        if (int rc = wavefront_step_multi(S.wf, S.wf_reqs.data() + a, (int) (b - a), S.tlas_cap,
+                                          S.blas_cap, S.p_rays + 2 * a, S.st, &launches))
+            return rc;
+        a = b;
+    }
+    PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
+    S.busy += now_s() - t0;
+    S.steps++;
+    for (size_t q = 0; q < n; q++) {
+        Req *r = S.active[q];
+        const int s1 = std::min(r->next + r->chunk, r->rs.max_spp);
+        S.samples += (int64_t) (s1 - r->next) * r->npix;
+        r->next = s1;
+        const unsigned long long rays = S.p_rays[2 * q] + S.p_rays[2 * q + 1];
+        r->rays += rays;
+        S.rays += rays;
+    }
+    return PRR_OK;
+}
+
 // One step over every running request; returns a status for the whole step.
 int run_step(Server &S) {
+    if (S.cfg.integrator == PRR_SERVER_WAVEFRONT)
+        return run_step_wavefront(S);
     const DevScene *d_scenes = S.d_scenes.as<DevScene>();
     size_t n_items = 0;
     for (Req *r : S.active)
@@ -297,6 +374,13 @@ int prr_server_create(const prr_server_config *config, prr_server **out) {
         S->cfg.max_active = 64;
     if (S->cfg.samples_per_step <= 0)
         S->cfg.samples_per_step = (int64_t) 1 << 20;
+    if (S->cfg.integrator != PRR_SERVER_WAVEFRONT && S->cfg.integrator != PRR_SERVER_MEGAKERNEL) {
+        delete S;
+        return fail(PRR_ERR_INVALID_ARGUMENT, "unknown server integrator");
+    }
+    if (S->cfg.paths_per_launch <= 0)
+        S->cfg.paths_per_launch = (int64_t) 1 << 24;
+    S->cfg.paths_per_launch = std::min<int64_t>(S->cfg.paths_per_launch, (int64_t) 1 << 30);
     cudaError_t e = cudaGetDevice(&S->device);
     if (e == cudaSuccess)
         e = cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking);
@@ -390,8 +474,11 @@ int prr_server_submit(prr_server *server, const prr_request *request, uint64_t *
     r->ww = r->rs.x1 - r->rs.x0;
     r->wh = r->rs.y1 - r->rs.y0;
     r->npix = r->ww * r->wh;
-    r->chunk = (int) std::max<int64_t>(1, std::min<int64_t>(r->rs.max_spp,
-                                                            S.cfg.samples_per_step / r->npix));
+    // wavefront steps also keep one request's chunk within a launch group
+    int64_t per_step = S.cfg.samples_per_step;
+    if (S.cfg.integrator == PRR_SERVER_WAVEFRONT)
+        per_step = std::min(per_step, S.cfg.paths_per_launch);
+    r->chunk = (int) std::max<int64_t>(1, std::min<int64_t>(r->rs.max_spp, per_step / r->npix));
     r->bytes = (size_t) r->npix * sizeof(float3) + (r->out_on_device ? 0 : (size_t) r->npix * 12);
     std::lock_guard<std::mutex> g(S.mu);
     if (S.stop)

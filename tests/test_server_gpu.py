@@ -1,8 +1,12 @@
-"""The render server: continuous batching over resident scenes. Each
-request's image is the same alone as in a mix (bit for bit), matches the
-plain renderer within float-summation tolerance, and admission respects the
-device budget; injected allocation failures, cancellations and timeouts are
-made on the host and leave the server serving."""
+"""The render server: continuous batching over resident scenes, on both step
+integrators. Each request's image is the same alone as in a mix (bit for
+bit); on wavefront steps (all running requests' paths in one set of ordered
+ray queues) it equals the plain renderer bit for bit, on megakernel steps
+within float-summation tolerance (chunk sums); admission respects the device
+budget; injected allocation failures, cancellations and timeouts are made on
+the host and leave the server serving."""
+import dataclasses
+
 import numpy as np
 import pytest
 import torch
@@ -36,16 +40,20 @@ def make_server(scene_set, **kw):
     return srv
 
 
-def test_same_alone_and_in_mix(scene_set):
-    alone = []
+@pytest.mark.parametrize("integrator,paths_per_launch", [
+    ("wavefront", 0), ("wavefront", 40000), ("megakernel", 0)])
+def test_same_alone_and_in_mix(scene_set, integrator, paths_per_launch):
+    kw = dict(integrator=integrator, paths_per_launch=paths_per_launch)
+    alone, alone_rays = [], []
     for sc, spp, depth, seed, win in JOBS:
-        srv = make_server(scene_set)
+        srv = make_server(scene_set, **kw)
         rid = srv.submit(sc, spp, depth, seed=seed, window=win)
         info = srv.wait(rid)
         assert info["status"] == "done"
         alone.append(srv.result(rid).copy())
+        alone_rays.append(info["rays"])
         srv.close()
-    srv = make_server(scene_set)
+    srv = make_server(scene_set, **kw)
     rids = []
     for k, (sc, spp, depth, seed, win) in enumerate(JOBS):
         if k % 2 == 0:  # half of them into device memory
@@ -63,20 +71,28 @@ def test_same_alone_and_in_mix(scene_set):
         got = srv.result(rid)
         got = got.cpu().numpy() if hasattr(got, "cpu") else got
         assert np.array_equal(got.view(np.uint32), alone[k].view(np.uint32)), k
+        assert infos[k]["rays"] == alone_rays[k] > 0, k
     st = srv.stats()
     assert st["completed"] == len(JOBS) and st["failed"] == 0 and st["steps"] > 0
+    assert st["rays"] == sum(alone_rays)
     srv.close()
-    # and each equals the plain renderer up to how the sample sums are grouped
+    # and each equals the plain renderer: bit for bit where samples are added
+    # one by one (wavefront), up to how the sums are grouped otherwise
     for k, (sc, spp, depth, seed, win) in enumerate(JOBS):
         ref, _ = scene_set[sc].render(spp, depth, seed=seed, window=win, slices=1)
-        assert np.allclose(alone[k], ref.cpu().numpy(), rtol=1e-5, atol=1e-6), k
+        ref = ref.cpu().numpy()
+        if integrator == "wavefront":
+            assert np.array_equal(alone[k].view(np.uint32), ref.view(np.uint32)), k
+        else:
+            assert np.allclose(alone[k], ref, rtol=1e-5, atol=1e-6), k
 
 
-def test_budget_faults_cancel_timeout(scene_set):
+@pytest.mark.parametrize("integrator", ["wavefront", "megakernel"])
+def test_budget_faults_cancel_timeout(scene_set, integrator):
     scene_bytes = sum(s.stats()["device_bytes"] for s in scene_set)
     # room for one 64x64 request at a time (film + host staging = 24 bytes/pixel)
     srv = make_server(scene_set, budget_bytes=scene_bytes + 64 * 64 * 24 + 100,
-                      fail_every_nth_admission=3)
+                      fail_every_nth_admission=3, integrator=integrator)
     rids = [srv.submit(0, 8, 5, seed=k) for k in range(6)]
     infos = [srv.wait(r) for r in rids]
     st = [i["status"] for i in infos]
@@ -100,3 +116,21 @@ def test_budget_faults_cancel_timeout(scene_set):
     assert srv.wait(ok)["status"] == "done"
     assert np.array_equal(srv.result(ok), srv.result(rids[0]))
     srv.close()
+
+
+def test_other_resolution(scene_set):
+    """A request at another resolution of the scene's camera equals the
+    renderer's output for the same camera at that resolution."""
+    srv = make_server(scene_set)
+    rid = srv.submit(1, 12, 8, seed=7, size=(120, 70), window=(10, 5, 90, 61))
+    assert srv.wait(rid)["status"] == "done"
+    got = srv.result(rid)
+    srv.close()
+    s = prr.Scene.from_desc(dataclasses.replace(scene_set[1].desc, width=120, height=70))
+    ref, _ = s.render(12, 8, seed=7, window=(10, 5, 90, 61), slices=1)
+    assert np.array_equal(got.view(np.uint32), ref.cpu().numpy().view(np.uint32))
+
+
+def test_unknown_integrator_rejected():
+    with pytest.raises(ValueError):
+        prr.Server(integrator="rasterizer")
