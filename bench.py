@@ -703,6 +703,8 @@ def run_serving(args, rank, world, on):
                    "total_samples": total_samples},
         "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
         "served_msamples_s": served_rate, "served_busy_msamples_s": busy_rate,
+        "worker_s": {"span": span, "steps": int(st["steps"]), "busy": st["busy_s"],
+                     "admit": st["admit_s"], "complete": st["complete_s"]},
         "steps": "wavefront (all running requests in one set of ordered ray queues)",
         "megakernel_steps": {"p50_s": float(np.percentile(mk, 50)),
                              "p99_s": float(np.percentile(mk, 99)),

@@ -348,6 +348,8 @@ typedef struct prr_server_stats {
     uint64_t rays;
     int64_t steps;
     double busy_s;                /* time inside GPU steps */
+    double admit_s;               /* worker time admitting requests (allocations) */
+    double complete_s;            /* worker time resolving and returning finished images */
     int64_t bytes_in_use;
     double now_s;
 } prr_server_stats;

@@ -1414,17 +1414,37 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     return PRR_OK;
 }
 
-int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n, int tlas_cap,
-                         int blas_cap, unsigned long long *rays_host, cudaStream_t st,
-                         int64_t *launches) {
+int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n,
+                         int64_t paths_per_launch, int tlas_cap, int blas_cap,
+                         unsigned long long *rays_host, cudaStream_t st, int64_t *launches) {
     if (n <= 0)
         return PRR_OK;
-    Wf w{};
-    int64_t P = 0, npix = 0;
-    int max_depth = 1;
-    std::vector<WfReq> table(n);
+    // the request table of the whole step in pinned memory, one copy up
+    const size_t table_bytes = (size_t) n * sizeof(WfReq);
+    if (table_bytes > ms.h_cap) {
+        if (ms.h_table)
+            cudaFreeHost(ms.h_table);
+        ms.h_table = nullptr;
+        ms.h_cap = std::max(table_bytes, 2 * ms.h_cap);
+        PRR_CUDA_TRY(cudaMallocHost(&ms.h_table, ms.h_cap));
+    }
+    PRR_CUDA_TRY(ms.reqs.ensure(ms.h_cap));
+    WfReq *table = static_cast<WfReq *>(ms.h_table);
+    // launch groups: consecutive requests of at most paths_per_launch paths
+    // (a request alone may exceed it); bases count from each group's start
+    struct Group {
+        int a, b, max_depth;
+        int64_t P, npix;
+    };
+    std::vector<Group> groups;
+    Group g{0, 0, 1, 0, 0};
     for (int k = 0; k < n; k++) {
         const WfStepReq &q = reqs[k];
+        const int64_t paths = (int64_t) q.ww * q.wh * q.nspp;
+        if (k > g.a && g.P + paths > paths_per_launch) {
+            groups.push_back(g);
+            g = Group{k, k, 1, 0, 0};
+        }
         WfReq &t = table[k];
         std::memset(&t, 0, sizeof(t));
         t.scene = q.scene;
@@ -1439,48 +1459,58 @@ int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n, int tla
         t.max_depth = q.max_depth;
         t.clamp = q.clamp;
         t.seed = q.seed;
-        t.path_base = P;
-        t.pix_base = npix;
+        t.path_base = g.P;
+        t.pix_base = g.npix;
         t.film = q.film;
-        P += (int64_t) t.npix * t.nspp;
-        npix += t.npix;
-        max_depth = std::max(max_depth, q.max_depth);
+        g.P += paths;
+        g.npix += t.npix;
+        g.max_depth = std::max(g.max_depth, q.max_depth);
+        g.b = k + 1;
     }
-    if (P >= ((int64_t) 1 << 31))
+    groups.push_back(g);
+    int64_t maxP = 0;
+    for (const Group &x : groups)
+        maxP = std::max(maxP, x.P);
+    if (maxP >= ((int64_t) 1 << 31))
         return fail(PRR_ERR_INVALID_ARGUMENT, "server step too large");
-    w.P = (int) P;
-    w.npix = 0; // no per-render film or active list in a server step
-    w.max_depth = max_depth;
-    w.ordered = 1;
-    w.n_reqs = n;
-    w.tlas_cap = tlas_cap;
-    w.blas_cap = blas_cap;
-    if (int rc = wf_layout(ms.state, w, (size_t) P, 1))
-        return rc;
-    PRR_CUDA_TRY(ms.reqs.ensure((size_t) n * sizeof(WfReq)));
-    w.reqs = ms.reqs.as<WfReq>();
-    WfShape L;
-    if (int rc = wf_shape<true>(w, ms.spill, 128, 8, 8, L))
-        return rc;
-    const WfParts parts = wf_parts(w);
-    PRR_CUDA_TRY(cudaMemcpyAsync(w.reqs, table.data(), (size_t) n * sizeof(WfReq),
-                                 cudaMemcpyHostToDevice, st));
-    PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) L.ntiles * kPartTile, st));
-    PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
-    if (int rc = wf_enqueue_bounces<true>(DevScene{}, w, L, parts, st))
-        return rc;
-    k_wf_film_multi<<<(int) std::min<int64_t>((npix + 255) / 256, (int64_t) device_sm_count() * 16),
-                      256, 0, st>>>(w, npix);
-    PRR_CUDA_TRY(cudaGetLastError());
+    PRR_CUDA_TRY(cudaMemcpyAsync(ms.reqs.ptr, table, table_bytes, cudaMemcpyHostToDevice, st));
+    int64_t nl = 0;
+    for (const Group &x : groups) {
+        Wf w{};
+        w.P = (int) x.P;
+        w.npix = 0; // no per-render film or active list in a server step
+        w.max_depth = x.max_depth;
+        w.ordered = 1;
+        w.reqs = ms.reqs.as<WfReq>() + x.a;
+        w.n_reqs = x.b - x.a;
+        w.tlas_cap = tlas_cap;
+        w.blas_cap = blas_cap;
+        if (int rc = wf_layout(ms.state, w, (size_t) maxP, 1))
+            return rc;
+        WfShape L;
+        if (int rc = wf_shape<true>(w, ms.spill, 128, 8, 8, L))
+            return rc;
+        const WfParts parts = wf_parts(w);
+        PRR_CUDA_TRY(cudaMemsetAsync(w.tag, 0xFF, (size_t) L.ntiles * kPartTile, st));
+        PRR_CUDA_TRY(cudaMemsetAsync(w.cnt, 0, kCntSlots * sizeof(unsigned), st));
+        if (int rc = wf_enqueue_bounces<true>(DevScene{}, w, L, parts, st))
+            return rc;
+        k_wf_film_multi<<<(int) std::min<int64_t>((x.npix + 255) / 256,
+                                                  (int64_t) device_sm_count() * 16),
+                          256, 0, st>>>(w, x.npix);
+        PRR_CUDA_TRY(cudaGetLastError());
+        // generate + per bounce (begin, extend, 3-kernel partition, miss,
+        // delta, surface, shadow, shadow_resolve, 3-kernel partition) + film
+        nl += 1 + (int64_t) (w.max_depth + 1) * 13 + 1;
+    }
     // the rays each request traced: one strided copy out of the table
     if (rays_host)
-        PRR_CUDA_TRY(cudaMemcpy2DAsync(rays_host, 2 * sizeof(unsigned long long), &w.reqs[0].rays,
-                                       sizeof(WfReq), 2 * sizeof(unsigned long long), n,
+        PRR_CUDA_TRY(cudaMemcpy2DAsync(rays_host, 2 * sizeof(unsigned long long),
+                                       &ms.reqs.as<WfReq>()[0].rays, sizeof(WfReq),
+                                       2 * sizeof(unsigned long long), n,
                                        cudaMemcpyDeviceToHost, st));
-    // generate + per bounce (begin, extend, 3-kernel partition, miss, delta,
-    // surface, shadow, shadow_resolve, 3-kernel partition) + film
     if (launches)
-        *launches = 1 + (int64_t) (w.max_depth + 1) * 13 + 1;
+        *launches = nl;
     return PRR_OK;
 }
 

@@ -164,16 +164,29 @@ struct WfStepReq {
     uint64_t seed;
     float3 *film; // ww*wh running sums (device)
 };
-// Device buffers a server keeps across its wavefront steps.
+// Buffers a server keeps across its wavefront steps: path state, stack
+// spill, and the request table (device, and pinned host for the upload).
 struct WfMultiState {
     DevBuf state, spill, reqs;
+    void *h_table = nullptr;
+    size_t h_cap = 0;
+    WfMultiState() = default;
+    WfMultiState(const WfMultiState &) = delete;
+    WfMultiState &operator=(const WfMultiState &) = delete;
+    ~WfMultiState() {
+        if (h_table)
+            cudaFreeHost(h_table);
+    }
 };
-// Traces one step of n requests as one set of ordered ray queues. Per
-// request, rays_host[2k], rays_host[2k+1] receive the closest and shadow rays
-// it traced (valid once the stream has drained); `launches` the kernel count.
-int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n, int tlas_cap,
-                         int blas_cap, unsigned long long *rays_host, cudaStream_t st,
-                         int64_t *launches);
+// Traces one step of n requests: consecutive requests of at most
+// paths_per_launch paths share one set of ordered ray queues (a request
+// alone may exceed it). Per request, rays_host[2k], rays_host[2k+1] receive
+// the closest and shadow rays it traced (valid once the stream has drained);
+// `launches` the kernel count. The step is ordered on `st`; the host does not
+// wait for it.
+int wavefront_step_multi(WfMultiState &ms, const WfStepReq *reqs, int n,
+                         int64_t paths_per_launch, int tlas_cap, int blas_cap,
+                         unsigned long long *rays_host, cudaStream_t st, int64_t *launches);
 
 int device_sm_count();
 DevCamera make_camera(const prr_camera &c, int width, int height);

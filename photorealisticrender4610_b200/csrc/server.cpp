@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <thread>
 #include <unordered_map>
 
@@ -48,7 +49,8 @@ struct Req {
     int next = 0, chunk = 1, npix = 0, ww = 0, wh = 0;
     DevCamera camera{};
     size_t bytes = 0;
-    DevBuf film, result;
+    void *film = nullptr, *result = nullptr; // device blocks from the server's pool
+    size_t film_cap = 0, result_cap = 0;
     unsigned long long rays = 0;
 };
 
@@ -85,10 +87,16 @@ struct Server {
     unsigned long long *p_rays = nullptr; // pinned, 2 per active request
     size_t cap_rays = 0;
 
+    // Device blocks of finished requests kept for later admissions: freeing
+    // and allocating device memory between steps would stall the worker.
+    std::multimap<size_t, void *> pool;
+    size_t pooled = 0;
+    static constexpr size_t kPoolCap = (size_t) 2 << 30;
+
     // stats
     int64_t submitted = 0, completed = 0, failed = 0, samples = 0, steps = 0;
     unsigned long long rays = 0;
-    double busy = 0;
+    double busy = 0, admit_time = 0, complete_time = 0;
 
     ~Server() {
         if (p_items)
@@ -97,17 +105,60 @@ struct Server {
             cudaFreeHost(p_reqs);
         if (p_rays)
             cudaFreeHost(p_rays);
+        for (auto &b : pool)
+            cudaFree(b.second);
         if (st)
             cudaStreamDestroy(st);
     }
 };
 
+// A block of at least n bytes: a pooled one up to twice that size, else a
+// new allocation (after giving the pool back when the device is full).
+cudaError_t pool_get(Server &S, size_t n, void **out, size_t *cap) {
+    auto it = S.pool.lower_bound(n);
+    if (it != S.pool.end() && it->first <= 2 * n) {
+        *out = it->second;
+        *cap = it->first;
+        S.pooled -= it->first;
+        S.pool.erase(it);
+        return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(out, n);
+    if (e == cudaErrorMemoryAllocation && !S.pool.empty()) {
+        cudaGetLastError();
+        for (auto &b : S.pool)
+            cudaFree(b.second);
+        S.pool.clear();
+        S.pooled = 0;
+        e = cudaMalloc(out, n);
+    }
+    *cap = e == cudaSuccess ? n : 0;
+    return e;
+}
+
+// Work on a returned block is ordered on the server's stream like all later
+// uses, so it can go straight back into the pool.
+void pool_put(Server &S, void *&p, size_t &cap) {
+    if (!p)
+        return;
+    S.pool.emplace(cap, p);
+    S.pooled += cap;
+    p = nullptr;
+    cap = 0;
+    while (S.pooled > Server::kPoolCap) {
+        auto big = std::prev(S.pool.end());
+        S.pooled -= big->first;
+        cudaFree(big->second);
+        S.pool.erase(big);
+    }
+}
+
 void finish_locked(Server &S, Req *r, int status, int error) {
     r->status = status;
     r->error = error;
     r->t_done = now_s();
-    r->film.release();
-    r->result.release();
+    pool_put(S, r->film, r->film_cap);
+    pool_put(S, r->result, r->result_cap);
     S.used -= r->bytes;
     if (status == PRR_REQUEST_DONE)
         S.completed++;
@@ -118,6 +169,7 @@ void finish_locked(Server &S, Req *r, int status, int error) {
 
 // Admit queued requests in arrival order while a slot and budget are free.
 void admit_locked(Server &S) {
+    const double t0 = now_s();
     while (!S.queue.empty() && (int) S.active.size() < S.cfg.max_active) {
         Req *r = S.queue.front();
         if (S.used + r->bytes > (size_t) S.cfg.device_budget_bytes)
@@ -128,11 +180,12 @@ void admit_locked(Server &S) {
         bool fail_alloc = S.cfg.fail_every_nth_admission > 0 &&
                           S.admissions % S.cfg.fail_every_nth_admission == 0;
         cudaError_t e = fail_alloc ? cudaErrorMemoryAllocation
-                                   : r->film.alloc((size_t) r->npix * sizeof(float3));
+                                   : pool_get(S, (size_t) r->npix * sizeof(float3), &r->film,
+                                              &r->film_cap);
         if (e == cudaSuccess)
-            e = cudaMemsetAsync(r->film.ptr, 0, (size_t) r->npix * sizeof(float3), S.st);
+            e = cudaMemsetAsync(r->film, 0, (size_t) r->npix * sizeof(float3), S.st);
         if (e == cudaSuccess && !r->out_on_device)
-            e = r->result.alloc((size_t) r->npix * 3 * sizeof(float));
+            e = pool_get(S, (size_t) r->npix * 3 * sizeof(float), &r->result, &r->result_cap);
         if (e != cudaSuccess) {
             cudaGetLastError();
             finish_locked(S, r, PRR_REQUEST_FAILED, PRR_ERR_OUT_OF_MEMORY);
@@ -142,6 +195,7 @@ void admit_locked(Server &S) {
         r->t_admit = now_s();
         S.active.push_back(r);
     }
+    S.admit_time += now_s() - t0;
 }
 
 int ensure_tables(Server &S, size_t items, size_t reqs) {
@@ -164,7 +218,7 @@ int ensure_tables(Server &S, size_t items, size_t reqs) {
 
 // One wavefront step over every running request: groups of requests (in
 // admission order) of at most paths_per_launch paths each, one after another
-// on the server's stream.
+// on the server's stream, then one wait for the stream.
 int run_step_wavefront(Server &S) {
     const DevScene *d_scenes = S.d_scenes.as<DevScene>();
     const size_t n = S.active.size();
@@ -190,26 +244,13 @@ int run_step_wavefront(Server &S) {
         d.max_depth = r->rs.max_depth;
         d.clamp = r->rs.indirect_clamp;
         d.seed = r->rs.seed;
-        d.film = r->film.as<float3>();
+        d.film = static_cast<float3 *>(r->film);
     }
-    const int64_t cap = S.cfg.paths_per_launch;
     const double t0 = now_s();
-    for (size_t a = 0; a < n;) {
-        size_t b = a;
-        int64_t paths = 0;
-        while (b < n) {
-            const int64_t p = (int64_t) S.wf_reqs[b].ww * S.wf_reqs[b].wh * S.wf_reqs[b].nspp;
-            if (b > a && paths + p > cap)
-                break;
-            paths += p;
-            b++;
-        }
-        int64_t launches = 0;
-        if (int rc = wavefront_step_multi(S.wf, S.wf_reqs.data() + a, (int) (b - a), S.tlas_cap,
-                                          S.blas_cap, S.p_rays + 2 * a, S.st, &launches))
-            return rc;
-        a = b;
-    }
+    int64_t launches = 0;
+    if (int rc = wavefront_step_multi(S.wf, S.wf_reqs.data(), (int) n, S.cfg.paths_per_launch,
+                                      S.tlas_cap, S.blas_cap, S.p_rays, S.st, &launches))
+        return rc;
     PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
     S.busy += now_s() - t0;
     S.steps++;
@@ -250,7 +291,7 @@ int run_step(Server &S) {
         d.max_depth = r->rs.max_depth;
         d.clamp = r->rs.indirect_clamp;
         d.seed = r->rs.seed;
-        d.film = r->film.as<float3>();
+        d.film = static_cast<float3 *>(r->film);
         d.rays = 0;
         const int tiles = serve_tiles(r->ww, r->wh);
         for (int t = 0; t < tiles; t++)
@@ -282,15 +323,18 @@ int run_step(Server &S) {
 
 // Resolve finished requests into their outputs.
 int complete(Server &S, std::vector<Req *> &done) {
+    const double t0 = now_s();
     for (Req *r : done) {
-        float *target = r->out_on_device ? r->out : r->result.as<float>();
-        if (int rc = serve_resolve(r->film.as<float3>(), r->npix, r->rs.max_spp, target, S.st))
+        float *target = r->out_on_device ? r->out : static_cast<float *>(r->result);
+        if (int rc = serve_resolve(static_cast<const float3 *>(r->film), r->npix, r->rs.max_spp,
+                                   target, S.st))
             return rc;
         if (!r->out_on_device)
-            PRR_CUDA_TRY(cudaMemcpyAsync(r->out, r->result.ptr, (size_t) r->npix * 3 * sizeof(float),
+            PRR_CUDA_TRY(cudaMemcpyAsync(r->out, r->result, (size_t) r->npix * 3 * sizeof(float),
                                          cudaMemcpyDeviceToHost, S.st));
     }
     PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
+    S.complete_time += now_s() - t0;
     return PRR_OK;
 }
 
@@ -567,6 +611,8 @@ int prr_server_stats_get(prr_server *server, prr_server_stats *out) {
     out->rays = S.rays;
     out->steps = S.steps;
     out->busy_s = S.busy;
+    out->admit_s = S.admit_time;
+    out->complete_s = S.complete_time;
     out->bytes_in_use = (int64_t) S.used;
     out->now_s = now_s();
     return PRR_OK;
