@@ -599,14 +599,14 @@ def run_caustics(args, rank, world, on):
 
 
 def serving_pool():
-    """Eight procedural scenes from about 10k to 2M triangles, built like the
-    museum-like scene (displaced icospheres under the HDR sky) and the query
-    set (a 1M / 1.5M triangle soup under the same sky)."""
-    import math
+    """Eight procedural scenes of about 10k, 30k, 100k, 300k, 600k, 1M, 1.5M
+    and 2M triangles, built like the museum-like scene (displaced icospheres
+    under the HDR sky: 2 / 6 level-4, 5 level-5, 4 level-6, 2 / 6 level-7
+    spheres) and the query set (1M / 1.5M triangle soups under the same sky)."""
     from photorealisticrender4610_b200 import scenes as sc
     pool = []
-    for level in (3, 4, 5, 6, 7):
-        pool.append(sc.museum_like(512, 512, level=level, env_size=(1024, 512)))
+    for level, spheres in ((4, 2), (4, 6), (5, 5), (6, 4), (7, 2)):
+        pool.append(sc.museum_like(512, 512, level=level, env_size=(1024, 512), spheres=spheres))
     for n in (1_000_000, 1_500_000):
         d = sc.SceneDesc(width=512, height=512, name=f"soup{n}")
         m = d.add_material(sc.Material(sc.DIFFUSE, (0.7, 0.6, 0.5), 0.6, 0.0))
@@ -615,7 +615,7 @@ def serving_pool():
         d.env = pool[0].env
         d.camera = sc.Camera(eye=(2.2, 1.6, 2.4), target=(0.5, 0.5, 0.5), fovv=40, fovh=45)
         pool.append(d)
-    pool.append(sc.caustics(512, 512, level=3))
+    pool.append(sc.museum_like(512, 512, level=7, env_size=(1024, 512)))
     return pool
 
 
@@ -645,8 +645,12 @@ def run_serving(args, rank, world, on):
     depth = 8
     total_samples = sum(w * h * spp for _, (w, h), spp in reqs)
 
-    host = [torch.empty((h, w, 3), dtype=torch.float32).pin_memory().numpy()
-            for _, (w, h), _ in reqs]
+    # outputs in pinned host memory; past 256 requests, a ring of 256 buffers
+    # of the largest size (a buffer is reused by every 256th request)
+    ring = min(n, 256)
+    big = max(w * h for _, (w, h), _ in reqs)
+    bufs = [torch.empty(big * 3, dtype=torch.float32).pin_memory().numpy() for _ in range(ring)]
+    host = [bufs[k % ring][:w * h * 3].reshape(h, w, 3) for k, (_, (w, h), _) in enumerate(reqs)]
 
     def serve(max_active, samples_per_step, arrive=arrive, integrator="wavefront"):
         """Replays the arrival schedule against a server; returns latencies,
@@ -680,15 +684,25 @@ def run_serving(args, rank, world, on):
         lat, span, st = serve(args.max_active, 1 << 20)
     served_rate = total_samples / span / 1e6
     busy_rate = total_samples / st["busy_s"] / 1e6
-    # the same schedule on megakernel steps (one launch over request tiles)
-    mk, mk_span, mk_st = serve(args.max_active, 1 << 20, integrator="megakernel")
-    # baseline: the same schedule, one request at a time in arrival order,
-    # each rendered by the plain megakernel
-    one, one_span, one_st = serve(1, 1 << 24, integrator="megakernel")
-    # a sustainable load: the same requests arriving at 70% of the measured
-    # busy throughput (mean work per request / capacity)
-    sus_rate = 0.7 * busy_rate * 1e6 / (total_samples / n)
-    sus, sus_span, sus_st = serve(args.max_active, 1 << 20, arrive * (args.rate / sus_rate))
+    arms = set(args.serving_arms.split(","))
+    if "all" in arms:
+        arms = {"megakernel", "one", "sustainable"}
+
+    def pct(lat_, span_, st_):
+        return {"p50_s": float(np.percentile(lat_, 50)), "p99_s": float(np.percentile(lat_, 99)),
+                "msamples_s": total_samples / span_ / 1e6,
+                "busy_msamples_s": total_samples / st_["busy_s"] / 1e6}
+    extra = {}
+    if "megakernel" in arms:  # the same schedule on megakernel steps (request tiles)
+        extra["megakernel_steps"] = pct(*serve(args.max_active, 1 << 20, integrator="megakernel"))
+    if "one" in arms:  # one request at a time in arrival order, plain megakernel
+        extra["one_at_a_time"] = pct(*serve(1, 1 << 24, integrator="megakernel"))
+    if "sustainable" in arms:
+        # the same requests arriving at 70% of the measured busy throughput
+        # (mean work per request / capacity)
+        sus_rate = 0.7 * busy_rate * 1e6 / (total_samples / n)
+        sus, sus_span, sus_st = serve(args.max_active, 1 << 20, arrive * (args.rate / sus_rate))
+        extra["sustainable"] = dict(pct(sus, sus_span, sus_st), rate_per_s=sus_rate, load=0.7)
     line = {
         "metric": "served p50/p99 latency (s) and Msamples/s", "value": float(np.percentile(lat, 99)),
         "unit": "s (p99 latency)", "n_gpus": world, "steps": n, "warmup": 1,
@@ -705,18 +719,8 @@ def run_serving(args, rank, world, on):
         "served_msamples_s": served_rate, "served_busy_msamples_s": busy_rate,
         "worker_s": {"span": span, "steps": int(st["steps"]), "busy": st["busy_s"],
                      "admit": st["admit_s"], "complete": st["complete_s"]},
-        "steps": "wavefront (all running requests in one set of ordered ray queues)",
-        "megakernel_steps": {"p50_s": float(np.percentile(mk, 50)),
-                             "p99_s": float(np.percentile(mk, 99)),
-                             "msamples_s": total_samples / mk_span / 1e6,
-                             "busy_msamples_s": total_samples / mk_st["busy_s"] / 1e6},
-        "one_at_a_time": {"p50_s": float(np.percentile(one, 50)),
-                          "p99_s": float(np.percentile(one, 99)),
-                          "msamples_s": total_samples / one_span / 1e6},
-        "sustainable": {"rate_per_s": sus_rate, "load": 0.7,
-                        "p50_s": float(np.percentile(sus, 50)),
-                        "p99_s": float(np.percentile(sus, 99)),
-                        "served_msamples_s": total_samples / sus_span / 1e6},
+        "server_steps": "wavefront (all running requests in one set of ordered ray queues)",
+        **extra,
         "failed": int(st["failed"]),
         "e2e": {"value": served_rate, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(np.mean([w * h * 12 for _, (w, h), _ in reqs]))},
@@ -740,6 +744,9 @@ def main():
     ap.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrivals per s")
     ap.add_argument("--max-spp", type=int, default=256, help="serving: spp upper bound")
     ap.add_argument("--max-active", type=int, default=64, help="serving: concurrent requests")
+    ap.add_argument("--serving-arms", default="all",
+                    help="serving: comparison runs beside the wavefront server, 'all' or a comma "
+                         "list of megakernel, one, sustainable (or 'none')")
     ap.add_argument("--size", default="", help="render workloads: WxH override")
     ap.add_argument("--spp", type=int, default=0, help="render workloads: spp override")
     ap.add_argument("--kernel-only", action="store_true",

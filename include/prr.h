@@ -312,11 +312,15 @@ typedef struct prr_server prr_server;
 typedef struct prr_server_config {
     int64_t device_budget_bytes; /* resident scenes + admitted requests (0: 120 GiB) */
     int max_active;              /* requests rendered at once (0: 64) */
-    int64_t samples_per_step;    /* samples per request per step (0: 1,048,576) */
+    int64_t samples_per_step;    /* megakernel steps: samples per request per step
+                                    (0: 1,048,576) */
     int fail_every_nth_admission;/* fault injection on the host for tests (0: off):
                                     every n-th admission fails its allocation */
     int integrator;              /* PRR_SERVER_WAVEFRONT (0) or PRR_SERVER_MEGAKERNEL */
-    int64_t paths_per_launch;    /* wavefront: paths per launch group (0: 16,777,216) */
+    int64_t paths_per_launch;    /* wavefront steps: paths per step (0: 16,777,216),
+                                    a quarter shared equally among the running
+                                    requests, the rest to those with the least
+                                    work left */
 } prr_server_config;
 /* Wavefront steps: the paths of every running request share one set of
  * ordered ray queues (one traversal launch per bounce for all of them).

@@ -13,10 +13,12 @@
 // each bounce is one traversal launch for all of them) or as one megakernel
 // launch over (request, 16x8 tile) items (k_serve.cu).
 //
-// A request's chunk size depends only on the request (samples_per_step / its
-// pixel count), and its film adds samples (wavefront: one by one, in sample
-// order, as a render of the request does) or chunk sums (megakernel) in
-// order, so its image is the same alone as in any mix.
+// On wavefront steps a request's film adds its samples one by one in sample
+// order, as a render of the request does, so its image does not depend on how
+// many samples each step takes: the scheduler splits each step's paths among
+// the running requests freely. On megakernel steps the film adds chunk sums,
+// and a request's chunk size depends only on the request (samples_per_step /
+// its pixel count). Either way its image is the same alone as in any mix.
 #include "prr_internal.h"
 #include "serve.h"
 
@@ -47,6 +49,7 @@ struct Req {
     int error = PRR_OK;
     double t_submit = 0, t_admit = 0, t_done = 0;
     int next = 0, chunk = 1, npix = 0, ww = 0, wh = 0;
+    int64_t credit = 0; // wavefront steps: paths earned towards the next samples
     DevCamera camera{};
     size_t bytes = 0;
     void *film = nullptr, *result = nullptr; // device blocks from the server's pool
@@ -84,6 +87,8 @@ struct Server {
     // wavefront steps
     WfMultiState wf;
     std::vector<WfStepReq> wf_reqs;
+    std::vector<int> chunks;
+    std::vector<size_t> order, stepped;
     unsigned long long *p_rays = nullptr; // pinned, 2 per active request
     size_t cap_rays = 0;
 
@@ -229,10 +234,54 @@ int run_step_wavefront(Server &S) {
         S.cap_rays = std::max(2 * n, 2 * S.cap_rays);
         PRR_CUDA_TRY(cudaMallocHost(&S.p_rays, S.cap_rays * sizeof(unsigned long long)));
     }
-    S.wf_reqs.resize(n);
+    // This step's samples per request (the image does not depend on them).
+    // A quarter of the step's paths is shared equally as credit: a request
+    // takes whole samples of its window once its credit pays for them, so a
+    // large window progresses every few steps without crowding the step. The
+    // rest goes to the requests with the least work left, so short requests
+    // leave in one step.
+    const int64_t budget = S.cfg.paths_per_launch;
+    const int64_t fair = std::max<int64_t>(1, budget / (4 * (int64_t) n));
+    S.chunks.assign(n, 0);
+    S.order.resize(n);
+    int64_t left = budget;
     for (size_t q = 0; q < n; q++) {
+        Req *r = S.active[q];
+        const int64_t rem = r->rs.max_spp - r->next;
+        r->credit = std::min(r->credit + fair, rem * r->npix);
+        const int64_t c = r->credit / r->npix;
+        S.chunks[q] = (int) c;
+        r->credit -= c * r->npix;
+        left -= c * r->npix;
+        S.order[q] = q;
+    }
+    std::sort(S.order.begin(), S.order.end(), [&](size_t a, size_t b) {
+        const Req *ra = S.active[a], *rb = S.active[b];
+        return (int64_t) (ra->rs.max_spp - ra->next) * ra->npix <
+               (int64_t) (rb->rs.max_spp - rb->next) * rb->npix;
+    });
+    bool any = false;
+    for (size_t i = 0; i < n; i++) {
+        const size_t q = S.order[i];
         const Req *r = S.active[q];
-        WfStepReq &d = S.wf_reqs[q];
+        const int64_t more = std::min<int64_t>(r->rs.max_spp - r->next - S.chunks[q],
+                                               std::max<int64_t>(0, left) / r->npix);
+        if (more > 0) {
+            S.chunks[q] += (int) more;
+            left -= more * r->npix;
+        }
+        any = any || S.chunks[q] > 0;
+    }
+    if (!any) // every window is larger than the step: one sample of the shortest
+        S.chunks[S.order[0]] = 1;
+    // the table holds the requests that take samples this step
+    S.wf_reqs.clear();
+    S.stepped.clear();
+    for (size_t q = 0; q < n; q++) {
+        if (S.chunks[q] == 0)
+            continue;
+        const Req *r = S.active[q];
+        WfStepReq d;
         d.scene = d_scenes + r->scene;
         d.camera = r->camera;
         d.x0 = r->rs.x0;
@@ -240,26 +289,29 @@ int run_step_wavefront(Server &S) {
         d.ww = r->ww;
         d.wh = r->wh;
         d.s0 = r->rs.sample_offset + r->next;
-        d.nspp = std::min(r->next + r->chunk, r->rs.max_spp) - r->next;
+        d.nspp = S.chunks[q];
         d.max_depth = r->rs.max_depth;
         d.clamp = r->rs.indirect_clamp;
         d.seed = r->rs.seed;
         d.film = static_cast<float3 *>(r->film);
+        S.wf_reqs.push_back(d);
+        S.stepped.push_back(q);
     }
     const double t0 = now_s();
     int64_t launches = 0;
-    if (int rc = wavefront_step_multi(S.wf, S.wf_reqs.data(), (int) n, S.cfg.paths_per_launch,
-                                      S.tlas_cap, S.blas_cap, S.p_rays, S.st, &launches))
+    if (int rc = wavefront_step_multi(S.wf, S.wf_reqs.data(), (int) S.wf_reqs.size(),
+                                      S.cfg.paths_per_launch, S.tlas_cap, S.blas_cap, S.p_rays,
+                                      S.st, &launches))
         return rc;
     PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
     S.busy += now_s() - t0;
     S.steps++;
-    for (size_t q = 0; q < n; q++) {
-        Req *r = S.active[q];
-        const int s1 = std::min(r->next + r->chunk, r->rs.max_spp);
-        S.samples += (int64_t) (s1 - r->next) * r->npix;
-        r->next = s1;
-        const unsigned long long rays = S.p_rays[2 * q] + S.p_rays[2 * q + 1];
+    for (size_t k = 0; k < S.stepped.size(); k++) {
+        Req *r = S.active[S.stepped[k]];
+        const int c = S.chunks[S.stepped[k]];
+        S.samples += (int64_t) c * r->npix;
+        r->next += c;
+        const unsigned long long rays = S.p_rays[2 * k] + S.p_rays[2 * k + 1];
         r->rays += rays;
         S.rays += rays;
     }
@@ -518,11 +570,10 @@ int prr_server_submit(prr_server *server, const prr_request *request, uint64_t *
     r->ww = r->rs.x1 - r->rs.x0;
     r->wh = r->rs.y1 - r->rs.y0;
     r->npix = r->ww * r->wh;
-    // wavefront steps also keep one request's chunk within a launch group
-    int64_t per_step = S.cfg.samples_per_step;
-    if (S.cfg.integrator == PRR_SERVER_WAVEFRONT)
-        per_step = std::min(per_step, S.cfg.paths_per_launch);
-    r->chunk = (int) std::max<int64_t>(1, std::min<int64_t>(r->rs.max_spp, per_step / r->npix));
+    // megakernel steps: a chunk that depends only on the request (its film
+    // adds chunk sums); wavefront steps choose samples per step (below)
+    r->chunk = (int) std::max<int64_t>(1, std::min<int64_t>(r->rs.max_spp,
+                                                            S.cfg.samples_per_step / r->npix));
     r->bytes = (size_t) r->npix * sizeof(float3) + (r->out_on_device ? 0 : (size_t) r->npix * 12);
     std::lock_guard<std::mutex> g(S.mu);
     if (S.stop)

@@ -398,18 +398,19 @@ def textured_showcase(width: int = 320, height: int = 240, env_size=(256, 128)) 
 
 
 def museum_like(width: int = 1920, height: int = 1080, level: int = 7, seed: int = 1,
-                env_size=(2048, 1024), amplitude: float = 0.05) -> SceneDesc:
-    """Six displaced level-``level`` icospheres (20*4^level triangles each) in a
-    3x2 grid on a ground quad; GGX alpha ~ U[0.05,0.8] (roughness = sqrt(alpha)),
-    metallic ~ Bernoulli(0.5), base colour ~ U[0.2,0.9]^3; sphere 4 is glass
-    (IOR 1.5); lit only by a procedural HDR sky."""
+                env_size=(2048, 1024), amplitude: float = 0.05, spheres: int = 6) -> SceneDesc:
+    """Six (or the first ``spheres``) displaced level-``level`` icospheres
+    (20*4^level triangles each) in a 3x2 grid on a ground quad; GGX alpha ~
+    U[0.05,0.8] (roughness = sqrt(alpha)), metallic ~ Bernoulli(0.5), base
+    colour ~ U[0.2,0.9]^3; sphere 4 is glass (IOR 1.5); lit only by a
+    procedural HDR sky."""
     rng = np.random.Generator(np.random.PCG64(seed))
     s = SceneDesc(width=width, height=height, name="museum_like")
     ground = s.add_material(Material(DIFFUSE, (0.5, 0.5, 0.5), 0.7, 0.0))
     s.objects.append(MeshObject(quad((-30, 0, 30), (30, 0, 30), (30, 0, -30), (-30, 0, -30)),
                                 ground))
     r = 0.8
-    for k in range(6):
+    for k in range(spheres):
         cx = (k % 3 - 1) * 2.2
         cz = (k // 3) * -2.2 + 1.0
         alpha = rng.uniform(0.05, 0.8)
