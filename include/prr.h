@@ -181,6 +181,18 @@ int prr_scene_set_material_textures(prr_scene *scene, int material, int base_col
  * without triangles add nothing. */
 int prr_scene_add_gltf(prr_scene *scene, const char *path, int material_type,
                        int override_material, int *out_first, int *out_count, int *out_undecoded);
+/* MeshTriangle(filename, offset, m) + Scene::Add (Triangle.cpp:4-32): the
+ * first mesh of an OBJ file read as the reference's bundled loader reads it
+ * (OBJ_Loader.hpp LoadFile), its face corners taken three at a time as
+ * triangles, positions + offset (NULL: none). The file must end in ".obj" and
+ * hold exactly one mesh (the reference asserts it), with a corner count that
+ * is a multiple of three. */
+int prr_scene_add_obj(prr_scene *scene, const char *path, const float *offset, int material,
+                      int *out_object);
+/* The triangles prr_scene_add_obj would add (ntri x 9 floats): with out_verts
+ * NULL only *out_ntri is set; else out_verts holds `capacity` triangles. */
+int prr_obj_read(const char *path, const float *offset, float *out_verts, int64_t capacity,
+                 int64_t *out_ntri);
 /* Host-side view of a mesh as added (before or after the build): ntri, the
  * kinds of per-corner data it carries (1 normals, 2 uvs, 4 tangents), and, for
  * non-NULL arrays, its triangles (ntri x 9), corner normals (ntri x 9), uvs

@@ -11,6 +11,8 @@
 //                                 Material.hpp:38-183
 //   Triangle(v0, v1, v2, m)       Triangle.hpp:27-32
 //   MeshTriangle(tris, bounds, m) Triangle.hpp:116-124
+//   MeshTriangle(filename, offset, m) (OBJ)
+//                                 Triangle.cpp:4-32
 //   Sphere(center, radius, m)     Sphere.hpp:14-16
 //   Texture; Triangle's per-corner data; Material textures
 //                                 TextureUtils.hpp:9-18, Triangle.hpp:17-23,
@@ -172,6 +174,9 @@ class MeshTriangle : public Object {
         : triangles(std::move(tris)), bounding_box(bounds) {
         m = mt;
     }
+    // MeshTriangle(filename, offset, m) (Triangle.cpp:4-32): the OBJ file's
+    // one mesh as the reference's bundled loader reads it, shifted by offset.
+    MeshTriangle(const std::string &filename, Vector3f offset, Material *mt);
 };
 
 class Sphere : public Object {
@@ -180,6 +185,28 @@ class Sphere : public Object {
     float radius;
     Sphere(const Vector3f &c, const float &r, Material *mt) : center(c), radius(r) { m = mt; }
 };
+
+inline MeshTriangle::MeshTriangle(const std::string &filename, Vector3f offset, Material *mt) {
+    m = mt;
+    const float off[3] = {offset.x, offset.y, offset.z};
+    int64_t nt = 0;
+    prr_detail::check(prr_obj_read(filename.c_str(), off, nullptr, 0, &nt));
+    std::vector<float> v((size_t) nt * 9);
+    prr_detail::check(prr_obj_read(filename.c_str(), off, v.data(), nt, &nt));
+    const float inf = std::numeric_limits<float>::infinity();
+    Vector3f lo(inf, inf, inf), hi(-inf, -inf, -inf);
+    triangles.reserve((size_t) nt);
+    for (int64_t i = 0; i < nt; i++) {
+        Vector3f c[3];
+        for (int j = 0; j < 3; j++) {
+            c[j] = Vector3f(v[i * 9 + j * 3], v[i * 9 + j * 3 + 1], v[i * 9 + j * 3 + 2]);
+            lo = Vector3f(std::min(lo.x, c[j].x), std::min(lo.y, c[j].y), std::min(lo.z, c[j].z));
+            hi = Vector3f(std::max(hi.x, c[j].x), std::max(hi.y, c[j].y), std::max(hi.z, c[j].z));
+        }
+        triangles.emplace_back(c[0], c[1], c[2], mt);
+    }
+    bounding_box = Bounds3(lo, hi);
+}
 
 enum class MaterialType { Diffuse, Glass, Mirror, Emit }; // GLTFLoader.hpp:10
 

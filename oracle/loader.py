@@ -210,6 +210,8 @@ class ReferenceOracle:
         L.prr_ref_scene_add_mesh.argtypes = [vp, _f32p, C.c_int64, C.c_int]
         L.prr_ref_scene_add_gltf.restype = C.c_int
         L.prr_ref_scene_add_gltf.argtypes = [vp, C.c_char_p, C.c_int]
+        L.prr_ref_scene_add_obj.restype = C.c_int
+        L.prr_ref_scene_add_obj.argtypes = [vp, C.c_char_p, _f32p, C.c_int]
         L.prr_ref_scene_export_mesh.restype = C.c_int64
         L.prr_ref_scene_export_mesh.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.prr_ref_scene_export_material.restype = C.c_int
@@ -558,6 +560,21 @@ class RefGltf:
         self.h = ref.L.prr_ref_scene_new()
         self.count = ref.L.prr_ref_scene_add_gltf(self.h, str(path).encode(),
                                                   self.TYPES[material_type])
+
+    @classmethod
+    def obj(cls, ref: ReferenceOracle, path, offset=(0.0, 0.0, 0.0)):
+        """MeshTriangle(filename, offset, m) of the reference on an OBJ file
+        (object 0). The file must hold exactly one mesh: the reference
+        asserts it and would end the process otherwise."""
+        self = cls.__new__(cls)
+        self.ref = ref
+        self.h = ref.L.prr_ref_scene_new()
+        m = ref.L.prr_ref_scene_add_material(self.h, 0, np.array(
+            [0.8, 0.8, 0.8, 0.5, 0.0, 1.5, 0.0, 0.0, 0.0], np.float32))
+        ref.L.prr_ref_scene_add_obj(self.h, str(path).encode(), np.ascontiguousarray(
+            offset, np.float32), m)
+        self.count = 1
+        return self
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -393,6 +393,18 @@ int prr_ref_scene_add_gltf(void *h, const char *path, int type) {
     return (int) meshes.size();
 }
 
+// MeshTriangle(filename, offset, m) + Scene::Add (Triangle.cpp:4-32): the OBJ
+// file read by the reference's own loader. Returns the object index.
+int prr_ref_scene_add_obj(void *h, const char *path, const float *offset, int mat) {
+    RefScene *rs = (RefScene *) h;
+    MeshTriangle *m = new MeshTriangle(std::string(path), Vector3f(offset[0], offset[1], offset[2]),
+                                       rs->materials.at(mat));
+    rs->scene.Add(m);
+    rs->objects.push_back(m);
+    rs->object_kind.push_back(0);
+    return (int) rs->objects.size() - 1;
+}
+
 // A mesh object's triangles as the reference holds them: v0 v1 v2, n0 n1 n2,
 // t0 t1 t2, tan0..2 with handedness; attr bit 1 = smooth normals, 4 = tangents.
 int64_t prr_ref_scene_export_mesh(void *h, int obj, int *attr, float *verts, float *normals,

@@ -5,7 +5,8 @@ hand-written CUDA behind a C ABI (include/prr.h), with a Python mirror of the
 reference's Scene / BVHAccel / Integrator / Renderer interface."""
 from ._lib import PrrError, header_symbols, load  # noqa: F401
 from . import scenes  # noqa: F401
-from .api import PhotonMap, Scene, Server, sample_count_image, tonemap, write_image  # noqa: F401
+from .api import (PhotonMap, Scene, Server, read_obj, sample_count_image,  # noqa: F401
+                  tonemap, write_image)
 
 __all__ = ["Scene", "PhotonMap", "Server", "PrrError", "load", "header_symbols", "scenes",
            "tonemap"]

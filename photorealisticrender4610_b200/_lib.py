@@ -102,6 +102,8 @@ _SIGS = {
     "prr_sample_count_image": (C.c_int, [_vp, C.c_int64, C.c_int, _vp]),
     "prr_scene_add_gltf": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int),
                                      C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "prr_scene_add_obj": (C.c_int, [_vp, C.c_char_p, _vp, C.c_int, C.POINTER(C.c_int)]),
+    "prr_obj_read": (C.c_int, [C.c_char_p, _vp, _vp, C.c_int64, C.POINTER(C.c_int64)]),
     "prr_scene_export_mesh": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int64), C.POINTER(C.c_int),
                                         _vp, _vp, _vp, _vp]),
     "prr_scene_export_material": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int), _vp, _vp]),

@@ -56,6 +56,19 @@ def sample_count_image(spp, max_spp: int) -> np.ndarray:
     return out
 
 
+def read_obj(path, offset=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """The (ntri, 9) float32 triangles MeshTriangle(filename, offset, m) makes
+    of an OBJ file."""
+    lib = _lib.load()
+    nt = C.c_int64()
+    off = _f3(offset)
+    check(lib.prr_obj_read(str(path).encode(), off, None, 0, C.byref(nt)))
+    out = np.empty((nt.value, 9), np.float32)
+    check(lib.prr_obj_read(str(path).encode(), off, C.c_void_p(out.ctypes.data), nt.value,
+                           C.byref(nt)))
+    return out
+
+
 def _normalize_rows(v: np.ndarray) -> np.ndarray:
     """normalize (Vector.hpp:103-111) row by row in float32: v * (1 / sqrt(|v|^2))."""
     x, y, z = v[:, 0], v[:, 1], v[:, 2]
@@ -182,6 +195,18 @@ class Scene:
                                                  None, None, None, None))
             self.objects.append(("mesh", nt.value))
         return {"first": first.value, "count": count.value, "undecoded_images": und.value}
+
+    def add_obj(self, path: str, material: int, offset=(0.0, 0.0, 0.0)) -> int:
+        """MeshTriangle(filename, offset, m) + Scene::Add: the OBJ file's one
+        mesh as the reference reads it; returns the object id."""
+        out = C.c_int()
+        check(self.lib.prr_scene_add_obj(self.h, str(path).encode(), _f3(offset), material,
+                                         C.byref(out)))
+        nt = C.c_int64()
+        check(self.lib.prr_scene_export_mesh(self.h, out.value, C.byref(nt), None, None, None,
+                                             None, None))
+        self.objects.append(("mesh", nt.value))
+        return out.value
 
     def export_mesh(self, obj: int) -> dict:
         """The mesh as added (host side): triangles and per-corner data."""

@@ -10,6 +10,7 @@ import pytest
 ROOT = Path(__file__).resolve().parents[1]
 SRC = ROOT / "tests" / "cpp" / "dropin_example.cpp"
 GLTF_SRC = ROOT / "tests" / "cpp" / "gltf_example.cpp"
+OBJ_SRC = ROOT / "tests" / "cpp" / "obj_example.cpp"
 LIBDIR = ROOT / "photorealisticrender4610_b200"
 
 
@@ -26,6 +27,7 @@ def build_example(tmp_path, src=SRC):
 def test_dropin_example_compiles(tmp_path, lib):
     assert build_example(tmp_path).exists()
     assert build_example(tmp_path, GLTF_SRC).exists()
+    assert build_example(tmp_path, OBJ_SRC).exists()
 
 
 @pytest.mark.gpu
@@ -77,4 +79,34 @@ def test_gltf_dropin_renders_like_the_python_api(tmp_path, cuda):
                                fovh=60.0), 96, 72)
     s.buildBVH()
     want, _ = s.render(64, 6, seed=3, mode="wavefront")
+    assert np.array_equal(fb.view(np.uint32), want.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_obj_dropin_renders_like_the_python_api(tmp_path, cuda):
+    """MeshTriangle(filename, offset, m) of the drop-in header on an OBJ
+    height field, rendered by Renderer::Render, equals the Python API's
+    add_obj scene at the same seed (plain mode, one slice per pixel)."""
+    import sys
+    sys.path.insert(0, str(ROOT / "tests"))
+    from test_obj import grid_obj
+    import photorealisticrender4610_b200 as prr
+    from photorealisticrender4610_b200 import scenes
+    path = tmp_path / "grid.obj"
+    path.write_text(grid_obj(9, seed=2))
+    exe = build_example(tmp_path, OBJ_SRC)
+    out = tmp_path / "fb.bin"
+    r = subprocess.run([str(exe), str(path), str(out)], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    fb = np.fromfile(out, np.float32).reshape(60, 80, 3)
+    s = prr.Scene()
+    m = s.add_material(0, [0.7, 0.6, 0.5, 0.5, 0.0, 1.5, 0.0, 0.0, 0.0])
+    s.add_obj(path, m, (-0.5, 0.0, -0.5))
+    lm = s.add_material(1, [0.8, 0.8, 0.8, 0.5, 0.0, 1.5, 15.0, 15.0, 15.0])
+    s.add_sphere((0.0, 1.2, 0.0), 0.2, lm)
+    s.set_camera(scenes.Camera(eye=(0.0, 1.6, 1.8), target=(0, 0, 0), up=(0, 1, 0), fovv=50.0,
+                               fovh=60.0), 80, 60)
+    s.buildBVH()
+    want, _ = s.render(32, 5, seed=5)
     assert np.array_equal(fb.view(np.uint32), want.cpu().numpy().view(np.uint32))
