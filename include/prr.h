@@ -314,6 +314,30 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream);
 
+/* ---- participating media (Volume.hpp, Volume.cpp) ----------------------
+ * The reference defines a homogeneous medium and the Henyey-Greenstein phase
+ * function, but its integrator never reads them (Scene::medium is not used by
+ * Integrator::castRay); they are provided as batch calls over device arrays.
+ * A medium is active when sigma_t > 1e-6 (Medium::active). */
+typedef struct prr_medium {
+    float sigma_a, sigma_s, sigma_t, g;
+    int bounded;                  /* 0: the medium fills all space */
+    float bounds_min[3], bounds_max[3];
+} prr_medium;
+#define PRR_MEDIUM_DUST 0 /* Medium::dust() */
+#define PRR_MEDIUM_FOG 1  /* Medium::fog() */
+int prr_medium_preset(int which, prr_medium *out);
+/* Medium::intersect (Volume.hpp:17-45) of n rays (o, d: n x 3): out_hit 0/1,
+ * entry and exit distances where hit (0 elsewhere). */
+int prr_medium_intersect(const prr_medium *medium, const float *o, const float *d, int64_t n,
+                         float *out_t_enter, float *out_t_exit, uint8_t *out_hit, void *stream);
+/* phaseHG(cos_theta[k], g) (Volume.cpp:3-6). */
+int prr_phase_hg(const float *cos_theta, int64_t n, float g, float *out, void *stream);
+/* samplePhaseHG(wo[k], g) (Volume.cpp:8-28); item k draws from stream
+ * (seed, k, 0). out_dirs: n x 3. */
+int prr_phase_hg_sample(const float *wo, int64_t n, float g, uint64_t seed, float *out_dirs,
+                        void *stream);
+
 /* ---- render server: continuous batching ---------------------------------
  * No counterpart in the reference (its Renderer renders one scene per
  * process). Requests are admitted in arrival order while a slot is free and

@@ -212,6 +212,15 @@ class ReferenceOracle:
         L.prr_ref_scene_add_gltf.argtypes = [vp, C.c_char_p, C.c_int]
         L.prr_ref_scene_add_obj.restype = C.c_int
         L.prr_ref_scene_add_obj.argtypes = [vp, C.c_char_p, _f32p, C.c_int]
+        L.prr_ref_medium_preset.restype = None
+        L.prr_ref_medium_preset.argtypes = [C.c_int, _f32p]
+        L.prr_ref_medium_intersect.restype = None
+        L.prr_ref_medium_intersect.argtypes = [C.c_int, _f32p, _f32p, _f32p, _f32p, C.c_int64,
+                                               _f32p, _f32p, vp]
+        L.prr_ref_phase_hg.restype = None
+        L.prr_ref_phase_hg.argtypes = [_f32p, C.c_int64, C.c_float, _f32p]
+        L.prr_ref_phase_hg_sample.restype = None
+        L.prr_ref_phase_hg_sample.argtypes = [_f32p, C.c_int64, C.c_float, C.c_uint64, _f32p]
         L.prr_ref_scene_export_mesh.restype = C.c_int64
         L.prr_ref_scene_export_mesh.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.prr_ref_scene_export_material.restype = C.c_int

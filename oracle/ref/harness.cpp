@@ -941,4 +941,49 @@ void prr_ref_photon_estimate(const float *rec, int64_t n, float radius, const fl
     }
 }
 
+// ---- participating media (Volume.hpp, Volume.cpp; unused by castRay)
+
+// Medium::dust() (0) or Medium::fog() (1): sigma_a, sigma_s, sigma_t, g.
+void prr_ref_medium_preset(int which, float *out) {
+    const Medium m = which == 0 ? Medium::dust() : Medium::fog();
+    out[0] = m.sigma_a;
+    out[1] = m.sigma_s;
+    out[2] = m.sigma_t;
+    out[3] = m.g;
+}
+
+void prr_ref_medium_intersect(int bounded, const float *lo, const float *hi, const float *o,
+                              const float *d, int64_t n, float *t_enter, float *t_exit,
+                              uint8_t *hit) {
+    Medium m;
+    m.bounded = bounded != 0;
+    m.bounds.pMin = Vector3f(lo[0], lo[1], lo[2]);
+    m.bounds.pMax = Vector3f(hi[0], hi[1], hi[2]);
+    for (int64_t i = 0; i < n; i++) {
+        const Ray r(Vector3f(o[i * 3], o[i * 3 + 1], o[i * 3 + 2]),
+                    Vector3f(d[i * 3], d[i * 3 + 1], d[i * 3 + 2]));
+        float te = 0.f, tx = 0.f;
+        const bool h = m.intersect(r, te, tx);
+        hit[i] = h ? 1 : 0;
+        t_enter[i] = h ? te : 0.f;
+        t_exit[i] = h ? tx : 0.f;
+    }
+}
+
+void prr_ref_phase_hg(const float *c, int64_t n, float g, float *out) {
+    for (int64_t i = 0; i < n; i++)
+        out[i] = phaseHG(c[i], g);
+}
+
+// samplePhaseHG(wo[i], g), item i drawing from stream (seed, i, 0).
+void prr_ref_phase_hg_sample(const float *wo, int64_t n, float g, uint64_t seed, float *out) {
+    for (int64_t i = 0; i < n; i++) {
+        ref_set_path(seed, (uint32_t) i, 0u);
+        const Vector3f w = samplePhaseHG(Vector3f(wo[i * 3], wo[i * 3 + 1], wo[i * 3 + 2]), g);
+        out[i * 3] = w.x;
+        out[i * 3 + 1] = w.y;
+        out[i * 3 + 2] = w.z;
+    }
+}
+
 } // extern "C"

@@ -5,8 +5,9 @@ hand-written CUDA behind a C ABI (include/prr.h), with a Python mirror of the
 reference's Scene / BVHAccel / Integrator / Renderer interface."""
 from ._lib import PrrError, header_symbols, load  # noqa: F401
 from . import scenes  # noqa: F401
-from .api import (PhotonMap, Scene, Server, read_obj, sample_count_image,  # noqa: F401
-                  tonemap, write_image)
+from .api import (PhotonMap, Scene, Server, medium_intersect, medium_preset,  # noqa: F401
+                  phase_hg, phase_hg_sample, read_obj, sample_count_image, tonemap,
+                  write_image)
 
 __all__ = ["Scene", "PhotonMap", "Server", "PrrError", "load", "header_symbols", "scenes",
            "tonemap"]

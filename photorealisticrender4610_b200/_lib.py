@@ -43,6 +43,12 @@ class prr_wavefront_config(C.Structure):
                 ("stack_smem", C.c_int), ("ordered", C.c_int)]
 
 
+class prr_medium(C.Structure):
+    _fields_ = [("sigma_a", C.c_float), ("sigma_s", C.c_float), ("sigma_t", C.c_float),
+                ("g", C.c_float), ("bounded", C.c_int), ("bounds_min", C.c_float * 3),
+                ("bounds_max", C.c_float * 3)]
+
+
 class prr_server_config(C.Structure):
     _fields_ = [("device_budget_bytes", C.c_int64), ("max_active", C.c_int),
                 ("samples_per_step", C.c_int64), ("fail_every_nth_admission", C.c_int),
@@ -135,6 +141,11 @@ _SIGS = {
     "prr_photon_gather": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp]),
     "prr_render_caustics": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int, _vp,
                                       _vp]),
+    "prr_medium_preset": (C.c_int, [C.c_int, C.POINTER(prr_medium)]),
+    "prr_medium_intersect": (C.c_int, [C.POINTER(prr_medium), _vp, _vp, C.c_int64, _vp, _vp,
+                                       _vp, _vp]),
+    "prr_phase_hg": (C.c_int, [_vp, C.c_int64, C.c_float, _vp, _vp]),
+    "prr_phase_hg_sample": (C.c_int, [_vp, C.c_int64, C.c_float, C.c_uint64, _vp, _vp]),
     "prr_server_create": (C.c_int, [C.POINTER(prr_server_config), C.POINTER(_vp)]),
     "prr_server_destroy": (C.c_int, [_vp]),
     "prr_server_add_scene": (C.c_int, [_vp, _vp, C.POINTER(C.c_int)]),

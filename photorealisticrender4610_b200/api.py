@@ -69,6 +69,61 @@ def read_obj(path, offset=(0.0, 0.0, 0.0)) -> np.ndarray:
     return out
 
 
+MEDIUM_PRESETS = {"dust": 0, "fog": 1}
+
+
+def medium_preset(name: str) -> dict:
+    """Medium::dust() / Medium::fog() (Volume.hpp:47-63) as a dict."""
+    m = _lib.prr_medium()
+    check(_lib.load().prr_medium_preset(MEDIUM_PRESETS[name], C.byref(m)))
+    return {"sigma_a": m.sigma_a, "sigma_s": m.sigma_s, "sigma_t": m.sigma_t, "g": m.g,
+            "bounded": False}
+
+
+def _medium(d: dict):
+    m = _lib.prr_medium()
+    for k in ("sigma_a", "sigma_s", "sigma_t", "g"):
+        setattr(m, k, float(d.get(k, 0.0)))
+    m.bounded = 1 if d.get("bounded") else 0
+    lo, hi = d.get("bounds", ((0.0,) * 3, (0.0,) * 3))
+    m.bounds_min = (C.c_float * 3)(*map(float, lo))
+    m.bounds_max = (C.c_float * 3)(*map(float, hi))
+    return m
+
+
+def medium_intersect(medium: dict, o, d, stream=None):
+    """Medium::intersect for (n, 3) float32 CUDA tensors: (t_enter, t_exit,
+    hit) with zeros where a ray misses the medium's box."""
+    import torch
+    n = o.shape[0]
+    te = torch.empty(n, dtype=torch.float32, device=o.device)
+    tx = torch.empty_like(te)
+    hit = torch.empty(n, dtype=torch.uint8, device=o.device)
+    m = _medium(medium)
+    check(_lib.load().prr_medium_intersect(C.byref(m), _ptr(o), _ptr(d), n, _ptr(te), _ptr(tx),
+                                           _ptr(hit), _stream(stream)))
+    return te, tx, hit
+
+
+def phase_hg(cos_theta, g: float, stream=None):
+    """phaseHG(cos_theta, g) (Volume.cpp:3-6) of a float32 CUDA tensor."""
+    import torch
+    out = torch.empty_like(cos_theta)
+    check(_lib.load().prr_phase_hg(_ptr(cos_theta), cos_theta.numel(), float(g), _ptr(out),
+                                   _stream(stream)))
+    return out
+
+
+def phase_hg_sample(wo, g: float, seed: int = 1, stream=None):
+    """samplePhaseHG(wo[k], g) (Volume.cpp:8-28) for an (n, 3) float32 CUDA
+    tensor; item k draws from stream (seed, k, 0)."""
+    import torch
+    out = torch.empty_like(wo)
+    check(_lib.load().prr_phase_hg_sample(_ptr(wo), wo.shape[0], float(g), seed, _ptr(out),
+                                          _stream(stream)))
+    return out
+
+
 def _normalize_rows(v: np.ndarray) -> np.ndarray:
     """normalize (Vector.hpp:103-111) row by row in float32: v * (1 / sqrt(|v|^2))."""
     x, y, z = v[:, 0], v[:, 1], v[:, 2]
