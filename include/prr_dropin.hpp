@@ -22,7 +22,9 @@
 //   Camera::create / fromBlender / init
 //                                 Camera.hpp:23-56
 //   Scene::Add / buildBVH / intersect / intersectP, envMap, camera,
-//   backgroundColor               Scene.hpp:15-41
+//   backgroundColor, medium       Scene.hpp:15-41
+//   Medium (dust, fog, active, intersect)
+//                                 Volume.hpp:7-63
 //   Integrator(scene, maxDepth, rr), castRay
 //                                 Integrator.hpp:15-23
 //   RenderSettings, Renderer::Render
@@ -374,12 +376,64 @@ struct Intersection {
     int primitive = -1; // triangle index within the mesh
 };
 
+// Medium (Volume.hpp:7-63): a homogeneous medium; like the reference's
+// integrator, rendering does not read Scene::medium. intersect is a one-ray
+// batch of prr_medium_intersect.
+struct Medium {
+    float sigma_a = 0.0f;
+    float sigma_s = 0.0f;
+    float sigma_t = 0.0f;
+    float g = 0.0f;
+    bool bounded = false;
+    Bounds3 bounds;
+    bool active() const { return sigma_t > 1e-6f; }
+    bool intersect(const Ray &ray, float &t_enter, float &t_exit) const {
+        prr_medium m{};
+        m.sigma_a = sigma_a;
+        m.sigma_s = sigma_s;
+        m.sigma_t = sigma_t;
+        m.g = g;
+        m.bounded = bounded ? 1 : 0;
+        const float lo[3] = {bounds.pMin.x, bounds.pMin.y, bounds.pMin.z};
+        const float hi[3] = {bounds.pMax.x, bounds.pMax.y, bounds.pMax.z};
+        std::copy(lo, lo + 3, m.bounds_min);
+        std::copy(hi, hi + 3, m.bounds_max);
+        const float o[3] = {ray.origin.x, ray.origin.y, ray.origin.z};
+        const float d[3] = {ray.direction.x, ray.direction.y, ray.direction.z};
+        prr_detail::DeviceArray<float> dO(3), dD(3), dE(1), dX(1);
+        prr_detail::DeviceArray<uint8_t> dH(1);
+        dO.put(o);
+        dD.put(d);
+        prr_detail::check(prr_medium_intersect(&m, dO.p, dD.p, 1, dE.p, dX.p, dH.p, nullptr));
+        uint8_t hit;
+        dH.get(&hit);
+        if (hit) {
+            dE.get(&t_enter);
+            dX.get(&t_exit);
+        }
+        return hit != 0;
+    }
+    static Medium preset(int which) {
+        prr_medium p{};
+        prr_detail::check(prr_medium_preset(which, &p));
+        Medium m;
+        m.sigma_a = p.sigma_a;
+        m.sigma_s = p.sigma_s;
+        m.sigma_t = p.sigma_t;
+        m.g = p.g;
+        return m;
+    }
+    static Medium dust() { return preset(PRR_MEDIUM_DUST); }
+    static Medium fog() { return preset(PRR_MEDIUM_FOG); }
+};
+
 class Scene {
   public:
     Vector3f backgroundColor = Vector3f(0.235294f, 0.67451f, 0.843137f);
     std::vector<Object *> objects;
     EnvMap envMap;
     Camera camera;
+    Medium medium; // Scene.hpp:25; not read by rendering, as in the reference
 
     Scene() { prr_detail::check(prr_scene_create(&h_)); }
     ~Scene() { prr_scene_destroy(h_); }

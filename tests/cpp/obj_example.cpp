@@ -22,6 +22,15 @@ int main(int argc, char **argv) {
     scene.camera.init(W, H);
     scene.buildBVH();
 
+    // the medium is carried like the reference's Scene::medium (rendering ignores it)
+    scene.medium = Medium::fog();
+    scene.medium.bounded = true;
+    scene.medium.bounds = Bounds3(Vector3f(-1.0f, -1.0f, -1.0f), Vector3f(1.0f, 1.0f, 1.0f));
+    float te = 0.f, tx = 0.f;
+    const bool inside = scene.medium.intersect(Ray(Vector3f(0.0f, 0.0f, 3.0f),
+                                                   Vector3f(0.0f, 0.0f, -1.0f)), te, tx);
+    std::printf("medium %d %g %g active %d\n", (int) inside, te, tx, (int) scene.medium.active());
+
     Integrator integrator(scene, 5, 0.8f);
     RenderSettings settings;
     settings.width = W;

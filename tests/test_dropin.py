@@ -99,6 +99,7 @@ def test_obj_dropin_renders_like_the_python_api(tmp_path, cuda):
     r = subprocess.run([str(exe), str(path), str(out)], cwd=tmp_path, capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
+    assert "medium 1 2 4 active 1" in r.stdout  # enters the unit box at t=2, leaves at 4
     fb = np.fromfile(out, np.float32).reshape(60, 80, 3)
     s = prr.Scene()
     m = s.add_material(0, [0.7, 0.6, 0.5, 0.5, 0.0, 1.5, 0.0, 0.0, 0.0])
