@@ -1,5 +1,6 @@
-// Device side of the render server: one launch renders the next sample chunk
-// of every admitted request at once. Each block takes one work item -- a
+// Device side of the render server's megakernel steps (the server's other
+// step kind runs on the wavefront integrator, k_wavefront.cu): one launch
+// renders the next sample chunk of every admitted request at once. Each block takes one work item -- a
 // (request, 16x8 pixel tile) pair -- from a table the host fills per step, so
 // requests of different scenes, sizes and sample counts share the launch.
 // Scenes stay resident: every request points at its scene's DevScene, kept in
