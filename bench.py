@@ -404,10 +404,10 @@ def run_render(args, rank, world, on):
         tuned = cfg
     else:
         # tune on enough samples per pixel (a power of two, so the candidate
-        # pass sizes divide it) that the largest candidate pass (32M paths)
+        # pass sizes divide it) that the largest candidate pass (64M paths)
         # fits in the tuning render, or on the whole frame
         tune_spp = 4
-        while tune_spp < spp and npix * tune_spp < (1 << 25):
+        while tune_spp < spp and npix * tune_spp < (1 << 26):
             tune_spp *= 2
         tuned = scene.autotune(min(tune_spp, spp), depth)
 

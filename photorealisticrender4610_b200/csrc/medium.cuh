@@ -14,9 +14,11 @@ struct DevMedium {
 };
 
 // Medium::intersect (Volume.hpp:17-45): slab entry and exit of the medium's
-// box (all of space when unbounded). The per-axis swap follows the
-// reference's flag, which is set for POSITIVE directions; std::max / std::min
-// keep their operand order (a NaN slab distance propagates as there).
+// box (all of space when unbounded). The box corner and the ray origin are
+// read through Vector3f's const operator[], which returns double
+// (Vector.hpp:67,78-80), so each slab distance is a double product rounded
+// once to float. The per-axis swap follows the reference's flag, which is set
+// for POSITIVE directions; std::max / std::min keep their operand order.
 __device__ __forceinline__ bool medium_intersect(const DevMedium &m, V3 o, V3 d, float &t_enter,
                                                  float &t_exit) {
     if (!m.bounded) {
@@ -30,8 +32,8 @@ __device__ __forceinline__ bool medium_intersect(const DevMedium &m, V3 o, V3 d,
 #pragma unroll
     for (int i = 0; i < 3; i++) {
         const float inv = 1.0f / dd[i];
-        float a = (m.lo[i] - oo[i]) * inv;
-        float b = (m.hi[i] - oo[i]) * inv;
+        float a = (float) (((double) m.lo[i] - (double) oo[i]) * (double) inv);
+        float b = (float) (((double) m.hi[i] - (double) oo[i]) * (double) inv);
         if (!(dd[i] > 0)) {
             const float t = a;
             a = b;
@@ -47,21 +49,19 @@ __device__ __forceinline__ bool medium_intersect(const DevMedium &m, V3 o, V3 d,
     return true;
 }
 
-// phaseHG (Volume.cpp:3-6): the normalisation 4*pi is a double product in
-// the reference, so the quotient is taken in double and rounded once; the
-// 1.5 power is evaluated in double and rounded to float, as a correctly
-// rounded powf returns it.
+// phaseHG (Volume.cpp:3-6), in float throughout (the reference's M_PI is a
+// float, global.hpp:9-10); the 1.5 power is evaluated in double and rounded
+// once, which is what a correctly rounded powf returns.
 __device__ __forceinline__ float phase_hg(float cos_theta, float g) {
     const float denom = 1.0f + g * g - 2.0f * g * cos_theta;
     const float p = (float) pow((double) denom, 1.5);
-    return (float) ((double) (1.0f - g * g) / (12.566370614359172 * (double) p));
+    return (1.0f - g * g) / (4.0f * PRR_PI * p);
 }
 
 // samplePhaseHG (Volume.cpp:8-28): one draw for cos(theta) (uniform when
-// |g| < 1e-3, else the inverted HG CDF), one for phi; the direction is built
-// in buildTBN(wo)'s frame and normalized. phi = 2*pi*u is a double product
-// stored as float; its cosine and sine are float functions in the reference,
-// taken here in double and rounded once.
+// |g| < 1e-3, else the inverted HG CDF), one for phi = 2*pi*u (float); the
+// direction is built in buildTBN(wo)'s frame and normalized. The float cosine
+// and sine of phi are taken in double and rounded once.
 __device__ __forceinline__ V3 sample_phase_hg(V3 wo, float g, Rng &rng) {
     float cos_theta;
     if (fabsf(g) < 1e-3f) {
@@ -72,7 +72,7 @@ __device__ __forceinline__ V3 sample_phase_hg(V3 wo, float g, Rng &rng) {
         cos_theta = (1.0f + g * g - sqr * sqr) / (2.0f * g);
     }
     const float sin_theta = sqrtf(smax(0.0f, 1.0f - cos_theta * cos_theta));
-    const float phi = (float) (6.283185307179586 * (double) rng.next());
+    const float phi = 2.0f * PRR_PI * rng.next();
     const Frame f = build_tbn(wo);
     const float cp = (float) cos((double) phi), sp = (float) sin((double) phi);
     return normalize((sin_theta * cp) * f.T + (sin_theta * sp) * f.B + cos_theta * wo);

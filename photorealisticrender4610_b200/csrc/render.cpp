@@ -97,7 +97,8 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
     PRR_CUDA_TRY(cudaEventCreate(&a));
     PRR_CUDA_TRY(cudaEventCreate(&b));
     const int64_t paths[] = {int64_t(1) << 20, int64_t(1) << 21, int64_t(1) << 22,
-                             int64_t(1) << 23, int64_t(1) << 24, int64_t(1) << 25};
+                             int64_t(1) << 23, int64_t(1) << 24, int64_t(1) << 25,
+                             int64_t(1) << 26};
     const int blocks[] = {64, 128, 256};
     float best_ms = 1e30f;
     prr_wavefront_config best{0, 0, 1, 0, 1};
