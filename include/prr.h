@@ -347,7 +347,7 @@ int prr_phase_hg_sample(const float *wo, int64_t n, float g, uint64_t seed, floa
 typedef struct prr_server prr_server;
 typedef struct prr_server_config {
     int64_t device_budget_bytes; /* resident scenes + admitted requests (0: 120 GiB);
-                                    the step state comes on top: about 340 bytes per
+                                    the step state comes on top: about 320 bytes per
                                     path of paths_per_launch, plus up to 2 GiB of
                                     pooled request blocks */
     int max_active;              /* requests rendered at once (0: 64) */
