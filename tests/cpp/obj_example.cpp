@@ -27,9 +27,14 @@ int main(int argc, char **argv) {
     scene.medium.bounded = true;
     scene.medium.bounds = Bounds3(Vector3f(-1.0f, -1.0f, -1.0f), Vector3f(1.0f, 1.0f, 1.0f));
     float te = 0.f, tx = 0.f;
-    const bool inside = scene.medium.intersect(Ray(Vector3f(0.0f, 0.0f, 3.0f),
-                                                   Vector3f(0.0f, 0.0f, -1.0f)), te, tx);
-    std::printf("medium %d %g %g active %d\n", (int) inside, te, tx, (int) scene.medium.active());
+    const float c = 0.57735026f; // 1/sqrt(3)
+    const bool diag = scene.medium.intersect(Ray(Vector3f(-3.0f), Vector3f(c, c, c)), te, tx);
+    std::printf("medium %d %g %g active %d\n", (int) diag, te, tx, (int) scene.medium.active());
+    // a direction with zero components: Medium::intersect swaps the slab ends
+    // of every axis whose direction is not positive, so this ray misses
+    const bool axis = scene.medium.intersect(Ray(Vector3f(0.0f, 0.0f, 3.0f),
+                                                 Vector3f(0.0f, 0.0f, -1.0f)), te, tx);
+    std::printf("axis-aligned %d\n", (int) axis);
 
     Integrator integrator(scene, 5, 0.8f);
     RenderSettings settings;

@@ -99,7 +99,10 @@ def test_obj_dropin_renders_like_the_python_api(tmp_path, cuda):
     r = subprocess.run([str(exe), str(path), str(out)], cwd=tmp_path, capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    assert "medium 1 2 4 active 1" in r.stdout  # enters the unit box at t=2, leaves at 4
+    # the diagonal ray enters the box at 2*sqrt(3) and leaves at 4*sqrt(3); the
+    # reference's intersect misses axis-aligned rays (their zero components)
+    assert "medium 1 3.4641 6.9282 active 1" in r.stdout, r.stdout
+    assert "axis-aligned 0" in r.stdout
     fb = np.fromfile(out, np.float32).reshape(60, 80, 3)
     s = prr.Scene()
     m = s.add_material(0, [0.7, 0.6, 0.5, 0.5, 0.0, 1.5, 0.0, 0.0, 0.0])
