@@ -194,12 +194,14 @@ def cpu_reference_rate(verts, o, d, n_sample, threads):
     rate, like the GPU number)."""
     from oracle import loader
     if "mesh" not in _CPU_MESH:
+        t0 = time.perf_counter()
         if loader.reference_available(fast=True):
             mesh, kind = loader.ReferenceOracle(fast=True).mesh(verts), "reference"
         else:
             mesh, kind = loader.PortOracle().mesh(verts), "port"
+        build_s = time.perf_counter() - t0
         mesh.intersect(o[:4096], d[:4096], threads=threads)
-        _CPU_MESH.update(kind=kind, mesh=mesh)
+        _CPU_MESH.update(kind=kind, mesh=mesh, build_s=build_s)
     mesh, kind = _CPU_MESH["mesh"], _CPU_MESH["kind"]
     t0 = time.perf_counter()
     mesh.intersect(o[:n_sample], d[:n_sample], threads=threads)
@@ -244,6 +246,12 @@ def run_ours(args, rank, world, on):
     dev = torch.device("cuda", torch.cuda.current_device())
     verts, o, d = workload_arrays()
     scene = prr.Scene.single_mesh(verts)
+    # the scene build (SAH tree on the host cores, then the upload), timed on a
+    # second build so the first one's context set-up is not counted
+    t0 = time.perf_counter()
+    second = prr.Scene.single_mesh(verts)
+    build_s = time.perf_counter() - t0
+    del second
     O = torch.from_numpy(o).to(dev)
     D = torch.from_numpy(d).to(dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
@@ -353,6 +361,8 @@ def run_ours(args, rank, world, on):
         "cpu_baseline": {"value": cpu_rate, "unit": "Mrays/s", "cores": threads,
                          "kind": cpu_kind, "sample": f"all {N_RAYS} query rays, one pass",
                          "one_core": {"value": cpu_rate_1, "sample": "first 131072 query rays"}},
+        "bvh_build_s": {"ours": build_s, "ours_threads": threads,
+                        "reference": _CPU_MESH.get("build_s"), "reference_threads": 1},
         "clocks": clocks,
         "gpu_launches": args.steps,
     }
