@@ -251,7 +251,12 @@ def run_ours(args, rank, world, on):
     t0 = time.perf_counter()
     second = prr.Scene.single_mesh(verts)
     build_s = time.perf_counter() - t0
+    # release it now (a collection during the timed steps would free device
+    # memory between them)
     del second
+    import gc
+    gc.collect()
+    torch.cuda.synchronize()
     O = torch.from_numpy(o).to(dev)
     D = torch.from_numpy(d).to(dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
