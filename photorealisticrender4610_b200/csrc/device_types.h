@@ -115,6 +115,12 @@ struct DevEnv {
     const float4 *pixels; // rgb + pad, row-major
     const float *cdf;     // width*height conditional CDFs
     const float *marginal;// height
+    // guide tables of the CDF searches: (height + 1) rows of guide_n + 1
+    // indices, the marginal's first; entry k of a table = lower_bound(cdf, k /
+    // guide_n); a table whose first entry is -1 is searched whole (its CDF is
+    // not non-decreasing). guide_n = 0: no tables.
+    const int32_t *guide;
+    int32_t guide_n;
     int32_t width, height;
     float total;          // totalLuminance
     int32_t loaded;

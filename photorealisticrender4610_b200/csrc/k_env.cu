@@ -7,7 +7,8 @@
 // thread per row; the row's pixels are first staged through shared memory
 // with coalesced loads, and the normalisation and write-back are spread over
 // the block. Rows run in parallel, one block each. The marginal CDF over the
-// row sums is the same sequential sum over rows.
+// row sums is the same sequential sum over rows. Guide tables for the
+// samplers' searches are built last.
 #include "prr_internal.h"
 
 namespace prr {
@@ -68,6 +69,44 @@ __global__ void k_env_marginal(const float *__restrict__ row_sums, int h,
         marginal[r] = (t > 0.f) ? acc[r] / t : acc[r];
 }
 
+// One block per table (block 0: the marginal, block r + 1: row r): entry k
+// = lower_bound(cdf, k / G), by the same search the samplers run; the
+// table's first entry becomes -1 when its CDF is not non-decreasing (NaN or
+// a decrease), so that the samplers search it whole.
+__global__ void k_env_guide(const float *__restrict__ cdf, const float *__restrict__ marginal,
+                            int w, int h, int G, int32_t *__restrict__ guide) {
+    const int b = blockIdx.x;
+    const float *a = b == 0 ? marginal : cdf + (size_t) (b - 1) * w;
+    const int n = b == 0 ? h : w;
+    int32_t *g = guide + (size_t) b * (G + 1);
+    __shared__ int bad;
+    if (threadIdx.x == 0)
+        bad = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i + 1 < n; i += blockDim.x)
+        if (!(a[i] <= a[i + 1]))
+            bad = 1;
+    if (threadIdx.x == 0 && !(a[0] >= 0.f))
+        bad = 1;
+    for (int k = threadIdx.x; k <= G; k += blockDim.x) {
+        const float t = (float) k / (float) G;
+        int lo = 0, len = n;
+        while (len > 0) {
+            const int half = len >> 1;
+            if (a[lo + half] < t) {
+                lo += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
+            }
+        }
+        g[k] = lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && bad)
+        g[0] = -1;
+}
+
 } // namespace
 
 int launch_env_cdf(Scene &s, cudaStream_t st) {
@@ -91,6 +130,9 @@ int launch_env_cdf(Scene &s, cudaStream_t st) {
     k_env_marginal<<<1, kEnvBlock, col_smem, st>>>(sums.as<float>(), h,
                                                    s.d_env_marginal.as<float>(),
                                                    sums.as<float>() + h);
+    PRR_CUDA_TRY(cudaGetLastError());
+    k_env_guide<<<h + 1, kEnvBlock, 0, st>>>(s.d_env_cdf.as<float>(), s.d_env_marginal.as<float>(),
+                                             w, h, kEnvGuide, s.d_env_guide.as<int32_t>());
     PRR_CUDA_TRY(cudaGetLastError());
     float total = 0.f;
     PRR_CUDA_TRY(cudaMemcpyAsync(&total, sums.as<float>() + h, sizeof(float),

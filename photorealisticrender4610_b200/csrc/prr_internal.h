@@ -101,7 +101,7 @@ struct Scene {
     DevBuf d_nodes, d_tris, d_verts, d_normals, d_objects, d_materials, d_emissives;
     std::vector<HostTexture> textures;
     DevBuf d_attr, d_texels, d_textures;
-    DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin;
+    DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin, d_env_guide;
     DevBuf d_scratch;      // staging for host-buffer entry points
     DevBuf d_render, d_render_spp; // per-slice partial sums / adaptive spp
     DevBuf d_counter;      // persistent-kernel work counters
@@ -145,6 +145,9 @@ int launch_scene_closest(const Scene &s, const float *o, const float *d, int64_t
                          int32_t *obj, int32_t *prim, float *t, float *geo, cudaStream_t st);
 int launch_scene_occluded(const Scene &s, const float *o, const float *d, const float *tmax,
                           int64_t n, uint8_t *hit, cudaStream_t st);
+// Buckets of the env CDF guide tables (a power of two: k / kEnvGuide and
+// u * kEnvGuide are exact in float).
+constexpr int kEnvGuide = 256;
 int launch_env_cdf(Scene &s, cudaStream_t st);
 int render_plain(Scene &s, const prr_render_settings &rs, float *out_rgb, int32_t *out_spp,
                  unsigned long long *out_rays, cudaStream_t st);

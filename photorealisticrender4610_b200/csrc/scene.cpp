@@ -459,9 +459,12 @@ int build_scene(Scene &s, cudaStream_t st) {
             return rc;
         PRR_CUDA_TRY(s.d_env_cdf.alloc((size_t) w * h * sizeof(float)));
         PRR_CUDA_TRY(s.d_env_marginal.alloc((size_t) h * sizeof(float)));
+        PRR_CUDA_TRY(s.d_env_guide.alloc((size_t) (h + 1) * (kEnvGuide + 1) * sizeof(int32_t)));
         D.env.pixels = s.d_env_px.as<float4>();
         D.env.cdf = s.d_env_cdf.as<float>();
         D.env.marginal = s.d_env_marginal.as<float>();
+        D.env.guide = s.d_env_guide.as<int32_t>();
+        D.env.guide_n = kEnvGuide;
         D.env.width = w;
         D.env.height = h;
         D.env.loaded = 1;
@@ -475,7 +478,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     s.device_bytes = s.d_attr.bytes + s.d_texels.bytes + s.d_textures.bytes +
                      s.d_nodes.bytes + s.d_tris.bytes + s.d_verts.bytes + s.d_normals.bytes +
                      s.d_objects.bytes + s.d_materials.bytes + s.d_emissives.bytes +
-                     s.d_env_px.bytes + s.d_env_cdf.bytes + s.d_env_marginal.bytes;
+                     s.d_env_px.bytes + s.d_env_cdf.bytes + s.d_env_marginal.bytes +
+                     s.d_env_guide.bytes;
     s.built = true;
     return PRR_OK;
 }

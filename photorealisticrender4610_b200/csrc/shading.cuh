@@ -552,13 +552,29 @@ __device__ __forceinline__ int lower_bound(const float *a, int n, float x) {
     }
     return lo;
 }
+// lower_bound over a non-decreasing CDF, started from its guide table: for u
+// in [k/G, (k+1)/G) the answer lies in [guide[k], guide[k+1]] (lower_bound is
+// monotone in the searched value), and the search of that sub-range returns
+// the same index as the search of the whole array, in a few steps instead of
+// log2(n). u * G is exact (G a power of two, u in [0, 1)).
+__device__ __forceinline__ int guided_lower_bound(const float *a, int n, float u,
+                                                  const int32_t *g, int G) {
+    if (G > 0 && __ldg(g) >= 0) {
+        const int k = min((int) (u * (float) G), G - 1);
+        const int lo = __ldg(g + k), hi = __ldg(g + k + 1);
+        return lo + lower_bound(a + lo, hi - lo, u);
+    }
+    return lower_bound(a, n, u);
+}
 // EnvMap::importanceSample (EnvMap.hpp:145-169)
 __device__ __forceinline__ V3 env_importance(const DevEnv &e, Rng &rng, float &pdf) {
     const float r1 = rng.next();
     const float r2 = rng.next();
-    int row = lower_bound(e.marginal, e.height, r1);
+    const int G = e.guide_n;
+    int row = guided_lower_bound(e.marginal, e.height, r1, e.guide, G);
     row = min(row, e.height - 1);
-    int col = lower_bound(e.cdf + (size_t) row * e.width, e.width, r2);
+    int col = guided_lower_bound(e.cdf + (size_t) row * e.width, e.width, r2,
+                                 G > 0 ? e.guide + (size_t) (row + 1) * (G + 1) : nullptr, G);
     col = min(col, e.width - 1);
     const float u = (col + 0.5f) / (float) e.width;
     const float v = (row + 0.5f) / (float) e.height;
