@@ -542,7 +542,8 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const int k = base + threadIdx.x;
-        bool cont = false, shadow = false;
+        bool cont = false, shadow = false, jl = false, je = false;
+        uint8_t oct = 0;
         int p = 0;
         if (k < n) {
             p = w.qsurf[k];
@@ -613,12 +614,20 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
                     }
                 }
                 if (shadow) {
-                    w.slo[p] = lo;
+                    // a ray's direction carries its flag (w = 0: none); its
+                    // origin and contribution are read only when set
                     w.sld[p] = ld;
-                    w.slc[p] = lc;
-                    w.seo[p] = eo;
                     w.sed[p] = ed;
-                    w.sec[p] = ec;
+                    if (ld.w != 0.f) {
+                        w.slo[p] = lo;
+                        w.slc[p] = lc;
+                    }
+                    if (ed.w != 0.f) {
+                        w.seo[p] = eo;
+                        w.sec[p] = ec;
+                    }
+                    jl = ld.w != 0.f;
+                    je = ed.w != 0.f;
                 }
                 BSDFSample bs;
                 if (m.kind == kMatDiffuse)
@@ -637,6 +646,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
                     const V3 off = dot(bs.wi, sd.f.N) >= 0.f ? sd.f.N : -sd.f.N;
                     st3(w.ro, p, hp + off * PRR_EPS);
                     st3(w.rd, p, bs.wi);
+                    oct = dir_octant(bs.wi);
                     st3(w.pend, p, scale, bs.pdf);
                     st3(w.prev, p, hp);
                     st3(w.beta, p, beta);
@@ -650,7 +660,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
         }
         if (w.ordered) {
             if (cont)
-                w.tag[p] = dir_octant(ld3(w.rd, p));
+                w.tag[p] = oct;
         } else {
             const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
             if (cont)
@@ -659,8 +669,6 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
         const int sslot = warp_append(w.cnt + kCntShadow, shadow);
         if (shadow)
             w.qshadow[sslot] = p;
-        const bool jl = shadow && w.sld[p].w != 0.f;
-        const bool je = shadow && w.sed[p].w != 0.f;
         const int j0 = warp_append(w.cnt + kCntShadowJobs, jl);
         if (jl)
             w.qjob[j0] = p * 2;
