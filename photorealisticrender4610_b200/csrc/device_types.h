@@ -138,6 +138,8 @@ struct DevScene {
     int32_t n_textures;
     const int32_t *emissives; // Scene::emissives, in object order
     int32_t n_objects, n_materials, n_emissives;
+    int32_t has_emissive_kind; // some material is of the emissive kind (hit-emission MIS
+                               // then needs the previous hit point)
     float total_emit_area;
     uint32_t tlas_root;
     float tlas_box[6];

@@ -550,6 +550,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
             const DevScene &S = scene_of<MULTI>(S0, w, p);
             Rng rng{w.rng[p]};
             V3 beta = ld3(w.beta, p), L = ld3(w.L, p);
+            const V3 L0 = L;
             const Inter in = load_inter(S, w, p);
             int it;
             bool spec;
@@ -648,9 +649,13 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
                     st3(w.rd, p, bs.wi);
                     oct = dir_octant(bs.wi);
                     st3(w.pend, p, scale, bs.pdf);
-                    st3(w.prev, p, hp);
+                    if (S.has_emissive_kind) // read only on an emissive hit
+                        st3(w.prev, p, hp);
                     st3(w.beta, p, beta);
-                    st3(w.L, p, L);
+                    if (__float_as_uint(L.x) != __float_as_uint(L0.x) ||
+                        __float_as_uint(L.y) != __float_as_uint(L0.y) ||
+                        __float_as_uint(L.z) != __float_as_uint(L0.z))
+                        st3(w.L, p, L); // changed only by emission at this hit
                     w.bounce[p] = it;
                     w.flags[p] = kFlagPending;
                     cont = true;

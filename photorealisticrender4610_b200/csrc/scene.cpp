@@ -428,6 +428,9 @@ int build_scene(Scene &s, cudaStream_t st) {
     D.n_objects = (int32_t) s.objects.size();
     D.n_materials = (int32_t) s.materials.size();
     D.n_emissives = (int32_t) emissives.size();
+    for (const HostMaterial &m : s.materials)
+        if (m.kind == kMatEmissive)
+            D.has_emissive_kind = 1;
     D.total_emit_area = emit_area;
     D.tlas_root = tlas_root;
     if (!s.objects.empty())
