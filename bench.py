@@ -99,6 +99,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up holds the driver for a while and stalls
+            # CUDA calls: let it deliver its first sample before any timing
+            deadline = time.time() + 10.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.05)
             time.sleep(0.3)
         except OSError:
             self.proc = None
