@@ -79,6 +79,12 @@ def max_over_ranks(x, on):
     return float(t.item())
 
 
+# GPU busy-wait queued before each timed step's start event (about 30 ms at
+# 1.97 GHz): a host stall shorter than this (a driver call held up by the
+# clock sampler) then falls before the step instead of inside it.
+SLEEP_CYCLES = 60_000_000
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -280,7 +286,7 @@ def run_ours(args, rank, world, on):
         times = []
         for _ in range(2):
             flush.zero_()
-            torch.cuda._sleep(20_000_000)
+            torch.cuda._sleep(SLEEP_CYCLES)
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
             scene.mesh_intersect(0, O, D, config=cfg)
@@ -304,11 +310,11 @@ def run_ours(args, rank, world, on):
         torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()
-            # keep the GPU busy (about 10 ms) while the host enqueues the timed
+            # keep the GPU busy (about 30 ms) while the host enqueues the timed
             # launch, so no host-side latency falls between the two events (the
             # driver calls of a launch can wait a few ms on the nvidia-smi
             # clock sampler)
-            torch.cuda._sleep(20_000_000)
+            torch.cuda._sleep(SLEEP_CYCLES)
             starts[k].record()
             hid, t = scene.mesh_intersect(0, O, D, config=best)
             ends[k].record()
@@ -438,7 +444,7 @@ def run_render(args, rank, world, on):
         rays = None
         for _ in range(steps):
             flush.zero_()
-            torch.cuda._sleep(20_000_000)
+            torch.cuda._sleep(SLEEP_CYCLES)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             img, cnt, rays = scene.render(spp, depth, seed=1, mode=mode, slices=0,
@@ -551,7 +557,7 @@ def run_caustics(args, rank, world, on):
 
     def step():
         flush.zero_()
-        torch.cuda._sleep(20_000_000)
+        torch.cuda._sleep(SLEEP_CYCLES)
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         ev[0].record()
         pm.emit(scene, n_ph, seed=1, max_depth=depth)
