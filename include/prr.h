@@ -106,7 +106,8 @@ typedef struct prr_render_settings {
 
 /* Wavefront launch shape (chosen by prr_autotune; zero fields = defaults). */
 typedef struct prr_wavefront_config {
-    int64_t paths_per_pass; /* paths in flight per pass (0: about 8M) */
+    int64_t paths_per_pass; /* paths in flight per pass (0: about 8M; at most 2^30; about
+                               320 bytes of device memory each) */
     int block_size;         /* threads per block of the traversal stages (0: 128) */
     int use_graphs;         /* 1: replay each pass from one captured CUDA graph */
     int stack_smem;         /* mesh-BVH stack entries per thread kept in shared memory;

@@ -64,9 +64,12 @@ extern "C" int prr_render(prr_scene *scene, const prr_render_settings *settings,
 extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config) {
     if (!scene || !config)
         return fail(PRR_ERR_INVALID_ARGUMENT, "scene and config are required");
-    if (config->paths_per_pass < 0 || config->block_size < 0 || config->block_size % 32 != 0 ||
-        config->block_size > 512 || config->stack_smem < 0)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "bad wavefront config");
+    if (config->paths_per_pass < 0 || config->paths_per_pass > (int64_t(1) << 30) ||
+        config->block_size < 0 || config->block_size % 32 != 0 || config->block_size > 512 ||
+        config->stack_smem < 0)
+        return fail(PRR_ERR_INVALID_ARGUMENT,
+                    "bad wavefront config (paths_per_pass <= 2^30, block_size a multiple of "
+                    "32 up to 512, stack_smem >= 0)");
     Scene &s = *reinterpret_cast<Scene *>(scene);
     std::lock_guard<std::mutex> g(s.mu);
     s.wf_paths = config->paths_per_pass;

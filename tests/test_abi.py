@@ -144,3 +144,16 @@ def test_scene_level_builder_against_reference_nth_element(ref):
             got, _ = bvh_build(pb, pa, 1)
             for k in NODE_KEYS:
                 assert np.array_equal(got[k], want[k]), (n, trial, k)
+
+
+@pytest.mark.parametrize("kw", [dict(paths_per_pass=(1 << 30) + 1), dict(paths_per_pass=-1),
+                                dict(block_size=48), dict(block_size=1024),
+                                dict(stack_smem=-2)])
+def test_wavefront_config_rejected(lib, kw):
+    """prr_scene_set_wavefront refuses launch shapes it cannot run (a pass of
+    more than 2^30 paths would also overflow its path indices)."""
+    import photorealisticrender4610_b200 as prr
+    s = prr.Scene()
+    with pytest.raises(prr.PrrError, match="wavefront config"):
+        s.set_wavefront(**kw)
+    s.set_wavefront(paths_per_pass=1 << 30, block_size=128, stack_smem=8)
