@@ -426,7 +426,7 @@ def run_render(args, rank, world, on):
     if args.launch:
         cfg = parse_launch(args.launch)
         scene.set_wavefront(cfg.get("paths", 0), cfg.get("block_size", 0), True,
-                            cfg.get("stack", 0), cfg.get("ordered", 1))
+                            cfg.get("stack", 0), cfg.get("ordered", 1), cfg.get("refill", 0))
         tuned = cfg
     else:
         # tune on enough samples per pixel (a power of two, so the candidate

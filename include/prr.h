@@ -114,6 +114,8 @@ typedef struct prr_wavefront_config {
                                deeper entries spill to a global buffer (0: the whole stack) */
     int ordered;            /* 1: rebuild the stage queues in path order (stable partition,
                                next rays grouped by direction octant); 0: append order */
+    int refill;             /* traversal stages: a warp takes new rays from its queue once
+                               this many of its lanes are idle (0: 8; at most 32) */
 } prr_wavefront_config;
 
 typedef struct prr_scene_stats {

@@ -40,7 +40,7 @@ class prr_trace_config(C.Structure):
 
 class prr_wavefront_config(C.Structure):
     _fields_ = [("paths_per_pass", C.c_int64), ("block_size", C.c_int), ("use_graphs", C.c_int),
-                ("stack_smem", C.c_int), ("ordered", C.c_int)]
+                ("stack_smem", C.c_int), ("ordered", C.c_int), ("refill", C.c_int)]
 
 
 class prr_medium(C.Structure):

@@ -469,9 +469,9 @@ class Scene:
         return rs
 
     def set_wavefront(self, paths_per_pass: int = 0, block_size: int = 0, use_graphs: bool = True,
-                      stack_smem: int = 0, ordered: bool = True):
+                      stack_smem: int = 0, ordered: bool = True, refill: int = 0):
         cfg = prr_wavefront_config(paths_per_pass, block_size, int(use_graphs), stack_smem,
-                                   int(ordered))
+                                   int(ordered), refill)
         check(self.lib.prr_scene_set_wavefront(self.h, C.byref(cfg)))
 
     def autotune(self, spp: int, max_depth: int, window=None, seed: int = 1, stream=None) -> dict:

@@ -66,10 +66,10 @@ extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_con
         return fail(PRR_ERR_INVALID_ARGUMENT, "scene and config are required");
     if (config->paths_per_pass < 0 || config->paths_per_pass > (int64_t(1) << 30) ||
         config->block_size < 0 || config->block_size % 32 != 0 || config->block_size > 512 ||
-        config->stack_smem < 0)
+        config->stack_smem < 0 || config->refill < 0 || config->refill > 32)
         return fail(PRR_ERR_INVALID_ARGUMENT,
                     "bad wavefront config (paths_per_pass <= 2^30, block_size a multiple of "
-                    "32 up to 512, stack_smem >= 0)");
+                    "32 up to 512, stack_smem >= 0, refill 0..32)");
     Scene &s = *reinterpret_cast<Scene *>(scene);
     std::lock_guard<std::mutex> g(s.mu);
     s.wf_paths = config->paths_per_pass;
@@ -77,6 +77,7 @@ extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_con
     s.wf_graphs = config->use_graphs != 0;
     s.wf_stack = config->stack_smem;
     s.wf_ordered = config->ordered != 0;
+    s.wf_refill = config->refill;
     return PRR_OK;
 }
 
@@ -104,7 +105,7 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
                              int64_t(1) << 26};
     const int blocks[] = {64, 128, 256};
     float best_ms = 1e30f;
-    prr_wavefront_config best{0, 0, 1, 0, 1};
+    prr_wavefront_config best{0, 0, 1, 0, 1, 0};
     int rc = PRR_OK;
     std::lock_guard<std::mutex> g(s.mu);
     auto trial = [&](const prr_wavefront_config &c) {
@@ -113,6 +114,7 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
         s.wf_graphs = true;
         s.wf_stack = c.stack_smem;
         s.wf_ordered = c.ordered != 0;
+        s.wf_refill = c.refill;
         float ms_min = 1e30f;
         for (int rep = 0; rep < 2 && rc == PRR_OK; rep++) {
             cudaEventRecord(a, st);
@@ -142,18 +144,24 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
         last = pp;
         for (int bl : blocks)
             if (rc == PRR_OK)
-                trial(prr_wavefront_config{pp, bl, 1, stack1, 1});
+                trial(prr_wavefront_config{pp, bl, 1, stack1, 1, 0});
     }
     // stage 2: at that shape, other shared stack depths (0: the whole stack)
     const prr_wavefront_config shape = best;
     for (int sk : {0, 16, 4, 2})
         if (rc == PRR_OK && sk < s.dev.blas_depth + 1 && sk != stack1)
-            trial(prr_wavefront_config{shape.paths_per_pass, shape.block_size, 1, sk, 1});
+            trial(prr_wavefront_config{shape.paths_per_pass, shape.block_size, 1, sk, 1, 0});
     // stage 3: append-order queues
     const prr_wavefront_config shape2 = best;
     if (rc == PRR_OK)
         trial(prr_wavefront_config{shape2.paths_per_pass, shape2.block_size, 1,
-                                   shape2.stack_smem, 0});
+                                   shape2.stack_smem, 0, 0});
+    // stage 4: the refill threshold of the traversal stages
+    const prr_wavefront_config shape3 = best;
+    for (int rf : {4, 12, 16})
+        if (rc == PRR_OK)
+            trial(prr_wavefront_config{shape3.paths_per_pass, shape3.block_size, 1,
+                                       shape3.stack_smem, shape3.ordered, rf});
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     if (rc)
@@ -163,6 +171,7 @@ extern "C" int prr_autotune(prr_scene *scene, const prr_render_settings *setting
     s.wf_graphs = true;
     s.wf_stack = best.stack_smem;
     s.wf_ordered = best.ordered != 0;
+    s.wf_refill = best.refill;
     if (out_best)
         *out_best = best;
     return PRR_OK;

@@ -148,7 +148,7 @@ def test_scene_level_builder_against_reference_nth_element(ref):
 
 @pytest.mark.parametrize("kw", [dict(paths_per_pass=(1 << 30) + 1), dict(paths_per_pass=-1),
                                 dict(block_size=48), dict(block_size=1024),
-                                dict(stack_smem=-2)])
+                                dict(stack_smem=-2), dict(refill=33)])
 def test_wavefront_config_rejected(lib, kw):
     """prr_scene_set_wavefront refuses launch shapes it cannot run (a pass of
     more than 2^30 paths would also overflow its path indices)."""

@@ -72,11 +72,24 @@ def test_wavefront_stack_spill(cuda, stack, ordered):
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
 
 
+@pytest.mark.parametrize("refill", [1, 4, 32])
+def test_wavefront_refill_threshold(cuda, refill):
+    # how many idle lanes a traversal warp waits for before taking new rays
+    # changes only the schedule: the same film as the plain renderer
+    desc = scenes.museum_like(80, 48, level=4, env_size=(256, 128))
+    s = prr.Scene.from_desc(desc)
+    ref, _ = s.render(8, 8, seed=6, slices=1)
+    s.set_wavefront(paths_per_pass=80 * 48 * 4, block_size=128, stack_smem=8, refill=refill)
+    out, _ = s.render(8, 8, seed=6, mode="wavefront")
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
+
+
 def test_autotune_tries_queue_order_and_stack_depth(cuda):
     desc = scenes.museum_like(96, 64, level=3, env_size=(256, 128))
     s = prr.Scene.from_desc(desc)
     best = s.autotune(2, 8)
     assert best["ordered"] in (0, 1) and best["stack_smem"] in (0, 16, 8, 4, 2)
+    assert best["refill"] in (0, 4, 12, 16)
     a, _ = s.render(4, 8, mode="wavefront")
     b, _ = s.render(4, 8, slices=1)
     assert np.array_equal(a.cpu().numpy(), b.cpu().numpy())
