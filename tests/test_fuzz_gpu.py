@@ -88,3 +88,33 @@ def test_matches_reference(ref, cuda, seed):
     err = rel_mse(img.cpu().numpy(), rimg)
     print(f"random scene {seed}: rMSE vs reference {err:.3e}")
     assert err < REL_MSE_TOL
+
+
+def test_server_mix_of_random_scenes(cuda):
+    """All six scenes resident in one server, requests of mixed size, window,
+    depth and spp submitted together: every served image equals a render of
+    that request alone (wavefront steps share ray queues across scenes with
+    and without sky, lights and glass)."""
+    import dataclasses
+    descs = [random_scene(seed) for seed in SEEDS]
+    scene_objs = [prr.Scene.from_desc(d) for d in descs]
+    srv = prr.Server(paths_per_launch=1 << 16)
+    for s in scene_objs:
+        srv.add_scene(s)
+    rng = np.random.default_rng(5)
+    jobs = []
+    for k in range(14):
+        sc = int(rng.integers(0, len(SEEDS)))
+        W, H = [(48, 40), (64, 48), (32, 24)][int(rng.integers(0, 3))]
+        x0, y0 = int(rng.integers(0, W // 2)), int(rng.integers(0, H // 2))
+        win = (x0, y0, int(rng.integers(x0 + 1, W + 1)), int(rng.integers(y0 + 1, H + 1)))
+        spp, depth = int(rng.integers(1, 24)), int(rng.integers(1, 8))
+        rid = srv.submit(sc, spp, depth, seed=100 + k, window=win, size=(W, H))
+        jobs.append((rid, sc, W, H, win, spp, depth, 100 + k))
+    for rid, sc, W, H, win, spp, depth, seed in jobs:
+        assert srv.wait(rid)["status"] == "done"
+        alone = prr.Scene.from_desc(dataclasses.replace(descs[sc], width=W, height=H))
+        want, _ = alone.render(spp, depth, seed=seed, window=win, slices=1)
+        got = srv.result(rid)
+        assert np.array_equal(got.view(np.uint32), want.cpu().numpy().view(np.uint32)), rid
+    srv.close()
