@@ -569,6 +569,12 @@ def run_caustics(args, rank, world, on):
         torch.cuda.synchronize()
         return [ev[i].elapsed_time(ev[i + 1]) for i in range(3)], img
 
+    def api_step():
+        """The same step as a user makes it: emit, build, render."""
+        pm.emit(scene, n_ph, seed=1, max_depth=depth)
+        pm.build(radius)
+        return pm.render_caustics(scene, spp, max_depth=depth, seed=1, k_nearest=k)
+
     for _ in range(args.warmup):
         step()
     with ClockSampler(dev.index) as clk:
@@ -583,9 +589,10 @@ def run_caustics(args, rank, world, on):
     host = torch.empty((desc.height, desc.width, 3), dtype=torch.float32).pin_memory()
     e2e = []
     for _ in range(max(2, min(args.steps, 3))):
+        flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, img = step()
+        img = api_step()
         host.copy_(img)
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)

@@ -38,6 +38,8 @@ struct PhotonMap {
     DevBuf order;    // n int32: photon index, sorted by (cell, index)
     DevBuf cell_of;  // n int32: cell of order[i]
     DevBuf start;    // res^3 int32: first position in `order` of each cell, -1 if empty
+    DevBuf sorted;   // n x 2 float4 in `order`: position + power r, power g b (gathers
+                     // read a cell's photons contiguously)
     DevBuf params;   // device copy of the grid parameters
     DevBuf scratch;
 };
@@ -298,14 +300,18 @@ __global__ void k_cell_keys(const float *rec, int64_t n, const GridParams *g,
     keys[i] = ((unsigned long long) cell << 32) | (unsigned long long) i;
 }
 
-__global__ void k_cell_table(const unsigned long long *keys, int64_t n, int32_t *order,
-                             int32_t *cell_of, int32_t *start) {
+__global__ void k_cell_table(const unsigned long long *keys, const float *rec, int64_t n,
+                             int32_t *order, int32_t *cell_of, int32_t *start, float4 *sorted) {
     const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const unsigned cell = (unsigned) (keys[i] >> 32);
-    order[i] = (int32_t) (keys[i] & 0xffffffffu);
+    const int32_t o = (int32_t) (keys[i] & 0xffffffffu);
+    order[i] = o;
     cell_of[i] = (int32_t) cell;
+    const float *p = rec + (size_t) o * 9;
+    sorted[2 * i] = make_float4(p[0], p[1], p[2], p[6]);
+    sorted[2 * i + 1] = make_float4(p[7], p[8], 0.f, 0.f);
     if (i == 0 || (unsigned) (keys[i - 1] >> 32) != cell)
         start[cell] = (int32_t) i;
 }
@@ -313,6 +319,7 @@ __global__ void k_cell_table(const unsigned long long *keys, int64_t n, int32_t 
 // ---------------------------------------------------------------- gather
 struct GridView {
     const float *rec;
+    const float4 *sorted;
     const int32_t *order, *cell_of, *start;
     const GridParams *g;
     int64_t n;
@@ -339,6 +346,13 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     z1 = min(g.res - 1, z1);
     V3 e = v3(0.f);
     int found = 0;
+    int worst = 0; // kNN: the first index of the largest kept distance, once k are kept
+    auto find_worst = [&] {
+        worst = 0;
+        for (int q = 1; q < k_nearest; q++)
+            if (kd[q] > kd[worst])
+                worst = q;
+    };
     for (int cx = x0; cx <= x1; cx++)
         for (int cy = y0; cy <= y1; cy++)
             for (int cz = z0; cz <= z1; cz++) {
@@ -346,25 +360,24 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
                 int s = v.start[cell];
                 if (s < 0)
                     continue;
+                // the cell's photons, in photon order, read from the cell-sorted copy
                 for (; s < v.n && v.cell_of[s] == cell; s++) {
-                    const float *p = v.rec + (size_t) v.order[s] * 9;
-                    const V3 d = v3(p[0], p[1], p[2]) - pos;
+                    const float4 pa = v.sorted[2 * s];
+                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
                     const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
                     if (dist <= r) {
-                        e = e + v3(p[6], p[7], p[8]);
+                        const float4 pb = v.sorted[2 * s + 1];
+                        e = e + v3(pa.w, pb.x, pb.y);
                         if (kd && found < k_nearest) {
                             kd[found] = dist;
                             kc[found] = v.order[s];
-                        } else if (kd) {
+                            if (found + 1 == k_nearest)
+                                find_worst();
+                        } else if (kd && dist < kd[worst]) {
                             // keep the k smallest distances (replace the largest)
-                            int worst = 0;
-                            for (int q = 1; q < k_nearest; q++)
-                                if (kd[q] > kd[worst])
-                                    worst = q;
-                            if (dist < kd[worst]) {
-                                kd[worst] = dist;
-                                kc[worst] = v.order[s];
-                            }
+                            kd[worst] = dist;
+                            kc[worst] = v.order[s];
+                            find_worst();
                         }
                         found++;
                     }
@@ -478,6 +491,7 @@ const PhotonMap *PM(const prr_photon_map *p) { return reinterpret_cast<const Pho
 GridView view(const PhotonMap &pm) {
     GridView v;
     v.rec = pm.rec.as<float>();
+    v.sorted = pm.sorted.as<float4>();
     v.order = pm.order.as<int32_t>();
     v.cell_of = pm.cell_of.as<int32_t>();
     v.start = pm.start.as<int32_t>();
@@ -619,8 +633,10 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     PRR_CUDA_TRY(pm.cell_of.ensure((size_t) n * sizeof(int32_t)));
     PRR_CUDA_TRY(pm.start.ensure(cells * sizeof(int32_t)));
     PRR_CUDA_TRY(cudaMemsetAsync(pm.start.ptr, 0xff, cells * sizeof(int32_t), st));
+    PRR_CUDA_TRY(pm.sorted.ensure((size_t) n * 2 * sizeof(float4)));
     k_cell_table<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
-        keys, n, pm.order.as<int32_t>(), pm.cell_of.as<int32_t>(), pm.start.as<int32_t>());
+        keys, pm.rec.as<float>(), n, pm.order.as<int32_t>(), pm.cell_of.as<int32_t>(),
+        pm.start.as<int32_t>(), pm.sorted.as<float4>());
     PRR_CUDA_TRY(cudaGetLastError());
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     pm.res = g.res;
