@@ -435,27 +435,35 @@ struct CausticArgs {
     uint64_t seed;
     int sample_offset;
     float *out;
+    float4 *samples; // npix x spp contributions, sample-major
 };
 
-__global__ void k_render_caustics(DevScene S, GridView v, CausticArgs a) {
+// One thread per (pixel, sample): sample n of window pixel q is item
+// n * npix + q, so neighbouring threads trace neighbouring pixels and the
+// uneven cost of gathers in and out of the caustics spreads over the grid.
+__global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     extern __shared__ uint2 smem[];
     SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
     SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= a.ww * a.wh)
-        return;
-    const int i = a.x0 + q % a.ww, j = a.y0 + q / a.ww;
-    const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) a.W;
+    const int64_t npix = (int64_t) a.ww * a.wh;
+    const int64_t total = npix * a.spp;
     float kd[kMaxK];
     int kc[kMaxK];
-    V3 acc = v3(0.f);
-    for (int n = 0; n < a.spp; n++) {
+    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t) gridDim.x * blockDim.x) {
+        const int n = (int) (t / npix);
+        const int q = (int) (t - (int64_t) n * npix);
+        const int i = a.x0 + q % a.ww, j = a.y0 + q / a.ww;
+        const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) a.W;
         Rng rng{path_state(a.seed, m, (uint32_t) (a.sample_offset + n))};
         const float xo = rng.next();
         const float yo = rng.next();
         Ray3 ray = generate_ray(S.camera, i, j, xo, yo, rng);
         V3 beta = v3(1.f);
+        V3 c = v3(0.f);
         for (int d = 0; d < a.max_depth; d++) {
+            tst.sp = 0;
+            bst.sp = 0;
             const Inter in = intersect(S, ray, tst, bst);
             if (!in.hit)
                 break;
@@ -476,13 +484,29 @@ __global__ void k_render_caustics(DevScene S, GridView v, CausticArgs a) {
             const V3 albedo = mt.tex_base >= 0
                                   ? sample_base_color(S.textures[mt.tex_base], in.a.u, in.a.v)
                                   : v3(mt.base[0], mt.base[1], mt.base[2]);
-            acc = acc + beta * (albedo / PRR_PI) * e;
+            c = beta * (albedo / PRR_PI) * e;
             break;
         }
+        a.samples[t] = make_float4(c.x, c.y, c.z, 0.f);
     }
-    a.out[(size_t) q * 3] = acc.x / (float) a.spp;
-    a.out[(size_t) q * 3 + 1] = acc.y / (float) a.spp;
-    a.out[(size_t) q * 3 + 2] = acc.z / (float) a.spp;
+}
+
+// The pixel's mean: its samples added in sample order (a sample without a
+// diffuse hit adds zero, which leaves the non-negative sum unchanged), so the
+// image is the one a per-pixel loop over its samples produces.
+__global__ void k_caustic_film(CausticArgs a) {
+    const int64_t npix = (int64_t) a.ww * a.wh;
+    const int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= npix)
+        return;
+    V3 acc = v3(0.f);
+    for (int n = 0; n < a.spp; n++) {
+        const float4 c = a.samples[(int64_t) n * npix + q];
+        acc = acc + v3(c.x, c.y, c.z);
+    }
+    a.out[q * 3] = acc.x / (float) a.spp;
+    a.out[q * 3 + 1] = acc.y / (float) a.spp;
+    a.out[q * 3 + 2] = acc.z / (float) a.spp;
 }
 
 PhotonMap *PM(prr_photon_map *p) { return reinterpret_cast<PhotonMap *>(p); }
@@ -726,12 +750,27 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
     if (smem > 200 * 1024)
         return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
     if (smem > 48 * 1024)
-        PRR_CUDA_TRY(cudaFuncSetAttribute(k_render_caustics,
+        PRR_CUDA_TRY(cudaFuncSetAttribute(k_caustic_samples,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    const int npix = a.ww * a.wh;
-    k_render_caustics<<<(npix + block - 1) / block, block, smem, (cudaStream_t) stream>>>(
-        s.dev, view(pm), a);
-    PRR_CUDA_TRY(cudaGetLastError());
+    const int64_t npix = (int64_t) a.ww * a.wh;
+    const int64_t total = npix * a.spp;
+    cudaStream_t st = (cudaStream_t) stream;
+    // per-call contributions from the stream-ordered pool: concurrent calls
+    // on other streams get their own
+    PRR_CUDA_TRY(cudaMallocAsync((void **) &a.samples, (size_t) total * sizeof(float4), st));
+    int bps = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_caustic_samples, block, smem);
+    const int64_t grid = std::min<int64_t>((total + block - 1) / block,
+                                           (int64_t) device_sm_count() * std::max(1, bps) * 8);
+    k_caustic_samples<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(a.samples, st);
+    if (e != cudaSuccess)
+        return fail(PRR_ERR_CUDA, std::string("caustic render: ") + cudaGetErrorString(e));
     return PRR_OK;
 }
 

@@ -95,3 +95,18 @@ def test_caustic_render(cuda):
     assert np.isfinite(img).all() and img.max() > 0
     img64 = pm.render_caustics(s, 4, k_nearest=64).cpu().numpy()
     assert np.isfinite(img64).all()
+
+
+def test_caustic_render_regression_fixture(cuda):
+    """The caustic render's images at fixed seeds, bit for bit against the
+    fixture written by tests/golden/make_caustics_fixture.py: every pixel is
+    the sum of its samples in sample order, however the work is scheduled."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+    import make_caustics_fixture as F
+    want = np.load(Path(__file__).resolve().parent / "golden" / "caustics_render.npz")
+    got = F.render_cases()
+    assert got["photons"][0] == want["photons"][0]
+    for name, _, _, _ in F.CASES:
+        assert np.array_equal(got[name].view(np.uint32), want[name].view(np.uint32)), name
