@@ -312,7 +312,10 @@ int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n,
                       float *out_rgb, void *stream);
 /* Caustic image: for every (pixel, sample) the camera ray follows the specular
  * chain (Integrator.cpp:143-169) to its first diffuse hit x, which returns
- * beta * baseColor/pi * E(x) from the photon map. out_rgb = window x 3. */
+ * beta * baseColor/pi * E(x) from the photon map. out_rgb = window x 3, each
+ * pixel the mean of its samples summed in sample order. Per call, 16 bytes per
+ * (pixel, sample) of scratch come from the stream-ordered allocator of
+ * `stream` and go back to it when the call's work is done. */
 int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream);
