@@ -314,7 +314,9 @@ int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n,
  * chain (Integrator.cpp:143-169) to its first diffuse hit x, which returns
  * beta * baseColor/pi * E(x) from the photon map. out_rgb = window x 3, each
  * pixel the mean of its samples summed in sample order. Per call, 16 bytes per
- * (pixel, sample) of scratch come from the stream-ordered allocator of
+ * (pixel, sample), at most 4 GiB (larger renders run in chunks of whole
+ * samples per pixel), come from a stream-ordered memory pool of the library
+ * (one per device; it keeps up to 4 GiB of freed blocks for later calls) on
  * `stream` and go back to it when the call's work is done. */
 int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,

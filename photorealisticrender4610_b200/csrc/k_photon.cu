@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 namespace prr {
 
@@ -435,7 +437,9 @@ struct CausticArgs {
     uint64_t seed;
     int sample_offset;
     float *out;
-    float4 *samples; // npix x spp contributions, sample-major
+    float4 *samples; // npix x chunk contributions, sample-major
+    float4 *acc;     // npix running sums across chunks
+    int s0, chunk;   // this launch's samples [s0, s0 + chunk) of each pixel
 };
 
 // One thread per (pixel, sample): sample n of window pixel q is item
@@ -446,13 +450,14 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
     SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
     const int64_t npix = (int64_t) a.ww * a.wh;
-    const int64_t total = npix * a.spp;
+    const int64_t total = npix * a.chunk;
     float kd[kMaxK];
     int kc[kMaxK];
     for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t) gridDim.x * blockDim.x) {
-        const int n = (int) (t / npix);
-        const int q = (int) (t - (int64_t) n * npix);
+        const int nc = (int) (t / npix);
+        const int q = (int) (t - (int64_t) nc * npix);
+        const int n = a.s0 + nc;
         const int i = a.x0 + q % a.ww, j = a.y0 + q / a.ww;
         const uint32_t m = (uint32_t) i + (uint32_t) j * (uint32_t) a.W;
         Rng rng{path_state(a.seed, m, (uint32_t) (a.sample_offset + n))};
@@ -491,22 +496,66 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     }
 }
 
-// The pixel's mean: its samples added in sample order (a sample without a
-// diffuse hit adds zero, which leaves the non-negative sum unchanged), so the
-// image is the one a per-pixel loop over its samples produces.
+// The pixel's sum: the chunk's samples added in sample order to the sums of
+// the chunks before (a sample without a diffuse hit adds zero, which leaves
+// the non-negative sum unchanged), so the image is the one a per-pixel loop
+// over its samples produces; the last chunk writes the mean.
 __global__ void k_caustic_film(CausticArgs a) {
     const int64_t npix = (int64_t) a.ww * a.wh;
     const int64_t q = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= npix)
         return;
     V3 acc = v3(0.f);
-    for (int n = 0; n < a.spp; n++) {
+    if (a.s0 > 0) {
+        const float4 p = a.acc[q];
+        acc = v3(p.x, p.y, p.z);
+    }
+    for (int n = 0; n < a.chunk; n++) {
         const float4 c = a.samples[(int64_t) n * npix + q];
         acc = acc + v3(c.x, c.y, c.z);
+    }
+    if (a.s0 + a.chunk < a.spp) {
+        a.acc[q] = make_float4(acc.x, acc.y, acc.z, 0.f);
+        return;
     }
     a.out[q * 3] = acc.x / (float) a.spp;
     a.out[q * 3 + 1] = acc.y / (float) a.spp;
     a.out[q * 3 + 2] = acc.z / (float) a.spp;
+}
+
+// Contributions held at once per call (16 bytes each): larger renders run in
+// chunks of whole samples per pixel.
+constexpr int64_t kCausticItems = int64_t(1) << 28;
+
+// The library's stream-ordered memory pool of a device: freed blocks stay in
+// it (up to a 4 GiB release threshold) for the next calls instead of going
+// back to the driver at every synchronisation, as the device's default pool
+// would do. Created on first use, one per device.
+cudaError_t library_pool(cudaMemPool_t *out) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return e;
+    std::lock_guard<std::mutex> g(mu);
+    if ((int) pools.size() <= dev)
+        pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        e = cudaMemPoolCreate(&p, &props);
+        if (e != cudaSuccess)
+            return e;
+        uint64_t keep = uint64_t(4) << 30;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
 }
 
 PhotonMap *PM(prr_photon_map *p) { return reinterpret_cast<PhotonMap *>(p); }
@@ -753,22 +802,38 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
         PRR_CUDA_TRY(cudaFuncSetAttribute(k_caustic_samples,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     const int64_t npix = (int64_t) a.ww * a.wh;
-    const int64_t total = npix * a.spp;
+    const int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(a.spp, kCausticItems / npix));
+    const int64_t items = npix * chunk;
     cudaStream_t st = (cudaStream_t) stream;
-    // per-call contributions from the stream-ordered pool: concurrent calls
-    // on other streams get their own
-    PRR_CUDA_TRY(cudaMallocAsync((void **) &a.samples, (size_t) total * sizeof(float4), st));
+    // per-call contributions (and, when chunked, running sums) from the
+    // library's stream-ordered pool: concurrent calls on other streams get
+    // their own
+    char *scratch = nullptr;
+    const size_t acc_bytes = chunk < a.spp ? (size_t) npix * sizeof(float4) : 0;
+    cudaMemPool_t pool;
+    PRR_CUDA_TRY(library_pool(&pool));
+    PRR_CUDA_TRY(cudaMallocFromPoolAsync((void **) &scratch,
+                                         (size_t) items * sizeof(float4) + acc_bytes, pool, st));
+    a.samples = reinterpret_cast<float4 *>(scratch);
+    a.acc = acc_bytes ? reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4))
+                      : nullptr;
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_caustic_samples, block, smem);
-    const int64_t grid = std::min<int64_t>((total + block - 1) / block,
-                                           (int64_t) device_sm_count() * std::max(1, bps) * 8);
-    k_caustic_samples<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) {
-        k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
+    cudaError_t e = cudaSuccess;
+    for (int s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
+        a.s0 = s0;
+        a.chunk = std::min(chunk, a.spp - s0);
+        const int64_t total = npix * a.chunk;
+        const int64_t grid = std::min<int64_t>(
+            (total + block - 1) / block, (int64_t) device_sm_count() * std::max(1, bps) * 8);
+        k_caustic_samples<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
         e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
+            e = cudaGetLastError();
+        }
     }
-    cudaFreeAsync(a.samples, st);
+    cudaFreeAsync(scratch, st);
     if (e != cudaSuccess)
         return fail(PRR_ERR_CUDA, std::string("caustic render: ") + cudaGetErrorString(e));
     return PRR_OK;

@@ -110,3 +110,17 @@ def test_caustic_render_regression_fixture(cuda):
     assert got["photons"][0] == want["photons"][0]
     for name, _, _, _ in F.CASES:
         assert np.array_equal(got[name].view(np.uint32), want[name].view(np.uint32)), name
+
+
+def test_caustic_render_in_chunks(cuda):
+    """A render of more (pixel, sample) contributions than one call holds at
+    once (1024 x 1024 x 520 > 2^28) runs in chunks of whole samples; its
+    pixels equal those of a window small enough for one chunk."""
+    desc = scenes.caustics(1024, 1024, level=2)
+    s = prr.Scene.from_desc(desc)
+    pm = prr.PhotonMap().emit(s, 100_000, seed=2).build(0.05)
+    full = pm.render_caustics(s, 520, max_depth=8, seed=4, k_nearest=16).cpu().numpy()
+    part = pm.render_caustics(s, 520, max_depth=8, seed=4, k_nearest=16,
+                              window=(300, 400, 700, 460)).cpu().numpy()
+    assert part.max() > 0
+    assert np.array_equal(full[400:460, 300:700].view(np.uint32), part.view(np.uint32))
