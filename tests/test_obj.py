@@ -115,3 +115,22 @@ def test_name_and_missing_file(tmp_path):
         prr.read_obj(p)
     with pytest.raises(prr.PrrError, match="cannot open"):
         prr.read_obj(tmp_path / "missing.obj")
+
+
+def test_c_abi_capacity_and_null_offset(tmp_path):
+    """prr_obj_read through the C ABI: the count query, a too-small output
+    (rejected) and a NULL offset (no shift)."""
+    import ctypes as C
+    from photorealisticrender4610_b200 import _lib
+    lib = _lib.load()
+    p = write(tmp_path, "tri.obj", "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 3\nf 2 4 3\n")
+    n = C.c_int64()
+    assert lib.prr_obj_read(str(p).encode(), None, None, 0, C.byref(n)) == 0
+    assert n.value == 2
+    out = np.zeros((2, 9), np.float32)
+    assert lib.prr_obj_read(str(p).encode(), None, C.c_void_p(out.ctypes.data), 1,
+                            C.byref(n)) < 0
+    assert lib.prr_obj_read(str(p).encode(), None, C.c_void_p(out.ctypes.data), 2,
+                            C.byref(n)) == 0
+    assert np.array_equal(out, np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0],
+                                         [1, 0, 0, 1, 1, 0, 0, 1, 0]], np.float32))
