@@ -219,12 +219,19 @@ def cpu_reference_rate(verts, o, d, n_sample, threads):
     return n_sample / (time.perf_counter() - t0) / 1e6, kind
 
 
+def query_config(world):
+    """The query-set workload as both arms name it."""
+    return {"workload": WORKLOAD, "rays_per_step": N_RAYS, "triangles": N_TRIS, "seed": 1,
+            "l2": "GPU arm: L2 flushed (512 MB write) before every timed step",
+            "parallelism": f"replica x{world}" if world > 1 else "1 GPU"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     verts, o, d = workload_arrays()
-    sample = min(N_RAYS, 1 << 20)
+    sample = N_RAYS
     for _ in range(args.warmup):
         cpu_reference_rate(verts, o, d, 1 << 16, threads)
     rates = []
@@ -240,9 +247,11 @@ def run_reference(args, rank, world):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total / max(1, args.steps) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_step": sample, "threads": threads},
+        "config": query_config(world),
+        "threads": threads,
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": threads, "kind": kind,
-                         "sample": f"{sample} of the {N_RAYS} query rays per step"},
+                         "sample": f"all {N_RAYS} query rays per step (the BVH built once, "
+                                   "untimed)"},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -338,7 +347,7 @@ def run_ours(args, rank, world, on):
     t_h = torch.empty(N_RAYS, dtype=torch.float32).pin_memory().numpy()
     scene.mesh_intersect_host(0, ho, hd, hid_h, t_h, config=best)
     e2e_ms = []
-    for _ in range(max(3, min(args.steps, 10))):
+    for _ in range(max(3, args.steps)):
         barrier(on)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -364,10 +373,9 @@ def run_ours(args, rank, world, on):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_step": N_RAYS, "triangles": N_TRIS,
-                   "seed": 1, "l2": "flushed (512 MB write) before every timed step",
-                   "launch": best, "parallelism": f"replica x{world}" if world > 1 else "1 GPU",
-                   "step_ms": [round(x, 3) for x in kernel_ms], "median_ms": ms_median},
+        "config": query_config(world),
+        "run": {"launch": best, "step_ms": [round(x, 3) for x in kernel_ms],
+                "median_ms": ms_median, "e2e_ms": [round(x, 3) for x in e2e_ms]},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 24,
                 "d2h_bytes_per_step": N_RAYS * 8},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -380,10 +388,30 @@ def run_ours(args, rank, world, on):
         "bvh_build_s": {"ours": build_s, "ours_threads": threads,
                         "reference": _CPU_MESH.get("build_s"), "reference_threads": 1},
         "clocks": clocks,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (6 if best.get("sort_rays") else 1),
     }
+    if world == 1 and args.extras != "none":
+        # the other north-star targets on the same box, as keys of this line
+        for name in args.extras.split(","):
+            t0 = time.perf_counter()
+            if name == "museum":
+                sub = render_result(args, rank, world, on, "museum", min(args.steps, 5), 3,
+                                    crop_check=True)
+            elif name == "caustics":
+                sub = caustics_result(args, rank, world, on, min(args.steps, 5), 3)
+            elif name == "serving":
+                sub = serving_result(args, rank, n_requests=60, arms_text="none")
+            else:
+                raise ValueError(f"unknown extra workload {name}")
+            sub = {k: v for k, v in sub.items() if k not in EXTRA_DROP}
+            sub["bench_s"] = time.perf_counter() - t0
+            line[name] = sub
     print(json.dumps(line), flush=True)
     return 0
+
+
+# keys of a workload's own line that its entry under the headline line leaves out
+EXTRA_DROP = ("n_gpus", "higher_is_better", "scaling", "vs_baseline", "dtype", "data")
 
 
 def _scenes():
@@ -405,13 +433,46 @@ RENDER_WORKLOADS = {
 }
 
 
+# Algorithmic bytes of a wavefront frame, per unit of work counted by
+# prr_render_counts: a closest-hit ray reads its origin and direction (24 B)
+# and writes its hit record (16 B); a shadow ray reads origin, direction and
+# tmax (28 B) and writes its visibility byte; each interior node visited reads
+# the two child boxes of one 64 B node, each triangle test the 36 B of v0, e1,
+# e2, each object leaf 16 B (sphere centre and radius, or a mesh's root). The
+# shading stages read and write per path-bounce the path state they need: a
+# surface hit 132 B (hit record, ray, throughput, radiance, RNG state, flags
+# in; next ray, throughput, radiance, RNG state out), a mirror/glass hit 104 B,
+# a miss 60 B; the film adds 12 B per pixel.
+FRAME_BYTES = {"closest_ray": 40, "shadow_ray": 29, "node": 64, "tri": 36, "object": 16,
+               "surface": 132, "delta": 104, "miss": 60, "pixel": 12}
+
+
+def frame_bytes(c, npix):
+    B = FRAME_BYTES
+    return (c["closest_rays"] * B["closest_ray"] + c["shadow_rays"] * B["shadow_ray"] +
+            (c["closest_nodes"] + c["shadow_nodes"]) * B["node"] +
+            (c["closest_tris"] + c["shadow_tris"]) * B["tri"] +
+            (c["closest_objects"] + c["shadow_objects"]) * B["object"] +
+            c["surface_hits"] * B["surface"] + c["delta_hits"] * B["delta"] +
+            c["misses"] * B["miss"] + npix * B["pixel"])
+
+
 def run_render(args, rank, world, on):
+    line = render_result(args, rank, world, on, args.workload, args.steps, args.warmup)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def render_result(args, rank, world, on, workload, steps, warmup, crop_check=False):
     """Samples/s of the plain megakernel and of the wavefront integrator on a
-    full frame (value = wavefront, the faster one; both reported)."""
+    full frame (value = wavefront, the faster one; both reported). Returns the
+    JSON line's dict on rank 0 (None elsewhere). crop_check adds the rMSE of a
+    32x32 crop at 4096 spp against the reference renderer."""
     import torch
     import photorealisticrender4610_b200 as prr
 
-    factory, spp, depth, desc_text, adaptive = RENDER_WORKLOADS[args.workload]
+    factory, spp, depth, desc_text, adaptive = RENDER_WORKLOADS[workload]
     min_spp, thr = adaptive if adaptive else (None, 0.05)
     dev = torch.device("cuda", torch.cuda.current_device())
     desc = factory()
@@ -457,21 +518,21 @@ def run_render(args, rank, world, on):
 
     if not args.kernel_only:
         timed("plain", 1)
-    timed("wavefront", args.warmup)
+    timed("wavefront", warmup)
     with ClockSampler(dev.index) as clk:
         barrier(on)
-        wf_ms, wf_img, wf_rays = timed("wavefront", args.steps)
+        wf_ms, wf_img, wf_rays = timed("wavefront", steps)
         barrier(on)
-    wf_launches = scene.stats()["last_render_launches"] * args.steps
+    wf_launches = scene.stats()["last_render_launches"] * steps
     if args.kernel_only:
         if rank == 0:
             print(json.dumps({"frame_ms": wf_ms,
                               "msamples_s": timed.samples / np.mean(wf_ms) / 1e3,
                               "launch": tuned}))
-        return 0
+        return None
     samples = timed.samples
     timed("plain", 1)
-    pl_ms, pl_img, pl_rays = timed("plain", max(1, min(args.steps, 3)))
+    pl_ms, pl_img, pl_rays = timed("plain", max(1, min(steps, 3)))
     wf_step = max_over_ranks(float(np.mean(wf_ms)), on)
     # the plain renderer is the comparison, not the headline: its median frame,
     # so one host stall longer than the queued busy-wait does not set the ratio
@@ -484,7 +545,7 @@ def run_render(args, rank, world, on):
     # end to end: the C ABI call plus the copy of the image to pinned host memory
     host = torch.empty((desc.height, desc.width, 3), dtype=torch.float32).pin_memory()
     e2e = []
-    for _ in range(max(2, min(args.steps, 3))):
+    for _ in range(max(3, steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         img, _ = scene.render(spp, depth, seed=1, mode="wavefront", min_spp=min_spp,
@@ -493,8 +554,38 @@ def run_render(args, rank, world, on):
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
     e2e_value = samples * world / (float(np.median(e2e)) * 1e-3) / 1e6
+    # the frame's work, counted by a separate (untimed) counting render
+    _, counts = scene.render_counts(spp, depth, seed=1, min_spp=min_spp, threshold=thr)
     if rank != 0:
-        return 0
+        return None
+    peak, peak_kind = measured_peaks()
+    alg = frame_bytes(counts, npix)
+    achieved = alg / (wf_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "basis": "algorithmic bytes of the whole wavefront frame (traversal steps "
+                         "and hit classes counted by prr_render_counts, bytes per unit in "
+                         "bench.FRAME_BYTES) / frame time",
+                "bytes_per_frame": alg, "bytes_per_unit": FRAME_BYTES,
+                "counts": counts,
+                "nodes_per_closest_ray": counts["closest_nodes"] / max(1, counts["closest_rays"]),
+                "tris_per_closest_ray": counts["closest_tris"] / max(1, counts["closest_rays"]),
+                "nodes_per_shadow_ray": counts["shadow_nodes"] / max(1, counts["shadow_rays"]),
+                "tris_per_shadow_ray": counts["shadow_tris"] / max(1, counts["shadow_rays"])}
+    crop = None
+    if crop_check:
+        from oracle import loader
+        if loader.reference_available():
+            win = (desc.width // 2 - 16, desc.height // 2 - 16, desc.width // 2 + 16,
+                   desc.height // 2 + 16)
+            gimg, _ = scene.render(4096, depth, seed=1, mode="wavefront", window=win)
+            rimg, _ = loader.ReferenceOracle().scene(desc).render(depth, 4096, 1, window=win)
+            g64 = gimg.cpu().numpy().astype(np.float64)
+            crop = {"window": list(win), "spp": 4096,
+                    "rel_mse": float(((g64 - rimg) ** 2).sum() / max((rimg.astype(np.float64) ** 2).sum(), 1e-30)),
+                    "against": "the reference renderer (its sources compiled in place, IEEE "
+                               "flags) on the same per-sample RNG streams"}
     threads = os.cpu_count() or 1
     cpu = None
     from oracle import loader
@@ -513,7 +604,7 @@ def run_render(args, rank, world, on):
                "sample": f"64x64 centre crop at {cspp} spp" + (" (adaptive)" if adaptive else "")}
     line = {
         "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": wf_step,
+        "steps": steps, "warmup": warmup, "ms_per_step": wf_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": desc_text, "mode": "wavefront", "autotuned": tuned,
@@ -526,13 +617,13 @@ def run_render(args, rank, world, on):
         "rays_per_frame": {"closest": int(rays[0]), "shadow": int(rays[1])},
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": npix * 12},
-        "roofline": None,
+        "roofline": roofline,
+        "crop_check": crop,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": wf_launches,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 CAUSTICS = ("caustics: glass sphere (r=1, IOR 1.5) over a diffuse plane, light of intensity 100 "
@@ -540,9 +631,25 @@ CAUSTICS = ("caustics: glass sphere (r=1, IOR 1.5) over a diffuse plane, light o
             "camera hit; 1024x1024, 32 spp, depth 8")
 
 
+# Algorithmic bytes of the caustic render kernel (the step's dominant one), per
+# unit counted by prr_render_caustics_counts: each (pixel, sample) writes its
+# 16 B contribution and the film stage reads it back; each photon a gather's
+# cell walk tests reads 16 B of the cell-sorted copy (position, power r), each
+# one inside the radius 16 B more (power g, b); the image is 12 B per pixel.
+CAUSTIC_BYTES = {"sample": 32, "photon_tested": 16, "photon_inside": 16, "pixel": 12}
+
+
 def run_caustics(args, rank, world, on):
+    line = caustics_result(args, rank, world, on, args.steps, args.warmup)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def caustics_result(args, rank, world, on, steps, warmup):
     """One step = trace 2M photons + build the photon grid + render the frame
-    with the caustic gather. value = camera samples/s of the whole step."""
+    with the caustic gather. value = camera samples/s of the whole step.
+    Returns the JSON line's dict on rank 0 (None elsewhere)."""
     import torch
     import photorealisticrender4610_b200 as prr
     from photorealisticrender4610_b200 import scenes
@@ -575,11 +682,11 @@ def run_caustics(args, rank, world, on):
         pm.build(radius)
         return pm.render_caustics(scene, spp, max_depth=depth, seed=1, k_nearest=k)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     with ClockSampler(dev.index) as clk:
         barrier(on)
-        phases = [step()[0] for _ in range(args.steps)]
+        phases = [step()[0] for _ in range(steps)]
         barrier(on)
     ph = np.array(phases)
     step_ms = max_over_ranks(float(ph.sum(1).mean()), on)
@@ -588,7 +695,7 @@ def run_caustics(args, rank, world, on):
     # end to end: the same step through the API plus the image copied to pinned host memory
     host = torch.empty((desc.height, desc.width, 3), dtype=torch.float32).pin_memory()
     e2e = []
-    for _ in range(max(2, min(args.steps, 3))):
+    for _ in range(max(3, steps)):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -597,8 +704,24 @@ def run_caustics(args, rank, world, on):
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
     e2e_value = npix * spp * world / (float(np.median(e2e)) * 1e-3) / 1e6
+    # the render's gather work, counted by a separate (untimed) counting render
+    _, counts = pm.render_caustics_counts(scene, spp, max_depth=depth, seed=1, k_nearest=k)
     if rank != 0:
-        return 0
+        return None
+    render_ms = float(ph[:, 2].mean())
+    B = CAUSTIC_BYTES
+    alg = (npix * spp * B["sample"] + counts["photons_tested"] * B["photon_tested"] +
+           counts["photons_inside"] * B["photon_inside"] + npix * B["pixel"])
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (render_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": profiled_traffic("k_caustic_samples"),
+                "peak_source": f"{peak_kind} hbm_gbs", "kernel": "k_caustic_samples + k_caustic_film",
+                "basis": "algorithmic bytes of the render + gather (gather work counted by "
+                         "prr_render_caustics_counts, bytes per unit in bench.CAUSTIC_BYTES) / "
+                         "its CUDA-event time",
+                "bytes_per_render": alg, "bytes_per_unit": CAUSTIC_BYTES, "counts": counts,
+                "photons_tested_per_gather": counts["photons_tested"] / max(1, counts["gathers"])}
     cpu = None
     from oracle import loader
     if loader.reference_available(fast=True):
@@ -612,7 +735,7 @@ def run_caustics(args, rank, world, on):
                "kind": "reference", "sample": f"{n_cpu} photons traced by Photon.cpp's trace"}
     line = {
         "metric": "Msamples/s", "value": value, "unit": "Msamples/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "steps": steps, "warmup": warmup, "ms_per_step": step_ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": CAUSTICS, "photons_stored": stored, "grid_res": grid_res,
@@ -622,13 +745,12 @@ def run_caustics(args, rank, world, on):
         "mphotons_s": n_ph / (float(ph[:, 0].mean()) * 1e-3) / 1e6,
         "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": npix * 12},
-        "roofline": None,
+        "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
         "gpu_launches": None,
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def serving_pool():
@@ -653,22 +775,30 @@ def serving_pool():
 
 
 def run_serving(args, rank, world, on):
+    line = serving_result(args, rank)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def serving_result(args, rank, n_requests=None, arms_text=None):
     """Continuous-batching server (wavefront steps) under Poisson arrivals,
     beside the same server on megakernel steps and the plain renderer run one
-    request at a time in arrival order."""
+    request at a time in arrival order. Returns the JSON line's dict on rank 0
+    (None elsewhere)."""
     import math
     import threading
     import torch
     import photorealisticrender4610_b200 as prr
 
     if rank != 0:
-        return 0
+        return None
     rng = np.random.Generator(np.random.PCG64(7))
     pool = serving_pool()
     scenes_ = [prr.Scene.from_desc(d) for d in pool]
     tris = [d.n_triangles() for d in pool]
     sizes = [(256, 256), (512, 512), (1024, 1024), (1920, 1080)]
-    n = args.requests
+    n = n_requests or args.requests
     gaps = rng.exponential(1.0 / args.rate, n)
     arrive = np.cumsum(gaps) - gaps[0]
     reqs = []
@@ -717,7 +847,7 @@ def run_serving(args, rank, world, on):
         lat, span, st = serve(args.max_active, 1 << 20)
     served_rate = total_samples / span / 1e6
     busy_rate = total_samples / st["busy_s"] / 1e6
-    arms = set(args.serving_arms.split(","))
+    arms = set((arms_text or args.serving_arms).split(","))
     if "all" in arms:
         arms = {"megakernel", "one", "sustainable"}
 
@@ -759,8 +889,7 @@ def run_serving(args, rank, world, on):
                 "d2h_bytes_per_step": int(np.mean([w * h * 12 for _, (w, h), _ in reqs]))},
         "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def main():
@@ -784,6 +913,9 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="render workloads: spp override")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the kernel only (no e2e, no CPU baseline): profiling runs")
+    ap.add_argument("--extras", default="museum,caustics,serving",
+                    help="query workload at 1 GPU: other workloads measured after the headline "
+                         "and added as keys of its line (comma list, or 'none')")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()

@@ -34,7 +34,7 @@ extern "C" {
 #define PRR_OK 0
 #define PRR_ERR_INVALID_ARGUMENT (-1)
 #define PRR_ERR_CUDA (-2)
-#define PRR_ERR_OUT_OF_MEMORY (-3)
+#define PRR_ERR_OUT_OF_MEMORY (-3) /* a device (or pinned host) allocation failed */
 #define PRR_ERR_NOT_BUILT (-4)
 #define PRR_ERR_UNSUPPORTED (-5)
 #define PRR_ERR_TIMEOUT (-6)
@@ -84,6 +84,13 @@ typedef struct prr_trace_config {
     int batch;        /* modes 2-3: refill threshold in idle lanes (0 = 8) */
     int leaf_batch;   /* mode 3: a triangle phase runs when this many lanes hold a
                          parked leaf (0 = 16) */
+    int sort_rays;    /* 0: trace rays in input order; 1-3: first reorder them by a
+                         coherence key (where each ray enters the mesh's root box and
+                         its direction, interleaved (1), direction-major (2) or
+                         entry-major (3)) so neighbouring lanes trace similar rays.
+                         Results are written at each ray's input index either way
+                         and do not depend on the order. Batches of 2^31 rays or
+                         more are traced in input order. */
 } prr_trace_config;
 
 #define PRR_RENDER_PLAIN 0     /* one megakernel thread per (pixel, sample range) */
@@ -306,8 +313,10 @@ int prr_photon_info(const prr_photon_map *map, int64_t *count, int32_t *grid_res
 int prr_photon_export(const prr_photon_map *map, float *records, int32_t *owner, void *stream);
 /* PhotonMap::estimateIrradiance (Photon.cpp:82-94) at n points (n x 3):
  * sum of the powers within the radius over pi r^2. k_nearest > 0 (<= 64) caps
- * it: with more than k photons in the radius, the k nearest over the disc
- * through the k-th (identical to the fixed radius otherwise). */
+ * it: with more than k photons in the radius, the powers of the k nearest
+ * (the k smallest (distance, photon index) pairs: of photons at equal distance
+ * the lower index is kept), added in photon order, over the disc through the
+ * k-th; identical to the fixed radius otherwise. */
 int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n, int k_nearest,
                       float *out_rgb, void *stream);
 /* Caustic image: for every (pixel, sample) the camera ray follows the specular
@@ -321,6 +330,13 @@ int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n,
 int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream);
+/* No counterpart in the reference: prr_render_caustics with counting kernels
+ * (the same image), for measurement. Waits for the stream; out[0..3] = camera
+ * hits traced, irradiance gathers, photons tested by the gathers' cell walks,
+ * photons found inside the radius. */
+int prr_render_caustics_counts(const prr_scene *scene, const prr_photon_map *pmap,
+                               const prr_render_settings *settings, int k_nearest,
+                               float *out_rgb, uint64_t out[4], void *stream);
 
 /* ---- participating media (Volume.hpp, Volume.cpp) ----------------------
  * The reference defines a homogeneous medium and the Henyey-Greenstein phase
@@ -427,12 +443,34 @@ int prr_server_stats_get(prr_server *server, prr_server_stats *out);
  * per-slice partial sums) is a fixed device array inside the library of
  * 2,097,152 partial sums (24 MiB), held on every GPU that loads the library
  * until the process exits. Windows of more than 2,097,152 pixels are rejected
- * with PRR_ERR_INVALID_ARGUMENT. The first call on a device looks up that
- * array's device address, so make it before any stream capture. All calls
+ * with PRR_ERR_INVALID_ARGUMENT, and so is an explicit settings->slices whose
+ * pixels x slices exceed that count (the automatic choice, slices <= 0, is
+ * reduced to fit instead). With the same settings, including the same
+ * explicit slices, its image equals prr_render's bit for bit. The first call
+ * on a device looks up that array's device address, so make it before any
+ * stream capture. All calls
  * share the array and keep its last contents: calls that overlap on the GPU
  * race, so order them (one stream, or events). out_rays is optional. */
 int prr_render_noalloc(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
                        uint64_t *out_rays, void *stream);
+
+/* Work of one render, counted by prr_render_counts: the rays traced, the
+ * traversal steps they took -- interior nodes of the scene and mesh BVHs,
+ * triangle tests, object leaves (mesh entries and sphere tests) -- and the
+ * closest hits by class (no hit, mirror/glass, other). */
+typedef struct prr_render_count {
+    uint64_t closest_rays, closest_nodes, closest_tris, closest_objects;
+    uint64_t shadow_rays, shadow_nodes, shadow_tris, shadow_objects;
+    uint64_t misses, delta_hits, surface_hits;
+} prr_render_count;
+
+/* No counterpart in the reference (its statistics are timings only): renders
+ * like prr_render in wavefront mode (the same image) with counting variants of
+ * the traversal stages, waits for the stream and fills *out. For measurement
+ * (bytes per ray and per path-bounce), not for timed renders: it runs without
+ * CUDA graphs and the counters cost a little. */
+int prr_render_counts(prr_scene *scene, const prr_render_settings *settings, float *out_rgb,
+                      prr_render_count *out, void *stream);
 
 /* Sets the wavefront launch shape used by prr_render in wavefront mode. */
 int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config);

@@ -23,6 +23,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
+# The one setting that locates the reference source tree on the build host
+# (compiled in place by oracle/Makefile; read by tests for its .glb assets).
+REFERENCE_ROOT = Path(os.environ.get("PRR_REFERENCE_ROOT", "/root/reference"))
 PORT_LIB = HERE / "libprr_oracle.so"
 
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -46,7 +49,7 @@ def build_reference(ref_root: str | None = None) -> bool:
     """Compile the reference sources in place into oracle/_ref/ (needs the
     reference tree, which exists only on the build host). The bridge library
     also needs the package's libprr.so, so it is built only when that exists."""
-    root = ref_root or os.environ.get("PRR_REFERENCE_ROOT", "/root/reference")
+    root = str(ref_root or REFERENCE_ROOT)
     if not Path(root, "BVH.cpp").exists():
         return False
     targets = ["ref"]
@@ -93,6 +96,9 @@ class PortOracle:
                                          C.POINTER(C.c_float)]
         L.prr_oracle_photon_estimate.argtypes = [_f32p, C.c_int64, C.c_float, _f32p, C.c_int64,
                                                  _f32p, C.POINTER(C.c_int32)]
+        L.prr_oracle_photon_estimate_knn.argtypes = [_f32p, C.c_int64, C.c_float, C.c_int, _f32p,
+                                                     C.c_int64, _f32p, _i32p,
+                                                     C.POINTER(C.c_int32)]
         self.L = L
 
     def rng_stream(self, seed, stream, index, n):
@@ -126,6 +132,18 @@ class PortOracle:
         res = C.c_int32()
         self.L.prr_oracle_photon_estimate(rec, len(rec), radius, q, len(q), out, C.byref(res))
         return out, res.value
+
+    def photon_estimate_knn(self, rec, radius, q, k):
+        """Irradiance capped at the k nearest photons (k = 0: fixed radius),
+        and the number of photons inside the radius of each query."""
+        rec = _c(rec, np.float32).reshape(-1, 9)
+        q = _c(q, np.float32).reshape(-1, 3)
+        out = np.empty((len(q), 3), np.float32)
+        inside = np.empty(len(q), np.int32)
+        res = C.c_int32()
+        self.L.prr_oracle_photon_estimate_knn(rec, len(rec), radius, k, q, len(q), out, inside,
+                                              C.byref(res))
+        return out, inside
 
 
 class PortMesh:
@@ -272,6 +290,11 @@ class ReferenceOracle:
                                                 _i32p, _u8p, vp]
         L.prr_ref_photon_estimate.argtypes = [_f32p, C.c_int64, C.c_float, _f32p, C.c_int64,
                                               _f32p, C.POINTER(C.c_int32), C.c_int]
+        L.prr_ref_photon_estimate_knn.argtypes = [_f32p, C.c_int64, C.c_float, C.c_int, _f32p,
+                                                  C.c_int64, _f32p, _i32p, C.c_int]
+        L.prr_ref_caustic_render.argtypes = [vp, _f32p, C.c_int64, C.c_float, C.c_int, C.c_int,
+                                             C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.c_int, _f32p, C.c_int]
         self.L = L
         self.fast = fast
 
@@ -304,6 +327,18 @@ class ReferenceOracle:
         self.L.prr_ref_photon_estimate(rec, len(rec), radius, q, len(q), out, C.byref(res),
                                        threads)
         return out, res.value
+
+    def photon_estimate_knn(self, rec, radius, q, k, threads=0):
+        """The k-nearest-capped estimate over the reference's own grid query
+        (k = 0 or at most k photons inside: estimateIrradiance itself), and the
+        number of photons inside the radius of each query."""
+        rec = _c(rec, np.float32).reshape(-1, 9)
+        q = _c(q, np.float32).reshape(-1, 3)
+        out = np.empty((len(q), 3), np.float32)
+        inside = np.empty(len(q), np.int32)
+        self.L.prr_ref_photon_estimate_knn(rec, len(rec), radius, k, q, len(q), out, inside,
+                                           threads)
+        return out, inside
 
 
 class RefMesh:
@@ -544,6 +579,19 @@ class RefScene:
         d = np.empty((n, 3), np.float32)
         self.ref.L.prr_ref_camera_rays(self.h, px, py, xo, yo, n, o, d)
         return o, d
+
+    def caustic_render(self, rec, radius, spp, k_nearest=0, max_depth=8, seed=1,
+                       sample_offset=0, window=None, threads=0):
+        """The caustic image of a photon array: each camera sample follows
+        castRay's delta chain to its first diffuse hit and takes
+        baseColor / pi * the (k-capped) irradiance there."""
+        rec = _c(rec, np.float32).reshape(-1, 9)
+        W, H = self.desc.width, self.desc.height
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        out = np.empty(((y1 - y0) * (x1 - x0), 3), np.float32)
+        self.ref.L.prr_ref_caustic_render(self.h, rec, len(rec), radius, k_nearest, max_depth,
+                                          spp, seed, sample_offset, x0, y0, x1, y1, out, threads)
+        return out.reshape(y1 - y0, x1 - x0, 3)
 
     def photon_emit(self, n_photons, seed, max_depth=30, threads=0):
         L = self.ref.L

@@ -902,12 +902,41 @@ void prr_oracle_env_cdf(const float *rgb, int w, int h, float *cdf, float *margi
 }
 
 /* ------------------------------------------------------------------------ */
-/* Photon grid + fixed-radius irradiance (Photon.cpp:24-94)                   */
+/* Photon grid + fixed-radius irradiance (Photon.cpp:24-94), and the          */
+/* k-nearest-capped variant: with more than k photons inside the radius, the  */
+/* k smallest (distance, photon index) pairs, their powers added in photon    */
+/* order, over pi r_k^2 (r_k the k-th smallest distance).                     */
 /* ------------------------------------------------------------------------ */
-void prr_oracle_photon_estimate(const float *rec, int64_t n, float radius, const float *q,
-                                int64_t nq, float *out, int32_t *grid_res) {
+typedef struct {
+    float d;
+    int64_t i;
+} knn_cand;
+
+static int knn_cmp(const void *a, const void *b) {
+    const knn_cand *x = (const knn_cand *) a, *y = (const knn_cand *) b;
+    if (x->d != y->d)
+        return x->d < y->d ? -1 : 1;
+    return x->i < y->i ? -1 : (x->i > y->i);
+}
+
+static int idx_cmp(const void *a, const void *b) {
+    const int64_t x = *(const int64_t *) a, y = *(const int64_t *) b;
+    return x < y ? -1 : (x > y);
+}
+
+/* pi r^2 as estimateIrradiance writes it (Photon.cpp:87): float throughout, as
+ * the reference redefines M_PI as a float literal (global.hpp:9-10) */
+static float disc_area(float r) {
+    return PRR_PI * r * r;
+}
+
+void prr_oracle_photon_estimate_knn(const float *rec, int64_t n, float radius, int k,
+                                    const float *q, int64_t nq, float *out, int32_t *inside,
+                                    int32_t *grid_res) {
     if (n <= 0) {
         memset(out, 0, sizeof(float) * 3 * nq);
+        if (inside)
+            memset(inside, 0, sizeof(int32_t) * nq);
         return;
     }
     v3 bmin = mk(rec[0], rec[1], rec[2]), bmax = bmin;
@@ -948,45 +977,80 @@ void prr_oracle_photon_estimate(const float *rec, int64_t n, float radius, const
     int64_t *order = (int64_t *) malloc(sizeof(int64_t) * n);
     for (int64_t i = 0; i < n; i++)
         order[fill[cell[i]]++] = i;
-    const float area = PRR_PI * radius * radius;
-#pragma omp parallel for schedule(dynamic, 256)
-    for (int64_t k = 0; k < nq; k++) {
-        v3 pos = mk(q[k * 3], q[k * 3 + 1], q[k * 3 + 2]);
-        int x0 = (int) ((pos.x - radius - bmin.x) / cs.x);
-        int y0 = (int) ((pos.y - radius - bmin.y) / cs.y);
-        int z0 = (int) ((pos.z - radius - bmin.z) / cs.z);
-        int x1 = (int) ((pos.x + radius - bmin.x) / cs.x);
-        int y1 = (int) ((pos.y + radius - bmin.y) / cs.y);
-        int z1 = (int) ((pos.z + radius - bmin.z) / cs.z);
-        x0 = x0 > 0 ? x0 : 0;
-        x1 = x1 < res - 1 ? x1 : res - 1;
-        y0 = y0 > 0 ? y0 : 0;
-        y1 = y1 < res - 1 ? y1 : res - 1;
-        z0 = z0 > 0 ? z0 : 0;
-        z1 = z1 < res - 1 ? z1 : res - 1;
-        v3 e = mk(0.f, 0.f, 0.f);
-        int any = 0;
-        for (int cx = x0; cx <= x1; cx++)
-            for (int cy = y0; cy <= y1; cy++)
-                for (int cz = z0; cz <= z1; cz++) {
-                    int64_t c = (int64_t) cx + (int64_t) cy * res + (int64_t) cz * res * res;
-                    for (int64_t s = start[c]; s < start[c + 1]; s++) {
-                        const float *p = rec + order[s] * 9;
-                        v3 dd = sub(mk(p[0], p[1], p[2]), pos);
-                        if (sqrtf(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z) <= radius) {
-                            e = add(e, mk(p[6], p[7], p[8]));
-                            any = 1;
+    const float area = disc_area(radius);
+#pragma omp parallel
+    {
+        int64_t cap = 1024;
+        knn_cand *cand = (knn_cand *) malloc(sizeof(knn_cand) * cap);
+        int64_t *keep = (int64_t *) malloc(sizeof(int64_t) * (k > 0 ? k : 1));
+#pragma omp for schedule(dynamic, 256)
+        for (int64_t j = 0; j < nq; j++) {
+            v3 pos = mk(q[j * 3], q[j * 3 + 1], q[j * 3 + 2]);
+            int x0 = (int) ((pos.x - radius - bmin.x) / cs.x);
+            int y0 = (int) ((pos.y - radius - bmin.y) / cs.y);
+            int z0 = (int) ((pos.z - radius - bmin.z) / cs.z);
+            int x1 = (int) ((pos.x + radius - bmin.x) / cs.x);
+            int y1 = (int) ((pos.y + radius - bmin.y) / cs.y);
+            int z1 = (int) ((pos.z + radius - bmin.z) / cs.z);
+            x0 = x0 > 0 ? x0 : 0;
+            x1 = x1 < res - 1 ? x1 : res - 1;
+            y0 = y0 > 0 ? y0 : 0;
+            y1 = y1 < res - 1 ? y1 : res - 1;
+            z0 = z0 > 0 ? z0 : 0;
+            z1 = z1 < res - 1 ? z1 : res - 1;
+            v3 e = mk(0.f, 0.f, 0.f);
+            int64_t found = 0;
+            for (int cx = x0; cx <= x1; cx++)
+                for (int cy = y0; cy <= y1; cy++)
+                    for (int cz = z0; cz <= z1; cz++) {
+                        int64_t c = (int64_t) cx + (int64_t) cy * res + (int64_t) cz * res * res;
+                        for (int64_t s = start[c]; s < start[c + 1]; s++) {
+                            const float *p = rec + order[s] * 9;
+                            v3 dd = sub(mk(p[0], p[1], p[2]), pos);
+                            float dist = sqrtf(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z);
+                            if (dist <= radius) {
+                                e = add(e, mk(p[6], p[7], p[8]));
+                                if (found == cap) {
+                                    cap *= 2;
+                                    cand = (knn_cand *) realloc(cand, sizeof(knn_cand) * cap);
+                                }
+                                cand[found].d = dist;
+                                cand[found].i = order[s];
+                                found++;
+                            }
                         }
                     }
+            if (inside)
+                inside[j] = (int32_t) found;
+            float a = area;
+            if (found == 0) {
+                e = mk(0.f, 0.f, 0.f);
+            } else if (k > 0 && found > k) {
+                qsort(cand, (size_t) found, sizeof(knn_cand), knn_cmp);
+                for (int t = 0; t < k; t++)
+                    keep[t] = cand[t].i;
+                qsort(keep, (size_t) k, sizeof(int64_t), idx_cmp);
+                e = mk(0.f, 0.f, 0.f);
+                for (int t = 0; t < k; t++) {
+                    const float *p = rec + keep[t] * 9;
+                    e = add(e, mk(p[6], p[7], p[8]));
                 }
-        if (!any)
-            e = mk(0.f, 0.f, 0.f);
-        out[k * 3] = e.x / area;
-        out[k * 3 + 1] = e.y / area;
-        out[k * 3 + 2] = e.z / area;
+                a = disc_area(cand[k - 1].d);
+            }
+            out[j * 3] = e.x / a;
+            out[j * 3 + 1] = e.y / a;
+            out[j * 3 + 2] = e.z / a;
+        }
+        free(cand);
+        free(keep);
     }
     free(cell);
     free(start);
     free(fill);
     free(order);
+}
+
+void prr_oracle_photon_estimate(const float *rec, int64_t n, float radius, const float *q,
+                                int64_t nq, float *out, int32_t *grid_res) {
+    prr_oracle_photon_estimate_knn(rec, n, radius, 0, q, nq, out, NULL, grid_res);
 }

@@ -64,6 +64,11 @@ void prr_oracle_env_cdf(const float *rgb, int w, int h, float *cdf, float *margi
  * rec: n x 9 floats (position, direction, power). */
 void prr_oracle_photon_estimate(const float *rec, int64_t n, float radius, const float *q,
                                 int64_t nq, float *out_rgb, int32_t *grid_res);
+/* The same with a k-nearest cap (k > 0; 0 = fixed radius); inside (optional)
+ * gets the number of photons inside the radius of each query. */
+void prr_oracle_photon_estimate_knn(const float *rec, int64_t n, float radius, int k,
+                                    const float *q, int64_t nq, float *out, int32_t *inside,
+                                    int32_t *grid_res);
 
 #ifdef __cplusplus
 }

@@ -941,6 +941,161 @@ void prr_ref_photon_estimate(const float *rec, int64_t n, float radius, const fl
     }
 }
 
+// ---------------------------------------------------------------------------
+// k-nearest-capped estimate and the caustic render at camera hits. Neither
+// exists in the reference (castRay never gathers photons; estimateIrradiance
+// is fixed-radius), so these restate the library's definition with the
+// reference's own pieces:
+//   candidates   PhotonGrid::query(pos, radius) on a grid built by
+//                PhotonGrid::build (Photon.cpp:24-81) from the given array;
+//   <= k inside  PhotonMap::estimateIrradiance itself (Photon.cpp:82-94);
+//   > k inside   brute force over the candidates: the k smallest
+//                (distance, photon index) pairs, distance as the query
+//                computes it ((p - x).norm()), their powers added in photon
+//                order, divided by pi r_k^2 written as estimateIrradiance
+//                writes pi r^2, r_k the k-th smallest distance.
+// The photon index travels in the direction field (unused by the estimate).
+// ---------------------------------------------------------------------------
+struct KnnMap {
+    PhotonMap pm;
+    std::vector<Vector3f> power; // in photon order
+};
+
+static KnnMap *knn_map_new(const float *rec, int64_t n, float radius) {
+    KnnMap *m = new KnnMap();
+    m->pm.photon_radius = radius;
+    m->pm.caustic_map.resize(n);
+    m->power.resize(n);
+    for (int64_t i = 0; i < n; i++) {
+        const float *r = rec + i * 9;
+        m->pm.caustic_map[i].position = Vector3f(r[0], r[1], r[2]);
+        m->pm.caustic_map[i].direction = Vector3f((float) i, 0.f, 0.f);
+        m->pm.caustic_map[i].power = Vector3f(r[6], r[7], r[8]);
+        m->pm.caustic_map[i].is_caustic = true;
+        m->power[i] = Vector3f(r[6], r[7], r[8]);
+    }
+    m->pm.build();
+    return m;
+}
+
+static Vector3f knn_estimate(const KnnMap &m, const Vector3f &pos, int k, int32_t *inside) {
+    thread_local std::vector<const Photon *> near;
+    thread_local std::vector<std::pair<float, int32_t>> cand;
+    m.pm.caustic_grid.query(pos, m.pm.photon_radius, near);
+    if (inside)
+        *inside = (int32_t) near.size();
+    if (k <= 0 || (int) near.size() <= k)
+        return m.pm.estimateIrradiance(pos, Vector3f(0, 1, 0));
+    cand.clear();
+    for (const Photon *p : near)
+        cand.emplace_back((p->position - pos).norm(), (int32_t) p->direction.x);
+    std::sort(cand.begin(), cand.end());
+    const float rk = cand[k - 1].first;
+    std::vector<int32_t> keep(k);
+    for (int q = 0; q < k; q++)
+        keep[q] = cand[q].second;
+    std::sort(keep.begin(), keep.end());
+    Vector3f e = {};
+    for (int32_t i : keep)
+        e += m.power[i];
+    float area = M_PI * rk * rk;
+    return e / area;
+}
+
+// Irradiance at nq points: fixed radius (k = 0) or capped at the k nearest;
+// out_inside (optional) gets the number of photons inside the radius.
+void prr_ref_photon_estimate_knn(const float *rec, int64_t n, float radius, int k, const float *q,
+                                 int64_t nq, float *out_rgb, int32_t *out_inside, int nthreads) {
+    KnnMap *m = knn_map_new(rec, n, radius);
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t j = 0; j < nq; j++) {
+        const Vector3f e = knn_estimate(*m, Vector3f(q[j * 3], q[j * 3 + 1], q[j * 3 + 2]), k,
+                                        out_inside ? out_inside + j : nullptr);
+        out_rgb[j * 3 + 0] = e.x;
+        out_rgb[j * 3 + 1] = e.y;
+        out_rgb[j * 3 + 2] = e.z;
+    }
+    delete m;
+}
+
+// The caustic radiance of a camera sample: the camera ray of Renderer.cpp:75-77
+// follows castRay's delta chain (Integrator.cpp:143-169: the material's own
+// sample, the pdf cut, beta *= f / pdf, the offset origin, the baseColor tint on
+// transmission) for at most max_depth hits; at the first non-delta, non-emissive
+// hit the estimate is beta * baseColor / pi * E(hit point), with baseColor from
+// the diffuse material's buildShadingData (Material.cpp:3-26). A miss, an
+// emitter or the depth limit contributes zero. Pixel m = i + j*W, sample n draws
+// stream (seed, m, sample_offset + n); the pixel value is the mean of its spp
+// samples added in sample order.
+void prr_ref_caustic_render(void *h, const float *rec, int64_t n, float radius, int k,
+                            int max_depth, int spp, uint64_t seed, int sample_offset, int x0,
+                            int y0, int x1, int y1, float *out_rgb, int nthreads) {
+    RefScene *rs = (RefScene *) h;
+    const int W = rs->width, H = rs->height;
+    KnnMap *m = knn_map_new(rec, n, radius);
+    const int ww = x1 - x0, wh = y1 - y0;
+    if (nthreads > 0)
+        omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t qp = 0; qp < (int64_t) ww * wh; qp++) {
+        const int i = x0 + (int) (qp % ww), j = y0 + (int) (qp / ww);
+        const int mpix = i + j * W;
+        Vector3f acc(0.f);
+        for (int s = 0; s < spp; s++) {
+            ref_set_path(seed, (uint32_t) mpix, (uint32_t) (sample_offset + s));
+            const float xOffset = get_random_float();
+            const float yOffset = get_random_float();
+            Ray ray = rs->scene.camera.generateRay(i, j, W, H, xOffset, yOffset);
+            Vector3f beta(1.f), c(0.f);
+            for (int d = 0; d < max_depth; d++) {
+                Intersection inter = rs->scene.intersect(ray);
+                if (!inter.happened)
+                    break;
+                Material *mat = inter.material;
+                if (mat->isEmissive())
+                    break;
+                const Vector3f geoNormal = inter.normal;
+                if (mat->isDelta()) {
+                    ShadingData sd = inter.hasTangent
+                                         ? mat->buildShadingData(inter.tcoords, geoNormal,
+                                                                 normalize(inter.tangent),
+                                                                 inter.tangentHandedness)
+                                         : mat->buildShadingData(inter.tcoords, geoNormal);
+                    BSDFSample bsdf = mat->sample(-ray.direction, sd);
+                    if (bsdf.pdf < 1e-6f)
+                        break;
+                    beta = beta * bsdf.f / bsdf.pdf;
+                    const bool trans = dotProduct(bsdf.wi, geoNormal) < 0.f;
+                    const Vector3f offset = trans ? -geoNormal : geoNormal;
+                    ray = Ray(inter.coords + offset * EPSILON, bsdf.wi);
+                    if (trans)
+                        beta = beta * sd.baseColor;
+                    continue;
+                }
+                DiffuseMaterial *dm = static_cast<DiffuseMaterial *>(mat);
+                const Vector3f sn = dotProduct(ray.direction, geoNormal) < 0.f ? geoNormal
+                                                                              : -geoNormal;
+                ShadingData sd = inter.hasTangent
+                                     ? dm->buildShadingData(inter.tcoords, sn,
+                                                            normalize(inter.tangent),
+                                                            inter.tangentHandedness)
+                                     : dm->buildShadingData(inter.tcoords, sn);
+                const Vector3f e = knn_estimate(*m, inter.coords, k, nullptr);
+                c = beta * (sd.baseColor / (float) M_PI) * e;
+                break;
+            }
+            acc += c;
+        }
+        acc = acc / (float) spp;
+        out_rgb[qp * 3 + 0] = acc.x;
+        out_rgb[qp * 3 + 1] = acc.y;
+        out_rgb[qp * 3 + 2] = acc.z;
+    }
+    delete m;
+}
+
 // ---- participating media (Volume.hpp, Volume.cpp; unused by castRay)
 
 // Medium::dust() (0) or Medium::fog() (1): sigma_a, sigma_s, sigma_t, g.

@@ -35,7 +35,7 @@ class prr_camera(C.Structure):
 
 class prr_trace_config(C.Structure):
     _fields_ = [("block_size", C.c_int), ("persistent", C.c_int), ("blocks_per_sm", C.c_int),
-                ("batch", C.c_int), ("leaf_batch", C.c_int)]
+                ("batch", C.c_int), ("leaf_batch", C.c_int), ("sort_rays", C.c_int)]
 
 
 class prr_wavefront_config(C.Structure):
@@ -74,6 +74,13 @@ class prr_scene_stats(C.Structure):
                 ("tlas_depth", C.c_int32), ("blas_depth", C.c_int32),
                 ("device_bytes", C.c_int64), ("total_emit_area", C.c_float),
                 ("last_render_launches", C.c_int64)]
+
+
+class prr_render_count(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "closest_rays", "closest_nodes", "closest_tris", "closest_objects",
+        "shadow_rays", "shadow_nodes", "shadow_tris", "shadow_objects",
+        "misses", "delta_hits", "surface_hits")]
 
 
 class prr_render_settings(C.Structure):
@@ -131,6 +138,8 @@ _SIGS = {
     "prr_scene_intersect": (C.c_int, [_vp, _vp, _vp, C.c_int64, _vp, _vp, _vp, _vp, _vp]),
     "prr_scene_occluded": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int64, _vp, _vp]),
     "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
+    "prr_render_counts": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp,
+                                    C.POINTER(prr_render_count), _vp]),
     "prr_photon_map_create": (C.c_int, [C.POINTER(_vp)]),
     "prr_photon_map_destroy": (C.c_int, [_vp]),
     "prr_photon_emit": (C.c_int, [_vp, _vp, C.c_int64, C.c_uint64, C.c_int, _vp]),
@@ -141,6 +150,8 @@ _SIGS = {
     "prr_photon_gather": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp]),
     "prr_render_caustics": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int, _vp,
                                       _vp]),
+    "prr_render_caustics_counts": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int,
+                                             _vp, _vp, _vp]),
     "prr_medium_preset": (C.c_int, [C.c_int, C.POINTER(prr_medium)]),
     "prr_medium_intersect": (C.c_int, [C.POINTER(prr_medium), _vp, _vp, C.c_int64, _vp, _vp,
                                        _vp, _vp]),

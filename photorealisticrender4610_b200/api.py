@@ -15,9 +15,9 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (check, prr_camera, prr_render_settings, prr_request, prr_request_info,
-                   prr_scene_stats, prr_server_config, prr_server_stats, prr_trace_config,
-                   prr_wavefront_config)
+from ._lib import (check, prr_camera, prr_render_count, prr_render_settings, prr_request,
+                   prr_request_info, prr_scene_stats, prr_server_config, prr_server_stats,
+                   prr_trace_config, prr_wavefront_config)
 
 RENDER_MODES = {"plain": 0, "wavefront": 1}
 TONEMAPPERS = {"raw": 0, "standard": 1, "agx": 2, "pbrneutral": 3, "aces": 4}
@@ -139,7 +139,7 @@ def _trace_config(config: dict | None):
         return None
     return prr_trace_config(config.get("block_size", 0), config.get("persistent", 0),
                             config.get("blocks_per_sm", 0), config.get("batch", 0),
-                            config.get("leaf_batch", 0))
+                            config.get("leaf_batch", 0), config.get("sort_rays", 0))
 
 
 def _ptr(t):
@@ -513,6 +513,22 @@ class Scene:
             return out, cnt, rays
         return out, cnt
 
+    def render_counts(self, spp: int, max_depth: int, seed: int = 1, min_spp: int | None = None,
+                      threshold: float = 0.05, window=None, indirect_clamp: float = 10.0,
+                      stream=None):
+        """A wavefront render with counting traversal stages: (image, dict of
+        rays, traversal steps and hit classes; see prr_render_count)."""
+        import torch
+        rs = self._settings(spp, max_depth, seed, min_spp, threshold, "wavefront", window,
+                            indirect_clamp, 0, 0)
+        x0, y0, x1, y1 = rs.x0, rs.y0, rs.x1, rs.y1
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
+        cnt = prr_render_count()
+        check(self.lib.prr_render_counts(self.h, C.byref(rs), _ptr(out), C.byref(cnt),
+                                         _stream(stream)))
+        return out, {k: int(getattr(cnt, k)) for k, _ in cnt._fields_}
+
     # ---- per-call reference methods, batched ----
     def cast_samples(self, px, py, sample, max_depth: int, seed: int = 1,
                      indirect_clamp: float = 10.0, stream=None):
@@ -644,6 +660,22 @@ class PhotonMap:
         check(self.lib.prr_render_caustics(scene.h, self.h, C.byref(rs), k_nearest, _ptr(out),
                                            _stream(stream)))
         return out
+
+    def render_caustics_counts(self, scene: Scene, spp: int, max_depth: int = 8, seed: int = 1,
+                               k_nearest: int = 0, window=None, stream=None):
+        """render_caustics with counting kernels: (image, dict of camera hits,
+        gathers, photons tested and photons inside the radius)."""
+        import torch
+        rs = scene._settings(spp, max_depth, seed, None, 0.05, "plain", window, 10.0, 0, 0)
+        W, H = scene.size
+        x0, y0, x1, y1 = window or (0, 0, W, H)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
+        cnt = (C.c_uint64 * 4)()
+        check(self.lib.prr_render_caustics_counts(scene.h, self.h, C.byref(rs), k_nearest,
+                                                  _ptr(out), cnt, _stream(stream)))
+        keys = ("hits", "gathers", "photons_tested", "photons_inside")
+        return out, dict(zip(keys, (int(x) for x in cnt)))
 
 
 REQUEST_STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}

@@ -328,10 +328,21 @@ struct GridView {
     float radius;
 };
 
+// pi r^2 as estimateIrradiance computes it (Photon.cpp:87): all in float,
+// since the reference redefines M_PI as a float literal (global.hpp:9-10).
+__device__ __forceinline__ float disc_area(float r) {
+    return PRR_PI * r * r;
+}
+
 // PhotonGrid::query + PhotonMap::estimateIrradiance (Photon.cpp:55-94). With
 // k_nearest > 0 and more than k photons inside the radius, the estimate uses
-// the k nearest and the disc through the k-th one instead.
-__device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc) {
+// the k nearest -- the k smallest (distance, photon index) pairs, so ties at
+// the k-th distance keep the lower photon index whatever the walk order --
+// and the disc through the k-th one: sum / (pi r_k^2), the kept photons added
+// in photon-array order.
+template <bool COUNT = false>
+__device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc,
+                         unsigned *tested = nullptr, unsigned *inside = nullptr) {
     const GridParams &g = *v.g;
     const float r = v.radius;
     int x0 = (int) ((pos.x - r - g.bmin[0]) / g.cs[0]);
@@ -348,11 +359,11 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     z1 = min(g.res - 1, z1);
     V3 e = v3(0.f);
     int found = 0;
-    int worst = 0; // kNN: the first index of the largest kept distance, once k are kept
+    int worst = 0; // kNN, once k are kept: the entry of the largest (distance, index)
     auto find_worst = [&] {
         worst = 0;
         for (int q = 1; q < k_nearest; q++)
-            if (kd[q] > kd[worst])
+            if (kd[q] > kd[worst] || (kd[q] == kd[worst] && kc[q] > kc[worst]))
                 worst = q;
     };
     for (int cx = x0; cx <= x1; cx++)
@@ -367,7 +378,11 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
                     const float4 pa = v.sorted[2 * s];
                     const V3 d = v3(pa.x, pa.y, pa.z) - pos;
                     const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+                    if constexpr (COUNT)
+                        (*tested)++;
                     if (dist <= r) {
+                        if constexpr (COUNT)
+                            (*inside)++;
                         const float4 pb = v.sorted[2 * s + 1];
                         e = e + v3(pa.w, pb.x, pb.y);
                         if (kd && found < k_nearest) {
@@ -375,11 +390,14 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
                             kc[found] = v.order[s];
                             if (found + 1 == k_nearest)
                                 find_worst();
-                        } else if (kd && dist < kd[worst]) {
-                            // keep the k smallest distances (replace the largest)
-                            kd[worst] = dist;
-                            kc[worst] = v.order[s];
-                            find_worst();
+                        } else if (kd && dist <= kd[worst]) {
+                            // keep the k smallest (distance, index) pairs
+                            const int idx = v.order[s];
+                            if (dist < kd[worst] || idx < kc[worst]) {
+                                kd[worst] = dist;
+                                kc[worst] = idx;
+                                find_worst();
+                            }
                         }
                         found++;
                     }
@@ -388,11 +406,7 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     if (found == 0)
         return v3(0.f);
     if (kd && found > k_nearest) {
-        // Jensen's estimate over the k nearest: sum / (pi r_k^2); the k kept
-        // photons are added in photon-array order for a fixed result
-        float rk = 0.f;
-        for (int q = 0; q < k_nearest; q++)
-            rk = fmaxf(rk, kd[q]);
+        const float rk = kd[worst];
         for (int a = 1; a < k_nearest; a++) {
             const int key = kc[a];
             int b = a - 1;
@@ -407,11 +421,9 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
             const float *p = v.rec + (size_t) kc[q] * 9;
             ek = ek + v3(p[6], p[7], p[8]);
         }
-        const float area = PRR_PI * rk * rk;
-        return ek / area;
+        return ek / disc_area(rk);
     }
-    const float area = PRR_PI * r * r;
-    return e / area;
+    return e / disc_area(r);
 }
 
 constexpr int kMaxK = 64;
@@ -440,11 +452,14 @@ struct CausticArgs {
     float4 *samples; // npix x chunk contributions, sample-major
     float4 *acc;     // npix running sums across chunks
     int s0, chunk;   // this launch's samples [s0, s0 + chunk) of each pixel
+    unsigned long long *stats; // counting variant: camera hits, gathers, photons
+                               // tested, photons inside the radius
 };
 
 // One thread per (pixel, sample): sample n of window pixel q is item
 // n * npix + q, so neighbouring threads trace neighbouring pixels and the
 // uneven cost of gathers in and out of the caustics spreads over the grid.
+template <bool COUNT>
 __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     extern __shared__ uint2 smem[];
     SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
@@ -453,6 +468,7 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     const int64_t total = npix * a.chunk;
     float kd[kMaxK];
     int kc[kMaxK];
+    unsigned cnt_[4] = {0, 0, 0, 0}; // hits, gathers, photons tested, photons inside
     for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t) gridDim.x * blockDim.x) {
         const int nc = (int) (t / npix);
@@ -472,12 +488,16 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
             const Inter in = intersect(S, ray, tst, bst);
             if (!in.hit)
                 break;
+            if constexpr (COUNT)
+                cnt_[0]++;
             const DevMaterial &mt = S.materials[in.mat];
             if (mt.kind == kMatEmissive)
                 break;
             if (mt.kind == kMatMirror || mt.kind == kMatGlass) {
                 const Shading sd = build_shading(S, mt, in.n, in.a);
                 const BSDFSample bs = delta_sample(mt, sd, -ray.d, rng);
+                if (bs.pdf < 1e-6f)
+                    break;
                 beta = beta * bs.f / bs.pdf;
                 const bool trans = dot(bs.wi, in.n) < 0.f;
                 ray = Ray3{in.p + (trans ? -in.n : in.n) * PRR_EPS, bs.wi};
@@ -485,7 +505,10 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
                     beta = beta * sd.base;
                 continue;
             }
-            const V3 e = irradiance(v, in.p, a.k_nearest, a.k_nearest > 0 ? kd : nullptr, kc);
+            if constexpr (COUNT)
+                cnt_[1]++;
+            const V3 e = irradiance<COUNT>(v, in.p, a.k_nearest, a.k_nearest > 0 ? kd : nullptr,
+                                           kc, cnt_ + 2, cnt_ + 3);
             const V3 albedo = mt.tex_base >= 0
                                   ? sample_base_color(S.textures[mt.tex_base], in.a.u, in.a.v)
                                   : v3(mt.base[0], mt.base[1], mt.base[2]);
@@ -493,6 +516,15 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
             break;
         }
         a.samples[t] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+    if constexpr (COUNT) {
+        for (int k = 0; k < 4; k++) {
+            unsigned long long x = cnt_[k];
+            for (int off = 16; off > 0; off >>= 1)
+                x += __shfl_down_sync(0xffffffffu, x, off);
+            if ((threadIdx.x & 31) == 0 && x)
+                atomicAdd(a.stats + k, x);
+        }
     }
 }
 
@@ -527,37 +559,6 @@ __global__ void k_caustic_film(CausticArgs a) {
 // chunks of whole samples per pixel.
 constexpr int64_t kCausticItems = int64_t(1) << 28;
 
-// The library's stream-ordered memory pool of a device: freed blocks stay in
-// it (up to a 4 GiB release threshold) for the next calls instead of going
-// back to the driver at every synchronisation, as the device's default pool
-// would do. Created on first use, one per device.
-cudaError_t library_pool(cudaMemPool_t *out) {
-    static std::mutex mu;
-    static std::vector<cudaMemPool_t> pools;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess)
-        return e;
-    std::lock_guard<std::mutex> g(mu);
-    if ((int) pools.size() <= dev)
-        pools.resize(dev + 1, nullptr);
-    if (!pools[dev]) {
-        cudaMemPoolProps props{};
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t p = nullptr;
-        e = cudaMemPoolCreate(&p, &props);
-        if (e != cudaSuccess)
-            return e;
-        uint64_t keep = uint64_t(4) << 30;
-        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
-        pools[dev] = p;
-    }
-    *out = pools[dev];
-    return cudaSuccess;
-}
-
 PhotonMap *PM(prr_photon_map *p) { return reinterpret_cast<PhotonMap *>(p); }
 const PhotonMap *PM(const prr_photon_map *p) { return reinterpret_cast<const PhotonMap *>(p); }
 
@@ -578,6 +579,87 @@ GridView view(const PhotonMap &pm) {
 } // namespace prr
 
 using namespace prr;
+
+namespace prr {
+namespace {
+
+int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
+                    const prr_render_settings *settings, int k_nearest, float *out_rgb,
+                    unsigned long long *stats, cudaStream_t st) {
+    if (!scene || !pmap || !settings || !out_rgb || k_nearest < 0 || k_nearest > kMaxK)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "bad caustic render arguments");
+    const Scene &s = *reinterpret_cast<const Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    const PhotonMap &pm = *PM(pmap);
+    if (!pm.built || pm.n == 0)
+        return fail(PRR_ERR_NOT_BUILT, "photon map empty or not built");
+    prr_render_settings rs = *settings;
+    rs.mode = PRR_RENDER_PLAIN;
+    rs.min_spp = rs.max_spp;
+    if (int rc = validate_render(s, rs))
+        return rc;
+    CausticArgs a{};
+    a.W = s.width;
+    a.x0 = rs.x0;
+    a.y0 = rs.y0;
+    a.ww = rs.x1 - rs.x0;
+    a.wh = rs.y1 - rs.y0;
+    a.spp = rs.max_spp;
+    a.max_depth = rs.max_depth;
+    a.k_nearest = k_nearest;
+    a.seed = rs.seed;
+    a.sample_offset = rs.sample_offset;
+    a.out = out_rgb;
+    a.stats = stats;
+    a.tlas_cap = s.dev.tlas_depth + 1;
+    const int block = 128;
+    const size_t smem = (size_t) (a.tlas_cap + s.dev.blas_depth + 1) * block * sizeof(uint2);
+    if (smem > 200 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
+    auto kern = stats ? k_caustic_samples<true> : k_caustic_samples<false>;
+    if (smem > 48 * 1024)
+        PRR_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int) smem));
+    const int64_t npix = (int64_t) a.ww * a.wh;
+    const int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(a.spp, kCausticItems / npix));
+    const int64_t items = npix * chunk;
+    // per-call contributions (and, when chunked, running sums) from the
+    // library's stream-ordered pool: concurrent calls on other streams get
+    // their own
+    char *scratch = nullptr;
+    const size_t acc_bytes = chunk < a.spp ? (size_t) npix * sizeof(float4) : 0;
+    cudaMemPool_t pool;
+    PRR_CUDA_TRY(library_pool(&pool));
+    PRR_CUDA_TRY(cudaMallocFromPoolAsync((void **) &scratch,
+                                         (size_t) items * sizeof(float4) + acc_bytes, pool, st));
+    a.samples = reinterpret_cast<float4 *>(scratch);
+    a.acc = acc_bytes ? reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4))
+                      : nullptr;
+    int bps = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
+    cudaError_t e = cudaSuccess;
+    for (int s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
+        a.s0 = s0;
+        a.chunk = std::min(chunk, a.spp - s0);
+        const int64_t total = npix * a.chunk;
+        const int64_t grid = std::min<int64_t>(
+            (total + block - 1) / block, (int64_t) device_sm_count() * std::max(1, bps) * 8);
+        kern<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
+            e = cudaGetLastError();
+        }
+    }
+    cudaFreeAsync(scratch, st);
+    if (e != cudaSuccess)
+        return fail(PRR_ERR_CUDA, std::string("caustic render: ") + cudaGetErrorString(e));
+    return PRR_OK;
+}
+
+} // namespace
+} // namespace prr
 
 extern "C" {
 
@@ -768,74 +850,24 @@ int prr_photon_gather(const prr_photon_map *pmap, const float *points, int64_t n
 int prr_render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream) {
-    if (!scene || !pmap || !settings || !out_rgb || k_nearest < 0 || k_nearest > kMaxK)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "bad caustic render arguments");
-    const Scene &s = *reinterpret_cast<const Scene *>(scene);
-    if (!s.built)
-        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
-    const PhotonMap &pm = *PM(pmap);
-    if (!pm.built || pm.n == 0)
-        return fail(PRR_ERR_NOT_BUILT, "photon map empty or not built");
-    prr_render_settings rs = *settings;
-    rs.mode = PRR_RENDER_PLAIN;
-    rs.min_spp = rs.max_spp;
-    if (int rc = validate_render(s, rs))
-        return rc;
-    CausticArgs a{};
-    a.W = s.width;
-    a.x0 = rs.x0;
-    a.y0 = rs.y0;
-    a.ww = rs.x1 - rs.x0;
-    a.wh = rs.y1 - rs.y0;
-    a.spp = rs.max_spp;
-    a.max_depth = rs.max_depth;
-    a.k_nearest = k_nearest;
-    a.seed = rs.seed;
-    a.sample_offset = rs.sample_offset;
-    a.out = out_rgb;
-    a.tlas_cap = s.dev.tlas_depth + 1;
-    const int block = 128;
-    const size_t smem = (size_t) (a.tlas_cap + s.dev.blas_depth + 1) * block * sizeof(uint2);
-    if (smem > 200 * 1024)
-        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stacks");
-    if (smem > 48 * 1024)
-        PRR_CUDA_TRY(cudaFuncSetAttribute(k_caustic_samples,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    const int64_t npix = (int64_t) a.ww * a.wh;
-    const int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(a.spp, kCausticItems / npix));
-    const int64_t items = npix * chunk;
+    return render_caustics(scene, pmap, settings, k_nearest, out_rgb, nullptr,
+                           (cudaStream_t) stream);
+}
+
+int prr_render_caustics_counts(const prr_scene *scene, const prr_photon_map *pmap,
+                               const prr_render_settings *settings, int k_nearest,
+                               float *out_rgb, uint64_t out[4], void *stream) {
+    if (!out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "out is required");
     cudaStream_t st = (cudaStream_t) stream;
-    // per-call contributions (and, when chunked, running sums) from the
-    // library's stream-ordered pool: concurrent calls on other streams get
-    // their own
-    char *scratch = nullptr;
-    const size_t acc_bytes = chunk < a.spp ? (size_t) npix * sizeof(float4) : 0;
-    cudaMemPool_t pool;
-    PRR_CUDA_TRY(library_pool(&pool));
-    PRR_CUDA_TRY(cudaMallocFromPoolAsync((void **) &scratch,
-                                         (size_t) items * sizeof(float4) + acc_bytes, pool, st));
-    a.samples = reinterpret_cast<float4 *>(scratch);
-    a.acc = acc_bytes ? reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4))
-                      : nullptr;
-    int bps = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_caustic_samples, block, smem);
-    cudaError_t e = cudaSuccess;
-    for (int s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
-        a.s0 = s0;
-        a.chunk = std::min(chunk, a.spp - s0);
-        const int64_t total = npix * a.chunk;
-        const int64_t grid = std::min<int64_t>(
-            (total + block - 1) / block, (int64_t) device_sm_count() * std::max(1, bps) * 8);
-        k_caustic_samples<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
-        e = cudaGetLastError();
-        if (e == cudaSuccess) {
-            k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
-            e = cudaGetLastError();
-        }
-    }
-    cudaFreeAsync(scratch, st);
-    if (e != cudaSuccess)
-        return fail(PRR_ERR_CUDA, std::string("caustic render: ") + cudaGetErrorString(e));
+    DevBuf buf;
+    PRR_CUDA_TRY(buf.alloc(4 * sizeof(unsigned long long)));
+    PRR_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, 4 * sizeof(unsigned long long), st));
+    if (int rc = render_caustics(scene, pmap, settings, k_nearest, out_rgb,
+                                 buf.as<unsigned long long>(), st))
+        return rc;
+    PRR_CUDA_TRY(cudaMemcpyAsync(out, buf.ptr, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
     return PRR_OK;
 }
 

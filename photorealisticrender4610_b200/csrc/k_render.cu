@@ -310,7 +310,16 @@ extern "C" int prr_render_noalloc(prr_scene *scene, const prr_render_settings *s
             slices *= 2;
     }
     slices = std::max(1, std::min(slices, rs.max_spp));
-    slices = (int) std::min<int64_t>(slices, kNoAllocPartials / npix);
+    if (npix * slices > kNoAllocPartials) {
+        // an explicit slice count fixes the summation order, so it is not cut
+        // silently; the automatic choice only aims to fill the GPU
+        if (rs.slices > 0)
+            return fail(PRR_ERR_INVALID_ARGUMENT,
+                        std::to_string(slices) + " slices of " + std::to_string(npix) +
+                            " pixels exceed the " + std::to_string(kNoAllocPartials) +
+                            " partial sums of the allocation-free renderer");
+        slices = (int) (kNoAllocPartials / npix);
+    }
     a.slices = slices;
     a.tlas_cap = S.tlas_depth + 1;
     const int bcap = S.blas_depth + 1;

@@ -57,7 +57,13 @@ struct MeshArgs {
     double *out_t64;
     unsigned long long *counter;
     int stack_stride;
+    const uint32_t *perm; // trace order -> input index (nullptr: input order)
 };
+
+// Input index of the ray traced in position i.
+__device__ __forceinline__ int64_t ray_at(const MeshArgs &a, int64_t i) {
+    return a.perm ? (int64_t) __ldg(a.perm + i) : i;
+}
 
 __device__ __forceinline__ void mesh_closest_one(const MeshArgs &a, SmemStack &st, int64_t i) {
     const RayD r = load_ray(a.O, a.D, i);
@@ -75,7 +81,7 @@ __global__ void k_mesh_closest(MeshArgs a) {
     SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
-        mesh_closest_one(a, st, i);
+        mesh_closest_one(a, st, ray_at(a, i));
 }
 
 // Persistent: each warp takes the next 32 rays from the counter until none
@@ -93,7 +99,7 @@ __global__ void k_mesh_closest_persistent(MeshArgs a) {
             break;
         const int64_t i = (int64_t) base + lane;
         if (i < a.n)
-            mesh_closest_one(a, st, i);
+            mesh_closest_one(a, st, ray_at(a, i));
     }
 }
 
@@ -136,8 +142,8 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
             if (idle) {
                 const int64_t ni = (int64_t) base + __popc(im & ((1u << lane) - 1u));
                 if (ni < a.n) {
-                    idx = ni;
-                    r = load_ray(a.O, a.D, ni);
+                    idx = ray_at(a, ni);
+                    r = load_ray(a.O, a.D, idx);
                     p = precompute(r);
                     best = kInf;
                     hit = -1;
@@ -280,8 +286,8 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
             if (idle) {
                 const int64_t ni = (int64_t) base + __popc(im & ((1u << lane) - 1u));
                 if (ni < a.n) {
-                    idx = ni;
-                    r = load_ray(a.O, a.D, ni);
+                    idx = ray_at(a, ni);
+                    r = load_ray(a.O, a.D, idx);
                     p = precompute(r);
                     best = kInf;
                     hit = -1;
@@ -468,6 +474,214 @@ __global__ void k_scene_occluded(DevScene S, const float *O, const float *D,
     }
 }
 
+// ---------------------------------------------------------------- ray order
+// Coherence reordering before a closest-hit batch. Each ray gets a 30-bit key
+// from where it enters the mesh's root box (its origin if it starts inside)
+// and its normalised direction, each quantised to 5 bits per axis; the
+// buckets are the key's top `bits` bits. A counting pass, an exclusive scan
+// and a scatter with one atomic per ray give a permutation grouped by bucket
+// (the order inside a bucket is whatever the atomics give: it does not matter,
+// because every ray's result is written at its own input index and the walk
+// of one ray does not depend on any other). Rays that miss the root box get
+// the last bucket.
+
+// bit k of v (k < 5) to bit 6k, for a 6-way interleave
+__device__ __forceinline__ uint32_t spread6(uint32_t v) {
+    uint32_t r = 0;
+#pragma unroll
+    for (int b = 0; b < 5; b++)
+        r |= ((v >> b) & 1u) << (6 * b);
+    return r;
+}
+
+// bit k of v (k < 5) to bit 3k, for a 3-way interleave
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+    uint32_t r = 0;
+#pragma unroll
+    for (int b = 0; b < 5; b++)
+        r |= ((v >> b) & 1u) << (3 * b);
+    return r;
+}
+
+__device__ __forceinline__ uint32_t quant5(float u) {
+    const float q = u * 32.f;
+    return q <= 0.f ? 0u : (q >= 31.f ? 31u : (uint32_t) q);
+}
+
+struct RayKeyArgs {
+    const float *O, *D;
+    int64_t n;
+    float box[6]; // root box [minX,maxX,minY,maxY,minZ,maxZ]
+    int mode;     // 1 interleaved, 2 direction-major, 3 entry-major
+    int shift;    // key >> shift = bucket
+    uint32_t *bucket;
+    uint32_t *count;
+};
+
+__global__ void k_ray_buckets(RayKeyArgs a) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    const RayD r = load_ray(a.O, a.D, i);
+    const RayPre p = precompute(r);
+    const float t = slab(a.box[0], a.box[1], a.box[2], a.box[3], a.box[4], a.box[5], p);
+    uint32_t key = (1u << 30) - 1u;
+    if (t < kInf) {
+        const float ex = (r.ox + r.dx * t - a.box[0]) / (a.box[1] - a.box[0]);
+        const float ey = (r.oy + r.dy * t - a.box[2]) / (a.box[3] - a.box[2]);
+        const float ez = (r.oz + r.dz * t - a.box[4]) / (a.box[5] - a.box[4]);
+        const float inv = rsqrtf(r.dx * r.dx + r.dy * r.dy + r.dz * r.dz);
+        const uint32_t qx = quant5(ex), qy = quant5(ey), qz = quant5(ez);
+        const uint32_t dx = quant5(0.5f + 0.5f * r.dx * inv);
+        const uint32_t dy = quant5(0.5f + 0.5f * r.dy * inv);
+        const uint32_t dz = quant5(0.5f + 0.5f * r.dz * inv);
+        const uint32_t e3 = spread3(qx) << 2 | spread3(qy) << 1 | spread3(qz);
+        const uint32_t d3 = spread3(dx) << 2 | spread3(dy) << 1 | spread3(dz);
+        if (a.mode == 2)
+            key = d3 << 15 | e3;
+        else if (a.mode == 3)
+            key = e3 << 15 | d3;
+        else
+            key = spread6(qx) << 5 | spread6(qy) << 4 | spread6(qz) << 3 | spread6(dx) << 2 |
+                  spread6(dy) << 1 | spread6(dz);
+    }
+    const uint32_t b = key >> a.shift;
+    a.bucket[i] = b;
+    atomicAdd(a.count + b, 1u);
+}
+
+// Exclusive scan of count[0, m) in place, in tiles of 4096 (1024 threads x 4):
+// tile sums first, then the sums' scan, then the tiles.
+constexpr int kScanTile = 4096;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *sh,
+                                                         uint32_t *total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? sh[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o)
+                w += y;
+        }
+        if (lane < nw)
+            sh[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t before = (warp > 0 ? sh[warp - 1] : 0u) + x - v;
+    if (total)
+        *total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__global__ void k_scan_tile_sums(const uint32_t *count, int64_t m, uint32_t *sums) {
+    __shared__ uint32_t sh[32];
+    const int64_t base = (int64_t) blockIdx.x * kScanTile + (int64_t) threadIdx.x * 4;
+    uint32_t v = 0;
+    for (int k = 0; k < 4; k++)
+        if (base + k < m)
+            v += count[base + k];
+    uint32_t total = 0;
+    block_exclusive_scan(v, sh, &total);
+    if (threadIdx.x == 0)
+        sums[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of the tile sums (at most 1024 tiles)
+__global__ void k_scan_sums(uint32_t *sums, int tiles) {
+    __shared__ uint32_t sh[32];
+    const uint32_t v = (int) threadIdx.x < tiles ? sums[threadIdx.x] : 0u;
+    const uint32_t e = block_exclusive_scan(v, sh, nullptr);
+    if ((int) threadIdx.x < tiles)
+        sums[threadIdx.x] = e;
+}
+
+__global__ void k_scan_tiles(uint32_t *count, int64_t m, const uint32_t *sums) {
+    __shared__ uint32_t sh[32];
+    const int64_t base = (int64_t) blockIdx.x * kScanTile + (int64_t) threadIdx.x * 4;
+    uint32_t c[4], v = 0;
+    for (int k = 0; k < 4; k++) {
+        c[k] = base + k < m ? count[base + k] : 0u;
+        v += c[k];
+    }
+    uint32_t run = sums[blockIdx.x] + block_exclusive_scan(v, sh, nullptr);
+    for (int k = 0; k < 4; k++)
+        if (base + k < m) {
+            count[base + k] = run;
+            run += c[k];
+        }
+}
+
+__global__ void k_ray_scatter(const uint32_t *bucket, int64_t n, uint32_t *offset,
+                              uint32_t *perm) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t pos = atomicAdd(offset + bucket[i], 1u);
+    perm[pos] = (uint32_t) i;
+}
+
+// Bucket bits for n rays: about 8 rays per bucket, 2^8 .. 2^22 buckets (the
+// scan handles at most 1024 tiles of 4096).
+int ray_bucket_bits(int64_t n) {
+    int b = 0;
+    while (b < 30 && (int64_t(1) << b) < n)
+        b++;
+    return std::max(8, std::min(22, b - 3));
+}
+
+// Device bytes of the reordering scratch for n rays.
+size_t ray_order_bytes(int64_t n) {
+    const int64_t m = int64_t(1) << ray_bucket_bits(n);
+    const int64_t tiles = (m + kScanTile - 1) / kScanTile;
+    return (size_t) (2 * n + m + tiles) * sizeof(uint32_t);
+}
+
+// Fills perm[0, n) with the coherence order of the rays (scratch from
+// ray_order_bytes(n), which starts with perm).
+int ray_order(const float *o, const float *d, int64_t n, const float box[6], int mode,
+              void *scratch, cudaStream_t st) {
+    const int bits = ray_bucket_bits(n);
+    const int64_t m = int64_t(1) << bits;
+    const int64_t tiles = (m + kScanTile - 1) / kScanTile;
+    uint32_t *perm = (uint32_t *) scratch;
+    uint32_t *bucket = perm + n;
+    uint32_t *count = bucket + n;
+    uint32_t *sums = count + m;
+    RayKeyArgs a;
+    a.O = o;
+    a.D = d;
+    a.n = n;
+    for (int k = 0; k < 6; k++)
+        a.box[k] = box[k];
+    a.mode = mode;
+    a.shift = 30 - bits;
+    a.bucket = bucket;
+    a.count = count;
+    PRR_CUDA_TRY(cudaMemsetAsync(count, 0, (size_t) m * sizeof(uint32_t), st));
+    const unsigned g = (unsigned) ((n + 255) / 256);
+    k_ray_buckets<<<g, 256, 0, st>>>(a);
+    k_scan_tile_sums<<<(unsigned) tiles, 1024, 0, st>>>(count, m, sums);
+    k_scan_sums<<<1, 1024, 0, st>>>(sums, (int) tiles);
+    k_scan_tiles<<<(unsigned) tiles, 1024, 0, st>>>(count, m, sums);
+    k_ray_scatter<<<g, 256, 0, st>>>(bucket, n, count, perm);
+    PRR_CUDA_TRY(cudaGetLastError());
+    return PRR_OK;
+}
+
 int stack_cap(int depth) {
     // entries outstanding <= deepest leaf depth; keep one spare slot
     return std::max(1, depth + 1);
@@ -506,37 +720,11 @@ int device_sm_count() {
     return sms;
 }
 
-int launch_mesh_closest(const Scene &s, int object, const float *o, const float *d, int64_t n,
-                        int32_t *id, float *t, double *t64, unsigned *counter,
-                        const prr_trace_config *cfg, cudaStream_t st) {
-    if (n == 0)
-        return PRR_OK;
-    const HostObject &obj = s.objects[object];
-    const DevObject *dobj = nullptr;
-    (void) dobj;
-    MeshArgs a;
-    a.nodes = s.dev.nodes;
-    a.tris = s.dev.tris;
-    a.verts = s.dev.verts;
-    a.root = obj.root;
-    a.O = o;
-    a.D = d;
-    a.n = n;
-    a.out_id = id;
-    a.out_t = t;
-    a.out_t64 = t64;
-    a.counter = (unsigned long long *) counter;
-    const int block = (cfg && cfg->block_size > 0) ? cfg->block_size : 128;
-    if (block % 32 != 0 || block > 1024)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 <= 1024");
-    const int cap = stack_cap(obj.bvh.max_depth);
-    a.stack_stride = block;
-    const size_t smem = (size_t) cap * block * sizeof(uint2);
-    if (smem > 227 * 1024)
-        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
-    const int mode = cfg ? cfg->persistent : 0;
-    if (mode < 0 || mode > 3)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1, 2 or 3");
+namespace {
+
+// The traversal launch of launch_mesh_closest.
+int trace_mesh_closest(MeshArgs &a, int mode, int block, size_t smem, unsigned *counter,
+                       const prr_trace_config *cfg, int64_t n, cudaStream_t st) {
     if (mode > 0) {
         if (!counter)
             return fail(PRR_ERR_INVALID_ARGUMENT, "persistent launch needs a counter");
@@ -569,6 +757,65 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     }
     PRR_CUDA_TRY(cudaGetLastError());
     return PRR_OK;
+}
+
+} // namespace
+
+int launch_mesh_closest(const Scene &s, int object, const float *o, const float *d, int64_t n,
+                        int32_t *id, float *t, double *t64, unsigned *counter,
+                        const prr_trace_config *cfg, cudaStream_t st) {
+    if (n == 0)
+        return PRR_OK;
+    const HostObject &obj = s.objects[object];
+    const DevObject *dobj = nullptr;
+    (void) dobj;
+    MeshArgs a;
+    a.nodes = s.dev.nodes;
+    a.tris = s.dev.tris;
+    a.verts = s.dev.verts;
+    a.root = obj.root;
+    a.O = o;
+    a.D = d;
+    a.n = n;
+    a.out_id = id;
+    a.out_t = t;
+    a.out_t64 = t64;
+    a.counter = (unsigned long long *) counter;
+    a.perm = nullptr;
+    const int block = (cfg && cfg->block_size > 0) ? cfg->block_size : 128;
+    if (block % 32 != 0 || block > 1024)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 <= 1024");
+    const int cap = stack_cap(obj.bvh.max_depth);
+    a.stack_stride = block;
+    const size_t smem = (size_t) cap * block * sizeof(uint2);
+    if (smem > 227 * 1024)
+        return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
+    const int mode = cfg ? cfg->persistent : 0;
+    if (mode < 0 || mode > 3)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1, 2 or 3");
+    const int sort = cfg ? cfg->sort_rays : 0;
+    if (sort < 0 || sort > 3)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "sort_rays must be 0, 1, 2 or 3");
+    // reordering scratch from the library's stream-ordered pool, released on
+    // the stream after the traversal (concurrent calls get their own)
+    void *order = nullptr;
+    if (sort > 0 && n < (int64_t(1) << 31)) {
+        cudaMemPool_t pool;
+        PRR_CUDA_TRY(library_pool(&pool));
+        PRR_CUDA_TRY(cudaMallocFromPoolAsync(&order, ray_order_bytes(n), pool, st));
+        float box[6];
+        for (int k = 0; k < 6; k++)
+            box[k] = obj.bvh.bounds[k];
+        if (int rc = ray_order(o, d, n, box, sort, order, st)) {
+            cudaFreeAsync(order, st);
+            return rc;
+        }
+        a.perm = (const uint32_t *) order;
+    }
+    const int rc = trace_mesh_closest(a, mode, block, smem, counter, cfg, n, st);
+    if (order)
+        cudaFreeAsync(order, st);
+    return rc;
 }
 
 int launch_mesh_occluded(const Scene &s, int object, const float *o, const float *d,

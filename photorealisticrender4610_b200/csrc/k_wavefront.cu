@@ -98,7 +98,36 @@ struct Wf {
     WfReq *reqs;
     int n_reqs;
     int *req;
+    // traversal counts (kStat* slots), filled only by the counting variants of
+    // the extend and shadow stages
+    unsigned long long *stats;
 };
+
+// Slots of Wf::stats: traversal work of closest-hit (extend) and shadow rays
+// (interior nodes of either BVH level, triangle tests, object leaves: mesh
+// entries and sphere tests) and the extend results by class.
+enum : int {
+    kStatClosestNodes = 0, kStatClosestTris = 1, kStatClosestObjects = 2,
+    kStatShadowNodes = 3, kStatShadowTris = 4, kStatShadowObjects = 5,
+    kStatMiss = 6, kStatDelta = 7, kStatSurface = 8, kStatSlots = 9
+};
+static_assert(kStatSlots == kWfStatSlots, "counter slots of prr_render_counts");
+
+// Adds a lane's counts to the stats slots [slot, slot + n), one atomic per
+// slot per warp.
+template <int N>
+__device__ __forceinline__ void flush_stats(unsigned long long *stats, int slot,
+                                            const unsigned (&c)[N]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        unsigned long long v = c[k];
+        for (int off = 16; off > 0; off >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0 && v)
+            atomicAdd(stats + slot + k, v);
+    }
+}
 
 // Per-path scene, clamp and depth: the kernel's own for a render, the path's
 // request's for a server step.
@@ -268,7 +297,7 @@ __device__ __forceinline__ const DevScene &lane_scene(const DevScene &S0, const 
         return S0;
 }
 
-template <bool MULTI>
+template <bool MULTI, bool STATS>
 __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int it, int refill) {
     extern __shared__ uint2 smem[];
     StackCol<uint2> tc, bc;
@@ -281,14 +310,22 @@ __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int i
     // this lane's ray's scene (server steps; a valid scene before the first ray)
     const DevScene *ls = MULTI ? w.reqs[0].scene : nullptr;
     ClosestWalk cw;
+    unsigned cnt_[6] = {0, 0, 0, 0, 0, 0}; // nodes, tris, objects, miss, delta, surface
     bool more = n > 0;
     if (!more)
         return;
     for (;;) {
         const bool idle = p < 0;
         const unsigned im = __ballot_sync(full, idle);
-        if (!more && im == full)
+        if (!more && im == full) {
+            if constexpr (STATS) {
+                const unsigned a[3] = {cnt_[0], cnt_[1], cnt_[2]};
+                const unsigned b[3] = {cnt_[3], cnt_[4], cnt_[5]};
+                flush_stats(w.stats, kStatClosestNodes, a);
+                flush_stats(w.stats, kStatMiss, b);
+            }
             break;
+        }
         if (more && __popc(im) >= refill) {
             const int cnt = __popc(im);
             unsigned base = 0;
@@ -314,8 +351,13 @@ __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int i
         }
         bool done = false;
         const DevScene &S = lane_scene<MULTI>(S0, ls);
-        if (p >= 0)
+        if (p >= 0) {
+            if constexpr (STATS) {
+                if (S.n_objects > 0)
+                    cnt_[cw.in_mesh ? (cw.ntri > 0 ? 1 : 0) : ((cw.tref & kLeafBit) ? 2 : 0)]++;
+            }
             done = S.n_objects == 0 || cw.step(S, tc, bc);
+        }
         int cls = -1;
         if (done) {
             w.hit[p] = make_int4(cw.hit_obj, cw.hit_tri, __float_as_int(cw.closest), 0);
@@ -325,6 +367,8 @@ __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int i
                 const int kind = S.materials[S.objects[cw.hit_obj].material].kind;
                 cls = (kind == kMatMirror || kind == kMatGlass) ? 1 : 2;
             }
+            if constexpr (STATS)
+                cnt_[3 + cls]++;
         }
         if (w.ordered) {
             if (cls >= 0)
@@ -684,7 +728,7 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
 }
 
 // ---- shadow: visibility of every queued NEE ray (persistent, per-lane refill)
-template <bool MULTI>
+template <bool MULTI, bool STATS>
 __device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int refill) {
     extern __shared__ uint32_t smem32[];
     StackCol<uint32_t> tc, bc;
@@ -698,6 +742,7 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int r
     AnyWalk aw;
     bool more = n > 0;
     unsigned rays = 0;
+    unsigned cnt_[3] = {0, 0, 0}; // nodes, tris, objects
     for (;;) {
         const bool idle = job < 0;
         const unsigned im = __ballot_sync(full, idle);
@@ -733,11 +778,17 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int r
                 count_req_rays(w, full, take, r, 1);
         }
         const DevScene &S = lane_scene<MULTI>(S0, ls);
+        if constexpr (STATS) {
+            if (job >= 0)
+                cnt_[aw.in_mesh ? (aw.ntri > 0 ? 1 : 0) : ((aw.tref & kLeafBit) ? 2 : 0)]++;
+        }
         if (job >= 0 && aw.step(S, tc, bc)) {
             w.vis[job] = aw.occluded ? 0 : 1;
             job = -1;
         }
     }
+    if constexpr (STATS)
+        flush_stats(w.stats, kStatShadowNodes, cnt_);
     for (int off = 16; off > 0; off >>= 1)
         rays += __shfl_down_sync(full, rays, off);
     if (lane == 0 && rays)
@@ -745,11 +796,12 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int r
                   (unsigned long long) rays);
 }
 
-template <bool MULTI> __global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
-    wf_extend<MULTI>(S, w, it, refill);
+template <bool MULTI, bool STATS = false>
+__global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
+    wf_extend<MULTI, STATS>(S, w, it, refill);
 }
-template <bool MULTI> __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
-    wf_shadow<MULTI>(S, w, refill);
+template <bool MULTI, bool STATS = false> __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
+    wf_shadow<MULTI, STATS>(S, w, refill);
 }
 
 // ---- add the visible NEE contributions, light first, then env, as castRay
@@ -1194,6 +1246,12 @@ int wf_shape(Wf &w, DevBuf &spill, int block_req, int stack_req, int refill_req,
     L.smem_sh = (size_t) (w.tlas_cap + w.blas_sm) * L.block * sizeof(uint32_t);
     L.ext = k_wf_extend<MULTI>;
     L.sh = k_wf_shadow<MULTI>;
+    if constexpr (!MULTI) {
+        if (w.stats) { // the counting variants (a separate, untimed render)
+            L.ext = k_wf_extend<false, true>;
+            L.sh = k_wf_shadow<false, true>;
+        }
+    }
     if (L.smem_ext > 48 * 1024)
         PRR_CUDA_TRY(cudaFuncSetAttribute((const void *) L.ext,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1334,6 +1392,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.min_spp = rs.min_spp;
     w.max_spp = rs.max_spp;
     w.threshold = rs.variance_threshold;
+    w.stats = s.wf_stats;
     WfShape L;
     if (int rc = wf_shape<false>(w, s.d_wf_spill, s.wf_block, s.wf_stack, s.wf_refill, L))
         return rc;
@@ -1376,7 +1435,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     if (!s.wf_plan)
         s.wf_plan = std::make_shared<WavefrontPlan>();
     WavefrontPlan &plan = *s.wf_plan;
-    if (s.wf_graphs && passes > 1) {
+    if (s.wf_graphs && passes > 1 && !w.stats) {
         if (plan.key != key || !plan.exec) {
             if (plan.exec) {
                 cudaGraphExecDestroy(plan.exec);

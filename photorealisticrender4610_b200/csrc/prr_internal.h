@@ -17,11 +17,23 @@ namespace prr {
 // ---- error reporting: every ABI call returns a status and leaves a message
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
+
+// The library's stream-ordered memory pool of the current device (per-call
+// scratch of the caustic render and of ray reordering): freed blocks stay in
+// it for later calls. Created on first use, one per device.
+cudaError_t library_pool(cudaMemPool_t *out);
+
+// 64-bit traversal counters of a counting wavefront render (prr_render_counts)
+constexpr int kWfStatSlots = 9;
+// A failed allocation (cudaMalloc, a pool allocation) reports
+// PRR_ERR_OUT_OF_MEMORY; every other CUDA error PRR_ERR_CUDA.
 #define PRR_CUDA_TRY(expr)                                                                        \
     do {                                                                                         \
         cudaError_t e__ = (expr);                                                                \
         if (e__ != cudaSuccess)                                                                  \
-            return ::prr::fail(PRR_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+            return ::prr::fail(e__ == cudaErrorMemoryAllocation ? PRR_ERR_OUT_OF_MEMORY           \
+                                                                : PRR_ERR_CUDA,                   \
+                               std::string(#expr) + ": " + cudaGetErrorString(e__));             \
     } while (0)
 
 // Owning device allocation.
@@ -114,6 +126,7 @@ struct Scene {
     int wf_stack = 0;      // mesh-stack entries per thread in shared memory (0 = whole stack)
     bool wf_ordered = false; // queues rebuilt in path order by a stable partition
     DevBuf d_wf_spill;     // global part of the traversal stacks
+    unsigned long long *wf_stats = nullptr; // set by prr_render_counts: count traversal work
     int64_t last_launches = 0; // kernels the last prr_render launched
     // Renders reuse the scratch above; each render waits for the previous
     // one's event before touching it, whatever stream either ran on.

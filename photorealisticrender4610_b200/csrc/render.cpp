@@ -61,6 +61,50 @@ extern "C" int prr_render(prr_scene *scene, const prr_render_settings *settings,
     return rc;
 }
 
+extern "C" int prr_render_counts(prr_scene *scene, const prr_render_settings *settings,
+                                 float *out_rgb, prr_render_count *out, void *stream) {
+    if (!scene || !settings || !out_rgb || !out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "scene, settings, out_rgb and out are required");
+    Scene &s = *reinterpret_cast<Scene *>(scene);
+    if (!s.built)
+        return fail(PRR_ERR_NOT_BUILT, "scene not built (call prr_scene_build)");
+    prr_render_settings rs = *settings;
+    rs.mode = PRR_RENDER_WAVEFRONT;
+    if (int rc = validate_render(s, rs))
+        return rc;
+    std::lock_guard<std::mutex> g(s.mu);
+    cudaStream_t st = (cudaStream_t) stream;
+    if (!s.scratch_done)
+        PRR_CUDA_TRY(cudaEventCreateWithFlags(&s.scratch_done, cudaEventDisableTiming));
+    else
+        PRR_CUDA_TRY(cudaStreamWaitEvent(st, s.scratch_done, 0));
+    DevBuf buf;
+    PRR_CUDA_TRY(buf.alloc((kWfStatSlots + 2) * sizeof(unsigned long long)));
+    PRR_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, (kWfStatSlots + 2) * sizeof(unsigned long long), st));
+    unsigned long long *stats = buf.as<unsigned long long>();
+    s.wf_stats = stats;
+    const int rc = render_wavefront(s, rs, out_rgb, nullptr, stats + kWfStatSlots, st);
+    s.wf_stats = nullptr;
+    PRR_CUDA_TRY(cudaEventRecord(s.scratch_done, st));
+    if (rc)
+        return rc;
+    unsigned long long h[kWfStatSlots + 2];
+    PRR_CUDA_TRY(cudaMemcpyAsync(h, stats, sizeof(h), cudaMemcpyDeviceToHost, st));
+    PRR_CUDA_TRY(cudaStreamSynchronize(st));
+    out->closest_rays = h[kWfStatSlots];
+    out->closest_nodes = h[0];
+    out->closest_tris = h[1];
+    out->closest_objects = h[2];
+    out->shadow_rays = h[kWfStatSlots + 1];
+    out->shadow_nodes = h[3];
+    out->shadow_tris = h[4];
+    out->shadow_objects = h[5];
+    out->misses = h[6];
+    out->delta_hits = h[7];
+    out->surface_hits = h[8];
+    return PRR_OK;
+}
+
 extern "C" int prr_scene_set_wavefront(prr_scene *scene, const prr_wavefront_config *config) {
     if (!scene || !config)
         return fail(PRR_ERR_INVALID_ARGUMENT, "scene and config are required");

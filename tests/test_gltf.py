@@ -15,7 +15,7 @@ import gltf_writer
 import photorealisticrender4610_b200 as prr
 from oracle import loader
 
-REF_ASSETS = Path("/root/reference/assets/models")
+REF_ASSETS = loader.REFERENCE_ROOT / "assets" / "models"
 
 pytestmark = pytest.mark.skipif(not loader.reference_available(),
                                 reason="reference oracle library not built")

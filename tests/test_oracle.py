@@ -81,3 +81,29 @@ def test_photon_estimate_restatement(port, ref):
     b, rb = ref.photon_estimate(rec, 0.05, q)
     assert ra == rb
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("k", [1, 8, 64])
+def test_photon_knn_restatement(port, ref, k):
+    """The C restatement of the k-nearest-capped estimate against the same
+    definition over the reference's own PhotonGrid::query and
+    estimateIrradiance, bit for bit, with ties at the k-th distance (every
+    photon stored twice at one spot) and queries holding more than k."""
+    rng = np.random.default_rng(9)
+    rec = np.zeros((20000, 9), np.float32)
+    rec[:, :3] = rng.uniform(-1, 1, (20000, 3)) * np.array([1, 0.05, 1])
+    rec[:, 6:] = rng.uniform(0, 1e-3, (20000, 3))
+    rec = np.concatenate([rec, rec])
+    rec[20000:, 6:] *= 1.5
+    q = (rng.uniform(-1, 1, (3000, 3)) * np.array([1, 0.05, 1])).astype(np.float32)
+    a, ia = port.photon_estimate_knn(rec, 0.06, q, k)
+    b, ib = ref.photon_estimate_knn(rec, 0.06, q, k)
+    assert (ib > k).sum() > 300
+    assert np.array_equal(ia, ib)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    # k = 0 and queries with at most k inside: estimateIrradiance itself
+    f, _ = ref.photon_estimate(rec, 0.06, q)
+    few = ib <= k
+    assert np.array_equal(a[few].view(np.uint32), f[few].view(np.uint32))
+    z, _ = port.photon_estimate_knn(rec, 0.06, q, 0)
+    assert np.array_equal(z.view(np.uint32), f.view(np.uint32))

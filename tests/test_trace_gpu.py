@@ -24,7 +24,11 @@ def dev(a, cuda):
                                     {"persistent": 2, "batch": 32, "block_size": 64},
                                     {"persistent": 3}, {"persistent": 3, "leaf_batch": 1},
                                     {"persistent": 3, "leaf_batch": 32, "batch": 4},
-                                    {"persistent": 3, "leaf_batch": 8, "block_size": 256}])
+                                    {"persistent": 3, "leaf_batch": 8, "block_size": 256},
+                                    {"persistent": 2, "sort_rays": 1},
+                                    {"persistent": 2, "batch": 12, "sort_rays": 2},
+                                    {"persistent": 1, "sort_rays": 3},
+                                    {"sort_rays": 1}, {"persistent": 3, "sort_rays": 1}])
 def test_mesh_intersect_bit_exact(golden, cuda, case, config):
     g = golden("mesh")
     p = f"mesh_{case}_"
@@ -48,7 +52,8 @@ def test_mesh_occluded_bit_exact(golden, cuda, case):
     assert np.array_equal(occ.cpu().numpy(), g[p + "occ"])
 
 
-@pytest.mark.parametrize("config", [None, {"persistent": 2}, {"persistent": 3}])
+@pytest.mark.parametrize("config", [None, {"persistent": 2}, {"persistent": 3},
+                                    {"persistent": 2, "batch": 12, "sort_rays": 1}])
 def test_mesh_intersect_host_buffers(golden, cuda, config):
     g = golden("mesh")
     p = "mesh_q3000_"
@@ -89,7 +94,10 @@ def test_query_set_full_size_against_restatement(port, cuda):
     assert np.isnan(t64[~hit]).all()
     # the persistent launch shapes give the same answer
     for cfg in ({"persistent": 1}, {"persistent": 2}, {"persistent": 2, "batch": 16},
-                {"persistent": 3}, {"persistent": 3, "leaf_batch": 24}):
+                {"persistent": 3}, {"persistent": 3, "leaf_batch": 24},
+                {"persistent": 2, "batch": 12, "sort_rays": 1},
+                {"persistent": 2, "batch": 12, "sort_rays": 2},
+                {"persistent": 2, "batch": 12, "sort_rays": 3}):
         hid2, t2, t642 = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), t64=True, config=cfg)
         assert np.array_equal(hid2.cpu().numpy(), rh)
         assert np.array_equal(t2.cpu().numpy().view(np.uint32), rt.view(np.uint32))
@@ -181,7 +189,7 @@ def test_edge_and_vertex_ties_all_launch_shapes(port, cuda):
     s = prr.Scene.single_mesh(v)
     rh, rt, _ = port.mesh(v).intersect(o, d)
     for cfg in (None, {"persistent": 2}, {"persistent": 3}, {"persistent": 3, "leaf_batch": 1},
-                {"persistent": 3, "leaf_batch": 32}):
+                {"persistent": 3, "leaf_batch": 32}, {"persistent": 2, "sort_rays": 1}):
         hid, t = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), config=cfg)
         assert np.array_equal(hid.cpu().numpy(), rh), cfg
         assert np.array_equal(t.cpu().numpy().view(np.uint32), rt.view(np.uint32)), cfg

@@ -138,3 +138,59 @@ def test_wavefront_adaptive_equals_plain(cuda, name, paths_spp, ordered):
     assert spp.min() >= lo and spp.max() <= hi and spp.min() < spp.max()
     assert np.array_equal(out.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
     assert s.stats()["last_render_launches"] > 0
+
+
+def test_render_counts_match_oracle_traversal(port, cuda):
+    """prr_render_counts: the same image as prr_render in wavefront mode, and
+    traversal counts equal to the oracle's walk of the same rays. A mirror soup
+    at depth 1 traces exactly the camera rays (the ray a delta bounce leaves
+    after the last iteration is not traced), so every counted interior node and
+    triangle test can be checked against the C restatement's counting walk
+    (BVH.cpp:311-415) on those rays, taken from the camera with the first two
+    draws of each (pixel, sample) stream."""
+    verts, _, _ = scenes.query_set(20_000, 1, seed=11)
+    desc = scenes.SceneDesc(width=64, height=48, name="mirror soup")
+    m = desc.add_material(scenes.Material(scenes.MIRROR, (0.9, 0.9, 0.9), 0.0, 0.0))
+    desc.objects.append(scenes.MeshObject(verts, m))
+    desc.camera = scenes.Camera(eye=(2.2, 1.6, 2.4), target=(0.5, 0.5, 0.5), fovv=40, fovh=45)
+    s = prr.Scene.from_desc(desc)
+    spp, seed = 2, 5
+    img, c = s.render_counts(spp, 1, seed=seed)
+    want, _, rays = s.render(spp, 1, seed=seed, mode="wavefront", count_rays=True)
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), want.cpu().numpy().view(np.uint32))
+    rays = rays.cpu().numpy()
+    n = desc.width * desc.height * spp
+    assert c["closest_rays"] == rays[0] == n
+    assert c["shadow_rays"] == rays[1] == 0
+    assert c["misses"] + c["delta_hits"] + c["surface_hits"] == n
+    assert c["surface_hits"] == 0 and c["delta_hits"] > n // 4
+    px, py, smp = np.meshgrid(np.arange(desc.width), np.arange(desc.height), np.arange(spp),
+                              indexing="ij")
+    px, py, smp = px.ravel(), py.ravel(), smp.ravel()
+    draws = np.array([port.rng_stream(seed, int(i + j * desc.width), int(k), 2)
+                      for i, j, k in zip(px, py, smp)], np.float32)
+    o, d = s.camera_rays(px, py, draws[:, 0], draws[:, 1])
+    o, d = o.cpu().numpy(), d.cpu().numpy()
+    hid, _, _, vis, tst = port.mesh(verts).intersect(o, d, stats=True)
+    assert (hid >= 0).sum() == c["delta_hits"]
+    # one object (the scene BVH's root is the mesh's leaf): one entry per ray
+    assert c["closest_objects"] == n
+    assert c["closest_nodes"] == int(vis.sum())
+    assert c["closest_tris"] == int(tst.sum())
+
+
+def test_render_counts_two_level_consistency(cuda):
+    """On a scene of meshes, spheres, emitters and the sky: the counting render
+    equals the timed renderer's image bit for bit, and its ray totals and hit
+    classes add up."""
+    desc = scenes.museum_like(96, 54, level=3, env_size=(256, 128))
+    s = prr.Scene.from_desc(desc)
+    img, c = s.render_counts(4, 8, seed=2)
+    want, _, rays = s.render(4, 8, seed=2, mode="wavefront", count_rays=True)
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), want.cpu().numpy().view(np.uint32))
+    rays = rays.cpu().numpy()
+    assert c["closest_rays"] == rays[0] and c["shadow_rays"] == rays[1]
+    assert c["misses"] + c["delta_hits"] + c["surface_hits"] == c["closest_rays"]
+    assert c["closest_objects"] >= c["closest_rays"] - c["misses"]
+    assert c["closest_nodes"] > c["closest_rays"] and c["closest_tris"] > 0
+    assert c["shadow_nodes"] > 0 and c["shadow_tris"] > 0

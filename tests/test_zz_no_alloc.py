@@ -21,16 +21,20 @@ from photorealisticrender4610_b200.api import _ptr, _stream
 pytestmark = pytest.mark.gpu
 
 
-def test_render_noalloc_matches_render(cuda):
+@pytest.mark.parametrize("slices", [4, 16])
+def test_render_noalloc_matches_render(cuda, slices):
+    """With the same settings and the same explicit slice count (which fixes
+    the order in which each pixel's samples are summed), the image equals
+    prr_render's bit for bit, on two calls in a row."""
     lib = _lib.load()
     desc = scenes.cornell_box(96, 64)
     s = prr.Scene.from_desc(desc)
-    want, _ = s.render(16, 5, seed=1)  # the allocating entry point, plain mode
-    want = want.cpu().numpy()
     for window in [None, (8, 4, 72, 52)]:
-        rs = s._settings(16, 5, 1, None, 0.05, "plain", window, 10.0, 0, 0)
+        # the allocating entry point, plain mode, same window and slices
+        want, _ = s.render(16, 5, seed=1, window=window, slices=slices)
+        ref = want.cpu().numpy()
+        rs = s._settings(16, 5, 1, None, 0.05, "plain", window, 10.0, 0, slices)
         x0, y0, x1, y1 = window or (0, 0, desc.width, desc.height)
-        ref = want[y0:y1, x0:x1]
         for call in range(2):
             out = torch.full(((y1 - y0), (x1 - x0), 3), float("nan"), dtype=torch.float32,
                              device=cuda)
@@ -39,8 +43,8 @@ def test_render_noalloc_matches_render(cuda):
             assert rc == 0, _lib.last_error()
             torch.cuda.synchronize()
             got = out.cpu().numpy()
-            # same tolerance as the slice-invariance test of test_render_gpu.py
-            assert np.allclose(got, ref, rtol=1e-5, atol=1e-6), (window, call)
+            assert got.shape == ref.shape
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), (window, call)
             assert int(rays[0].item()) > 0
 
 
@@ -55,3 +59,9 @@ def test_render_noalloc_rejects_oversized_windows(cuda):
     assert "exceeds" in _lib.last_error()
     rs2 = s._settings(4, 5, 1, 2, 0.05, "plain", (0, 0, 32, 32), 10.0, 0, 0)
     assert lib.prr_render_noalloc(s.h, C.byref(rs2), _ptr(out), None, _stream(None)) == -5
+    # an explicit slice count is never cut silently: 1,000,000 pixels x 4 slices
+    # do not fit in the 2,097,152 partial sums
+    rs3 = s._settings(8, 5, 1, None, 0.05, "plain", (0, 0, 1000, 1000), 10.0, 0, 4)
+    rc = lib.prr_render_noalloc(s.h, C.byref(rs3), _ptr(out), None, _stream(None))
+    assert rc == _lib.PRR_OK - 1, _lib.last_error()
+    assert "slices" in _lib.last_error()
