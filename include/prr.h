@@ -229,6 +229,17 @@ int prr_scene_set_camera(prr_scene *scene, const prr_camera *camera, int width, 
  * device, EnvMap.hpp:189-224), and the upload of everything. */
 int prr_scene_build(prr_scene *scene, void *stream);
 int prr_scene_stats_get(const prr_scene *scene, prr_scene_stats *out);
+/* The device-side checks of the checked build (libprr_checked.so, compiled
+ * with -DPRR_CHECKED), no counterpart in the reference: every node and
+ * triangle fetch of the traversal kernels is tested against the array's
+ * length, every stack push against its column's depth (the tree depth + 1),
+ * every wavefront queue length and append against the queue's capacity. A
+ * failed test keeps the access in bounds and records out[0] = the first error
+ * (1 node index, 2 triangle index, 3 stack depth, 4 queue slot or length),
+ * out[1] = its offending value, out[2] = the number of failed tests, in the
+ * scene's status words. Waits for the device; reset != 0 clears the words.
+ * Returns 1 in the checked build, 0 in the normal one (whose words stay 0). */
+int prr_check_status(prr_scene *scene, uint32_t out[3], int reset);
 /* The reference-layout flattened tree of one mesh (object >= 0) or of the
  * scene BVH (object == -1): BVHNode bounds/first_child/meta, nodeAreas and
  * orderedPrims (BVH.hpp:34-67, :129-135). Any output may be NULL. Returns the

@@ -1,16 +1,20 @@
 """ctypes binding to libprr.so (the C ABI declared in include/prr.h).
 
 The library is built in-tree (``photorealisticrender4610_b200/build.py``).
-Loading fails loudly when it is missing: there is no CPU fallback.
+Loading fails loudly when it is missing: there is no CPU fallback. With
+PRR_LIBRARY=checked in the environment the checked build (libprr_checked.so,
+device-side bounds tests reported by prr_check_status) is loaded instead.
 """
 from __future__ import annotations
 
 import ctypes as C
+import os
 import re
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libprr.so"
+LIB_PATH = PKG / ("libprr_checked.so" if os.environ.get("PRR_LIBRARY") == "checked"
+                  else "libprr.so")
 HEADER_DIR = PKG.parent / "include"
 
 PRR_OK = 0
@@ -140,6 +144,7 @@ _SIGS = {
     "prr_render": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp, _vp, _vp, _vp]),
     "prr_render_counts": (C.c_int, [_vp, C.POINTER(prr_render_settings), _vp,
                                     C.POINTER(prr_render_count), _vp]),
+    "prr_check_status": (C.c_int, [_vp, _vp, C.c_int]),
     "prr_photon_map_create": (C.c_int, [C.POINTER(_vp)]),
     "prr_photon_map_destroy": (C.c_int, [_vp]),
     "prr_photon_emit": (C.c_int, [_vp, _vp, C.c_int64, C.c_uint64, C.c_int, _vp]),

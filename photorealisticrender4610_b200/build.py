@@ -20,6 +20,10 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libprr.so"
+# the checked build: the same sources with -DPRR_CHECKED (device-side bounds
+# tests on node, triangle, stack and queue indices, reported by prr_check_status)
+BUILD_CHECKED = PKG / "_build_checked"
+LIB_CHECKED = PKG / "libprr_checked.so"
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -56,36 +60,41 @@ def _run(cmd, verbose):
         sys.stderr.write(r.stdout + r.stderr)
 
 
-def build(verbose: bool = False, ptxas_verbose: bool = False, jobs: int = 8) -> Path:
-    """Compile every kernel and host unit and link libprr.so; returns its path."""
+def build(verbose: bool = False, ptxas_verbose: bool = False, jobs: int = 8,
+          checked: bool = False) -> Path:
+    """Compile every kernel and host unit and link libprr.so (checked=True:
+    libprr_checked.so with -DPRR_CHECKED); returns its path."""
     if not Path(NVCC).exists():
         raise RuntimeError(f"nvcc not found at {NVCC}")
-    BUILD.mkdir(exist_ok=True)
+    out_dir, lib = (BUILD_CHECKED, LIB_CHECKED) if checked else (BUILD, LIB)
+    define = ["-DPRR_CHECKED"] if checked else []
+    out_dir.mkdir(exist_ok=True)
     cu, cpp, headers = _sources()
     cmds, objs = [], []
     for src in cu:
-        obj = BUILD / (src.stem + ".cu.o")
+        obj = out_dir / (src.stem + ".cu.o")
         objs.append(obj)
         if _stale(obj, src, headers):
             extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-            cmds.append([NVCC, *ARCH, *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)])
+            cmds.append([NVCC, *ARCH, *NVCC_FLAGS, *define, *extra, "-c", str(src), "-o",
+                         str(obj)])
     for src in cpp:
-        obj = BUILD / (src.stem + ".o")
+        obj = out_dir / (src.stem + ".o")
         objs.append(obj)
         if _stale(obj, src, headers):
-            cmds.append([CXX, *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
+            cmds.append([CXX, *CXX_FLAGS, *define, "-c", str(src), "-o", str(obj)])
     if cmds:
         from concurrent.futures import ThreadPoolExecutor
         with ThreadPoolExecutor(max_workers=jobs) as ex:
             list(ex.map(lambda c: _run(c, verbose), cmds))
-    if cmds or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        tmp = LIB.with_suffix(".so.tmp")
+    if cmds or not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        tmp = lib.with_suffix(".so.tmp")
         _run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *map(str, objs),
               "-Xcompiler", "-pthread", "-lz"], verbose)
-        shutil.move(str(tmp), str(LIB))
-    return LIB
+        shutil.move(str(tmp), str(lib))
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, ptxas_verbose="--ptxas" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, ptxas_verbose="--ptxas" in sys.argv,
+                checked="--checked" in sys.argv))

@@ -50,16 +50,22 @@ struct alignas(64) WNode {
 static_assert(sizeof(WNode) == 64, "WNode must be 64 bytes");
 
 // One triangle in leaf order (orderedPrims order): v0, e1 = v1-v0, e2 = v2-v0
-// exactly as Triangle's constructor computes them (Triangle.hpp:27-31).
-struct alignas(16) Tri {
+// exactly as Triangle's constructor computes them (Triangle.hpp:27-31). The
+// intersection test reads 36 bytes: the first eight floats as one 32-byte
+// record (one memory sector), e2.z from a parallel float array (a sector there
+// covers eight neighbouring triangles, so a leaf's four usually share one).
+// The input id and the area live in a third array (TriMeta), read once per
+// hit or only by light sampling.
+struct alignas(32) Tri {
     float v0x, v0y, v0z, e1x;
     float e1y, e1z, e2x, e2y;
-    float e2z;
+};
+static_assert(sizeof(Tri) == 32, "Tri must be 32 bytes");
+
+struct TriMeta {
     int32_t id;         // index of the triangle in its mesh's input order
-    uint32_t reserved;
     float area;         // Triangle::area (Triangle.hpp:31)
 };
-static_assert(sizeof(Tri) == 48, "Tri must be 48 bytes");
 
 enum ObjectKind : int32_t { kObjMesh = 0, kObjSphere = 1 };
 enum MaterialKind : int32_t { kMatDiffuse = 0, kMatEmissive = 1, kMatMirror = 2, kMatGlass = 3 };
@@ -129,6 +135,8 @@ struct DevEnv {
 struct DevScene {
     const WNode *nodes;
     const Tri *tris;
+    const float *tri_e2z;      // e2.z of each triangle (completes Tri)
+    const TriMeta *tri_meta;   // input id and area of each triangle
     const float *verts;   // original v0,v1,v2 per triangle, leaf order (sampling, fp64 re-solve)
     const float *normals; // Triangle::normal per triangle, leaf order
     const DevObject *objects;
@@ -148,6 +156,10 @@ struct DevScene {
     float background[3];
     DevCamera camera;
     DevEnv env;
+    // bounds of the node and triangle arrays and the scene's status words,
+    // read only by the checked build (compiled with -DPRR_CHECKED)
+    uint32_t n_nodes, n_tris;
+    uint32_t *check;
 };
 
 } // namespace prr

@@ -25,7 +25,7 @@ __device__ __forceinline__ void finalize_attr(const DevScene &S, const DevObject
     if (!o.attr)
         return;
     float t, u, v;
-    tri_hit(load_tri(S.tris, (uint32_t) tri), r, t, u, v);
+    tri_hit(load_tri(S, (uint32_t) tri), r, t, u, v);
     const float w0 = 1.f - u - v;
     const float *R = S.attr + (size_t) (o.attr_base + (tri - o.tri_base)) * kAttrFloats;
     if (o.attr & kAttrUV) {

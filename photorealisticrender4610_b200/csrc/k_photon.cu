@@ -77,8 +77,9 @@ __device__ __forceinline__ V3 sample_cosine(V3 N, Rng &rng) {
 
 __global__ void k_photon_emit(DevScene S, EmitArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_photons)
         return;
@@ -462,8 +463,9 @@ struct CausticArgs {
 template <bool COUNT>
 __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t npix = (int64_t) a.ww * a.wh;
     const int64_t total = npix * a.chunk;
     float kd[kMaxK];

@@ -16,8 +16,9 @@ __global__ void k_cast_samples(DevScene S, const int32_t *__restrict__ px,
                                int64_t n, uint64_t seed, int max_depth, float clamp,
                                float *__restrict__ out, int tlas_cap) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n)
         return;
@@ -40,8 +41,9 @@ __global__ void k_cast_rays(DevScene S, const float *__restrict__ O, const float
                             int64_t n, uint64_t seed, int max_depth, float clamp,
                             float *__restrict__ out, int tlas_cap) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n)
         return;

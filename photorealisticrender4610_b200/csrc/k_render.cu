@@ -53,8 +53,9 @@ __device__ __forceinline__ void count_rays(unsigned long long *rays, const PathC
 
 __global__ void __launch_bounds__(kTileW *kTileH) k_render_plain(DevScene S, RenderArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int tiles_x = (a.ww + kTileW - 1) / kTileW;
     const int tile = blockIdx.x;
     const int lx = (tile % tiles_x) * kTileW + (int) (threadIdx.x % kTileW);
@@ -87,8 +88,9 @@ __global__ void __launch_bounds__(kTileW *kTileH) k_render_plain(DevScene S, Ren
 
 __global__ void __launch_bounds__(kTileW *kTileH) k_render_adaptive(DevScene S, RenderArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int tiles_x = (a.ww + kTileW - 1) / kTileW;
     const int tile = blockIdx.x;
     const int lx = (tile % tiles_x) * kTileW + (int) (threadIdx.x % kTileW);

@@ -48,6 +48,8 @@ __device__ double tri_t64(const float *__restrict__ v, const RayD &r) {
 struct MeshArgs {
     const WNode *nodes;
     const Tri *tris;
+    const float *e2z;
+    const TriMeta *meta;
     const float *verts;
     uint32_t root;
     const float *O, *D;
@@ -57,8 +59,29 @@ struct MeshArgs {
     double *out_t64;
     unsigned long long *counter;
     int stack_stride;
+    int stack_cap;        // entries of a thread's stack column
+    TraceBounds B;        // array bounds and status words (checked build)
     const uint32_t *perm; // trace order -> input index (nullptr: input order)
 };
+
+// Push onto this thread's stack column; the checked build tests the depth.
+#ifdef PRR_CHECKED
+#define PRR_COL_PUSH(val)                                                                          \
+    do {                                                                                           \
+        if (sp < a.stack_cap) {                                                                    \
+            col[sp * stride] = (val);                                                              \
+            sp++;                                                                                  \
+        } else {                                                                                   \
+            check_fail(a.B.check, kCheckStack, (uint32_t) sp);                                     \
+        }                                                                                          \
+    } while (0)
+#else
+#define PRR_COL_PUSH(val)                                                                          \
+    do {                                                                                           \
+        col[sp * stride] = (val);                                                                  \
+        sp++;                                                                                      \
+    } while (0)
+#endif
 
 // Input index of the ray traced in position i.
 __device__ __forceinline__ int64_t ray_at(const MeshArgs &a, int64_t i) {
@@ -69,8 +92,8 @@ __device__ __forceinline__ void mesh_closest_one(const MeshArgs &a, SmemStack &s
     const RayD r = load_ray(a.O, a.D, i);
     const RayPre p = precompute(r);
     float t = kInf, u = 0.f, v = 0.f;
-    const int hit = blas_closest(a.nodes, a.tris, a.root, r, p, st, t, u, v);
-    a.out_id[i] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+    const int hit = blas_closest(a.nodes, a.tris, a.e2z, a.root, r, p, st, t, u, v, a.B);
+    a.out_id[i] = hit >= 0 ? __ldg(&a.meta[hit].id) : -1;
     a.out_t[i] = t;
     if (a.out_t64)
         a.out_t64[i] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r) : __longlong_as_double(0x7ff8000000000000LL);
@@ -78,7 +101,7 @@ __device__ __forceinline__ void mesh_closest_one(const MeshArgs &a, SmemStack &s
 
 __global__ void k_mesh_closest(MeshArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0, a.stack_cap, a.B.check};
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride)
         mesh_closest_one(a, st, ray_at(a, i));
@@ -88,7 +111,7 @@ __global__ void k_mesh_closest(MeshArgs a) {
 // are left. The counter is zeroed on the stream before the launch.
 __global__ void k_mesh_closest_persistent(MeshArgs a) {
     extern __shared__ uint2 smem[];
-    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0, a.stack_cap, a.B.check};
     const int lane = threadIdx.x & 31;
     for (;;) {
         unsigned long long base = 0;
@@ -162,7 +185,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
             continue;
         bool pop = false;
         if (ntri > 0) {
-            const TriV T = load_tri(a.tris, tri);
+            const TriV T = load_tri(a.tris, a.e2z, tri, a.B);
             float t, u, v;
             if (tri_hit(T, r, t, u, v) && t < best) {
                 best = t;
@@ -172,7 +195,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
             ntri--;
             pop = ntri == 0;
         } else {
-            const NodeV n = load_node(a.nodes, ref);
+            const NodeV n = load_node(a.nodes, ref, a.B);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             uint32_t next = 0;
@@ -180,8 +203,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
             if (tl <= tr) {
                 if (tl < best) {
                     if (tr < best) {
-                        col[sp * stride] = make_uint2(n.link.y, __float_as_uint(tr));
-                        sp++;
+                        PRR_COL_PUSH(make_uint2(n.link.y, __float_as_uint(tr)));
                     }
                     next = n.link.x;
                     down = true;
@@ -189,8 +211,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
             } else {
                 if (tr < best) {
                     if (tl < best) {
-                        col[sp * stride] = make_uint2(n.link.x, __float_as_uint(tl));
-                        sp++;
+                        PRR_COL_PUSH(make_uint2(n.link.x, __float_as_uint(tl)));
                     }
                     next = n.link.y;
                     down = true;
@@ -227,7 +248,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
                     ref = next;
                 }
             } else {
-                a.out_id[idx] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+                a.out_id[idx] = hit >= 0 ? __ldg(&a.meta[hit].id) : -1;
                 a.out_t[idx] = best;
                 if (a.out_t64)
                     a.out_t64[idx] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r)
@@ -308,7 +329,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
             if (tw) {
                 if (pt < best) {
                     pt = -kInf; // the leaf passed; its other triangles follow unconditionally
-                    const TriV T = load_tri(a.tris, ptri);
+                    const TriV T = load_tri(a.tris, a.e2z, ptri, a.B);
                     float t, u, v;
                     if (tri_hit(T, r, t, u, v) && t < best) {
                         best = t;
@@ -322,7 +343,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
             }
         } else if (nw) {
             if (ref != kNoRef && !(ref & kLeafBit)) {
-                const NodeV n = load_node(a.nodes, ref);
+                const NodeV n = load_node(a.nodes, ref, a.B);
                 const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
                 const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
                 uint32_t next = kNoRef;
@@ -330,8 +351,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
                 if (tl <= tr) {
                     if (tl < best) {
                         if (tr < best) {
-                            col[sp * stride] = make_uint2(n.link.y, __float_as_uint(tr));
-                            sp++;
+                            PRR_COL_PUSH(make_uint2(n.link.y, __float_as_uint(tr)));
                         }
                         next = n.link.x;
                         next_t = tl;
@@ -339,8 +359,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
                 } else {
                     if (tr < best) {
                         if (tl < best) {
-                            col[sp * stride] = make_uint2(n.link.x, __float_as_uint(tl));
-                            sp++;
+                            PRR_COL_PUSH(make_uint2(n.link.x, __float_as_uint(tl)));
                         }
                         next = n.link.y;
                         next_t = tr;
@@ -365,7 +384,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
             }
         }
         if (act && ref == kNoRef && sp == 0 && pcnt == 0) {
-            a.out_id[idx] = hit >= 0 ? __ldg(&a.tris[hit].id) : -1;
+            a.out_id[idx] = hit >= 0 ? __ldg(&a.meta[hit].id) : -1;
             a.out_t[idx] = best;
             if (a.out_t64)
                 a.out_t64[idx] = hit >= 0 ? tri_t64(a.verts + (size_t) hit * 9, r)
@@ -375,16 +394,20 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
     }
 }
 
-__global__ void k_mesh_occluded(const WNode *nodes, const Tri *tris, uint32_t root,
+__global__ void k_mesh_occluded(const WNode *nodes, const Tri *tris, const float *e2z,
+                                uint32_t root,
                                 DevObject obj, const float *O, const float *D,
-                                const float *__restrict__ tmax, int64_t n, uint8_t *out) {
+                                const float *__restrict__ tmax, int64_t n, uint8_t *out,
+                                TraceBounds B, int stack_cap) {
     extern __shared__ uint2 smem[];
-    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack st{smem + threadIdx.x, (int) blockDim.x, 0, stack_cap, B.check};
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const RayD r = load_ray(O, D, i);
         const RayPre p = precompute(r);
-        out[i] = blas_occluded(nodes, tris, root, obj.root_box, r, p, st, __ldg(tmax + i)) ? 1 : 0;
+        out[i] = blas_occluded(nodes, tris, e2z, root, obj.root_box, r, p, st, __ldg(tmax + i), B)
+                     ? 1
+                     : 0;
     }
 }
 
@@ -392,8 +415,9 @@ __global__ void k_scene_closest(DevScene S, const float *O, const float *D, int6
                                 int32_t *out_obj, int32_t *out_prim, float *out_t, float *geo,
                                 int tlas_cap) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const RayD r = load_ray(O, D, i);
@@ -410,14 +434,14 @@ __global__ void k_scene_closest(DevScene S, const float *O, const float *D, int6
         const float cx = r.ox + r.dx * h.t, cy = r.oy + r.dy * h.t, cz = r.oz + r.dz * h.t;
         float nx, ny, nz;
         if (o.kind == kObjMesh) {
-            out_prim[i] = __ldg(&S.tris[h.tri].id);
+            out_prim[i] = __ldg(&S.tri_meta[h.tri].id);
             nx = S.normals[(size_t) h.tri * 3 + 0];
             ny = S.normals[(size_t) h.tri * 3 + 1];
             nz = S.normals[(size_t) h.tri * 3 + 2];
             if (o.attr & kAttrNormals) {
                 // Triangle::finalize (Triangle.cpp:44-47): normalize(n0*w0 + n1*u + n2*v)
                 float t, u, v;
-                tri_hit(load_tri(S.tris, (uint32_t) h.tri), r, t, u, v);
+                tri_hit(load_tri(S, (uint32_t) h.tri), r, t, u, v);
                 const float w0 = 1.f - u - v;
                 const float *R = S.attr + (size_t) (o.attr_base + (h.tri - o.tri_base)) * kAttrFloats;
                 float x = R[0] * w0 + R[3] * u + R[6] * v;
@@ -464,8 +488,9 @@ __global__ void k_scene_occluded(DevScene S, const float *O, const float *D,
                                  const float *__restrict__ tmax, int64_t n, uint8_t *out,
                                  int tlas_cap) {
     extern __shared__ uint2 smem[];
-    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0};
-    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0};
+    SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
+    SmemStack bst{smem + (size_t) tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,
+                  S.blas_depth + 1, S.check};
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const RayD r = load_ray(O, D, i);
@@ -682,6 +707,10 @@ int ray_order(const float *o, const float *d, int64_t n, const float box[6], int
     return PRR_OK;
 }
 
+TraceBounds host_bounds(const DevScene &S) {
+    return TraceBounds{S.n_nodes, S.n_tris, S.check};
+}
+
 int stack_cap(int depth) {
     // entries outstanding <= deepest leaf depth; keep one spare slot
     return std::max(1, depth + 1);
@@ -772,6 +801,8 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     MeshArgs a;
     a.nodes = s.dev.nodes;
     a.tris = s.dev.tris;
+    a.e2z = s.dev.tri_e2z;
+    a.meta = s.dev.tri_meta;
     a.verts = s.dev.verts;
     a.root = obj.root;
     a.O = o;
@@ -787,6 +818,8 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
         return fail(PRR_ERR_INVALID_ARGUMENT, "block_size must be a multiple of 32 <= 1024");
     const int cap = stack_cap(obj.bvh.max_depth);
     a.stack_stride = block;
+    a.stack_cap = cap;
+    a.B = host_bounds(s.dev);
     const size_t smem = (size_t) cap * block * sizeof(uint2);
     if (smem > 227 * 1024)
         return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
@@ -832,8 +865,11 @@ int launch_mesh_occluded(const Scene &s, int object, const float *o, const float
         return fail(PRR_ERR_UNSUPPORTED, "BVH too deep for the shared-memory stack");
     if (int rc = set_smem((const void *) k_mesh_occluded, smem))
         return rc;
-    k_mesh_occluded<<<grid_for(n, block), block, smem, st>>>(s.dev.nodes, s.dev.tris, obj.root,
-                                                             dobj, o, d, tmax, n, hit);
+    k_mesh_occluded<<<grid_for(n, block), block, smem, st>>>(s.dev.nodes, s.dev.tris,
+                                                             s.dev.tri_e2z, obj.root,
+                                                             dobj, o, d, tmax, n, hit,
+                                                             host_bounds(s.dev),
+                                                             stack_cap(obj.bvh.max_depth));
     PRR_CUDA_TRY(cudaGetLastError());
     return PRR_OK;
 }

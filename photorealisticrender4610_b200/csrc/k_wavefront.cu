@@ -101,7 +101,37 @@ struct Wf {
     // traversal counts (kStat* slots), filled only by the counting variants of
     // the extend and shadow stages
     unsigned long long *stats;
+    uint32_t *check; // status words of the checked build (nullptr: not reported)
 };
+
+// q[slot] = v for an appended queue entry; the checked build tests the slot
+// against the queue's capacity (and drops and reports an entry beyond it).
+__device__ __forceinline__ void queue_put(const Wf &w, int *q, int slot, int64_t cap, int v) {
+#ifdef PRR_CHECKED
+    if (slot < 0 || (int64_t) slot >= cap) {
+        check_fail(w.check, kCheckQueue, (uint32_t) slot);
+        return;
+    }
+#endif
+    (void) w;
+    (void) cap;
+    q[slot] = v;
+}
+
+// A queue's length as a stage reads it. The checked build tests it against
+// the queue's capacity (and reports and clamps a longer one).
+__device__ __forceinline__ int queue_len(const Wf &w, unsigned n, int64_t cap) {
+#ifdef PRR_CHECKED
+    if ((int64_t) n > cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            check_fail(w.check, kCheckQueue, n);
+        return (int) cap;
+    }
+#endif
+    (void) w;
+    (void) cap;
+    return (int) n;
+}
 
 // Slots of Wf::stats: traversal work of closest-hit (extend) and shadow rays
 // (interior nodes of either BVH level, triangle tests, object leaves: mesh
@@ -284,9 +314,9 @@ __global__ void k_wf_begin(Wf w, int it) {
 template <class E>
 __device__ __forceinline__ void make_stacks(const Wf &w, E *smem, StackCol<E> &tc,
                                             StackCol<E> &bc) {
-    tc = StackCol<E>{smem + threadIdx.x, nullptr, w.tlas_cap};
+    tc = StackCol<E>{smem + threadIdx.x, nullptr, w.tlas_cap, w.tlas_cap, w.check};
     bc = StackCol<E>{smem + (size_t) w.tlas_cap * blockDim.x + threadIdx.x, (E *) w.spill,
-                     w.blas_sm};
+                     w.blas_sm, w.blas_cap, w.check};
 }
 
 template <bool MULTI>
@@ -303,7 +333,7 @@ __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int i
     StackCol<uint2> tc, bc;
     make_stacks(w, smem, tc, bc);
     const int *qin = w.qray[it & 1];
-    const int n = (int) w.cnt[kCntRay0 + (it & 1)];
+    const int n = queue_len(w, w.cnt[kCntRay0 + (it & 1)], w.P);
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int p = -1;
@@ -378,11 +408,11 @@ __device__ __forceinline__ void wf_extend(const DevScene &S0, const Wf &w, int i
             const int b = warp_append(w.cnt + kCntDelta, cls == 1);
             const int c = warp_append(w.cnt + kCntSurf, cls == 2);
             if (cls == 0)
-                w.qmiss[a] = p;
+                queue_put(w, w.qmiss, a, w.P, p);
             else if (cls == 1)
-                w.qdelta[b] = p;
+                queue_put(w, w.qdelta, b, w.P, p);
             else if (cls == 2)
-                w.qsurf[c] = p;
+                queue_put(w, w.qsurf, c, w.P, p);
         }
         if (done)
             p = -1;
@@ -496,7 +526,7 @@ __device__ __forceinline__ bool enter_iteration(const DevScene &S, const Wf &w, 
 
 // ---- miss: the path leaves the scene
 template <bool MULTI> __global__ void k_wf_miss(DevScene S0, Wf w) {
-    const int n = (int) w.cnt[kCntMiss];
+    const int n = queue_len(w, w.cnt[kCntMiss], w.P);
     const int stride = gridDim.x * blockDim.x;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const int p = w.qmiss[k];
@@ -517,7 +547,7 @@ template <bool MULTI> __global__ void k_wf_miss(DevScene S0, Wf w) {
 
 // ---- delta: one step of the specular chain
 template <bool MULTI> __global__ void k_wf_delta(DevScene S0, Wf w, int it_next) {
-    const int n = (int) w.cnt[kCntDelta];
+    const int n = queue_len(w, w.cnt[kCntDelta], w.P);
     int *qout = w.qray[it_next & 1];
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -571,7 +601,7 @@ template <bool MULTI> __global__ void k_wf_delta(DevScene S0, Wf w, int it_next)
         } else {
             const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
             if (cont)
-                qout[slot] = p;
+                queue_put(w, qout, slot, w.P, p);
         }
     }
 }
@@ -581,7 +611,7 @@ template <bool MULTI> __global__ void k_wf_delta(DevScene S0, Wf w, int it_next)
 // state and scene data, so resident warps matter more than a few spills.
 template <bool MULTI>
 __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it_next) {
-    const int n = (int) w.cnt[kCntSurf];
+    const int n = queue_len(w, w.cnt[kCntSurf], w.P);
     int *qout = w.qray[it_next & 1];
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -713,17 +743,17 @@ __global__ void __launch_bounds__(128, 8) k_wf_surface(DevScene S0, Wf w, int it
         } else {
             const int slot = warp_append(w.cnt + kCntRay0 + (it_next & 1), cont);
             if (cont)
-                qout[slot] = p;
+                queue_put(w, qout, slot, w.P, p);
         }
         const int sslot = warp_append(w.cnt + kCntShadow, shadow);
         if (shadow)
-            w.qshadow[sslot] = p;
+            queue_put(w, w.qshadow, sslot, w.P, p);
         const int j0 = warp_append(w.cnt + kCntShadowJobs, jl);
         if (jl)
-            w.qjob[j0] = p * 2;
+            queue_put(w, w.qjob, j0, 2 * (int64_t) w.P, p * 2);
         const int j1 = warp_append(w.cnt + kCntShadowJobs, je);
         if (je)
-            w.qjob[j1] = p * 2 + 1;
+            queue_put(w, w.qjob, j1, 2 * (int64_t) w.P, p * 2 + 1);
     }
 }
 
@@ -733,7 +763,7 @@ __device__ __forceinline__ void wf_shadow(const DevScene &S0, const Wf &w, int r
     extern __shared__ uint32_t smem32[];
     StackCol<uint32_t> tc, bc;
     make_stacks(w, smem32, tc, bc);
-    const int n = (int) w.cnt[kCntShadowJobs];
+    const int n = queue_len(w, w.cnt[kCntShadowJobs], 2 * (int64_t) w.P);
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int job = -1;
@@ -806,7 +836,7 @@ template <bool MULTI, bool STATS = false> __global__ void k_wf_shadow(DevScene S
 
 // ---- add the visible NEE contributions, light first, then env, as castRay
 template <bool MULTI> __global__ void k_wf_shadow_resolve(Wf w) {
-    const int n = (int) w.cnt[kCntShadow];
+    const int n = queue_len(w, w.cnt[kCntShadow], w.P);
     const int stride = gridDim.x * blockDim.x;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
         const int p = w.qshadow[k];
@@ -1393,6 +1423,7 @@ int render_wavefront(Scene &s, const prr_render_settings &rs, float *out_rgb, in
     w.max_spp = rs.max_spp;
     w.threshold = rs.variance_threshold;
     w.stats = s.wf_stats;
+    w.check = S.check;
     WfShape L;
     if (int rc = wf_shape<false>(w, s.d_wf_spill, s.wf_block, s.wf_stack, s.wf_refill, L))
         return rc;

@@ -110,13 +110,15 @@ struct Scene {
     int64_t n_tris = 0;
     size_t device_bytes = 0;
 
-    DevBuf d_nodes, d_tris, d_verts, d_normals, d_objects, d_materials, d_emissives;
+    DevBuf d_nodes, d_tris, d_tri_e2z, d_tri_meta, d_verts, d_normals, d_objects, d_materials,
+        d_emissives;
     std::vector<HostTexture> textures;
     DevBuf d_attr, d_texels, d_textures;
     DevBuf d_env_px, d_env_cdf, d_env_marginal, d_env_rowsin, d_env_guide;
     DevBuf d_scratch;      // staging for host-buffer entry points
     DevBuf d_render, d_render_spp; // per-slice partial sums / adaptive spp
     DevBuf d_counter;      // persistent-kernel work counters
+    DevBuf d_check;        // status words of the checked build's device-side tests
     DevBuf d_wavefront;    // wavefront path state, queues and film
     std::shared_ptr<WavefrontPlan> wf_plan; // captured pass graph
     int64_t wf_paths = 0;  // paths in flight per pass (0 = automatic)

@@ -205,6 +205,8 @@ int build_scene(Scene &s, cudaStream_t st) {
 
     // ---- device triangle arrays in leaf order ----
     std::vector<Tri> tris;
+    std::vector<float> tri_e2z;
+    std::vector<TriMeta> tri_meta;
     std::vector<float> verts, normals;
     std::vector<WNode> nodes;
     int64_t ntri = 0;
@@ -213,6 +215,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     if (ntri >= kMaxTriangles)
         return fail(PRR_ERR_UNSUPPORTED, "too many triangles (limit 2^29 per scene)");
     tris.resize(ntri);
+    tri_e2z.resize(ntri);
+    tri_meta.resize(ntri);
     verts.resize((size_t) ntri * 9);
     normals.resize((size_t) ntri * 3);
     int base = 0;
@@ -236,12 +240,12 @@ int build_scene(Scene &s, cudaStream_t st) {
             t.e1z = e1z;
             t.e2x = e2x;
             t.e2y = e2y;
-            t.e2z = e2z;
-            t.id = id;
-            t.reserved = 0;
+            tri_e2z[base + j] = e2z;
+            TriMeta &tm = tri_meta[base + j];
+            tm.id = id;
             const float cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z,
                         cz = e1x * e2y - e1y * e2x;
-            t.area = std::sqrt(cx * cx + cy * cy + cz * cz) * 0.5f;
+            tm.area = std::sqrt(cx * cx + cy * cy + cz * cz) * 0.5f;
             // normalize(crossProduct(e1, e2)) (Vector.hpp:103-111)
             const float m2 = cx * cx + cy * cy + cz * cz;
             float nx = cx, ny = cy, nz = cz;
@@ -402,6 +406,10 @@ int build_scene(Scene &s, cudaStream_t st) {
         return rc;
     if (int rc = upload(s.d_tris, tris))
         return rc;
+    if (int rc = upload(s.d_tri_e2z, tri_e2z))
+        return rc;
+    if (int rc = upload(s.d_tri_meta, tri_meta))
+        return rc;
     if (int rc = upload(s.d_verts, verts))
         return rc;
     if (int rc = upload(s.d_normals, normals))
@@ -417,6 +425,14 @@ int build_scene(Scene &s, cudaStream_t st) {
     std::memset(&D, 0, sizeof(D));
     D.nodes = s.d_nodes.as<WNode>();
     D.tris = s.d_tris.as<Tri>();
+    D.tri_e2z = s.d_tri_e2z.as<float>();
+    D.tri_meta = s.d_tri_meta.as<TriMeta>();
+    D.n_nodes = (uint32_t) nodes.size();
+    D.n_tris = (uint32_t) ntri;
+    // status words of the checked build's device-side tests (prr_check_status)
+    PRR_CUDA_TRY(s.d_check.alloc(4 * sizeof(uint32_t)));
+    PRR_CUDA_TRY(cudaMemset(s.d_check.ptr, 0, 4 * sizeof(uint32_t)));
+    D.check = s.d_check.as<uint32_t>();
     D.verts = s.d_verts.as<float>();
     D.normals = s.d_normals.as<float>();
     D.objects = s.d_objects.as<DevObject>();
@@ -479,7 +495,8 @@ int build_scene(Scene &s, cudaStream_t st) {
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     s.n_tris = ntri;
     s.device_bytes = s.d_attr.bytes + s.d_texels.bytes + s.d_textures.bytes +
-                     s.d_nodes.bytes + s.d_tris.bytes + s.d_verts.bytes + s.d_normals.bytes +
+                     s.d_nodes.bytes + s.d_tris.bytes + s.d_tri_e2z.bytes + s.d_tri_meta.bytes +
+                     s.d_verts.bytes + s.d_normals.bytes +
                      s.d_objects.bytes + s.d_materials.bytes + s.d_emissives.bytes +
                      s.d_env_px.bytes + s.d_env_cdf.bytes + s.d_env_marginal.bytes +
                      s.d_env_guide.bytes;
@@ -816,6 +833,24 @@ static int check_mesh(const prr_scene *scene, int object) {
     if (object < 0 || object >= (int) s->objects.size() || s->objects[object].kind != kObjMesh)
         return fail(PRR_ERR_INVALID_ARGUMENT, "object is not a mesh");
     return PRR_OK;
+}
+
+int prr_check_status(prr_scene *scene, uint32_t *out, int reset) {
+    if (int rc = check_scene(scene, true))
+        return rc;
+    Scene *s = S(scene);
+    uint32_t h[4] = {0, 0, 0, 0};
+    PRR_CUDA_TRY(cudaDeviceSynchronize());
+    PRR_CUDA_TRY(cudaMemcpy(h, s->d_check.ptr, sizeof(h), cudaMemcpyDeviceToHost));
+    if (out)
+        std::memcpy(out, h, 3 * sizeof(uint32_t));
+    if (reset)
+        PRR_CUDA_TRY(cudaMemset(s->d_check.ptr, 0, sizeof(h)));
+#ifdef PRR_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 int prr_mesh_intersect(const prr_scene *scene, int object, const float *o, const float *d,

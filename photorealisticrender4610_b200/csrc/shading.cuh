@@ -602,7 +602,7 @@ __device__ __forceinline__ LightPoint mesh_sample(const DevScene &S, const DevOb
             const uint32_t first = leaf_first(ref), cnt = leaf_count(ref);
             tri = first + cnt - 1;
             for (uint32_t i = 0; i < cnt; i++) {
-                p -= __ldg(&S.tris[first + i].area);
+                p -= __ldg(&S.tri_meta[first + i].area);
                 if (p <= 0.f || i == cnt - 1) {
                     tri = first + i;
                     break;

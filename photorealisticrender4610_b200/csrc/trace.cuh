@@ -12,6 +12,16 @@
 //
 // Stacks live in shared memory, one column per thread ([depth][block]
 // layout), so a warp's pushes and pops hit distinct banks.
+//
+// Checked build (-DPRR_CHECKED): every node and triangle fetch is tested
+// against the array's length and every stack push against the column's
+// depth. A failed test records an error code (first one wins), the offending
+// value and a count in the scene's status words and keeps the access in
+// bounds (an out-of-range node reads as two empty boxes, a triangle as a
+// degenerate one that never hits, an overflowing push is dropped), so the
+// kernel runs to its end and the host reads the status (prr_check_status).
+// Nothing traps and nothing waits. In the normal build the tests compile to
+// nothing.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -20,6 +30,28 @@
 namespace prr {
 
 #define kInf (__int_as_float(0x7f800000))
+
+// Error codes of the checked build's status words.
+enum : uint32_t { kCheckNode = 1, kCheckTri = 2, kCheckStack = 3, kCheckQueue = 4 };
+
+// status[0] = first error code, status[1] = its value, status[2] = errors seen
+__device__ __forceinline__ void check_fail(uint32_t *status, uint32_t code, uint32_t value) {
+    if (!status)
+        return;
+    if (atomicCAS(status, 0u, code) == 0u)
+        atomicExch(status + 1, value);
+    atomicAdd(status + 2, 1u);
+}
+
+// What a checked fetch tests against.
+struct TraceBounds {
+    uint32_t n_nodes, n_tris;
+    uint32_t *check;
+};
+
+__device__ __forceinline__ TraceBounds bounds_of(const DevScene &S) {
+    return TraceBounds{S.n_nodes, S.n_tris, S.check};
+}
 
 struct RayD {
     float ox, oy, oz;
@@ -92,13 +124,52 @@ struct TriV {
     float4 p, q, r;
 };
 
-__device__ __forceinline__ TriV load_tri(const Tri *tris, uint32_t idx) {
+__device__ __forceinline__ TriV load_tri(const Tri *tris, const float *e2z, uint32_t idx) {
     const float4 *t = reinterpret_cast<const float4 *>(tris + idx);
     TriV v;
     v.p = __ldg(t);
     v.q = __ldg(t + 1);
-    v.r = __ldg(t + 2);
+    v.r = make_float4(__ldg(e2z + idx), 0.f, 0.f, 0.f);
     return v;
+}
+
+// Checked forms: the plain fetch unless the build is checked and the index is
+// out of range.
+__device__ __forceinline__ NodeV load_node(const WNode *nodes, uint32_t idx,
+                                           const TraceBounds &B) {
+#ifdef PRR_CHECKED
+    if (idx >= B.n_nodes) {
+        check_fail(B.check, kCheckNode, idx);
+        NodeV n; // two empty boxes: no slab test enters them
+        n.a = make_float4(kInf, -kInf, kInf, -kInf);
+        n.b = make_float4(kInf, -kInf, kInf, -kInf);
+        n.c = make_float4(kInf, -kInf, kInf, -kInf);
+        n.link = make_uint4(0u, 0u, 0u, 0u);
+        return n;
+    }
+#endif
+    return load_node(nodes, idx);
+}
+
+__device__ __forceinline__ TriV load_tri(const Tri *tris, const float *e2z, uint32_t idx,
+                                         const TraceBounds &B) {
+#ifdef PRR_CHECKED
+    if (idx >= B.n_tris) {
+        check_fail(B.check, kCheckTri, idx);
+        TriV v; // all zero: det = 0 fails the parallel test
+        v.p = v.q = v.r = make_float4(0.f, 0.f, 0.f, 0.f);
+        return v;
+    }
+#endif
+    return load_tri(tris, e2z, idx);
+}
+
+__device__ __forceinline__ NodeV load_node(const DevScene &S, uint32_t idx) {
+    return load_node(S.nodes, idx, bounds_of(S));
+}
+
+__device__ __forceinline__ TriV load_tri(const DevScene &S, uint32_t idx) {
+    return load_tri(S.tris, S.tri_e2z, idx, bounds_of(S));
 }
 
 // Triangle::hitTest (Triangle.hpp:46-64), evaluated without early exits. The
@@ -161,17 +232,31 @@ template <class E> struct StackCol {
     E *sm;
     E *gl;
     int cap;
+    int total = 1 << 30;     // entries in both parts (tested by the checked build)
+    uint32_t *check = nullptr;
     __device__ __forceinline__ E *spill_at(int k) const {
         return gl + (size_t) (k - cap) * (gridDim.x * blockDim.x) + blockIdx.x * blockDim.x +
                threadIdx.x;
     }
     __device__ __forceinline__ void put(int k, E v) const {
+#ifdef PRR_CHECKED
+        if (k >= total || k < 0) {
+            check_fail(check, kCheckStack, (uint32_t) k);
+            return;
+        }
+#endif
         if (k < cap)
             sm[k * blockDim.x] = v;
         else
             *spill_at(k) = v;
     }
     __device__ __forceinline__ E get(int k) const {
+#ifdef PRR_CHECKED
+        if (k >= total || k < 0) {
+            check_fail(check, kCheckStack, (uint32_t) k);
+            return E{};
+        }
+#endif
         return k < cap ? sm[k * blockDim.x] : *spill_at(k);
     }
 };
@@ -181,7 +266,15 @@ struct SmemStack {
     uint2 *base; // &smem[tid]; entry k at base[k * stride]
     int stride;
     int sp;
+    int cap = 1 << 30;         // entries in the column (tested by the checked build)
+    uint32_t *check = nullptr; // where the checked build reports
     __device__ __forceinline__ void push(uint32_t ref, float t) {
+#ifdef PRR_CHECKED
+        if (sp >= cap) {
+            check_fail(check, kCheckStack, (uint32_t) sp);
+            return;
+        }
+#endif
         base[sp * stride] = make_uint2(ref, __float_as_uint(t));
         sp++;
     }
@@ -195,15 +288,17 @@ struct SmemStack {
 // best_t enters as +inf (every mesh-level search starts fresh, BVH.cpp:331).
 // Returns the winning triangle's global leaf-order index, or -1.
 __device__ __forceinline__ int blas_closest(const WNode *__restrict__ nodes,
-                                            const Tri *__restrict__ tris, uint32_t root,
+                                            const Tri *__restrict__ tris,
+                                            const float *__restrict__ e2z, uint32_t root,
                                             const RayD &r, const RayPre &p, SmemStack &st,
-                                            float &best_t, float &best_u, float &best_v) {
+                                            float &best_t, float &best_u, float &best_v,
+                                            const TraceBounds &B) {
     const int sp0 = st.sp;
     uint32_t ref = root;
     int hit = -1;
     for (;;) {
         if (!(ref & kLeafBit)) {
-            const NodeV n = load_node(nodes, ref);
+            const NodeV n = load_node(nodes, ref, B);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             if (tl <= tr) {
@@ -225,7 +320,7 @@ __device__ __forceinline__ int blas_closest(const WNode *__restrict__ nodes,
             const uint32_t first = leaf_first(ref);
             const uint32_t cnt = leaf_count(ref);
             for (uint32_t i = 0; i < cnt; i++) {
-                const TriV T = load_tri(tris, first + i);
+                const TriV T = load_tri(tris, e2z, first + i, B);
                 float t, u, v;
                 if (tri_hit(T, r, t, u, v) && t < best_t) {
                     best_t = t;
@@ -253,16 +348,18 @@ __device__ __forceinline__ int blas_closest(const WNode *__restrict__ nodes,
 // where the reference tests them (far child at push, near child at the top of
 // the next iteration), so exactly the same subtrees are entered.
 __device__ __forceinline__ bool blas_occluded(const WNode *__restrict__ nodes,
-                                              const Tri *__restrict__ tris, uint32_t root,
+                                              const Tri *__restrict__ tris,
+                                              const float *__restrict__ e2z, uint32_t root,
                                               const float *root_box, const RayD &r,
-                                              const RayPre &p, SmemStack &st, float tmax) {
+                                              const RayPre &p, SmemStack &st, float tmax,
+                                              const TraceBounds &B) {
     if (!(slab6(root_box, p) < tmax))
         return false;
     const int sp0 = st.sp;
     uint32_t ref = root;
     for (;;) {
         if (!(ref & kLeafBit)) {
-            const NodeV n = load_node(nodes, ref);
+            const NodeV n = load_node(nodes, ref, B);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             const uint32_t axis = n.link.z;
@@ -282,7 +379,7 @@ __device__ __forceinline__ bool blas_occluded(const WNode *__restrict__ nodes,
             const uint32_t first = leaf_first(ref);
             const uint32_t cnt = leaf_count(ref);
             for (uint32_t i = 0; i < cnt; i++) {
-                const TriV T = load_tri(tris, first + i);
+                const TriV T = load_tri(tris, e2z, first + i, B);
                 if (tri_occludes(T, r, tmax)) {
                     st.sp = sp0;
                     return true;
@@ -355,7 +452,7 @@ __device__ __forceinline__ SceneHit scene_closest(const DevScene &S, const RayD 
     uint32_t ref = S.tlas_root;
     for (;;) {
         if (!(ref & kLeafBit)) {
-            const NodeV n = load_node(S.nodes, ref);
+            const NodeV n = load_node(S, ref);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             if (tl <= tr) {
@@ -378,7 +475,8 @@ __device__ __forceinline__ SceneHit scene_closest(const DevScene &S, const RayD 
             const DevObject &o = S.objects[k];
             if (o.kind == kObjMesh) {
                 float t = kInf, u = 0.f, v = 0.f;
-                const int tri = blas_closest(S.nodes, S.tris, o.root, r, p, bst, t, u, v);
+                const int tri = blas_closest(S.nodes, S.tris, S.tri_e2z, o.root, r, p, bst, t, u, v,
+                                             bounds_of(S));
                 if (tri >= 0 && t < closest) {
                     closest = t;
                     h.obj = k;
@@ -425,7 +523,7 @@ __device__ __forceinline__ bool scene_occluded(const DevScene &S, const RayD &r,
     uint32_t ref = S.tlas_root;
     for (;;) {
         if (!(ref & kLeafBit)) {
-            const NodeV n = load_node(S.nodes, ref);
+            const NodeV n = load_node(S, ref);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             const uint32_t axis = n.link.z;
@@ -444,7 +542,8 @@ __device__ __forceinline__ bool scene_occluded(const DevScene &S, const RayD &r,
             const DevObject &o = S.objects[ref & ~kLeafBit];
             bool occ;
             if (o.kind == kObjMesh) {
-                occ = blas_occluded(S.nodes, S.tris, o.root, o.root_box, r, p, bst, tmax) &&
+                occ = blas_occluded(S.nodes, S.tris, S.tri_e2z, o.root, o.root_box, r, p, bst, tmax,
+                                    bounds_of(S)) &&
                       (1e-3f < tmax);
             } else {
                 float t;

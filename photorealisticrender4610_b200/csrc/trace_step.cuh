@@ -65,7 +65,7 @@ struct ClosestWalk {
         if (in_mesh) {
             bool pop = false;
             if (ntri > 0) {
-                const TriV T = load_tri(S.tris, tri);
+                const TriV T = load_tri(S, tri);
                 float t, u, v;
                 if (tri_hit(T, r, t, u, v) && t < bbest) {
                     bbest = t;
@@ -75,7 +75,7 @@ struct ClosestWalk {
                 ntri--;
                 pop = ntri == 0;
             } else {
-                const NodeV n = load_node(S.nodes, bref);
+                const NodeV n = load_node(S, bref);
                 const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
                 const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
                 if (tl <= tr) {
@@ -115,7 +115,7 @@ struct ClosestWalk {
             return scene_pop(tc);
         }
         if (!(tref & kLeafBit)) {
-            const NodeV n = load_node(S.nodes, tref);
+            const NodeV n = load_node(S, tref);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             if (tl <= tr) {
@@ -205,7 +205,7 @@ struct AnyWalk {
                                          const StackCol<uint32_t> &bc) {
         if (in_mesh) {
             if (ntri > 0) {
-                const TriV T = load_tri(S.tris, tri);
+                const TriV T = load_tri(S, tri);
                 if (tri_occludes(T, r, tmax)) {
                     // MeshTriangle::intersectT answers 1e-3; the scene-level
                     // caller then needs 1e-3 < tMax
@@ -221,7 +221,7 @@ struct AnyWalk {
                 if (ntri > 0)
                     return false;
             } else {
-                const NodeV n = load_node(S.nodes, bref);
+                const NodeV n = load_node(S, bref);
                 const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
                 const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
                 const uint32_t axis = n.link.z;
@@ -246,7 +246,7 @@ struct AnyWalk {
             return scene_pop(tc);
         }
         if (!(tref & kLeafBit)) {
-            const NodeV n = load_node(S.nodes, tref);
+            const NodeV n = load_node(S, tref);
             const float tl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, p);
             const float tr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, p);
             const uint32_t axis = n.link.z;

@@ -20,6 +20,18 @@ def test_exports_every_declared_symbol(lib):
     assert lib.prr_abi_version() == 1
 
 
+def test_checked_build_exports_every_declared_symbol():
+    """The checked build (device-side bounds tests) is the same ABI."""
+    import ctypes
+    from photorealisticrender4610_b200 import build
+    if not build.LIB_CHECKED.exists():
+        pytest.skip("checked library not built")
+    lib = ctypes.CDLL(str(build.LIB_CHECKED))
+    missing = [n for n in prr.header_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert lib.prr_abi_version() == 1
+
+
 def test_error_paths(lib):
     s = prr.Scene()
     with pytest.raises(prr.PrrError, match="NOT_BUILT"):
