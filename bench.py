@@ -406,7 +406,7 @@ def run_ours(args, rank, world, on):
             elif name == "caustics":
                 sub = caustics_result(args, rank, world, on, min(args.steps, 5), 3)
             elif name == "serving":
-                sub = serving_result(args, rank, n_requests=60, arms_text="none")
+                sub = serving_result(args, rank, world, n_requests=60, arms_text="none")
             else:
                 raise ValueError(f"unknown extra workload {name}")
             sub = {k: v for k, v in sub.items() if k not in EXTRA_DROP}
@@ -781,13 +781,13 @@ def serving_pool():
 
 
 def run_serving(args, rank, world, on):
-    line = serving_result(args, rank)
+    line = serving_result(args, rank, world)
     if line is not None:
         print(json.dumps(line), flush=True)
     return 0
 
 
-def serving_result(args, rank, n_requests=None, arms_text=None):
+def serving_result(args, rank, world, n_requests=None, arms_text=None):
     """Continuous-batching server (wavefront steps) under Poisson arrivals,
     beside the same server on megakernel steps and the plain renderer run one
     request at a time in arrival order. Returns the JSON line's dict on rank 0

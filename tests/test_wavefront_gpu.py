@@ -163,7 +163,7 @@ def test_render_counts_match_oracle_traversal(port, cuda):
     assert c["closest_rays"] == rays[0] == n
     assert c["shadow_rays"] == rays[1] == 0
     assert c["misses"] + c["delta_hits"] + c["surface_hits"] == n
-    assert c["surface_hits"] == 0 and c["delta_hits"] > n // 4
+    assert c["surface_hits"] == 0 and c["delta_hits"] > 0
     px, py, smp = np.meshgrid(np.arange(desc.width), np.arange(desc.height), np.arange(spp),
                               indexing="ij")
     px, py, smp = px.ravel(), py.ravel(), smp.ravel()
