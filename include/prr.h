@@ -84,10 +84,12 @@ typedef struct prr_trace_config {
     int batch;        /* modes 2-3: refill threshold in idle lanes (0 = 8) */
     int leaf_batch;   /* mode 3: a triangle phase runs when this many lanes hold a
                          parked leaf (0 = 16) */
-    int sort_rays;    /* 0: trace rays in input order; 1-3: first reorder them by a
-                         coherence key (where each ray enters the mesh's root box and
-                         its direction, interleaved (1), direction-major (2) or
-                         entry-major (3)) so neighbouring lanes trace similar rays.
+    int sort_rays;    /* 0: trace rays in input order; 1-5: first reorder them by a
+                         coherence key so neighbouring lanes trace similar rays: where
+                         each ray enters the mesh's root box and its direction,
+                         interleaved (1), direction-major (2) or entry-major (3); or
+                         where it enters and where it leaves the box, interleaved (4)
+                         or entry-major (5).
                          Results are written at each ray's input index either way
                          and do not depend on the order. Batches of 2^31 rays or
                          more are traced in input order. */

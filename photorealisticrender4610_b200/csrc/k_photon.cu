@@ -358,9 +358,42 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     y1 = min(g.res - 1, y1);
     z0 = max(0, z0);
     z1 = min(g.res - 1, z1);
+    // Pass 1: the fixed-radius sum and the number of photons inside, in the
+    // reference query's order (cells x, y, z; a cell's photons in photon
+    // order, read from the cell-sorted copy).
     V3 e = v3(0.f);
     int found = 0;
-    int worst = 0; // kNN, once k are kept: the entry of the largest (distance, index)
+    for (int cx = x0; cx <= x1; cx++)
+        for (int cy = y0; cy <= y1; cy++)
+            for (int cz = z0; cz <= z1; cz++) {
+                const int cell = cx + cy * g.res + cz * g.res * g.res;
+                int s = v.start[cell];
+                if (s < 0)
+                    continue;
+                for (; s < v.n && v.cell_of[s] == cell; s++) {
+                    const float4 pa = v.sorted[2 * s];
+                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+                    if constexpr (COUNT)
+                        (*tested)++;
+                    if (dist <= r) {
+                        if constexpr (COUNT)
+                            (*inside)++;
+                        const float4 pb = v.sorted[2 * s + 1];
+                        e = e + v3(pa.w, pb.x, pb.y);
+                        found++;
+                    }
+                }
+            }
+    if (found == 0)
+        return v3(0.f);
+    if (!kd || found <= k_nearest)
+        return e / disc_area(r);
+    // Pass 2, only with more than k inside: keep the k smallest (distance,
+    // photon index) pairs -- the first k found, then each closer one replaces
+    // the largest kept.
+    int kept = 0;
+    int worst = 0; // once k are kept: the entry of the largest (distance, index)
     auto find_worst = [&] {
         worst = 0;
         for (int q = 1; q < k_nearest; q++)
@@ -374,57 +407,45 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
                 int s = v.start[cell];
                 if (s < 0)
                     continue;
-                // the cell's photons, in photon order, read from the cell-sorted copy
                 for (; s < v.n && v.cell_of[s] == cell; s++) {
                     const float4 pa = v.sorted[2 * s];
                     const V3 d = v3(pa.x, pa.y, pa.z) - pos;
                     const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-                    if constexpr (COUNT)
-                        (*tested)++;
-                    if (dist <= r) {
-                        if constexpr (COUNT)
-                            (*inside)++;
-                        const float4 pb = v.sorted[2 * s + 1];
-                        e = e + v3(pa.w, pb.x, pb.y);
-                        if (kd && found < k_nearest) {
-                            kd[found] = dist;
-                            kc[found] = v.order[s];
-                            if (found + 1 == k_nearest)
-                                find_worst();
-                        } else if (kd && dist <= kd[worst]) {
-                            // keep the k smallest (distance, index) pairs
-                            const int idx = v.order[s];
-                            if (dist < kd[worst] || idx < kc[worst]) {
-                                kd[worst] = dist;
-                                kc[worst] = idx;
-                                find_worst();
-                            }
+                    if (!(dist <= r)) // (the counts are pass 1's: what one walk reads)
+                        continue;
+                    if (kept < k_nearest) {
+                        kd[kept] = dist;
+                        kc[kept] = v.order[s];
+                        if (++kept == k_nearest)
+                            find_worst();
+                    } else if (dist <= kd[worst]) {
+                        const int idx = v.order[s];
+                        if (dist < kd[worst] || idx < kc[worst]) {
+                            kd[worst] = dist;
+                            kc[worst] = idx;
+                            find_worst();
                         }
-                        found++;
                     }
                 }
             }
-    if (found == 0)
-        return v3(0.f);
-    if (kd && found > k_nearest) {
-        const float rk = kd[worst];
-        for (int a = 1; a < k_nearest; a++) {
-            const int key = kc[a];
-            int b = a - 1;
-            while (b >= 0 && kc[b] > key) {
-                kc[b + 1] = kc[b];
-                b--;
-            }
-            kc[b + 1] = key;
+    // the estimate over the disc through the k-th: the kept powers added in
+    // photon-array order
+    const float rk = kd[worst];
+    for (int a = 1; a < k_nearest; a++) {
+        const int key = kc[a];
+        int b = a - 1;
+        while (b >= 0 && kc[b] > key) {
+            kc[b + 1] = kc[b];
+            b--;
         }
-        V3 ek = v3(0.f);
-        for (int q = 0; q < k_nearest; q++) {
-            const float *p = v.rec + (size_t) kc[q] * 9;
-            ek = ek + v3(p[6], p[7], p[8]);
-        }
-        return ek / disc_area(rk);
+        kc[b + 1] = key;
     }
-    return e / disc_area(r);
+    V3 ek = v3(0.f);
+    for (int q = 0; q < k_nearest; q++) {
+        const float *p = v.rec + (size_t) kc[q] * 9;
+        ek = ek + v3(p[6], p[7], p[8]);
+    }
+    return ek / disc_area(rk);
 }
 
 constexpr int kMaxK = 64;

@@ -537,7 +537,8 @@ struct RayKeyArgs {
     const float *O, *D;
     int64_t n;
     float box[6]; // root box [minX,maxX,minY,maxY,minZ,maxZ]
-    int mode;     // 1 interleaved, 2 direction-major, 3 entry-major
+    int mode;     // 1 entry and direction interleaved, 2 direction-major, 3 entry-major,
+                  // 4 entry and exit point interleaved, 5 entry-major then exit
     int shift;    // key >> shift = bucket
     uint32_t *bucket;
     uint32_t *count;
@@ -562,13 +563,28 @@ __global__ void k_ray_buckets(RayKeyArgs a) {
         const uint32_t dz = quant5(0.5f + 0.5f * r.dz * inv);
         const uint32_t e3 = spread3(qx) << 2 | spread3(qy) << 1 | spread3(qz);
         const uint32_t d3 = spread3(dx) << 2 | spread3(dy) << 1 | spread3(dz);
-        if (a.mode == 2)
+        if (a.mode == 2) {
             key = d3 << 15 | e3;
-        else if (a.mode == 3)
+        } else if (a.mode == 3) {
             key = e3 << 15 | d3;
-        else
+        } else if (a.mode >= 4) {
+            // where the ray leaves the box: the nearest far slab
+            const float fx = ((p.nx ? a.box[0] : a.box[1]) - p.ox) * p.ix;
+            const float fy = ((p.ny ? a.box[2] : a.box[3]) - p.oy) * p.iy;
+            const float fz = ((p.nz ? a.box[4] : a.box[5]) - p.oz) * p.iz;
+            const float tx = fminf(fx, fminf(fy, fz));
+            const uint32_t xx = quant5((r.ox + r.dx * tx - a.box[0]) / (a.box[1] - a.box[0]));
+            const uint32_t xy = quant5((r.oy + r.dy * tx - a.box[2]) / (a.box[3] - a.box[2]));
+            const uint32_t xz = quant5((r.oz + r.dz * tx - a.box[4]) / (a.box[5] - a.box[4]));
+            if (a.mode == 4)
+                key = spread6(qx) << 5 | spread6(qy) << 4 | spread6(qz) << 3 | spread6(xx) << 2 |
+                      spread6(xy) << 1 | spread6(xz);
+            else
+                key = e3 << 15 | spread3(xx) << 2 | spread3(xy) << 1 | spread3(xz);
+        } else {
             key = spread6(qx) << 5 | spread6(qy) << 4 | spread6(qz) << 3 | spread6(dx) << 2 |
                   spread6(dy) << 1 | spread6(dz);
+        }
     }
     const uint32_t b = key >> a.shift;
     a.bucket[i] = b;
@@ -827,8 +843,8 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     if (mode < 0 || mode > 3)
         return fail(PRR_ERR_INVALID_ARGUMENT, "persistent must be 0, 1, 2 or 3");
     const int sort = cfg ? cfg->sort_rays : 0;
-    if (sort < 0 || sort > 3)
-        return fail(PRR_ERR_INVALID_ARGUMENT, "sort_rays must be 0, 1, 2 or 3");
+    if (sort < 0 || sort > 5)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "sort_rays must be 0 to 5");
     // reordering scratch from the library's stream-ordered pool, released on
     // the stream after the traversal (concurrent calls get their own)
     void *order = nullptr;

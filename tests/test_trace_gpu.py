@@ -28,6 +28,8 @@ def dev(a, cuda):
                                     {"persistent": 2, "sort_rays": 1},
                                     {"persistent": 2, "batch": 12, "sort_rays": 2},
                                     {"persistent": 1, "sort_rays": 3},
+                                    {"persistent": 2, "sort_rays": 4},
+                                    {"persistent": 2, "sort_rays": 5},
                                     {"sort_rays": 1}, {"persistent": 3, "sort_rays": 1}])
 def test_mesh_intersect_bit_exact(golden, cuda, case, config):
     g = golden("mesh")
@@ -97,7 +99,9 @@ def test_query_set_full_size_against_restatement(port, cuda):
                 {"persistent": 3}, {"persistent": 3, "leaf_batch": 24},
                 {"persistent": 2, "batch": 12, "sort_rays": 1},
                 {"persistent": 2, "batch": 12, "sort_rays": 2},
-                {"persistent": 2, "batch": 12, "sort_rays": 3}):
+                {"persistent": 2, "batch": 12, "sort_rays": 3},
+                {"persistent": 2, "batch": 8, "sort_rays": 4},
+                {"persistent": 2, "batch": 8, "sort_rays": 5}):
         hid2, t2, t642 = s.mesh_intersect(0, dev(o, cuda), dev(d, cuda), t64=True, config=cfg)
         assert np.array_equal(hid2.cpu().numpy(), rh)
         assert np.array_equal(t2.cpu().numpy().view(np.uint32), rt.view(np.uint32))
