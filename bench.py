@@ -290,7 +290,7 @@ def run_ours(args, rank, world, on):
             configs.append({"block_size": block, "persistent": 3, "batch": 8, "leaf_batch": leaf})
     # the same launch shapes after a coherence reordering of the rays (inside
     # the timed call)
-    for sort in (1, 2, 3):
+    for sort in (1, 3, 4, 5):
         for refill in (8, 12, 16):
             configs.append({"block_size": 128, "persistent": 2, "batch": refill, "sort_rays": sort})
         configs.append({"block_size": 128, "persistent": 1, "sort_rays": sort})
