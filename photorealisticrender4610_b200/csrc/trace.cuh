@@ -110,13 +110,29 @@ struct NodeV {
     uint4 link;
 };
 
+// 32 bytes from 32-byte aligned read-only global memory in one load
+// instruction (sm_100's 256-bit vector load): half a node, or a whole Tri
+// record. Builds with -DPRR_LDG128 use two 128-bit loads instead.
+__device__ __forceinline__ void ldg256(const void *p, float4 &lo, float4 &hi) {
+#ifdef PRR_LDG128
+    lo = __ldg(reinterpret_cast<const float4 *>(p));
+    hi = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+#else
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(lo.x), "=f"(lo.y), "=f"(lo.z), "=f"(lo.w), "=f"(hi.x), "=f"(hi.y), "=f"(hi.z),
+          "=f"(hi.w)
+        : "l"(p));
+#endif
+}
+
 __device__ __forceinline__ NodeV load_node(const WNode *nodes, uint32_t idx) {
-    const float4 *q = reinterpret_cast<const float4 *>(nodes + idx);
+    const WNode *q = nodes + idx;
     NodeV n;
-    n.a = __ldg(q);
-    n.b = __ldg(q + 1);
-    n.c = __ldg(q + 2);
-    n.link = __ldg(reinterpret_cast<const uint4 *>(q + 3));
+    float4 l;
+    ldg256(q, n.a, n.b);
+    ldg256(reinterpret_cast<const float4 *>(q) + 2, n.c, l);
+    n.link = make_uint4(__float_as_uint(l.x), __float_as_uint(l.y), __float_as_uint(l.z),
+                        __float_as_uint(l.w));
     return n;
 }
 
@@ -125,10 +141,8 @@ struct TriV {
 };
 
 __device__ __forceinline__ TriV load_tri(const Tri *tris, const float *e2z, uint32_t idx) {
-    const float4 *t = reinterpret_cast<const float4 *>(tris + idx);
     TriV v;
-    v.p = __ldg(t);
-    v.q = __ldg(t + 1);
+    ldg256(tris + idx, v.p, v.q);
     v.r = make_float4(__ldg(e2z + idx), 0.f, 0.f, 0.f);
     return v;
 }
