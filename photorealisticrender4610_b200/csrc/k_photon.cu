@@ -233,9 +233,18 @@ __global__ void k_gather_records(const unsigned long long *keys, const float *sr
 }
 
 // ---------------------------------------------------------------- grid
+// kOccWords 32-bit words hold one bit per slab of an axis (res <= 200)
+constexpr int kOccWords = 7;
+
 struct GridParams {
     float bmin[3], bmax[3], cs[3];
     int res;
+    // occupancy of the grid's slabs along x, y and z: bit c of occ[a] is set
+    // when some photon lies in a cell whose coordinate on axis a is c. A cell
+    // can hold photons only if its three slabs are occupied, so the gathers
+    // skip the other cells without reading the cell table (the same cells in
+    // the same order as the reference's walk, minus ones known to be empty).
+    uint32_t occ[3][kOccWords];
 };
 
 __global__ void k_bounds(const float *rec, int64_t n, float *partial) {
@@ -278,6 +287,8 @@ __global__ void k_grid_params(const float *partial, int nb, float radius, GridPa
     for (int k = 0; k < 3; k++) {
         g->bmin[k] = mn[k] - 0.01f;
         g->bmax[k] = mx[k] + 0.01f;
+        for (int w = 0; w < kOccWords; w++)
+            g->occ[k][w] = 0u;
     }
     const float ex = g->bmax[0] - g->bmin[0], ey = g->bmax[1] - g->bmin[1],
                 ez = g->bmax[2] - g->bmin[2];
@@ -301,6 +312,21 @@ __global__ void k_cell_keys(const float *rec, int64_t n, const GridParams *g,
     const int cz = (int) (float) (int) ((rec[i * 9 + 2] - g->bmin[2]) / g->cs[2]);
     const unsigned cell = (unsigned) (cx + cy * res + cz * res * res);
     keys[i] = ((unsigned long long) cell << 32) | (unsigned long long) i;
+}
+
+// the slabs each photon's cell occupies (one atomic per axis per photon whose
+// cell differs from its predecessor's in the sorted order)
+__global__ void k_cell_occupancy(const unsigned long long *keys, int64_t n, GridParams *g) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned cell = (unsigned) (keys[i] >> 32);
+    if (i > 0 && (unsigned) (keys[i - 1] >> 32) == cell)
+        return;
+    const unsigned res = (unsigned) g->res;
+    const unsigned c[3] = {cell % res, (cell / res) % res, cell / (res * res)};
+    for (int a = 0; a < 3; a++)
+        atomicOr(&g->occ[a][c[a] >> 5], 1u << (c[a] & 31));
 }
 
 __global__ void k_cell_table(const unsigned long long *keys, const float *rec, int64_t n,
@@ -341,6 +367,40 @@ __device__ __forceinline__ float disc_area(float r) {
 // the k-th distance keep the lower photon index whatever the walk order --
 // and the disc through the k-th one: sum / (pi r_k^2), the kept photons added
 // in photon-array order.
+// The first occupied slab of an axis in [c, hi], or hi + 1.
+__device__ __forceinline__ int next_slab(const uint32_t *occ, int c, int hi) {
+    while (c <= hi) {
+        const uint32_t w = occ[c >> 5] >> (c & 31);
+        if (w) {
+            c += __ffs(w) - 1;
+            return c <= hi ? c : hi + 1;
+        }
+        c = (c | 31) + 1;
+    }
+    return hi + 1;
+}
+
+// Calls f(s) for every photon of the cells in the box [x0,x1] x [y0,y1] x
+// [z0,z1], in the reference query's order (cells by x, then y, then z; a
+// cell's photons in photon order; s indexes the cell-sorted arrays). Slabs
+// without photons are skipped before the cell table is read.
+template <class F>
+__device__ __forceinline__ void walk_cells(const GridView &v, const GridParams &g, int x0, int x1,
+                                           int y0, int y1, int z0, int z1, F &&f) {
+    for (int cx = next_slab(g.occ[0], x0, x1); cx <= x1; cx = next_slab(g.occ[0], cx + 1, x1))
+        for (int cy = next_slab(g.occ[1], y0, y1); cy <= y1;
+             cy = next_slab(g.occ[1], cy + 1, y1))
+            for (int cz = next_slab(g.occ[2], z0, z1); cz <= z1;
+                 cz = next_slab(g.occ[2], cz + 1, z1)) {
+                const int cell = cx + cy * g.res + cz * g.res * g.res;
+                int s = v.start[cell];
+                if (s < 0)
+                    continue;
+                for (; s < v.n && v.cell_of[s] == cell; s++)
+                    f(s);
+            }
+}
+
 template <bool COUNT = false>
 __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc,
                          unsigned *tested = nullptr, unsigned *inside = nullptr) {
@@ -359,39 +419,30 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     z0 = max(0, z0);
     z1 = min(g.res - 1, z1);
     // Pass 1: the fixed-radius sum and the number of photons inside, in the
-    // reference query's order (cells x, y, z; a cell's photons in photon
-    // order, read from the cell-sorted copy).
+    // reference query's order.
     V3 e = v3(0.f);
     int found = 0;
-    for (int cx = x0; cx <= x1; cx++)
-        for (int cy = y0; cy <= y1; cy++)
-            for (int cz = z0; cz <= z1; cz++) {
-                const int cell = cx + cy * g.res + cz * g.res * g.res;
-                int s = v.start[cell];
-                if (s < 0)
-                    continue;
-                for (; s < v.n && v.cell_of[s] == cell; s++) {
-                    const float4 pa = v.sorted[2 * s];
-                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-                    if constexpr (COUNT)
-                        (*tested)++;
-                    if (dist <= r) {
-                        if constexpr (COUNT)
-                            (*inside)++;
-                        const float4 pb = v.sorted[2 * s + 1];
-                        e = e + v3(pa.w, pb.x, pb.y);
-                        found++;
-                    }
-                }
-            }
+    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+        const float4 pa = v.sorted[2 * s];
+        const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+        const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        if constexpr (COUNT)
+            (*tested)++;
+        if (dist <= r) {
+            if constexpr (COUNT)
+                (*inside)++;
+            const float4 pb = v.sorted[2 * s + 1];
+            e = e + v3(pa.w, pb.x, pb.y);
+            found++;
+        }
+    });
     if (found == 0)
         return v3(0.f);
     if (!kd || found <= k_nearest)
         return e / disc_area(r);
     // Pass 2, only with more than k inside: keep the k smallest (distance,
     // photon index) pairs -- the first k found, then each closer one replaces
-    // the largest kept.
+    // the largest kept. (The counts are pass 1's: what one walk reads.)
     int kept = 0;
     int worst = 0; // once k are kept: the entry of the largest (distance, index)
     auto find_worst = [&] {
@@ -400,34 +451,26 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
             if (kd[q] > kd[worst] || (kd[q] == kd[worst] && kc[q] > kc[worst]))
                 worst = q;
     };
-    for (int cx = x0; cx <= x1; cx++)
-        for (int cy = y0; cy <= y1; cy++)
-            for (int cz = z0; cz <= z1; cz++) {
-                const int cell = cx + cy * g.res + cz * g.res * g.res;
-                int s = v.start[cell];
-                if (s < 0)
-                    continue;
-                for (; s < v.n && v.cell_of[s] == cell; s++) {
-                    const float4 pa = v.sorted[2 * s];
-                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-                    if (!(dist <= r)) // (the counts are pass 1's: what one walk reads)
-                        continue;
-                    if (kept < k_nearest) {
-                        kd[kept] = dist;
-                        kc[kept] = v.order[s];
-                        if (++kept == k_nearest)
-                            find_worst();
-                    } else if (dist <= kd[worst]) {
-                        const int idx = v.order[s];
-                        if (dist < kd[worst] || idx < kc[worst]) {
-                            kd[worst] = dist;
-                            kc[worst] = idx;
-                            find_worst();
-                        }
-                    }
-                }
+    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+        const float4 pa = v.sorted[2 * s];
+        const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+        const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        if (!(dist <= r))
+            return;
+        if (kept < k_nearest) {
+            kd[kept] = dist;
+            kc[kept] = v.order[s];
+            if (++kept == k_nearest)
+                find_worst();
+        } else if (dist <= kd[worst]) {
+            const int idx = v.order[s];
+            if (dist < kd[worst] || idx < kc[worst]) {
+                kd[worst] = dist;
+                kc[worst] = idx;
+                find_worst();
             }
+        }
+    });
     // the estimate over the disc through the k-th: the kept powers added in
     // photon-array order
     const float rk = kd[worst];
@@ -815,6 +858,8 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     k_cell_table<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
         keys, pm.rec.as<float>(), n, pm.order.as<int32_t>(), pm.cell_of.as<int32_t>(),
         pm.start.as<int32_t>(), pm.sorted.as<float4>());
+    k_cell_occupancy<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(keys, n,
+                                                                     pm.params.as<GridParams>());
     PRR_CUDA_TRY(cudaGetLastError());
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     pm.res = g.res;
