@@ -519,11 +519,13 @@ struct CausticArgs {
     int s0, chunk;   // this launch's samples [s0, s0 + chunk) of each pixel
     unsigned long long *stats; // counting variant: camera hits, gathers, photons
                                // tested, photons inside the radius
+    unsigned long long *next;  // work counter of this launch (zeroed before it)
 };
 
-// One thread per (pixel, sample): sample n of window pixel q is item
-// n * npix + q, so neighbouring threads trace neighbouring pixels and the
-// uneven cost of gathers in and out of the caustics spreads over the grid.
+// One (pixel, sample) item per thread at a time: sample n of window pixel q is
+// item n * npix + q, so a warp's lanes trace neighbouring pixels; its result
+// goes to slot n * npix + q, so the image does not depend on which thread
+// took which item.
 template <bool COUNT>
 __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     extern __shared__ uint2 smem[];
@@ -535,8 +537,21 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     float kd[kMaxK];
     int kc[kMaxK];
     unsigned cnt_[4] = {0, 0, 0, 0}; // hits, gathers, photons tested, photons inside
-    for (int64_t t = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t) gridDim.x * blockDim.x) {
+    // Persistent warps take the next 32 items from the launch's counter: a
+    // sample through the glass sphere or with a dense k-nearest gather costs
+    // many times a plain floor hit, so a fixed share per thread would leave
+    // most warps waiting on a few slow ones.
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long base = 0;
+        if (lane == 0)
+            base = atomicAdd(a.next, 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if ((int64_t) base >= total)
+            break;
+        const int64_t t = (int64_t) base + lane;
+        if (t >= total)
+            continue;
         const int nc = (int) (t / npix);
         const int q = (int) (t - (int64_t) nc * npix);
         const int n = a.s0 + nc;
@@ -698,10 +713,13 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
     cudaMemPool_t pool;
     PRR_CUDA_TRY(library_pool(&pool));
     PRR_CUDA_TRY(cudaMallocFromPoolAsync((void **) &scratch,
-                                         (size_t) items * sizeof(float4) + acc_bytes, pool, st));
+                                         (size_t) items * sizeof(float4) + acc_bytes + 256, pool,
+                                         st));
     a.samples = reinterpret_cast<float4 *>(scratch);
     a.acc = acc_bytes ? reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4))
                       : nullptr;
+    a.next = reinterpret_cast<unsigned long long *>(scratch + (size_t) items * sizeof(float4) +
+                                                    acc_bytes);
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
     cudaError_t e = cudaSuccess;
@@ -709,10 +727,13 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
         a.s0 = s0;
         a.chunk = std::min(chunk, a.spp - s0);
         const int64_t total = npix * a.chunk;
-        const int64_t grid = std::min<int64_t>(
-            (total + block - 1) / block, (int64_t) device_sm_count() * std::max(1, bps) * 8);
-        kern<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
-        e = cudaGetLastError();
+        const int64_t grid = std::min<int64_t>((total + block - 1) / block,
+                                               (int64_t) device_sm_count() * std::max(1, bps));
+        e = cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess) {
+            kern<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
+            e = cudaGetLastError();
+        }
         if (e == cudaSuccess) {
             k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
             e = cudaGetLastError();
