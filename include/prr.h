@@ -328,8 +328,8 @@ int prr_photon_export(const prr_photon_map *map, float *records, int32_t *owner,
  * sum of the powers within the radius over pi r^2. k_nearest > 0 (<= 64) caps
  * it: with more than k photons in the radius, the powers of the k nearest
  * (the k smallest (distance, photon index) pairs: of photons at equal distance
- * the lower index is kept), added in photon order, over the disc through the
- * k-th; identical to the fixed radius otherwise. */
+ * the lower index is kept), added in the order the grid query walks them, over
+ * the disc through the k-th; identical to the fixed radius otherwise. */
 int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n, int k_nearest,
                       float *out_rgb, void *stream);
 /* Caustic image: for every (pixel, sample) the camera ray follows the specular

@@ -904,8 +904,8 @@ void prr_oracle_env_cdf(const float *rgb, int w, int h, float *cdf, float *margi
 /* ------------------------------------------------------------------------ */
 /* Photon grid + fixed-radius irradiance (Photon.cpp:24-94), and the          */
 /* k-nearest-capped variant: with more than k photons inside the radius, the  */
-/* k smallest (distance, photon index) pairs, their powers added in photon    */
-/* order, over pi r_k^2 (r_k the k-th smallest distance).                     */
+/* k smallest (distance, photon index) pairs, their powers added in the walk  */
+/* order of the query, over pi r_k^2 (r_k the k-th smallest distance).        */
 /* ------------------------------------------------------------------------ */
 typedef struct {
     float d;
@@ -917,11 +917,6 @@ static int knn_cmp(const void *a, const void *b) {
     if (x->d != y->d)
         return x->d < y->d ? -1 : 1;
     return x->i < y->i ? -1 : (x->i > y->i);
-}
-
-static int idx_cmp(const void *a, const void *b) {
-    const int64_t x = *(const int64_t *) a, y = *(const int64_t *) b;
-    return x < y ? -1 : (x > y);
 }
 
 /* pi r^2 as estimateIrradiance writes it (Photon.cpp:87): float throughout, as
@@ -980,9 +975,9 @@ void prr_oracle_photon_estimate_knn(const float *rec, int64_t n, float radius, i
     const float area = disc_area(radius);
 #pragma omp parallel
     {
-        int64_t cap = 1024;
+        int64_t cap = 1024, sorted_cap = 0;
         knn_cand *cand = (knn_cand *) malloc(sizeof(knn_cand) * cap);
-        int64_t *keep = (int64_t *) malloc(sizeof(int64_t) * (k > 0 ? k : 1));
+        knn_cand *sorted = NULL;
 #pragma omp for schedule(dynamic, 256)
         for (int64_t j = 0; j < nq; j++) {
             v3 pos = mk(q[j * 3], q[j * 3 + 1], q[j * 3 + 2]);
@@ -1026,23 +1021,30 @@ void prr_oracle_photon_estimate_knn(const float *rec, int64_t n, float radius, i
             if (found == 0) {
                 e = mk(0.f, 0.f, 0.f);
             } else if (k > 0 && found > k) {
-                qsort(cand, (size_t) found, sizeof(knn_cand), knn_cmp);
-                for (int t = 0; t < k; t++)
-                    keep[t] = cand[t].i;
-                qsort(keep, (size_t) k, sizeof(int64_t), idx_cmp);
-                e = mk(0.f, 0.f, 0.f);
-                for (int t = 0; t < k; t++) {
-                    const float *p = rec + keep[t] * 9;
-                    e = add(e, mk(p[6], p[7], p[8]));
+                /* cand holds the candidates in walk order; the k-th smallest
+                 * pair by a sorted copy, then the walk-order sum of the pairs
+                 * at or below it */
+                if (sorted_cap < found) {
+                    sorted_cap = found;
+                    sorted = (knn_cand *) realloc(sorted, sizeof(knn_cand) * sorted_cap);
                 }
-                a = disc_area(cand[k - 1].d);
+                memcpy(sorted, cand, sizeof(knn_cand) * (size_t) found);
+                qsort(sorted, (size_t) found, sizeof(knn_cand), knn_cmp);
+                const knn_cand kth = sorted[k - 1];
+                e = mk(0.f, 0.f, 0.f);
+                for (int64_t t = 0; t < found; t++)
+                    if (knn_cmp(&cand[t], &kth) <= 0) {
+                        const float *p = rec + cand[t].i * 9;
+                        e = add(e, mk(p[6], p[7], p[8]));
+                    }
+                a = disc_area(kth.d);
             }
             out[j * 3] = e.x / a;
             out[j * 3 + 1] = e.y / a;
             out[j * 3 + 2] = e.z / a;
         }
         free(cand);
-        free(keep);
+        free(sorted);
     }
     free(cell);
     free(start);

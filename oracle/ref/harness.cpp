@@ -951,9 +951,10 @@ void prr_ref_photon_estimate(const float *rec, int64_t n, float radius, const fl
 //   <= k inside  PhotonMap::estimateIrradiance itself (Photon.cpp:82-94);
 //   > k inside   brute force over the candidates: the k smallest
 //                (distance, photon index) pairs, distance as the query
-//                computes it ((p - x).norm()), their powers added in photon
-//                order, divided by pi r_k^2 written as estimateIrradiance
-//                writes pi r^2, r_k the k-th smallest distance.
+//                computes it ((p - x).norm()), their powers added in the
+//                order the query returns them (as estimateIrradiance adds),
+//                divided by pi r_k^2 written as estimateIrradiance writes
+//                pi r^2, r_k the k-th smallest distance.
 // The photon index travels in the direction field (unused by the estimate).
 // ---------------------------------------------------------------------------
 struct KnnMap {
@@ -989,15 +990,14 @@ static Vector3f knn_estimate(const KnnMap &m, const Vector3f &pos, int k, int32_
     cand.clear();
     for (const Photon *p : near)
         cand.emplace_back((p->position - pos).norm(), (int32_t) p->direction.x);
-    std::sort(cand.begin(), cand.end());
-    const float rk = cand[k - 1].first;
-    std::vector<int32_t> keep(k);
-    for (int q = 0; q < k; q++)
-        keep[q] = cand[q].second;
-    std::sort(keep.begin(), keep.end());
+    std::vector<std::pair<float, int32_t>> sorted(cand);
+    std::sort(sorted.begin(), sorted.end());
+    const std::pair<float, int32_t> kth = sorted[k - 1];
+    const float rk = kth.first;
     Vector3f e = {};
-    for (int32_t i : keep)
-        e += m.power[i];
+    for (size_t q = 0; q < near.size(); q++)
+        if (cand[q] <= kth)
+            e += near[q]->power;
     float area = M_PI * rk * rk;
     return e / area;
 }

@@ -366,7 +366,7 @@ __device__ __forceinline__ float disc_area(float r) {
 // the k nearest -- the k smallest (distance, photon index) pairs, so ties at
 // the k-th distance keep the lower photon index whatever the walk order --
 // and the disc through the k-th one: sum / (pi r_k^2), the kept photons added
-// in photon-array order.
+// in the order the query walks them (as estimateIrradiance adds its photons).
 // The first occupied slab of an axis in [c, hi], or hi + 1.
 __device__ __forceinline__ int next_slab(const uint32_t *occ, int c, int hi) {
     while (c <= hi) {
@@ -440,54 +440,63 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
         return v3(0.f);
     if (!kd || found <= k_nearest)
         return e / disc_area(r);
-    // Pass 2, only with more than k inside: keep the k smallest (distance,
-    // photon index) pairs -- the first k found, then each closer one replaces
-    // the largest kept. (The counts are pass 1's: what one walk reads.)
-    int kept = 0;
-    int worst = 0; // once k are kept: the entry of the largest (distance, index)
-    auto find_worst = [&] {
-        worst = 0;
-        for (int q = 1; q < k_nearest; q++)
-            if (kd[q] > kd[worst] || (kd[q] == kd[worst] && kc[q] > kc[worst]))
-                worst = q;
+    // Pass 2, only with more than k inside: the k smallest (distance, photon
+    // index) pairs in a max-heap (the largest kept pair at its root), then
+    // pass 3 adds the powers of the photons at or below the root pair, in
+    // the walk's order, over the disc through the k-th.
+    auto below = [](float da, int ia, float db, int ib) {
+        return da < db || (da == db && ia < ib);
     };
+    int kept = 0;
     walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
         const float4 pa = v.sorted[2 * s];
         const V3 d = v3(pa.x, pa.y, pa.z) - pos;
         const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-        if (!(dist <= r))
+        if (!(dist <= r) || (kept == k_nearest && dist > kd[0]))
             return;
-        if (kept < k_nearest) {
-            kd[kept] = dist;
-            kc[kept] = v.order[s];
-            if (++kept == k_nearest)
-                find_worst();
-        } else if (dist <= kd[worst]) {
-            const int idx = v.order[s];
-            if (dist < kd[worst] || idx < kc[worst]) {
-                kd[worst] = dist;
-                kc[worst] = idx;
-                find_worst();
+        const int idx = v.order[s];
+        if (kept < k_nearest) { // push and sift up
+            int c = kept++;
+            while (c > 0) {
+                const int up = (c - 1) >> 1;
+                if (!below(kd[up], kc[up], dist, idx))
+                    break;
+                kd[c] = kd[up];
+                kc[c] = kc[up];
+                c = up;
             }
+            kd[c] = dist;
+            kc[c] = idx;
+        } else if (below(dist, idx, kd[0], kc[0])) { // replace the root and sift down
+            int c = 0;
+            for (;;) {
+                int m = 2 * c + 1;
+                if (m >= k_nearest)
+                    break;
+                if (m + 1 < k_nearest && below(kd[m], kc[m], kd[m + 1], kc[m + 1]))
+                    m++;
+                if (!below(dist, idx, kd[m], kc[m]))
+                    break;
+                kd[c] = kd[m];
+                kc[c] = kc[m];
+                c = m;
+            }
+            kd[c] = dist;
+            kc[c] = idx;
         }
     });
-    // the estimate over the disc through the k-th: the kept powers added in
-    // photon-array order
-    const float rk = kd[worst];
-    for (int a = 1; a < k_nearest; a++) {
-        const int key = kc[a];
-        int b = a - 1;
-        while (b >= 0 && kc[b] > key) {
-            kc[b + 1] = kc[b];
-            b--;
-        }
-        kc[b + 1] = key;
-    }
+    const float rk = kd[0];
+    const int ik = kc[0];
     V3 ek = v3(0.f);
-    for (int q = 0; q < k_nearest; q++) {
-        const float *p = v.rec + (size_t) kc[q] * 9;
-        ek = ek + v3(p[6], p[7], p[8]);
-    }
+    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+        const float4 pa = v.sorted[2 * s];
+        const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+        const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        if (dist < rk || (dist == rk && v.order[s] <= ik)) {
+            const float4 pb = v.sorted[2 * s + 1];
+            ek = ek + v3(pa.w, pb.x, pb.y);
+        }
+    });
     return ek / disc_area(rk);
 }
 

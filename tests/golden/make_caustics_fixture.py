@@ -2,7 +2,8 @@
 of the small caustics scene at fixed seeds, as a bit-for-bit regression
 fixture for changes to how the caustic render kernel schedules its work (the
 image is defined by per-pixel sums of the samples in sample order, whatever
-the schedule). Generated on a GPU with the one-thread-per-pixel kernel:
+the schedule). Generated on a GPU (last when the k-nearest estimate came to add
+its kept photons in the grid query's order):
 
     python tests/golden/make_caustics_fixture.py [out.npz]
 
