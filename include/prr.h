@@ -336,20 +336,23 @@ int prr_photon_gather(const prr_photon_map *map, const float *points, int64_t n,
  * chain (Integrator.cpp:143-169) to its first diffuse hit x, which returns
  * beta * baseColor/pi * E(x) from the photon map. out_rgb = window x 3, each
  * pixel the mean of its samples summed in sample order. Per call, 16 bytes per
- * (pixel, sample), at most 4 GiB (larger renders run in chunks of whole
- * samples per pixel), come from a stream-ordered memory pool of the library
+ * (pixel, sample) of at most 2^28 at once (larger renders run in chunks of
+ * whole samples per pixel), 4 more with k_nearest > 0 (a queue of the
+ * gathers with more than k photons inside, selected by a second kernel), come
+ * from a stream-ordered memory pool of the library
  * (one per device; it keeps up to 4 GiB of freed blocks for later calls) on
  * `stream` and go back to it when the call's work is done. */
 int prr_render_caustics(const prr_scene *scene, const prr_photon_map *map,
                         const prr_render_settings *settings, int k_nearest, float *out_rgb,
                         void *stream);
 /* No counterpart in the reference: prr_render_caustics with counting kernels
- * (the same image), for measurement. Waits for the stream; out[0..3] = camera
+ * (the same image), for measurement. Waits for the stream; out[0..4] = camera
  * hits traced, irradiance gathers, photons tested by the gathers' cell walks,
- * photons found inside the radius. */
+ * photons found inside the radius, gathers with more than k photons inside
+ * (the ones the k-nearest selection runs for). */
 int prr_render_caustics_counts(const prr_scene *scene, const prr_photon_map *pmap,
                                const prr_render_settings *settings, int k_nearest,
-                               float *out_rgb, uint64_t out[4], void *stream);
+                               float *out_rgb, uint64_t out[5], void *stream);
 
 /* ---- participating media (Volume.hpp, Volume.cpp) ----------------------
  * The reference defines a homogeneous medium and the Henyey-Greenstein phase

@@ -671,10 +671,10 @@ class PhotonMap:
         x0, y0, x1, y1 = window or (0, 0, W, H)
         dev = torch.device("cuda", torch.cuda.current_device())
         out = torch.empty(((y1 - y0), (x1 - x0), 3), dtype=torch.float32, device=dev)
-        cnt = (C.c_uint64 * 4)()
+        cnt = (C.c_uint64 * 5)()
         check(self.lib.prr_render_caustics_counts(scene.h, self.h, C.byref(rs), k_nearest,
                                                   _ptr(out), cnt, _stream(stream)))
-        keys = ("hits", "gathers", "photons_tested", "photons_inside")
+        keys = ("hits", "gathers", "photons_tested", "photons_inside", "dense_gathers")
         return out, dict(zip(keys, (int(x) for x in cnt)))
 
 

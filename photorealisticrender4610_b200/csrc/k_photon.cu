@@ -361,12 +361,6 @@ __device__ __forceinline__ float disc_area(float r) {
     return PRR_PI * r * r;
 }
 
-// PhotonGrid::query + PhotonMap::estimateIrradiance (Photon.cpp:55-94). With
-// k_nearest > 0 and more than k photons inside the radius, the estimate uses
-// the k nearest -- the k smallest (distance, photon index) pairs, so ties at
-// the k-th distance keep the lower photon index whatever the walk order --
-// and the disc through the k-th one: sum / (pi r_k^2), the kept photons added
-// in the order the query walks them (as estimateIrradiance adds its photons).
 // The first occupied slab of an axis in [c, hi], or hi + 1.
 __device__ __forceinline__ int next_slab(const uint32_t *occ, int c, int hi) {
     while (c <= hi) {
@@ -401,28 +395,38 @@ __device__ __forceinline__ void walk_cells(const GridView &v, const GridParams &
             }
 }
 
+// The cell box of a query at pos (PhotonGrid::query, Photon.cpp:58-72).
+struct GatherBox {
+    int x0, x1, y0, y1, z0, z1;
+};
+
+__device__ __forceinline__ GatherBox gather_box(const GridParams &g, V3 pos, float r) {
+    GatherBox b;
+    b.x0 = (int) ((pos.x - r - g.bmin[0]) / g.cs[0]);
+    b.y0 = (int) ((pos.y - r - g.bmin[1]) / g.cs[1]);
+    b.z0 = (int) ((pos.z - r - g.bmin[2]) / g.cs[2]);
+    b.x1 = (int) ((pos.x + r - g.bmin[0]) / g.cs[0]);
+    b.y1 = (int) ((pos.y + r - g.bmin[1]) / g.cs[1]);
+    b.z1 = (int) ((pos.z + r - g.bmin[2]) / g.cs[2]);
+    b.x0 = max(0, b.x0);
+    b.x1 = min(g.res - 1, b.x1);
+    b.y0 = max(0, b.y0);
+    b.y1 = min(g.res - 1, b.y1);
+    b.z0 = max(0, b.z0);
+    b.z1 = min(g.res - 1, b.z1);
+    return b;
+}
+
+// Pass 1 of a gather: the sum of the powers within the radius and their
+// number, in the reference query's order.
 template <bool COUNT = false>
-__device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc,
-                         unsigned *tested = nullptr, unsigned *inside = nullptr) {
-    const GridParams &g = *v.g;
+__device__ __forceinline__ V3 radius_sum(const GridView &v, const GatherBox &b, V3 pos,
+                                         int &found, unsigned *tested = nullptr,
+                                         unsigned *inside = nullptr) {
     const float r = v.radius;
-    int x0 = (int) ((pos.x - r - g.bmin[0]) / g.cs[0]);
-    int y0 = (int) ((pos.y - r - g.bmin[1]) / g.cs[1]);
-    int z0 = (int) ((pos.z - r - g.bmin[2]) / g.cs[2]);
-    int x1 = (int) ((pos.x + r - g.bmin[0]) / g.cs[0]);
-    int y1 = (int) ((pos.y + r - g.bmin[1]) / g.cs[1]);
-    int z1 = (int) ((pos.z + r - g.bmin[2]) / g.cs[2]);
-    x0 = max(0, x0);
-    x1 = min(g.res - 1, x1);
-    y0 = max(0, y0);
-    y1 = min(g.res - 1, y1);
-    z0 = max(0, z0);
-    z1 = min(g.res - 1, z1);
-    // Pass 1: the fixed-radius sum and the number of photons inside, in the
-    // reference query's order.
     V3 e = v3(0.f);
-    int found = 0;
-    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+    found = 0;
+    walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
         const float4 pa = v.sorted[2 * s];
         const V3 d = v3(pa.x, pa.y, pa.z) - pos;
         const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
@@ -436,19 +440,21 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
             found++;
         }
     });
-    if (found == 0)
-        return v3(0.f);
-    if (!kd || found <= k_nearest)
-        return e / disc_area(r);
-    // Pass 2, only with more than k inside: the k smallest (distance, photon
-    // index) pairs in a max-heap (the largest kept pair at its root), then
-    // pass 3 adds the powers of the photons at or below the root pair, in
-    // the walk's order, over the disc through the k-th.
+    return e;
+}
+
+// Passes 2 and 3 of a gather with more than k photons inside: the k smallest
+// (distance, photon index) pairs in a max-heap (the largest kept pair at its
+// root), then the powers of the photons at or below the root pair added in
+// the walk's order, over the disc through the k-th.
+__device__ V3 knn_estimate(const GridView &v, const GatherBox &b, V3 pos, int k_nearest,
+                           float *kd, int *kc) {
+    const float r = v.radius;
     auto below = [](float da, int ia, float db, int ib) {
         return da < db || (da == db && ia < ib);
     };
     int kept = 0;
-    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+    walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
         const float4 pa = v.sorted[2 * s];
         const V3 d = v3(pa.x, pa.y, pa.z) - pos;
         const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
@@ -488,7 +494,7 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
     const float rk = kd[0];
     const int ik = kc[0];
     V3 ek = v3(0.f);
-    walk_cells(v, g, x0, x1, y0, y1, z0, z1, [&](int s) {
+    walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
         const float4 pa = v.sorted[2 * s];
         const V3 d = v3(pa.x, pa.y, pa.z) - pos;
         const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
@@ -498,6 +504,23 @@ __device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, in
         }
     });
     return ek / disc_area(rk);
+}
+
+// PhotonGrid::query + PhotonMap::estimateIrradiance (Photon.cpp:55-94). With
+// k_nearest > 0 and more than k photons inside the radius, the estimate uses
+// the k nearest -- the k smallest (distance, photon index) pairs, so ties at
+// the k-th distance keep the lower photon index whatever the walk order --
+// and the disc through the k-th one: sum / (pi r_k^2), the kept photons added
+// in the order the query walks them (as estimateIrradiance adds its photons).
+__device__ V3 irradiance(const GridView &v, V3 pos, int k_nearest, float *kd, int *kc) {
+    const GatherBox b = gather_box(*v.g, pos, v.radius);
+    int found = 0;
+    const V3 e = radius_sum(v, b, pos, found);
+    if (found == 0)
+        return v3(0.f);
+    if (!kd || found <= k_nearest)
+        return e / disc_area(v.radius);
+    return knn_estimate(v, b, pos, k_nearest, kd, kc);
 }
 
 constexpr int kMaxK = 64;
@@ -527,9 +550,31 @@ struct CausticArgs {
     float4 *acc;     // npix running sums across chunks
     int s0, chunk;   // this launch's samples [s0, s0 + chunk) of each pixel
     unsigned long long *stats; // counting variant: camera hits, gathers, photons
-                               // tested, photons inside the radius
+                               // tested, photons inside the radius, dense gathers
     unsigned long long *next;  // work counter of this launch (zeroed before it)
+    // gathers with more than k photons inside, selected by k_caustic_dense:
+    // 2 float4 per entry (hit point + item index bits, beta * baseColor / pi)
+    float4 *dense;
+    unsigned *dense_count;     // entries queued (zeroed before each launch)
+    int64_t dense_cap;
 };
+
+// The dense gathers of one launch, one per thread: the k-nearest selection
+// of knn_estimate, and the item's contribution scale * E(x), the same
+// product as the render kernel forms for the other items.
+__global__ void k_caustic_dense(GridView v, CausticArgs a) {
+    const int64_t n = min((int64_t) *a.dense_count, a.dense_cap);
+    float kd[kMaxK];
+    int kc[kMaxK];
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t) gridDim.x * blockDim.x) {
+        const float4 p = a.dense[2 * i], sc = a.dense[2 * i + 1];
+        const V3 pos = v3(p.x, p.y, p.z);
+        const GatherBox b = gather_box(*v.g, pos, v.radius);
+        const V3 c = v3(sc.x, sc.y, sc.z) * knn_estimate(v, b, pos, a.k_nearest, kd, kc);
+        a.samples[__float_as_int(p.w)] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+}
 
 // One (pixel, sample) item per thread at a time: sample n of window pixel q is
 // item n * npix + q, so a warp's lanes trace neighbouring pixels; its result
@@ -545,7 +590,8 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     const int64_t total = npix * a.chunk;
     float kd[kMaxK];
     int kc[kMaxK];
-    unsigned cnt_[4] = {0, 0, 0, 0}; // hits, gathers, photons tested, photons inside
+    unsigned cnt_[5] = {0, 0, 0, 0, 0}; // hits, gathers, photons tested, photons inside,
+                                        // gathers with more than k inside
     // Persistent warps take the next 32 items from the launch's counter: a
     // sample through the glass sphere or with a dense k-nearest gather costs
     // many times a plain floor hit, so a fixed share per thread would leave
@@ -572,6 +618,7 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
         Ray3 ray = generate_ray(S.camera, i, j, xo, yo, rng);
         V3 beta = v3(1.f);
         V3 c = v3(0.f);
+        bool deferred = false;
         for (int d = 0; d < a.max_depth; d++) {
             tst.sp = 0;
             bst.sp = 0;
@@ -597,18 +644,41 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
             }
             if constexpr (COUNT)
                 cnt_[1]++;
-            const V3 e = irradiance<COUNT>(v, in.p, a.k_nearest, a.k_nearest > 0 ? kd : nullptr,
-                                           kc, cnt_ + 2, cnt_ + 3);
             const V3 albedo = mt.tex_base >= 0
                                   ? sample_base_color(S.textures[mt.tex_base], in.a.u, in.a.v)
                                   : v3(mt.base[0], mt.base[1], mt.base[2]);
-            c = beta * (albedo / PRR_PI) * e;
+            const V3 scale = beta * (albedo / PRR_PI);
+            const GatherBox b = gather_box(*v.g, in.p, v.radius);
+            int found = 0;
+            V3 e = radius_sum<COUNT>(v, b, in.p, found, cnt_ + 2, cnt_ + 3);
+            if (found == 0) {
+                e = v3(0.f);
+            } else if (a.k_nearest == 0 || found <= a.k_nearest) {
+                e = e / disc_area(v.radius);
+            } else {
+                if constexpr (COUNT)
+                    cnt_[4]++;
+                // more than k inside: the selection goes to the dense queue,
+                // whose kernel runs such gathers side by side (here one lane
+                // would hold its warp); a full queue selects in place
+                const unsigned slot = atomicAdd(a.dense_count, 1u);
+                if ((int64_t) slot < a.dense_cap) {
+                    a.dense[2 * (size_t) slot] =
+                        make_float4(in.p.x, in.p.y, in.p.z, __int_as_float((int) t));
+                    a.dense[2 * (size_t) slot + 1] = make_float4(scale.x, scale.y, scale.z, 0.f);
+                    deferred = true;
+                    break;
+                }
+                e = knn_estimate(v, b, in.p, a.k_nearest, kd, kc);
+            }
+            c = scale * e;
             break;
         }
-        a.samples[t] = make_float4(c.x, c.y, c.z, 0.f);
+        if (!deferred)
+            a.samples[t] = make_float4(c.x, c.y, c.z, 0.f);
     }
     if constexpr (COUNT) {
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < 5; k++) {
             unsigned long long x = cnt_[k];
             for (int off = 16; off > 0; off >>= 1)
                 x += __shfl_down_sync(0xffffffffu, x, off);
@@ -717,18 +787,24 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
     // per-call contributions (and, when chunked, running sums) from the
     // library's stream-ordered pool: concurrent calls on other streams get
     // their own
+    // (and the dense-gather queue: room for an eighth of the items, 32 B each;
+    // a launch with more dense gathers selects the rest in place)
     char *scratch = nullptr;
     const size_t acc_bytes = chunk < a.spp ? (size_t) npix * sizeof(float4) : 0;
+    a.dense_cap = k_nearest > 0 ? std::max<int64_t>(1024, items / 8) : 0;
+    const size_t dense_bytes = (size_t) a.dense_cap * 2 * sizeof(float4);
     cudaMemPool_t pool;
     PRR_CUDA_TRY(library_pool(&pool));
-    PRR_CUDA_TRY(cudaMallocFromPoolAsync((void **) &scratch,
-                                         (size_t) items * sizeof(float4) + acc_bytes + 256, pool,
-                                         st));
+    PRR_CUDA_TRY(cudaMallocFromPoolAsync(
+        (void **) &scratch, (size_t) items * sizeof(float4) + acc_bytes + dense_bytes + 256, pool,
+        st));
     a.samples = reinterpret_cast<float4 *>(scratch);
     a.acc = acc_bytes ? reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4))
                       : nullptr;
-    a.next = reinterpret_cast<unsigned long long *>(scratch + (size_t) items * sizeof(float4) +
-                                                    acc_bytes);
+    a.dense = reinterpret_cast<float4 *>(scratch + (size_t) items * sizeof(float4) + acc_bytes);
+    char *tail = scratch + (size_t) items * sizeof(float4) + acc_bytes + dense_bytes;
+    a.next = reinterpret_cast<unsigned long long *>(tail);
+    a.dense_count = reinterpret_cast<unsigned *>(tail + sizeof(unsigned long long));
     int bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
     cudaError_t e = cudaSuccess;
@@ -738,9 +814,13 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
         const int64_t total = npix * a.chunk;
         const int64_t grid = std::min<int64_t>((total + block - 1) / block,
                                                (int64_t) device_sm_count() * std::max(1, bps));
-        e = cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), st);
+        e = cudaMemsetAsync(tail, 0, 2 * sizeof(unsigned long long), st);
         if (e == cudaSuccess) {
             kern<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && a.dense_cap > 0) {
+            k_caustic_dense<<<(unsigned) (device_sm_count() * 8), 128, 0, st>>>(view(pm), a);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) {
@@ -954,17 +1034,17 @@ int prr_render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
 
 int prr_render_caustics_counts(const prr_scene *scene, const prr_photon_map *pmap,
                                const prr_render_settings *settings, int k_nearest,
-                               float *out_rgb, uint64_t out[4], void *stream) {
+                               float *out_rgb, uint64_t out[5], void *stream) {
     if (!out)
         return fail(PRR_ERR_INVALID_ARGUMENT, "out is required");
     cudaStream_t st = (cudaStream_t) stream;
     DevBuf buf;
-    PRR_CUDA_TRY(buf.alloc(4 * sizeof(unsigned long long)));
-    PRR_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, 4 * sizeof(unsigned long long), st));
+    PRR_CUDA_TRY(buf.alloc(5 * sizeof(unsigned long long)));
+    PRR_CUDA_TRY(cudaMemsetAsync(buf.ptr, 0, 5 * sizeof(unsigned long long), st));
     if (int rc = render_caustics(scene, pmap, settings, k_nearest, out_rgb,
                                  buf.as<unsigned long long>(), st))
         return rc;
-    PRR_CUDA_TRY(cudaMemcpyAsync(out, buf.ptr, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    PRR_CUDA_TRY(cudaMemcpyAsync(out, buf.ptr, 5 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     return PRR_OK;
 }
