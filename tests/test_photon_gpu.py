@@ -223,3 +223,21 @@ def test_caustic_render_counts(cuda):
         assert np.array_equal(img2.cpu().numpy().view(np.uint32), img.view(np.uint32))
         assert 0 < c["gathers"] <= 64 * 64 * 4 and c["gathers"] <= c["hits"]
         assert 0 < c["photons_inside"] <= c["photons_tested"]
+        assert c["dense_gathers"] <= c["gathers"] and (k > 0 or c["dense_gathers"] == 0)
+
+
+def test_caustic_dense_queue_and_in_place_agree(cuda):
+    """Gathers with more than k photons inside are selected by a second kernel
+    from a queue with room for an eighth of a launch's items; beyond that they
+    select in place. A 64x64 render at r = 0.3 (nearly every gather dense)
+    overflows the queue; one-row windows of the same render fit in it: the
+    pixels agree bit for bit."""
+    desc = scenes.caustics(64, 64, level=2)
+    s = prr.Scene.from_desc(desc)
+    pm = prr.PhotonMap().emit(s, 100_000, seed=1).build(0.3)
+    full, c = pm.render_caustics_counts(s, 4, k_nearest=16)
+    full = full.cpu().numpy()
+    assert c["dense_gathers"] > 2048, c  # more than the launch's queue holds
+    for y in (0, 21, 40, 63):
+        row = pm.render_caustics(s, 4, k_nearest=16, window=(0, y, 64, y + 1)).cpu().numpy()
+        assert np.array_equal(row.view(np.uint32), full[y:y + 1].view(np.uint32)), y
