@@ -559,20 +559,140 @@ struct CausticArgs {
     int64_t dense_cap;
 };
 
-// The dense gathers of one launch, one per thread: the k-nearest selection
-// of knn_estimate, and the item's contribution scale * E(x), the same
-// product as the render kernel forms for the other items.
+// In-radius photons a lane of k_caustic_dense keeps in registers (a gather
+// with more than 32 x this many walks its cells again for every count).
+constexpr int kDenseRegs = 12;
+
+// walk_cells with the photons of each cell shared out over a warp: lane l
+// takes the cell's photons l, l + 32, ... (every lane walks the same cells).
+template <class F>
+__device__ __forceinline__ void walk_cells_warp(const GridView &v, const GatherBox &b, int lane,
+                                                F &&f) {
+    const GridParams &g = *v.g;
+    for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
+         cx = next_slab(g.occ[0], cx + 1, b.x1))
+        for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
+             cy = next_slab(g.occ[1], cy + 1, b.y1))
+            for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
+                 cz = next_slab(g.occ[2], cz + 1, b.z1)) {
+                const int cell = cx + cy * g.res + cz * g.res * g.res;
+                const int s0 = v.start[cell];
+                if (s0 < 0)
+                    continue;
+                for (int s = s0 + lane; s < v.n && v.cell_of[s] == cell; s += 32)
+                    f(s);
+            }
+}
+
+// The dense gathers of one launch, one warp each. The warp finds the k-th
+// smallest (distance, photon index) pair by bisection -- on the distance's
+// bits (non-negative floats order as their bit patterns), then, when several
+// photons share the k-th distance, on the index -- counting candidates kept
+// in registers (or, for a gather with too many, by walking the cells again);
+// then lane 0 adds the powers at or below that pair in the walk's order, as
+// knn_estimate does, and writes scale * E(x), the product the render kernel
+// forms for the other items.
 __global__ void k_caustic_dense(GridView v, CausticArgs a) {
     const int64_t n = min((int64_t) *a.dense_count, a.dense_cap);
-    float kd[kMaxK];
-    int kc[kMaxK];
-    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t) gridDim.x * blockDim.x) {
-        const float4 p = a.dense[2 * i], sc = a.dense[2 * i + 1];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
+    const float r = v.radius;
+    const int k = a.k_nearest;
+    for (int64_t e = warp; e < n; e += nwarps) {
+        const float4 p = a.dense[2 * e], sc = a.dense[2 * e + 1];
         const V3 pos = v3(p.x, p.y, p.z);
-        const GatherBox b = gather_box(*v.g, pos, v.radius);
-        const V3 c = v3(sc.x, sc.y, sc.z) * knn_estimate(v, b, pos, a.k_nearest, kd, kc);
-        a.samples[__float_as_int(p.w)] = make_float4(c.x, c.y, c.z, 0.f);
+        const GatherBox b = gather_box(*v.g, pos, r);
+        uint32_t cd[kDenseRegs];
+        int ci[kDenseRegs];
+        int cnt = 0;
+        walk_cells_warp(v, b, lane, [&](int s) {
+            const float4 pa = v.sorted[2 * s];
+            const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+            const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+            if (!(dist <= r))
+                return;
+            const int idx = v.order[s];
+#pragma unroll
+            for (int j = 0; j < kDenseRegs; j++)
+                if (j == cnt) {
+                    cd[j] = __float_as_uint(dist);
+                    ci[j] = idx;
+                }
+            cnt++;
+        });
+        const bool cached = !__any_sync(full, cnt > kDenseRegs);
+        // candidates with pred(distance bits, index), summed over the warp
+        auto count = [&](auto pred) -> int {
+            int c = 0;
+            if (cached) {
+#pragma unroll
+                for (int j = 0; j < kDenseRegs; j++)
+                    if (j < cnt && pred(cd[j], ci[j]))
+                        c++;
+            } else {
+                walk_cells_warp(v, b, lane, [&](int s) {
+                    const float4 pa = v.sorted[2 * s];
+                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+                    if (dist <= r && pred(__float_as_uint(dist), v.order[s]))
+                        c++;
+                });
+            }
+            return (int) __reduce_add_sync(full, (unsigned) c);
+        };
+        // the k-th smallest distance: the least D with count(dist <= D) >= k,
+        // between the smallest and the largest candidate distance
+        uint32_t lo = 0, hi = __float_as_uint(r);
+        if (cached) {
+            uint32_t kmin = 0xffffffffu, kmax = 0u;
+#pragma unroll
+            for (int j = 0; j < kDenseRegs; j++)
+                if (j < cnt) {
+                    kmin = min(kmin, cd[j]);
+                    kmax = max(kmax, cd[j]);
+                }
+            lo = __reduce_min_sync(full, kmin);
+            hi = __reduce_max_sync(full, kmax);
+        }
+        while (lo < hi) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (count([&](uint32_t key, int) { return key <= mid; }) >= k)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        const uint32_t dk = lo;
+        // of the photons at distance D, the lowest (k - count(dist < D)) indices
+        // (all of them unless more share the k-th distance)
+        const int m = k - count([&](uint32_t key, int) { return key < dk; });
+        const int eq = count([&](uint32_t key, int) { return key == dk; });
+        int ilo = eq == m ? 0x7fffffff : 0, ihi = 0x7fffffff;
+        while (ilo < ihi) {
+            const int mid = ilo + (ihi - ilo) / 2;
+            if (count([&](uint32_t key, int idx) { return key == dk && idx <= mid; }) >= m)
+                ihi = mid;
+            else
+                ilo = mid + 1;
+        }
+        if (lane == 0) {
+            const float rk = __uint_as_float(dk);
+            const int ik = ilo;
+            V3 ek = v3(0.f);
+            walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
+                const float4 pa = v.sorted[2 * s];
+                const V3 d = v3(pa.x, pa.y, pa.z) - pos;
+                const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+                if (dist < rk || (dist == rk && v.order[s] <= ik)) {
+                    const float4 pb = v.sorted[2 * s + 1];
+                    ek = ek + v3(pa.w, pb.x, pb.y);
+                }
+            });
+            const V3 c = v3(sc.x, sc.y, sc.z) * (ek / disc_area(rk));
+            a.samples[__float_as_int(p.w)] = make_float4(c.x, c.y, c.z, 0.f);
+        }
+        __syncwarp();
     }
 }
 
