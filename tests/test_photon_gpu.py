@@ -226,14 +226,13 @@ def test_caustic_render_counts(cuda):
         assert c["dense_gathers"] <= c["gathers"] and (k > 0 or c["dense_gathers"] == 0)
 
 
-def test_caustic_dense_queue_and_in_place_agree(cuda):
+def test_caustic_dense_queue_and_in_place_agree(ref, cuda):
     """Gathers with more than k photons inside are selected by a second kernel
     from a queue with room for an eighth of a launch's items; beyond that they
     select in place. A 64x64 render at r = 0.5 and k = 4 (most gathers dense)
     overflows the queue; one-row windows of the same render fit in it: the
-    pixels agree bit for bit, and with the one-thread selection of the
-    standalone gather at the same points (k_caustic_dense selects with a whole
-    warp per gather)."""
+    pixels agree bit for bit. Both paths against the oracle's render pass on
+    the same photons: rMSE <= 1e-3 and most pixels equal to the bit."""
     desc = scenes.caustics(64, 64, level=2)
     s = prr.Scene.from_desc(desc)
     pm = prr.PhotonMap().emit(s, 100_000, seed=1).build(0.5)
@@ -243,3 +242,7 @@ def test_caustic_dense_queue_and_in_place_agree(cuda):
     for y in (0, 21, 40, 63):
         row = pm.render_caustics(s, 4, k_nearest=4, window=(0, y, 64, y + 1)).cpu().numpy()
         assert np.array_equal(row.view(np.uint32), full[y:y + 1].view(np.uint32)), y
+    rec, _ = pm.export()
+    want = ref.scene(desc).caustic_render(rec, 0.5, 4, k_nearest=4)
+    assert rel_mse(full, want) < 1e-3
+    assert (full.view(np.uint32) == want.view(np.uint32)).all(axis=2).mean() > 0.9
