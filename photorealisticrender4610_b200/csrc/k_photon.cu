@@ -559,10 +559,6 @@ struct CausticArgs {
     int64_t dense_cap;
 };
 
-// In-radius photons a lane of k_caustic_dense keeps in registers (a gather
-// with more than 32 x this many walks its cells again for every count).
-constexpr int kDenseRegs = 12;
-
 // walk_cells with the photons of each cell shared out over a warp: lane l
 // takes the cell's photons l, l + 32, ... (every lane walks the same cells).
 template <class F>
@@ -584,111 +580,151 @@ __device__ __forceinline__ void walk_cells_warp(const GridView &v, const GatherB
             }
 }
 
-// The dense gathers of one launch, one warp each. The warp finds the k-th
-// smallest (distance, photon index) pair by bisection -- on the distance's
-// bits (non-negative floats order as their bit patterns), then, when several
-// photons share the k-th distance, on the index -- counting candidates kept
-// in registers (or, for a gather with too many, by walking the cells again);
-// then lane 0 adds the powers at or below that pair in the walk's order, as
-// knn_estimate does, and writes scale * E(x), the product the render kernel
-// forms for the other items.
-__global__ void k_caustic_dense(GridView v, CausticArgs a) {
+// The value of rank `want` (1-based) among the candidates' 32-bit keys, by a
+// radix select over the key's bytes from the top: each pass histograms one
+// byte of the candidates that match the bytes found so far into the warp's
+// 256 shared-memory bins and keeps the bin holding the wanted rank. On
+// return want is the rank within the candidates whose key equals the result,
+// and *equal is how many have that key. key_of(s, key) gives candidate s's
+// key (false: not a candidate).
+template <class K>
+__device__ uint32_t warp_radix_select(const GridView &v, const GatherBox &b, int lane,
+                                      unsigned *bins, int &want, int *equal, K &&key_of) {
+    const unsigned full = 0xffffffffu;
+    uint32_t prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int q = lane; q < 256; q += 32)
+            bins[q] = 0u;
+        __syncwarp();
+        walk_cells_warp(v, b, lane, [&](int s) {
+            uint32_t key;
+            if (key_of(s, key) && (key & mask) == prefix)
+                atomicAdd(&bins[(key >> shift) & 255u], 1u);
+        });
+        __syncwarp();
+        // the bin holding rank `want`: each lane sums 8 bins, a warp scan
+        // finds the lane, the lane finds the bin
+        unsigned own = 0;
+        for (int q = 0; q < 8; q++)
+            own += bins[lane * 8 + q];
+        unsigned incl = own;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(full, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        const unsigned before = incl - own;
+        const bool holds = before < (unsigned) want && (unsigned) want <= incl;
+        const int src = __ffs(__ballot_sync(full, holds)) - 1;
+        int bin = 0;
+        unsigned below = 0, in_bin = 0;
+        if (holds) {
+            unsigned run = before;
+            for (int q = 0; q < 8; q++) {
+                const unsigned c = bins[lane * 8 + q];
+                if ((unsigned) want <= run + c) {
+                    bin = lane * 8 + q;
+                    below = run;
+                    in_bin = c;
+                    break;
+                }
+                run += c;
+            }
+        }
+        bin = __shfl_sync(full, bin, src);
+        below = __shfl_sync(full, below, src);
+        in_bin = __shfl_sync(full, in_bin, src);
+        want -= (int) below;
+        prefix |= (uint32_t) bin << shift;
+        mask |= 255u << shift;
+        *equal = (int) in_bin;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+// The dense gathers of one launch, one warp each (4 per block of 128). The
+// k-th smallest (distance, photon index) pair by radix selects over the
+// distance's bits (non-negative floats order as their bit patterns) and,
+// when several photons share the k-th distance, over the index; then the
+// kept photons -- at or below that pair -- are added in the walk's order,
+// 32 photons tested at a time and only the kept ones added one by one, as
+// knn_estimate adds them; the item gets scale * E(x), the product the render
+// kernel forms for the other items.
+__global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a) {
+    __shared__ unsigned bins_all[4][256];
+    unsigned *bins = bins_all[threadIdx.x >> 5];
     const int64_t n = min((int64_t) *a.dense_count, a.dense_cap);
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
     const float r = v.radius;
-    const int k = a.k_nearest;
     for (int64_t e = warp; e < n; e += nwarps) {
         const float4 p = a.dense[2 * e], sc = a.dense[2 * e + 1];
         const V3 pos = v3(p.x, p.y, p.z);
         const GatherBox b = gather_box(*v.g, pos, r);
-        uint32_t cd[kDenseRegs];
-        int ci[kDenseRegs];
-        int cnt = 0;
-        walk_cells_warp(v, b, lane, [&](int s) {
+        auto dist_of = [&](int s) {
             const float4 pa = v.sorted[2 * s];
             const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-            const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-            if (!(dist <= r))
-                return;
-            const int idx = v.order[s];
-#pragma unroll
-            for (int j = 0; j < kDenseRegs; j++)
-                if (j == cnt) {
-                    cd[j] = __float_as_uint(dist);
-                    ci[j] = idx;
-                }
-            cnt++;
-        });
-        const bool cached = !__any_sync(full, cnt > kDenseRegs);
-        // candidates with pred(distance bits, index), summed over the warp
-        auto count = [&](auto pred) -> int {
-            int c = 0;
-            if (cached) {
-#pragma unroll
-                for (int j = 0; j < kDenseRegs; j++)
-                    if (j < cnt && pred(cd[j], ci[j]))
-                        c++;
-            } else {
-                walk_cells_warp(v, b, lane, [&](int s) {
-                    const float4 pa = v.sorted[2 * s];
-                    const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-                    const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-                    if (dist <= r && pred(__float_as_uint(dist), v.order[s]))
-                        c++;
-                });
-            }
-            return (int) __reduce_add_sync(full, (unsigned) c);
+            return sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
         };
-        // the k-th smallest distance: the least D with count(dist <= D) >= k,
-        // between the smallest and the largest candidate distance
-        uint32_t lo = 0, hi = __float_as_uint(r);
-        if (cached) {
-            uint32_t kmin = 0xffffffffu, kmax = 0u;
-#pragma unroll
-            for (int j = 0; j < kDenseRegs; j++)
-                if (j < cnt) {
-                    kmin = min(kmin, cd[j]);
-                    kmax = max(kmax, cd[j]);
+        int want = a.k_nearest, equal = 0;
+        const uint32_t dk = warp_radix_select(v, b, lane, bins, want, &equal,
+                                              [&](int s, uint32_t &key) {
+                                                  const float dist = dist_of(s);
+                                                  key = __float_as_uint(dist);
+                                                  return dist <= r;
+                                              });
+        // of the photons at the k-th distance, keep the lowest `want` indices
+        int ik = 0x7fffffff;
+        if (equal > want) {
+            int eq2 = 0;
+            ik = (int) warp_radix_select(v, b, lane, bins, want, &eq2,
+                                         [&](int s, uint32_t &key) {
+                                             key = (uint32_t) v.order[s];
+                                             return __float_as_uint(dist_of(s)) == dk;
+                                         });
+        }
+        const float rk = __uint_as_float(dk);
+        // the ordered sum of the kept powers (lane 0 holds it)
+        V3 ek = v3(0.f);
+        const GridParams &g = *v.g;
+        for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
+             cx = next_slab(g.occ[0], cx + 1, b.x1))
+            for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
+                 cy = next_slab(g.occ[1], cy + 1, b.y1))
+                for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
+                     cz = next_slab(g.occ[2], cz + 1, b.z1)) {
+                    const int cell = cx + cy * g.res + cz * g.res * g.res;
+                    const int s0 = v.start[cell];
+                    if (s0 < 0)
+                        continue;
+                    for (int base = s0;; base += 32) {
+                        const int s = base + lane;
+                        const bool in_cell = s < v.n && v.cell_of[s] == cell;
+                        if (!__any_sync(full, in_cell))
+                            break;
+                        bool keep = false;
+                        V3 pw = v3(0.f);
+                        if (in_cell) {
+                            const float dist = dist_of(s);
+                            keep = dist < rk || (dist == rk && v.order[s] <= ik);
+                            if (keep) {
+                                const float4 pa = v.sorted[2 * s];
+                                const float4 pb = v.sorted[2 * s + 1];
+                                pw = v3(pa.w, pb.x, pb.y);
+                            }
+                        }
+                        for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
+                            const int l = __ffs(km) - 1;
+                            const V3 q = v3(__shfl_sync(full, pw.x, l), __shfl_sync(full, pw.y, l),
+                                            __shfl_sync(full, pw.z, l));
+                            ek = ek + q;
+                        }
+                    }
                 }
-            lo = __reduce_min_sync(full, kmin);
-            hi = __reduce_max_sync(full, kmax);
-        }
-        while (lo < hi) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            if (count([&](uint32_t key, int) { return key <= mid; }) >= k)
-                hi = mid;
-            else
-                lo = mid + 1;
-        }
-        const uint32_t dk = lo;
-        // of the photons at distance D, the lowest (k - count(dist < D)) indices
-        // (all of them unless more share the k-th distance)
-        const int m = k - count([&](uint32_t key, int) { return key < dk; });
-        const int eq = count([&](uint32_t key, int) { return key == dk; });
-        int ilo = eq == m ? 0x7fffffff : 0, ihi = 0x7fffffff;
-        while (ilo < ihi) {
-            const int mid = ilo + (ihi - ilo) / 2;
-            if (count([&](uint32_t key, int idx) { return key == dk && idx <= mid; }) >= m)
-                ihi = mid;
-            else
-                ilo = mid + 1;
-        }
         if (lane == 0) {
-            const float rk = __uint_as_float(dk);
-            const int ik = ilo;
-            V3 ek = v3(0.f);
-            walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
-                const float4 pa = v.sorted[2 * s];
-                const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-                const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-                if (dist < rk || (dist == rk && v.order[s] <= ik)) {
-                    const float4 pb = v.sorted[2 * s + 1];
-                    ek = ek + v3(pa.w, pb.x, pb.y);
-                }
-            });
             const V3 c = v3(sc.x, sc.y, sc.z) * (ek / disc_area(rk));
             a.samples[__float_as_int(p.w)] = make_float4(c.x, c.y, c.z, 0.f);
         }
