@@ -228,21 +228,28 @@ def test_caustic_render_counts(cuda):
 
 def test_caustic_dense_queue_and_in_place_agree(ref, cuda):
     """Gathers with more than k photons inside are selected by a second kernel
-    from a queue with room for an eighth of a launch's items; beyond that they
-    select in place. A 64x64 render at r = 0.5 and k = 4 (most gathers dense)
-    overflows the queue; one-row windows of the same render fit in it: the
-    pixels agree bit for bit. Both paths against the oracle's render pass on
-    the same photons: rMSE <= 1e-3 and most pixels equal to the bit."""
+    (a warp per gather) from a queue with room for an eighth of a launch's
+    items, at least 1024; beyond that they select in place (one thread each).
+    A 16x16 window over the caustic at 16 spp (4,096 items, most of them dense
+    gathers) overflows the queue; one-row windows of it fit: the pixels agree
+    bit for bit. Both paths against the oracle's render pass on the same
+    photons: rMSE <= 1e-3 and most pixels equal to the bit."""
     desc = scenes.caustics(64, 64, level=2)
     s = prr.Scene.from_desc(desc)
     pm = prr.PhotonMap().emit(s, 100_000, seed=1).build(0.5)
-    full, c = pm.render_caustics_counts(s, 4, k_nearest=4)
+    # the 16x16 window of the brightest caustic
+    lum = pm.render_caustics(s, 2, k_nearest=0).cpu().numpy().sum(axis=2)
+    sums = [(lum[y:y + 16, x:x + 16].sum(), x, y) for y in range(0, 49, 4) for x in range(0, 49, 4)]
+    _, x0, y0 = max(sums)
+    win = (x0, y0, x0 + 16, y0 + 16)
+    full, c = pm.render_caustics_counts(s, 16, k_nearest=4, window=win)
     full = full.cpu().numpy()
-    assert c["dense_gathers"] > 2048, c  # more than the launch's queue holds
-    for y in (0, 21, 40, 63):
-        row = pm.render_caustics(s, 4, k_nearest=4, window=(0, y, 64, y + 1)).cpu().numpy()
-        assert np.array_equal(row.view(np.uint32), full[y:y + 1].view(np.uint32)), y
+    assert c["dense_gathers"] > max(1024, 16 * 16 * 16 // 8), c  # more than the queue holds
+    for y in range(y0, y0 + 16, 5):
+        row = pm.render_caustics(s, 16, k_nearest=4, window=(x0, y, x0 + 16, y + 1)).cpu().numpy()
+        assert np.array_equal(row.view(np.uint32), full[y - y0:y - y0 + 1].view(np.uint32)), y
     rec, _ = pm.export()
-    want = ref.scene(desc).caustic_render(rec, 0.5, 4, k_nearest=4)
+    want = ref.scene(desc).caustic_render(rec, 0.5, 16, k_nearest=4, window=win)
+    assert want.max() > 0
     assert rel_mse(full, want) < 1e-3
     assert (full.view(np.uint32) == want.view(np.uint32)).all(axis=2).mean() > 0.9
