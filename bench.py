@@ -714,7 +714,9 @@ def caustics_result(args, rank, world, on, steps, warmup):
         step()
     with ClockSampler(dev.index) as clk:
         barrier(on)
+        launches0 = pm.launches()
         phases = [step()[0] for _ in range(steps)]
+        launches = pm.launches() - launches0
         barrier(on)
     ph = np.array(phases)
     step_ms = max_over_ranks(float(ph.sum(1).mean()), on)
@@ -776,7 +778,7 @@ def caustics_result(args, rank, world, on, steps, warmup):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
-        "gpu_launches": None,
+        "gpu_launches": launches,
     }
     return line
 

@@ -322,6 +322,10 @@ int prr_photon_set(prr_photon_map *map, const float *records, int64_t n, void *s
  * (Photon.cpp:24-53, :189). */
 int prr_photon_build(prr_photon_map *map, float radius, void *stream);
 int prr_photon_info(const prr_photon_map *map, int64_t *count, int32_t *grid_res);
+/* Kernels launched so far by the calls on this photon map (emit, build,
+ * gather, caustic render): a running count for launch accounting, no
+ * counterpart in the reference (whose photon map runs on the host). */
+int prr_photon_launches(const prr_photon_map *map, int64_t *out);
 /* Copies the records (n x 9) and their emitting photon indices (n). */
 int prr_photon_export(const prr_photon_map *map, float *records, int32_t *owner, void *stream);
 /* PhotonMap::estimateIrradiance (Photon.cpp:82-94) at n points (n x 3):

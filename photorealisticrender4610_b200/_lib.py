@@ -151,6 +151,7 @@ _SIGS = {
     "prr_photon_set": (C.c_int, [_vp, _vp, C.c_int64, _vp]),
     "prr_photon_build": (C.c_int, [_vp, C.c_float, _vp]),
     "prr_photon_info": (C.c_int, [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "prr_photon_launches": (C.c_int, [_vp, C.POINTER(C.c_int64)]),
     "prr_photon_export": (C.c_int, [_vp, _vp, _vp, _vp]),
     "prr_photon_gather": (C.c_int, [_vp, _vp, C.c_int64, C.c_int, _vp, _vp]),
     "prr_render_caustics": (C.c_int, [_vp, _vp, C.POINTER(prr_render_settings), C.c_int, _vp,

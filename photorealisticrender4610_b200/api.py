@@ -632,6 +632,12 @@ class PhotonMap:
         check(self.lib.prr_photon_info(self.h, C.byref(n), C.byref(res)))
         return n.value, res.value
 
+    def launches(self) -> int:
+        """Kernels launched so far by the calls on this photon map."""
+        n = C.c_int64()
+        check(self.lib.prr_photon_launches(self.h, C.byref(n)))
+        return n.value
+
     def export(self):
         n, _ = self.info()
         rec = np.empty((n, 9), np.float32)

@@ -22,6 +22,7 @@
 #include "prr_internal.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -44,6 +45,9 @@ struct PhotonMap {
                      // read a cell's photons contiguously)
     DevBuf params;   // device copy of the grid parameters
     DevBuf scratch;
+    // kernels launched by calls on this map (emit, build, gather, caustic
+    // render); renders take the map read-only, hence mutable
+    mutable std::atomic<int64_t> launches{0};
 };
 
 namespace {
@@ -199,16 +203,21 @@ __global__ void k_bitonic_shared(unsigned long long *keys, int64_t k, int j0) {
     keys[base + threadIdx.x + 1024] = t[threadIdx.x + 1024];
 }
 
-// Sorts keys[0, n2) ascending; n2 is a power of two >= 2048.
-int bitonic_sort(unsigned long long *keys, int64_t n2, cudaStream_t st) {
+// Sorts keys[0, n2) ascending; n2 is a power of two >= 2048. Adds its kernel
+// launches to *launches.
+int bitonic_sort(unsigned long long *keys, int64_t n2, cudaStream_t st,
+                 std::atomic<int64_t> *launches) {
     const int tb = 256;
     const unsigned grid = (unsigned) ((n2 + tb - 1) / tb);
+    int64_t count = 0;
     for (int64_t k = 2; k <= n2; k <<= 1) {
         int64_t j = k >> 1;
-        for (; j >= 1024; j >>= 1)
+        for (; j >= 1024; j >>= 1, count++)
             k_bitonic_global<<<grid, tb, 0, st>>>(keys, j, k, n2);
         k_bitonic_shared<<<(unsigned) (n2 / 2048), 1024, 0, st>>>(keys, k, (int) j);
+        count++;
     }
+    *launches += count;
     PRR_CUDA_TRY(cudaGetLastError());
     return PRR_OK;
 }
@@ -553,10 +562,12 @@ struct CausticArgs {
                                // tested, photons inside the radius, dense gathers
     unsigned long long *next;  // work counter of this launch (zeroed before it)
     // gathers with more than k photons inside, selected by k_caustic_dense:
-    // 2 float4 per entry (hit point + item index bits, beta * baseColor / pi)
+    // 2 float4 per entry (hit point + item index bits, beta * baseColor / pi
+    // + the number of photons inside the radius as int bits)
     float4 *dense;
     unsigned *dense_count;     // entries queued (zeroed before each launch)
     int64_t dense_cap;
+    unsigned long long *dense_next; // k_caustic_dense's work counter (zeroed too)
 };
 
 // walk_cells with the photons of each cell shared out over a warp: lane l
@@ -585,18 +596,19 @@ __device__ __forceinline__ void walk_cells_warp(const GridView &v, const GatherB
 // byte of the candidates that match the bytes found so far into the warp's
 // 256 shared-memory bins and keeps the bin holding the wanted rank. On
 // return want is the rank within the candidates whose key equals the result,
-// and *equal is how many have that key. key_of(s, key) gives candidate s's
-// key (false: not a candidate).
-template <class K>
-__device__ uint32_t warp_radix_select(const GridView &v, const GatherBox &b, int lane,
-                                      unsigned *bins, int &want, int *equal, K &&key_of) {
+// and *equal is how many have that key. walk(f) calls f(s) for this lane's
+// share of the items; key_of(s, key) gives item s's key (false: not a
+// candidate).
+template <class Walk, class K>
+__device__ uint32_t warp_radix_select(Walk &&walk, int lane, unsigned *bins, int &want,
+                                      int *equal, K &&key_of) {
     const unsigned full = 0xffffffffu;
     uint32_t prefix = 0, mask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int q = lane; q < 256; q += 32)
             bins[q] = 0u;
         __syncwarp();
-        walk_cells_warp(v, b, lane, [&](int s) {
+        walk([&](int s) {
             uint32_t key;
             if (key_of(s, key) && (key & mask) == prefix)
                 atomicAdd(&bins[(key >> shift) & 255u], 1u);
@@ -643,89 +655,218 @@ __device__ uint32_t warp_radix_select(const GridView &v, const GatherBox &b, int
     return prefix;
 }
 
-// The dense gathers of one launch, one warp each (4 per block of 128). The
-// k-th smallest (distance, photon index) pair by radix selects over the
-// distance's bits (non-negative floats order as their bit patterns) and,
-// when several photons share the k-th distance, over the index; then the
-// kept photons -- at or below that pair -- are added in the walk's order,
-// 32 photons tested at a time and only the kept ones added one by one, as
-// knn_estimate adds them; the item gets scale * E(x), the product the render
-// kernel forms for the other items.
+// Candidates per warp that k_caustic_dense holds in shared memory.
+constexpr int kDenseCands = 1024;
+// Collection walks k_caustic_dense tries before it selects by walking cells.
+constexpr int kDenseTries = 4;
+
+// The cells of `big` that can hold photons within t of pos: the cell box of
+// the disc of radius t, one cell wider on every side (so rounding in the cell
+// arithmetic cannot leave such a photon out), cut to `big`. Walked in the
+// same nested x, y, z order, its cells come in the order `big` visits them.
+__device__ __forceinline__ GatherBox sub_box(const GridParams &g, const GatherBox &big, V3 pos,
+                                             float t) {
+    const GatherBox s = gather_box(g, pos, t);
+    GatherBox b;
+    b.x0 = max(big.x0, s.x0 - 1);
+    b.x1 = min(big.x1, s.x1 + 1);
+    b.y0 = max(big.y0, s.y0 - 1);
+    b.y1 = min(big.y1, s.y1 + 1);
+    b.z0 = max(big.z0, s.z0 - 1);
+    b.z1 = min(big.z1, s.z1 + 1);
+    return b;
+}
+
+// The dense gathers of one launch, one warp each (4 per block of 128, the
+// next entry from a counter). The k-th smallest (distance, photon index)
+// pair, then the kept photons -- at or below that pair -- added in the
+// walk's order, as knn_estimate adds them; the item gets scale * E(x), the
+// product the render kernel forms for the other items.
+//
+// Collection first: one walk over the cells that can hold photons within a
+// threshold t <= r stores every photon at distance <= t, in walk order, as
+// (distance bits, sorted slot) in the warp's shared memory. When at least k
+// photons lie within t, the k nearest within r are the k nearest of these
+// (any pair at or below the k-th has distance <= t), so the selection and
+// the ordered sum run over shared memory. t starts where about 3k of the
+// `found` photons inside r would lie if they were spread evenly over the
+// disc, and is widened (fewer than k within t) or narrowed (more than the
+// warp holds) for up to kDenseTries walks. Failing that the warp selects by
+// radix passes that walk the cells of the whole query box: one per byte of
+// the distance's bits (non-negative floats order as their bit patterns), one
+// more per byte of the photon index when several photons share the k-th
+// distance, and the ordered sum in a last walk, 32 photons tested per round.
 __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a) {
     __shared__ unsigned bins_all[4][256];
+    __shared__ uint2 cand_all[4][kDenseCands];
     unsigned *bins = bins_all[threadIdx.x >> 5];
+    uint2 *cand = cand_all[threadIdx.x >> 5];
     const int64_t n = min((int64_t) *a.dense_count, a.dense_cap);
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t) gridDim.x * blockDim.x) >> 5;
     const float r = v.radius;
-    for (int64_t e = warp; e < n; e += nwarps) {
+    const int k = a.k_nearest;
+    const GridParams &g = *v.g;
+    for (;;) {
+        unsigned long long e = 0;
+        if (lane == 0)
+            e = atomicAdd(a.dense_next, 1ull);
+        e = __shfl_sync(full, e, 0);
+        if ((int64_t) e >= n)
+            break;
         const float4 p = a.dense[2 * e], sc = a.dense[2 * e + 1];
         const V3 pos = v3(p.x, p.y, p.z);
-        const GatherBox b = gather_box(*v.g, pos, r);
+        const int found = __float_as_int(sc.w); // photons inside r (> k)
+        const GatherBox big = gather_box(g, pos, r);
         auto dist_of = [&](int s) {
             const float4 pa = v.sorted[2 * s];
             const V3 d = v3(pa.x, pa.y, pa.z) - pos;
             return sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
         };
-        int want = a.k_nearest, equal = 0;
-        const uint32_t dk = warp_radix_select(v, b, lane, bins, want, &equal,
-                                              [&](int s, uint32_t &key) {
-                                                  const float dist = dist_of(s);
-                                                  key = __float_as_uint(dist);
-                                                  return dist <= r;
-                                              });
-        // of the photons at the k-th distance, keep the lowest `want` indices
-        int ik = 0x7fffffff;
-        if (equal > want) {
-            int eq2 = 0;
-            ik = (int) warp_radix_select(v, b, lane, bins, want, &eq2,
-                                         [&](int s, uint32_t &key) {
-                                             key = (uint32_t) v.order[s];
-                                             return __float_as_uint(dist_of(s)) == dk;
-                                         });
-        }
-        const float rk = __uint_as_float(dk);
-        // the ordered sum of the kept powers (lane 0 holds it)
-        V3 ek = v3(0.f);
-        const GridParams &g = *v.g;
-        for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
-             cx = next_slab(g.occ[0], cx + 1, b.x1))
-            for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
-                 cy = next_slab(g.occ[1], cy + 1, b.y1))
-                for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
-                     cz = next_slab(g.occ[2], cz + 1, b.z1)) {
-                    const int cell = cx + cy * g.res + cz * g.res * g.res;
-                    const int s0 = v.start[cell];
-                    if (s0 < 0)
-                        continue;
-                    for (int base = s0;; base += 32) {
-                        const int s = base + lane;
-                        const bool in_cell = s < v.n && v.cell_of[s] == cell;
-                        if (!__any_sync(full, in_cell))
-                            break;
-                        bool keep = false;
-                        V3 pw = v3(0.f);
-                        if (in_cell) {
-                            const float dist = dist_of(s);
-                            keep = dist < rk || (dist == rk && v.order[s] <= ik);
-                            if (keep) {
-                                const float4 pa = v.sorted[2 * s];
-                                const float4 pb = v.sorted[2 * s + 1];
-                                pw = v3(pa.w, pb.x, pb.y);
+        float t = r * sqrtf(fminf(1.f, 3.f * (float) k / (float) found));
+        int count = -1; // photons collected in shared memory (-1: none usable)
+        for (int attempt = 0; attempt < kDenseTries; attempt++) {
+            const GatherBox b = sub_box(g, big, pos, t);
+            int c = 0;
+            for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
+                 cx = next_slab(g.occ[0], cx + 1, b.x1))
+                for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
+                     cy = next_slab(g.occ[1], cy + 1, b.y1))
+                    for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
+                         cz = next_slab(g.occ[2], cz + 1, b.z1)) {
+                        const int cell = cx + cy * g.res + cz * g.res * g.res;
+                        const int s0 = v.start[cell];
+                        if (s0 < 0)
+                            continue;
+                        for (int base = s0;; base += 32) {
+                            const int s = base + lane;
+                            const bool in_cell = s < v.n && v.cell_of[s] == cell;
+                            if (!__any_sync(full, in_cell))
+                                break;
+                            float dist = 0.f;
+                            bool take = false;
+                            if (in_cell) {
+                                dist = dist_of(s);
+                                take = dist <= t;
                             }
-                        }
-                        for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
-                            const int l = __ffs(km) - 1;
-                            const V3 q = v3(__shfl_sync(full, pw.x, l), __shfl_sync(full, pw.y, l),
-                                            __shfl_sync(full, pw.z, l));
-                            ek = ek + q;
+                            const unsigned m = __ballot_sync(full, take);
+                            const int at = c + __popc(m & ((1u << lane) - 1u));
+                            if (take && at < kDenseCands)
+                                cand[at] = make_uint2(__float_as_uint(dist), (unsigned) s);
+                            c += __popc(m);
                         }
                     }
+            __syncwarp();
+            if (c >= k && c <= kDenseCands) {
+                count = c;
+                break;
+            }
+            if (c < k) {
+                if (t >= r)
+                    break; // cannot happen while found > k
+                t = fminf(r, t * sqrtf(2.f * (float) k / (float) max(c, 1)));
+            } else {
+                t = t * sqrtf(0.5f * (float) kDenseCands / (float) c);
+            }
+        }
+        int want = k, equal = 0;
+        uint32_t dk;
+        int ik = 0x7fffffff;
+        V3 ek = v3(0.f);
+        if (count >= 0) {
+            auto walk = [&](auto &&f) {
+                for (int q = lane; q < count; q += 32)
+                    f(q);
+            };
+            dk = warp_radix_select(walk, lane, bins, want, &equal, [&](int q, uint32_t &key) {
+                key = cand[q].x;
+                return true;
+            });
+            // of the photons at the k-th distance, keep the lowest `want` indices
+            if (equal > want) {
+                int eq2 = 0;
+                ik = (int) warp_radix_select(walk, lane, bins, want, &eq2,
+                                             [&](int q, uint32_t &key) {
+                                                 key = (uint32_t) v.order[cand[q].y];
+                                                 return cand[q].x == dk;
+                                             });
+            }
+            // the ordered sum of the kept powers (lane 0 holds it)
+            for (int base = 0; base < count; base += 32) {
+                const int q = base + lane;
+                bool keep = false;
+                V3 pw = v3(0.f);
+                if (q < count) {
+                    const uint2 cq = cand[q];
+                    keep = cq.x < dk || (cq.x == dk && v.order[cq.y] <= ik);
+                    if (keep) {
+                        const float4 pa = v.sorted[2 * cq.y];
+                        const float4 pb = v.sorted[2 * cq.y + 1];
+                        pw = v3(pa.w, pb.x, pb.y);
+                    }
                 }
+                for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
+                    const int l = __ffs(km) - 1;
+                    const V3 w = v3(__shfl_sync(full, pw.x, l), __shfl_sync(full, pw.y, l),
+                                    __shfl_sync(full, pw.z, l));
+                    ek = ek + w;
+                }
+            }
+        } else {
+            const GatherBox &b = big;
+            auto walk = [&](auto &&f) { walk_cells_warp(v, b, lane, f); };
+            dk = warp_radix_select(walk, lane, bins, want, &equal, [&](int s, uint32_t &key) {
+                const float dist = dist_of(s);
+                key = __float_as_uint(dist);
+                return dist <= r;
+            });
+            if (equal > want) {
+                int eq2 = 0;
+                ik = (int) warp_radix_select(walk, lane, bins, want, &eq2,
+                                             [&](int s, uint32_t &key) {
+                                                 key = (uint32_t) v.order[s];
+                                                 return __float_as_uint(dist_of(s)) == dk;
+                                             });
+            }
+            const float rk = __uint_as_float(dk);
+            for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
+                 cx = next_slab(g.occ[0], cx + 1, b.x1))
+                for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
+                     cy = next_slab(g.occ[1], cy + 1, b.y1))
+                    for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
+                         cz = next_slab(g.occ[2], cz + 1, b.z1)) {
+                        const int cell = cx + cy * g.res + cz * g.res * g.res;
+                        const int s0 = v.start[cell];
+                        if (s0 < 0)
+                            continue;
+                        for (int base = s0;; base += 32) {
+                            const int s = base + lane;
+                            const bool in_cell = s < v.n && v.cell_of[s] == cell;
+                            if (!__any_sync(full, in_cell))
+                                break;
+                            bool keep = false;
+                            V3 pw = v3(0.f);
+                            if (in_cell) {
+                                const float dist = dist_of(s);
+                                keep = dist < rk || (dist == rk && v.order[s] <= ik);
+                                if (keep) {
+                                    const float4 pa = v.sorted[2 * s];
+                                    const float4 pb = v.sorted[2 * s + 1];
+                                    pw = v3(pa.w, pb.x, pb.y);
+                                }
+                            }
+                            for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
+                                const int l = __ffs(km) - 1;
+                                const V3 w = v3(__shfl_sync(full, pw.x, l),
+                                                __shfl_sync(full, pw.y, l),
+                                                __shfl_sync(full, pw.z, l));
+                                ek = ek + w;
+                            }
+                        }
+                    }
+        }
         if (lane == 0) {
-            const V3 c = v3(sc.x, sc.y, sc.z) * (ek / disc_area(rk));
+            const V3 c = v3(sc.x, sc.y, sc.z) * (ek / disc_area(__uint_as_float(dk)));
             a.samples[__float_as_int(p.w)] = make_float4(c.x, c.y, c.z, 0.f);
         }
         __syncwarp();
@@ -821,7 +962,8 @@ __global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
                 if ((int64_t) slot < a.dense_cap) {
                     a.dense[2 * (size_t) slot] =
                         make_float4(in.p.x, in.p.y, in.p.z, __int_as_float((int) t));
-                    a.dense[2 * (size_t) slot + 1] = make_float4(scale.x, scale.y, scale.z, 0.f);
+                    a.dense[2 * (size_t) slot + 1] =
+                        make_float4(scale.x, scale.y, scale.z, __int_as_float(found));
                     deferred = true;
                     break;
                 }
@@ -961,8 +1103,11 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
     char *tail = scratch + (size_t) items * sizeof(float4) + acc_bytes + dense_bytes;
     a.next = reinterpret_cast<unsigned long long *>(tail);
     a.dense_count = reinterpret_cast<unsigned *>(tail + sizeof(unsigned long long));
-    int bps = 1;
+    a.dense_next = reinterpret_cast<unsigned long long *>(tail + 2 * sizeof(unsigned long long));
+    int bps = 1, dense_bps = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, block, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dense_bps, k_caustic_dense, 128, 0);
+    dense_bps = std::max(1, dense_bps);
     cudaError_t e = cudaSuccess;
     for (int s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
         a.s0 = s0;
@@ -970,17 +1115,21 @@ int render_caustics(const prr_scene *scene, const prr_photon_map *pmap,
         const int64_t total = npix * a.chunk;
         const int64_t grid = std::min<int64_t>((total + block - 1) / block,
                                                (int64_t) device_sm_count() * std::max(1, bps));
-        e = cudaMemsetAsync(tail, 0, 2 * sizeof(unsigned long long), st);
+        e = cudaMemsetAsync(tail, 0, 3 * sizeof(unsigned long long), st);
         if (e == cudaSuccess) {
             kern<<<(unsigned) grid, block, smem, st>>>(s.dev, view(pm), a);
+            pm.launches++;
             e = cudaGetLastError();
         }
         if (e == cudaSuccess && a.dense_cap > 0) {
-            k_caustic_dense<<<(unsigned) (device_sm_count() * 8), 128, 0, st>>>(view(pm), a);
+            k_caustic_dense<<<(unsigned) (device_sm_count() * dense_bps), 128, 0, st>>>(view(pm),
+                                                                                       a);
+            pm.launches++;
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) {
             k_caustic_film<<<(unsigned) ((npix + 255) / 256), 256, 0, st>>>(a);
+            pm.launches++;
             e = cudaGetLastError();
         }
     }
@@ -1039,6 +1188,7 @@ int prr_photon_emit(prr_photon_map *pmap, const prr_scene *scene, int64_t num_ph
         PRR_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(unsigned), st));
         EmitArgs a{num_photons, seed, max_depth, rec, keys, count, capacity, tcap};
         k_photon_emit<<<(unsigned) ((num_photons + block - 1) / block), block, smem, st>>>(s.dev, a);
+        pm.launches++;
         PRR_CUDA_TRY(cudaGetLastError());
         unsigned stored = 0;
         PRR_CUDA_TRY(cudaMemcpyAsync(&stored, count, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -1049,15 +1199,19 @@ int prr_photon_emit(prr_photon_map *pmap, const prr_scene *scene, int64_t num_ph
         }
         const int64_t n = stored;
         const int64_t np2 = pow2_at_least(std::max<int64_t>(n, 1));
-        if (np2 > n)
+        if (np2 > n) {
             k_fill_keys<<<(unsigned) ((np2 - n + 255) / 256), 256, 0, st>>>(keys, n, np2);
-        if (int rc = bitonic_sort(keys, np2, st))
+            pm.launches++;
+        }
+        if (int rc = bitonic_sort(keys, np2, st, &pm.launches))
             return rc;
         PRR_CUDA_TRY(pm.rec.ensure((size_t) std::max<int64_t>(n, 1) * 9 * sizeof(float)));
         PRR_CUDA_TRY(pm.owner.ensure((size_t) std::max<int64_t>(n, 1) * sizeof(int32_t)));
-        if (n > 0)
+        if (n > 0) {
             k_gather_records<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
                 keys, rec, n, pm.rec.as<float>(), pm.owner.as<int32_t>());
+            pm.launches++;
+        }
         PRR_CUDA_TRY(cudaGetLastError());
         PRR_CUDA_TRY(cudaStreamSynchronize(st));
         pm.n = n;
@@ -1107,10 +1261,13 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     k_grid_params<<<1, 1, 0, st>>>(partial, nb, radius, pm.params.as<GridParams>());
     k_cell_keys<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(pm.rec.as<float>(), n,
                                                               pm.params.as<GridParams>(), keys);
-    if (n2 > n)
+    pm.launches += 3;
+    if (n2 > n) {
         k_fill_keys<<<(unsigned) ((n2 - n + 255) / 256), 256, 0, st>>>(keys, n, n2);
+        pm.launches++;
+    }
     PRR_CUDA_TRY(cudaGetLastError());
-    if (int rc = bitonic_sort(keys, n2, st))
+    if (int rc = bitonic_sort(keys, n2, st, &pm.launches))
         return rc;
     GridParams g;
     PRR_CUDA_TRY(cudaMemcpyAsync(&g, pm.params.ptr, sizeof(g), cudaMemcpyDeviceToHost, st));
@@ -1126,6 +1283,7 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
         pm.start.as<int32_t>(), pm.sorted.as<float4>());
     k_cell_occupancy<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(keys, n,
                                                                      pm.params.as<GridParams>());
+    pm.launches += 2;
     PRR_CUDA_TRY(cudaGetLastError());
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     pm.res = g.res;
@@ -1143,6 +1301,13 @@ int prr_photon_info(const prr_photon_map *pmap, int64_t *count, int32_t *grid_re
         *count = pm.n;
     if (grid_res)
         *grid_res = pm.res;
+    return PRR_OK;
+}
+
+int prr_photon_launches(const prr_photon_map *pmap, int64_t *out) {
+    if (!pmap || !out)
+        return fail(PRR_ERR_INVALID_ARGUMENT, "photon map or out is NULL");
+    *out = PM(pmap)->launches.load();
     return PRR_OK;
 }
 
@@ -1177,6 +1342,7 @@ int prr_photon_gather(const prr_photon_map *pmap, const float *points, int64_t n
     }
     k_photon_gather<<<(unsigned) ((n + 127) / 128), 128, 0, st>>>(view(pm), points, n, k_nearest,
                                                                    out_rgb);
+    pm.launches++;
     PRR_CUDA_TRY(cudaGetLastError());
     return PRR_OK;
 }

@@ -253,3 +253,69 @@ def test_caustic_dense_queue_and_in_place_agree(ref, cuda):
     assert want.max() > 0
     assert rel_mse(full, want) < 1e-3
     assert (full.view(np.uint32) == want.view(np.uint32)).all(axis=2).mean() > 0.9
+
+
+@pytest.mark.parametrize("case", ["doubled", "pile"])
+def test_caustic_dense_selection_paths(ref, cuda, case):
+    """The dense-gather kernel selects among the photons it collects into
+    shared memory within a threshold distance, and walks the whole query box
+    instead when no threshold leaves between k and its capacity (1,024)
+    photons. Two photon arrays made from an emitted map: every photon doubled
+    (ties at the k-th distance, settled by the photon index, in shared
+    memory), and a pile of 3,000 coincident photons at the caustic's densest
+    spot (more than the capacity at every threshold that reaches the pile, so
+    gathers near it take the box walk, with ties among the pile). Pixels
+    against the in-place selection (a window whose dense gathers overflow the
+    queue against one-row windows that fit) bit for bit, and against the
+    oracle's render pass."""
+    desc = scenes.caustics(64, 64, level=2)
+    s = prr.Scene.from_desc(desc)
+    rec, _ = prr.PhotonMap().emit(s, 100_000, seed=1).build(0.05).export()
+    radius, k, spp = 0.1, 16, 16
+    if case == "doubled":
+        rec = np.concatenate([rec, rec])
+        rec[len(rec) // 2:, 6:] *= 1.5
+    else:
+        p = rec[:, :3].astype(np.float64)
+        d2 = ((p[:, None, :] - p[None, ::4, :]) ** 2).sum(axis=2)
+        focus = int(np.argmax((d2 < 0.05 ** 2).sum(axis=0))) * 4
+        pile = np.repeat(rec[focus:focus + 1], 3000, axis=0)
+        pile[:, 6:] *= np.linspace(0.5, 1.5, 3000, dtype=np.float32)[:, None]
+        rec = np.concatenate([rec[:focus], pile, rec[focus:]])
+    pm = prr.PhotonMap().set(rec).build(radius)
+    lum = pm.render_caustics(s, 2, k_nearest=0).cpu().numpy().sum(axis=2)
+    sums = [(lum[y:y + 16, x:x + 16].sum(), x, y) for y in range(0, 49, 4) for x in range(0, 49, 4)]
+    _, x0, y0 = max(sums)
+    win = (x0, y0, x0 + 16, y0 + 16)
+    full, c = pm.render_caustics_counts(s, spp, k_nearest=k, window=win)
+    full = full.cpu().numpy()
+    assert c["dense_gathers"] > max(1024, 16 * 16 * spp // 8), c
+    for y in range(y0, y0 + 16, 3):
+        row = pm.render_caustics(s, spp, k_nearest=k, window=(x0, y, x0 + 16, y + 1)).cpu().numpy()
+        assert np.array_equal(row.view(np.uint32), full[y - y0:y - y0 + 1].view(np.uint32)), y
+    want = ref.scene(desc).caustic_render(rec, radius, spp, k_nearest=k, window=win)
+    assert want.max() > 0
+    assert rel_mse(full, want) < 1e-3
+    assert (full.view(np.uint32) == want.view(np.uint32)).all(axis=2).mean() > 0.9
+
+
+def test_photon_map_counts_its_launches(cuda):
+    """prr_photon_launches counts the kernels of every call on the map: a
+    one-chunk caustic render launches the sample kernel and the film, plus
+    the dense-gather kernel when k > 0."""
+    desc = scenes.caustics(64, 64, level=2)
+    s = prr.Scene.from_desc(desc)
+    pm = prr.PhotonMap()
+    assert pm.launches() == 0
+    pm.emit(s, 100_000, seed=1)
+    n0 = pm.launches()
+    assert n0 >= 2
+    pm.build(0.05)
+    n1 = pm.launches()
+    assert n1 >= n0 + 5
+    pm.render_caustics(s, 4, k_nearest=0)
+    assert pm.launches() == n1 + 2
+    pm.render_caustics(s, 4, k_nearest=16)
+    assert pm.launches() == n1 + 5
+    pm.gather(np.zeros((8, 3), np.float32))
+    assert pm.launches() == n1 + 6
