@@ -271,7 +271,7 @@ def test_caustic_dense_selection_paths(ref, cuda, case):
     desc = scenes.caustics(64, 64, level=2)
     s = prr.Scene.from_desc(desc)
     rec, _ = prr.PhotonMap().emit(s, 100_000, seed=1).build(0.05).export()
-    radius, k, spp = 0.1, 16, 16
+    radius, k, spp = 0.3, 16, 16
     if case == "doubled":
         rec = np.concatenate([rec, rec])
         rec[len(rec) // 2:, 6:] *= 1.5
