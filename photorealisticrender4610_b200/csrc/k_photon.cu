@@ -876,9 +876,10 @@ __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a
 // One (pixel, sample) item per thread at a time: sample n of window pixel q is
 // item n * npix + q, so a warp's lanes trace neighbouring pixels; its result
 // goes to slot n * npix + q, so the image does not depend on which thread
-// took which item.
+// took which item. Held to 64 registers (8 resident blocks of 128 instead of
+// 7; the in-place k-nearest arrays live in local memory either way).
 template <bool COUNT>
-__global__ void k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
+__global__ void __launch_bounds__(128, 8) k_caustic_samples(DevScene S, GridView v, CausticArgs a) {
     extern __shared__ uint2 smem[];
     SmemStack tst{smem + threadIdx.x, (int) blockDim.x, 0, S.tlas_depth + 1, S.check};
     SmemStack bst{smem + (size_t) a.tlas_cap * blockDim.x + threadIdx.x, (int) blockDim.x, 0,

@@ -143,7 +143,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
     const unsigned full = 0xffffffffu;
     int64_t idx = -1;
     RayD r{};
-    RayPre p{};
+    RayPair p{};
     float best = kInf;
     int hit = -1;
     uint32_t ref = 0, tri = 0, ntri = 0;
@@ -167,7 +167,7 @@ __global__ void k_mesh_closest_refill(MeshArgs a, int refill) {
                 if (ni < a.n) {
                     idx = ray_at(a, ni);
                     r = load_ray(a.O, a.D, idx);
-                    p = precompute(r);
+                    p = precompute_pair(r);
                     best = kInf;
                     hit = -1;
                     sp = 0;

@@ -114,6 +114,63 @@ __device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, fl
     return tmin <= tmax ? tmin : kInf;
 }
 
+// The same precomputation with the origin and the reciprocal direction held
+// twice per axis, as the register pairs of sm_100's packed float2 arithmetic:
+// one packed subtract and one packed multiply give an axis's distances to both
+// of its planes. Used by the query-set kernel, which has the registers for
+// the pairs (in the wavefront stages the six extra registers cost a resident
+// block per SM, more than the packed arithmetic saves).
+struct RayPair {
+    float2 o2x, o2y, o2z; // (o, o) per axis
+    float2 i2x, i2y, i2z; // (1/d, 1/d) per axis
+    bool nx, ny, nz;      // octant: direction negative on that axis
+};
+
+__device__ __forceinline__ RayPair precompute_pair(const RayD &r) {
+    const RayPre q = precompute(r);
+    RayPair p;
+    p.o2x = make_float2(q.ox, q.ox);
+    p.o2y = make_float2(q.oy, q.oy);
+    p.o2z = make_float2(q.oz, q.oz);
+    p.i2x = make_float2(q.ix, q.ix);
+    p.i2y = make_float2(q.iy, q.iy);
+    p.i2z = make_float2(q.iz, q.iz);
+    p.nx = q.nx;
+    p.ny = q.ny;
+    p.nz = q.nz;
+    return p;
+}
+
+// (a.x - b.x, a.y - b.y), each rounded to nearest like the scalar subtract.
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 a2, b2, d2;\n\t"
+        "mov.b64 a2, {%2, %3};\n\t"
+        "mov.b64 b2, {%4, %5};\n\t"
+        "sub.rn.f32x2 d2, a2, b2;\n\t"
+        "mov.b64 {%0, %1}, d2;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// slab() on the packed form: per axis (t at the min plane, t at the max
+// plane) as (plane - o) * inv, each lane the float the scalar form computes;
+// the octant then picks which of the two enters, as the reference picks the
+// plane before subtracting.
+__device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, float z0, float z1,
+                                      const RayPair &p) {
+    const float2 tx = __fmul2_rn(fsub2(make_float2(x0, x1), p.o2x), p.i2x);
+    const float2 ty = __fmul2_rn(fsub2(make_float2(y0, y1), p.o2y), p.i2y);
+    const float2 tz = __fmul2_rn(fsub2(make_float2(z0, z1), p.o2z), p.i2z);
+    const float t0x = p.nx ? tx.y : tx.x, t1x = p.nx ? tx.x : tx.y;
+    const float t0y = p.ny ? ty.y : ty.x, t1y = p.ny ? ty.x : ty.y;
+    const float t0z = p.nz ? tz.y : tz.x, t1z = p.nz ? tz.x : tz.y;
+    const float tmin = fmax3(fmaxf(0.f, t0x), t0y, t0z);
+    const float tmax = fmin3(fminf(kInf, t1x), t1y, t1z);
+    return tmin <= tmax ? tmin : kInf;
+}
+
 __device__ __forceinline__ float slab6(const float *b, const RayPre &p) {
     return slab(b[0], b[1], b[2], b[3], b[4], b[5], p);
 }
