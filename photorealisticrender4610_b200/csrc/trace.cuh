@@ -117,9 +117,10 @@ __device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, fl
 // The same precomputation with the origin and the reciprocal direction held
 // twice per axis, as the register pairs of sm_100's packed float2 arithmetic:
 // one packed subtract and one packed multiply give an axis's distances to both
-// of its planes. Used by the query-set kernel, which has the registers for
-// the pairs (in the wavefront stages the six extra registers cost a resident
-// block per SM, more than the packed arithmetic saves).
+// of its planes. Used by the query-set kernel and by the any-hit walk of the
+// wavefront's shadow stage, which have the registers for the pairs (in the
+// closest-hit walk of the extend stage the six extra registers cost a
+// resident block per SM, more than the packed arithmetic saves).
 struct RayPair {
     float2 o2x, o2y, o2z; // (o, o) per axis
     float2 i2x, i2y, i2z; // (1/d, 1/d) per axis
@@ -172,6 +173,10 @@ __device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, fl
 }
 
 __device__ __forceinline__ float slab6(const float *b, const RayPre &p) {
+    return slab(b[0], b[1], b[2], b[3], b[4], b[5], p);
+}
+
+__device__ __forceinline__ float slab6(const float *b, const RayPair &p) {
     return slab(b[0], b[1], b[2], b[3], b[4], b[5], p);
 }
 

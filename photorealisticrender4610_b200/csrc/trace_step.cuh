@@ -160,7 +160,7 @@ struct ClosestWalk {
 // Sphere intersectT (BVH.cpp:421-473, Triangle.hpp:141-147, Object.hpp:24-29).
 struct AnyWalk {
     RayD r;
-    RayPre p;
+    RayPair p;
     float tmax;
     uint32_t tref;
     int tsp;
@@ -172,7 +172,7 @@ struct AnyWalk {
     // false when the scene's root box already misses
     __device__ __forceinline__ bool start(const DevScene &S, const RayD &ray, float t_max) {
         r = ray;
-        p = precompute(ray);
+        p = precompute_pair(ray);
         tmax = t_max;
         tref = S.tlas_root;
         tsp = 0;
