@@ -858,6 +858,7 @@ def serving_result(args, rank, world, n_requests=None, arms_text=None):
         for s_ in scenes_:
             srv.add_scene(s_)
         srv.wait(srv.submit(0, 2, depth, size=(64, 64)))  # warm-up
+        launches0 = srv.stats()["launches"]
         ids = [None] * n
         t_start = time.perf_counter()
 
@@ -873,6 +874,7 @@ def serving_result(args, rank, world, n_requests=None, arms_text=None):
         th.join()
         infos = [srv.wait(i) for i in ids]
         st = srv.stats()
+        st["timed_launches"] = st["launches"] - launches0
         srv.close()
         lat = np.array([i["done_s"] - i["submit_s"] for i in infos])
         span = max(i["done_s"] for i in infos) - min(i["submit_s"] for i in infos)
@@ -920,6 +922,7 @@ def serving_result(args, rank, world, n_requests=None, arms_text=None):
         "server_steps": "wavefront (all running requests in one set of ordered ray queues)",
         **extra,
         "failed": int(st["failed"]),
+        "gpu_launches": int(st["timed_launches"]),
         "e2e": {"value": served_rate, "unit": "Msamples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(np.mean([w * h * 12 for _, (w, h), _ in reqs]))},
         "clocks": clk.summary(),

@@ -439,6 +439,7 @@ typedef struct prr_server_stats {
     double complete_s;            /* worker time resolving and returning finished images */
     int64_t bytes_in_use;
     double now_s;
+    int64_t launches;             /* kernels launched by the worker so far */
 } prr_server_stats;
 int prr_server_create(const prr_server_config *config, prr_server **out);
 /* Cancels queued requests, finishes running ones, joins the worker. */

@@ -70,7 +70,7 @@ class prr_server_stats(C.Structure):
                 ("active", C.c_int64), ("queued", C.c_int64), ("samples", C.c_int64),
                 ("rays", C.c_uint64), ("steps", C.c_int64), ("busy_s", C.c_double),
                 ("admit_s", C.c_double), ("complete_s", C.c_double),
-                ("bytes_in_use", C.c_int64), ("now_s", C.c_double)]
+                ("bytes_in_use", C.c_int64), ("now_s", C.c_double), ("launches", C.c_int64)]
 
 
 class prr_scene_stats(C.Structure):

@@ -99,7 +99,7 @@ struct Server {
     static constexpr size_t kPoolCap = (size_t) 2 << 30;
 
     // stats
-    int64_t submitted = 0, completed = 0, failed = 0, samples = 0, steps = 0;
+    int64_t submitted = 0, completed = 0, failed = 0, samples = 0, steps = 0, launches = 0;
     unsigned long long rays = 0;
     double busy = 0, admit_time = 0, complete_time = 0;
 
@@ -306,6 +306,7 @@ int run_step_wavefront(Server &S) {
     PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
     S.busy += now_s() - t0;
     S.steps++;
+    S.launches += launches;
     for (size_t k = 0; k < S.stepped.size(); k++) {
         Req *r = S.active[S.stepped[k]];
         const int c = S.chunks[S.stepped[k]];
@@ -362,6 +363,7 @@ int run_step(Server &S) {
     PRR_CUDA_TRY(cudaStreamSynchronize(S.st));
     S.busy += now_s() - t0;
     S.steps++;
+    S.launches += n_items > 0 ? 1 : 0;
     for (size_t q = 0; q < S.active.size(); q++) {
         Req *r = S.active[q];
         const int s1 = std::min(r->next + r->chunk, r->rs.max_spp);
@@ -381,6 +383,7 @@ int complete(Server &S, std::vector<Req *> &done) {
         if (int rc = serve_resolve(static_cast<const float3 *>(r->film), r->npix, r->rs.max_spp,
                                    target, S.st))
             return rc;
+        S.launches++;
         if (!r->out_on_device)
             PRR_CUDA_TRY(cudaMemcpyAsync(r->out, r->result, (size_t) r->npix * 3 * sizeof(float),
                                          cudaMemcpyDeviceToHost, S.st));
@@ -666,6 +669,7 @@ int prr_server_stats_get(prr_server *server, prr_server_stats *out) {
     out->complete_s = S.complete_time;
     out->bytes_in_use = (int64_t) S.used;
     out->now_s = now_s();
+    out->launches = S.launches;
     return PRR_OK;
 }
 

@@ -80,6 +80,8 @@ def test_same_alone_and_in_mix(scene_set, integrator, paths_per_launch):
     st = srv.stats()
     assert st["completed"] == len(JOBS) and st["failed"] == 0 and st["steps"] > 0
     assert st["rays"] == sum(alone_rays)
+    # at least one kernel per step and one resolve per finished request
+    assert st["launches"] >= st["steps"] + len(JOBS)
     srv.close()
     # and each equals the plain renderer: bit for bit where samples are added
     # one by one (wavefront), up to how the sums are grouped otherwise
