@@ -830,6 +830,13 @@ template <bool MULTI, bool STATS = false>
 __global__ void k_wf_extend(DevScene S, Wf w, int it, int refill) {
     wf_extend<MULTI, STATS>(S, w, it, refill);
 }
+// The server's extend stage (paths of several requests; the request index
+// selects scene and camera) held to 56 registers: 9 resident blocks of 128
+// instead of 8 at the 64 it takes otherwise, without spills. (The one-scene
+// stage already fits in 56, and a cap there made it slower.)
+__global__ void __maxnreg__(56) k_wf_extend_multi(DevScene S, Wf w, int it, int refill) {
+    wf_extend<true, false>(S, w, it, refill);
+}
 template <bool MULTI, bool STATS = false> __global__ void k_wf_shadow(DevScene S, Wf w, int refill) {
     wf_shadow<MULTI, STATS>(S, w, refill);
 }
@@ -1274,7 +1281,7 @@ int wf_shape(Wf &w, DevBuf &spill, int block_req, int stack_req, int refill_req,
     w.blas_sm = std::max(1, std::min(w.blas_sm, max_sm_entries - w.tlas_cap));
     L.smem_ext = (size_t) (w.tlas_cap + w.blas_sm) * L.block * sizeof(uint2);
     L.smem_sh = (size_t) (w.tlas_cap + w.blas_sm) * L.block * sizeof(uint32_t);
-    L.ext = k_wf_extend<MULTI>;
+    L.ext = MULTI ? k_wf_extend_multi : k_wf_extend<false>;
     L.sh = k_wf_shadow<MULTI>;
     if constexpr (!MULTI) {
         if (w.stats) { // the counting variants (a separate, untimed render)
