@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -36,6 +37,7 @@ struct PhotonMap {
     // grid
     bool built = false;
     float radius = 0.01f; // PhotonMap::photon_radius default (Photon.hpp:36)
+    float inside_sq = 1e-4f; // the largest float s with sqrtf(s) <= radius
     int res = 0;
     float bmin[3] = {0, 0, 0}, cs[3] = {1, 1, 1};
     DevBuf order;    // n int32: photon index, sorted by (cell, index)
@@ -222,6 +224,25 @@ int bitonic_sort(unsigned long long *keys, int64_t n2, cudaStream_t st,
     return PRR_OK;
 }
 
+// The largest float s with sqrtf(s) <= r (r finite and > 0): the threshold
+// on a squared distance that decides `sqrtf(d.d) <= r` without the square
+// root (IEEE sqrt is correctly rounded and monotone, on the host as on the
+// device built with IEEE sqrt).
+float inside_square(float r) {
+    if (!std::isfinite(r))
+        return r;
+    float t = r * r;
+    while (t > 0.f && std::sqrt(t) > r)
+        t = std::nextafter(t, 0.f);
+    for (;;) {
+        const float n = std::nextafter(t, INFINITY);
+        if (!(std::sqrt(n) <= r))
+            break;
+        t = n;
+    }
+    return t;
+}
+
 int64_t pow2_at_least(int64_t n) {
     int64_t p = 2048;
     while (p < n)
@@ -362,6 +383,9 @@ struct GridView {
     const GridParams *g;
     int64_t n;
     float radius;
+    // the largest float s with sqrtf(s) <= radius: sqrtf is correctly
+    // rounded and monotone, so |d| <= radius exactly when d.d <= inside_sq
+    float inside_sq;
 };
 
 // pi r^2 as estimateIrradiance computes it (Photon.cpp:87): all in float,
@@ -432,16 +456,16 @@ template <bool COUNT = false>
 __device__ __forceinline__ V3 radius_sum(const GridView &v, const GatherBox &b, V3 pos,
                                          int &found, unsigned *tested = nullptr,
                                          unsigned *inside = nullptr) {
-    const float r = v.radius;
     V3 e = v3(0.f);
     found = 0;
     walk_cells(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int s) {
         const float4 pa = v.sorted[2 * s];
         const V3 d = v3(pa.x, pa.y, pa.z) - pos;
-        const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        // sqrtf(d.d) <= r, decided on d.d
+        const float dd = d.x * d.x + d.y * d.y + d.z * d.z;
         if constexpr (COUNT)
             (*tested)++;
-        if (dist <= r) {
+        if (dd <= v.inside_sq) {
             if constexpr (COUNT)
                 (*inside)++;
             const float4 pb = v.sorted[2 * s + 1];
@@ -1031,6 +1055,7 @@ GridView view(const PhotonMap &pm) {
     v.g = pm.params.as<GridParams>();
     v.n = pm.n;
     v.radius = pm.radius;
+    v.inside_sq = pm.inside_sq;
     return v;
 }
 
@@ -1246,6 +1271,7 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     PhotonMap &pm = *PM(pmap);
     cudaStream_t st = (cudaStream_t) stream;
     pm.radius = radius;
+    pm.inside_sq = inside_square(radius);
     PRR_CUDA_TRY(pm.params.ensure(sizeof(GridParams)));
     if (pm.n == 0) {
         pm.built = true;

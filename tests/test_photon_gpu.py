@@ -319,3 +319,36 @@ def test_photon_map_counts_its_launches(cuda):
     assert pm.launches() == n1 + 5
     pm.gather(np.zeros((8, 3), np.float32))
     assert pm.launches() == n1 + 6
+
+
+def test_gather_radius_boundary_bit_exact(ref, port, cuda):
+    """The fixed-radius test decides sqrtf(d.d) <= r on d.d against the
+    largest float whose square root is at most r. Photons on rings whose
+    radii step through r by a tenth of an ulp at a time (so the computed
+    distance falls on either side of r, and on it), around several query
+    points: the sums equal the reference estimator's bit for bit, with and
+    without the k-nearest cap."""
+    rng = np.random.default_rng(11)
+    r = np.float32(0.05)
+    q = rng.uniform(-1, 1, (8, 3)).astype(np.float32) * np.float32([1, 0.05, 1])
+    recs = []
+    for j in range(len(q)):
+        u = rng.normal(size=(300, 3))
+        u = (u / np.linalg.norm(u, axis=1, keepdims=True)).astype(np.float32)
+        s = (r * (1 + (np.arange(300, dtype=np.float32) - 150) * np.float32(1e-8))).astype(np.float32)
+        rec = np.zeros((300, 9), np.float32)
+        rec[:, :3] = q[j] + u * s[:, None]
+        rec[:, 6:] = rng.uniform(0, 1e-3, (300, 3))
+        recs.append(rec)
+    rec = np.concatenate(recs + [random_photons(5000, 12)[0]])
+    d = (rec[None, :, :3] - q[:, None, :]).astype(np.float32)
+    dist = np.sqrt((d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2])
+    assert ((dist == r).sum() > 0) and ((np.abs(dist - r) <= 4e-9).sum() > 100)
+    pm = prr.PhotonMap().set(rec).build(float(r))
+    want, _ = ref.photon_estimate(rec, float(r), q)
+    got = pm.gather(q).cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    want16, inside = ref.photon_estimate_knn(rec, float(r), q, 16)
+    assert (inside > 16).all()
+    got16 = pm.gather(q, k_nearest=16).cpu().numpy()
+    assert np.array_equal(got16.view(np.uint32), want16.view(np.uint32))
