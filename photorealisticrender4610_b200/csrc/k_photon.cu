@@ -41,10 +41,10 @@ struct PhotonMap {
     int res = 0;
     float bmin[3] = {0, 0, 0}, cs[3] = {1, 1, 1};
     DevBuf order;    // n int32: photon index, sorted by (cell, index)
-    DevBuf cell_of;  // n int32: cell of order[i]
     DevBuf start;    // res^3 int32: first position in `order` of each cell, -1 if empty
-    DevBuf sorted;   // n x 2 float4 in `order`: position + power r, power g b (gathers
-                     // read a cell's photons contiguously)
+    DevBuf sorted;   // n x 2 float4 in `order`: position + power r, then power g b + the
+                     // slot's cell as int bits (gathers read a cell's photons
+                     // contiguously and stop where the cell changes)
     DevBuf params;   // device copy of the grid parameters
     DevBuf scratch;
     // kernels launched by calls on this map (emit, build, gather, caustic
@@ -360,17 +360,16 @@ __global__ void k_cell_occupancy(const unsigned long long *keys, int64_t n, Grid
 }
 
 __global__ void k_cell_table(const unsigned long long *keys, const float *rec, int64_t n,
-                             int32_t *order, int32_t *cell_of, int32_t *start, float4 *sorted) {
+                             int32_t *order, int32_t *start, float4 *sorted) {
     const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const unsigned cell = (unsigned) (keys[i] >> 32);
     const int32_t o = (int32_t) (keys[i] & 0xffffffffu);
     order[i] = o;
-    cell_of[i] = (int32_t) cell;
     const float *p = rec + (size_t) o * 9;
     sorted[2 * i] = make_float4(p[0], p[1], p[2], p[6]);
-    sorted[2 * i + 1] = make_float4(p[7], p[8], 0.f, 0.f);
+    sorted[2 * i + 1] = make_float4(p[7], p[8], __int_as_float((int) cell), 0.f);
     if (i == 0 || (unsigned) (keys[i - 1] >> 32) != cell)
         start[cell] = (int32_t) i;
 }
@@ -379,7 +378,7 @@ __global__ void k_cell_table(const unsigned long long *keys, const float *rec, i
 struct GridView {
     const float *rec;
     const float4 *sorted;
-    const int32_t *order, *cell_of, *start;
+    const int32_t *order, *start;
     const GridParams *g;
     int64_t n;
     float radius;
@@ -387,6 +386,12 @@ struct GridView {
     // rounded and monotone, so |d| <= radius exactly when d.d <= inside_sq
     float inside_sq;
 };
+
+// The cell of sorted slot s (kept beside the slot's power, in the sector a
+// gather reads anyway).
+__device__ __forceinline__ int cell_at(const GridView &v, int64_t s) {
+    return __float_as_int(v.sorted[2 * s + 1].z);
+}
 
 // pi r^2 as estimateIrradiance computes it (Photon.cpp:87): all in float,
 // since the reference redefines M_PI as a float literal (global.hpp:9-10).
@@ -423,7 +428,7 @@ __device__ __forceinline__ void walk_cells(const GridView &v, const GridParams &
                 int s = v.start[cell];
                 if (s < 0)
                     continue;
-                for (; s < v.n && v.cell_of[s] == cell; s++)
+                for (; s < v.n && cell_at(v, s) == cell; s++)
                     f(s);
             }
 }
@@ -610,7 +615,7 @@ __device__ __forceinline__ void walk_cells_warp(const GridView &v, const GatherB
                 const int s0 = v.start[cell];
                 if (s0 < 0)
                     continue;
-                for (int s = s0 + lane; s < v.n && v.cell_of[s] == cell; s += 32)
+                for (int s = s0 + lane; s < v.n && cell_at(v, s) == cell; s += 32)
                     f(s);
             }
 }
@@ -764,7 +769,7 @@ __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a
                             continue;
                         for (int base = s0;; base += 32) {
                             const int s = base + lane;
-                            const bool in_cell = s < v.n && v.cell_of[s] == cell;
+                            const bool in_cell = s < v.n && cell_at(v, s) == cell;
                             if (!__any_sync(full, in_cell))
                                 break;
                             float dist = 0.f;
@@ -865,7 +870,7 @@ __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a
                             continue;
                         for (int base = s0;; base += 32) {
                             const int s = base + lane;
-                            const bool in_cell = s < v.n && v.cell_of[s] == cell;
+                            const bool in_cell = s < v.n && cell_at(v, s) == cell;
                             if (!__any_sync(full, in_cell))
                                 break;
                             bool keep = false;
@@ -1050,7 +1055,6 @@ GridView view(const PhotonMap &pm) {
     v.rec = pm.rec.as<float>();
     v.sorted = pm.sorted.as<float4>();
     v.order = pm.order.as<int32_t>();
-    v.cell_of = pm.cell_of.as<int32_t>();
     v.start = pm.start.as<int32_t>();
     v.g = pm.params.as<GridParams>();
     v.n = pm.n;
@@ -1301,12 +1305,11 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     const size_t cells = (size_t) g.res * g.res * g.res;
     PRR_CUDA_TRY(pm.order.ensure((size_t) n * sizeof(int32_t)));
-    PRR_CUDA_TRY(pm.cell_of.ensure((size_t) n * sizeof(int32_t)));
     PRR_CUDA_TRY(pm.start.ensure(cells * sizeof(int32_t)));
     PRR_CUDA_TRY(cudaMemsetAsync(pm.start.ptr, 0xff, cells * sizeof(int32_t), st));
     PRR_CUDA_TRY(pm.sorted.ensure((size_t) n * 2 * sizeof(float4)));
     k_cell_table<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
-        keys, pm.rec.as<float>(), n, pm.order.as<int32_t>(), pm.cell_of.as<int32_t>(),
+        keys, pm.rec.as<float>(), n, pm.order.as<int32_t>(),
         pm.start.as<int32_t>(), pm.sorted.as<float4>());
     k_cell_occupancy<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(keys, n,
                                                                      pm.params.as<GridParams>());
