@@ -259,7 +259,7 @@ def test_caustic_dense_queue_and_in_place_agree(ref, cuda):
 def test_caustic_dense_selection_paths(ref, cuda, case):
     """The dense-gather kernel selects among the photons it collects into
     shared memory within a threshold distance, and walks the whole query box
-    instead when no threshold leaves between k and its capacity (1,024)
+    instead when no threshold leaves between k and its capacity (512)
     photons. Two photon arrays made from an emitted map: every photon doubled
     (ties at the k-th distance, settled by the photon index, in shared
     memory), and a pile of 3,000 coincident photons at the caustic's densest
