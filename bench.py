@@ -399,7 +399,9 @@ def run_ours(args, rank, world, on):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": query_config(world),
-        "run": {"launch": best, "e2e_launch": e2e_cfg, "step_ms": [round(x, 3) for x in kernel_ms],
+        "run": {"launch": best, "e2e_launch": e2e_cfg,
+                "tuned_fastest": [[round(ms, 3), c] for ms, c in sorted(tuned, key=lambda x: x[0])[:6]],
+                "step_ms": [round(x, 3) for x in kernel_ms],
                 "median_ms": ms_median, "e2e_ms": [round(x, 3) for x in e2e_ms]},
         "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": N_RAYS * 24,
                 "d2h_bytes_per_step": N_RAYS * 8},

@@ -281,7 +281,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
     const unsigned full = 0xffffffffu;
     int64_t idx = -1;
     RayD r{};
-    RayPre p{};
+    RayPair p{};
     float best = kInf;
     int hit = -1;
     uint32_t ref = kNoRef; // walk position: interior node, leaf waiting for the slot, or none
@@ -309,7 +309,7 @@ __global__ void k_mesh_closest_phased(MeshArgs a, int refill, int tri_min) {
                 if (ni < a.n) {
                     idx = ray_at(a, ni);
                     r = load_ray(a.O, a.D, idx);
-                    p = precompute(r);
+                    p = precompute_pair(r);
                     best = kInf;
                     hit = -1;
                     sp = 0;

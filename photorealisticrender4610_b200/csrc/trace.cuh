@@ -117,7 +117,7 @@ __device__ __forceinline__ float slab(float x0, float x1, float y0, float y1, fl
 // The same precomputation with the origin and the reciprocal direction held
 // twice per axis, as the register pairs of sm_100's packed float2 arithmetic:
 // one packed subtract and one packed multiply give an axis's distances to both
-// of its planes. Used by the query-set kernel and by the any-hit walk of the
+// of its planes. Used by the query-set kernels and by the any-hit walk of the
 // wavefront's shadow stage, which have the registers for the pairs (in the
 // closest-hit walk of the extend stage the six extra registers cost a
 // resident block per SM, more than the packed arithmetic saves).
