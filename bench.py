@@ -325,13 +325,13 @@ def run_ours(args, rank, world, on):
     with ClockSampler(dev.index if world == 1 else int(os.environ.get("LOCAL_RANK", 0))) as clk:
         barrier(on)
         torch.cuda.synchronize()
+        # keep the GPU busy (about 0.3 s) while the host enqueues all K steps,
+        # so no host-side latency falls between a step's two events: a driver
+        # call can wait tens of ms on the nvidia-smi clock sampler, which a
+        # per-step cushion did not always cover
+        torch.cuda._sleep(SLEEP_CYCLES * 10)
         for k in range(args.steps):
             flush.zero_()
-            # keep the GPU busy (about 30 ms) while the host enqueues the timed
-            # launch, so no host-side latency falls between the two events (the
-            # driver calls of a launch can wait a few ms on the nvidia-smi
-            # clock sampler)
-            torch.cuda._sleep(SLEEP_CYCLES)
             starts[k].record()
             hid, t = scene.mesh_intersect(0, O, D, config=best)
             ends[k].record()
