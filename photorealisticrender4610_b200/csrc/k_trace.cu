@@ -812,8 +812,6 @@ int launch_mesh_closest(const Scene &s, int object, const float *o, const float 
     if (n == 0)
         return PRR_OK;
     const HostObject &obj = s.objects[object];
-    const DevObject *dobj = nullptr;
-    (void) dobj;
     MeshArgs a;
     a.nodes = s.dev.nodes;
     a.tris = s.dev.tris;

@@ -85,7 +85,7 @@ struct HostObject {
     float radius = 0.f;
     // filled by build
     FlatBVH bvh;
-    PrimBox bounds;
+    PrimBox bounds{};
     float area = 0.f;
     int tri_base = 0;
     uint32_t root = 0;
