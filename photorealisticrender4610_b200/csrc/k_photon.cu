@@ -17,9 +17,12 @@
 // the same order as the reference and gets the same float sum.
 //
 // Sorting: an in-house bitonic sort over 64-bit keys (global passes for long
-// strides, shared-memory passes for strides below 1024).
+// strides, shared-memory passes for strides below 2048), in one cooperative
+// launch when the device holds all of its blocks at once.
 #include "integrator.cuh"
 #include "prr_internal.h"
+
+#include <cooperative_groups.h>
 
 #include <algorithm>
 #include <atomic>
@@ -27,6 +30,8 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
+
+namespace cg = cooperative_groups;
 
 namespace prr {
 
@@ -205,10 +210,96 @@ __global__ void k_bitonic_shared(unsigned long long *keys, int64_t k, int j0) {
     keys[base + threadIdx.x + 1024] = t[threadIdx.x + 1024];
 }
 
-// Sorts keys[0, n2) ascending; n2 is a power of two >= 2048. Adds its kernel
-// launches to *launches.
+// The whole bitonic sort of n2 keys in one cooperative launch of n2 / 2048
+// blocks: block b keeps keys [2048 b, 2048 b + 2048) in shared memory for the
+// strides below 2048 of every stage, and the strides of 2048 and more run on
+// global memory between grid-wide barriers (the launch guarantees that all
+// blocks are resident, so the barriers complete). The same compare-exchange
+// network as k_bitonic_global + k_bitonic_shared, in the same order.
+__global__ void __launch_bounds__(1024) k_bitonic_coop(unsigned long long *keys, int64_t n2) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ unsigned long long t[2048];
+    const int64_t base = (int64_t) blockIdx.x * 2048;
+    const int64_t nthreads = (int64_t) gridDim.x * blockDim.x;
+    const int64_t gtid = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    t[threadIdx.x] = keys[base + threadIdx.x];
+    t[threadIdx.x + 1024] = keys[base + threadIdx.x + 1024];
+    __syncthreads();
+    for (int64_t k = 2; k <= n2; k <<= 1) {
+        int64_t j = k >> 1;
+        if (j >= 2048) {
+            keys[base + threadIdx.x] = t[threadIdx.x];
+            keys[base + threadIdx.x + 1024] = t[threadIdx.x + 1024];
+            grid.sync();
+            for (; j >= 2048; j >>= 1) {
+                for (int64_t i = gtid; i < n2; i += nthreads) {
+                    const int64_t l = i ^ j;
+                    if (l > i) {
+                        const bool up = (i & k) == 0;
+                        const unsigned long long a = keys[i], b = keys[l];
+                        if ((a > b) == up) {
+                            keys[i] = b;
+                            keys[l] = a;
+                        }
+                    }
+                }
+                grid.sync();
+            }
+            t[threadIdx.x] = keys[base + threadIdx.x];
+            t[threadIdx.x + 1024] = keys[base + threadIdx.x + 1024];
+            __syncthreads();
+        }
+        for (; j > 0; j >>= 1) {
+            for (int h = 0; h < 2; h++) {
+                const int i = (int) threadIdx.x + h * 1024;
+                const int l = i ^ (int) j;
+                if (l > i) {
+                    const bool up = ((base + i) & k) == 0;
+                    const unsigned long long a = t[i], b = t[l];
+                    if ((a > b) == up) {
+                        t[i] = b;
+                        t[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    keys[base + threadIdx.x] = t[threadIdx.x];
+    keys[base + threadIdx.x + 1024] = t[threadIdx.x + 1024];
+}
+
+// Blocks of k_bitonic_coop that can be resident at once on this device (0:
+// no cooperative launch).
+int64_t coop_sort_blocks() {
+    static const int64_t blocks = [] {
+        int dev = 0, coop = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess ||
+            !coop ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bitonic_coop, 1024, 0) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return int64_t(0);
+        }
+        return (int64_t) per_sm * device_sm_count();
+    }();
+    return blocks;
+}
+
+// Sorts keys[0, n2) ascending; n2 is a power of two >= 2048. One cooperative
+// launch when the device holds all n2 / 2048 blocks at once, else a launch
+// per stage (and per large stride). Adds its kernel launches to *launches.
 int bitonic_sort(unsigned long long *keys, int64_t n2, cudaStream_t st,
                  std::atomic<int64_t> *launches) {
+    if (n2 / 2048 <= coop_sort_blocks()) {
+        void *args[] = {(void *) &keys, (void *) &n2};
+        PRR_CUDA_TRY(cudaLaunchCooperativeKernel((const void *) k_bitonic_coop,
+                                                 dim3((unsigned) (n2 / 2048)), dim3(1024), args,
+                                                 0, st));
+        *launches += 1;
+        return PRR_OK;
+    }
     const int tb = 256;
     const unsigned grid = (unsigned) ((n2 + tb - 1) / tb);
     int64_t count = 0;
