@@ -11,10 +11,14 @@
 //
 // Grid: the reference bins photons into an unordered_map keyed by cell index
 // with per-cell vectors in insertion order, and a query walks the cell box in
-// x, y, z order. Here photons are sorted by (cell, position in the photon
-// array) -- unique keys, so the order is fully determined -- and a per-cell
-// start table replaces the hash map. A query therefore adds the same photons in
-// the same order as the reference and gets the same float sum.
+// x, y, z order. Here cells are numbered in that walk order (x slowest, z
+// fastest) and photons sorted by (cell, position in the photon array) --
+// unique keys, so the order is fully determined. A table of lower bounds
+// (for each cell, the first sorted slot of that cell or a later one) replaces
+// the hash map: the cells (cx, cy, z0..z1) of a query box are consecutive, so
+// a column of the box is one slot range, read with two lookups. A query
+// therefore adds the same photons in the same order as the reference and gets
+// the same float sum.
 //
 // Sorting: an in-house bitonic sort over 64-bit keys (global passes for long
 // strides, shared-memory passes for strides below 2048), in one cooperative
@@ -46,7 +50,9 @@ struct PhotonMap {
     int res = 0;
     float bmin[3] = {0, 0, 0}, cs[3] = {1, 1, 1};
     DevBuf order;    // n int32: photon index, sorted by (cell, index)
-    DevBuf start;    // res^3 int32: first position in `order` of each cell, -1 if empty
+    DevBuf first;    // res^3 + 1 int32: first sorted slot of each cell or a later one
+                     // (cells in the walk's order: x slowest, z fastest), n past the last
+    DevBuf tiles;    // suffix minima of the cell table's tiles (build scratch)
     DevBuf sorted;   // n x 2 float4 in `order`: position + power r, then power g b + the
                      // slot's cell as int bits (gathers read a cell's photons
                      // contiguously and stop where the cell changes)
@@ -431,7 +437,9 @@ __global__ void k_cell_keys(const float *rec, int64_t n, const GridParams *g,
     const int cx = (int) (float) (int) ((rec[i * 9 + 0] - g->bmin[0]) / g->cs[0]);
     const int cy = (int) (float) (int) ((rec[i * 9 + 1] - g->bmin[1]) / g->cs[1]);
     const int cz = (int) (float) (int) ((rec[i * 9 + 2] - g->bmin[2]) / g->cs[2]);
-    const unsigned cell = (unsigned) (cx + cy * res + cz * res * res);
+    // cells numbered in the walk's order (x slowest, z fastest), so the cells
+    // (cx, cy, z0..z1) of one column are consecutive keys
+    const unsigned cell = (unsigned) (cz + cy * res + cx * res * res);
     keys[i] = ((unsigned long long) cell << 32) | (unsigned long long) i;
 }
 
@@ -445,13 +453,16 @@ __global__ void k_cell_occupancy(const unsigned long long *keys, int64_t n, Grid
     if (i > 0 && (unsigned) (keys[i - 1] >> 32) == cell)
         return;
     const unsigned res = (unsigned) g->res;
-    const unsigned c[3] = {cell % res, (cell / res) % res, cell / (res * res)};
+    const unsigned c[3] = {cell / (res * res), (cell / res) % res, cell % res};
     for (int a = 0; a < 3; a++)
         atomicOr(&g->occ[a][c[a] >> 5], 1u << (c[a] & 31));
 }
 
+// The sorted copy and, at the first slot of each occupied cell, that slot in
+// the cell's entry of `first` (the other entries hold a value above any slot;
+// k_first_* then turn the table into lower bounds).
 __global__ void k_cell_table(const unsigned long long *keys, const float *rec, int64_t n,
-                             int32_t *order, int32_t *start, float4 *sorted) {
+                             int32_t *order, int32_t *first, float4 *sorted) {
     const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
@@ -460,16 +471,103 @@ __global__ void k_cell_table(const unsigned long long *keys, const float *rec, i
     order[i] = o;
     const float *p = rec + (size_t) o * 9;
     sorted[2 * i] = make_float4(p[0], p[1], p[2], p[6]);
-    sorted[2 * i + 1] = make_float4(p[7], p[8], __int_as_float((int) cell), 0.f);
+    sorted[2 * i + 1] = make_float4(p[7], p[8], 0.f, 0.f);
     if (i == 0 || (unsigned) (keys[i - 1] >> 32) != cell)
-        start[cell] = (int32_t) i;
+        first[cell] = (int32_t) i;
+}
+
+// Lower bounds over the cell table: first[c] becomes the first sorted slot
+// whose cell is c or later (n when there is none), by a suffix minimum over
+// the cells in tiles of 4096: within each tile here, across tiles in
+// k_first_tile_mins, both applied in k_first_apply.
+constexpr int kFirstTile = 4096;
+
+// Suffix minimum over the threads of a block: thread t gets the minimum of v
+// over threads t + 1 .. blockDim.x - 1 (INT_MAX for the last); *total = the
+// minimum over all threads.
+__device__ int block_suffix_min_excl(int v, int *total) {
+    __shared__ int warp_suf[32];
+    __shared__ int thread_suf[1024];
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_down_sync(full, v, o);
+        if (lane + o < 32)
+            v = min(v, y);
+    }
+    if (lane == 0)
+        warp_suf[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < nw ? warp_suf[lane] : INT_MAX;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_down_sync(full, w, o);
+            if (lane + o < 32)
+                w = min(w, y);
+        }
+        warp_suf[lane] = w;
+    }
+    __syncthreads();
+    thread_suf[threadIdx.x] = min(v, wid + 1 < nw ? warp_suf[wid + 1] : INT_MAX);
+    __syncthreads();
+    const int excl =
+        threadIdx.x + 1 < blockDim.x ? thread_suf[threadIdx.x + 1] : INT_MAX;
+    *total = warp_suf[0];
+    __syncthreads();
+    return excl;
+}
+
+__global__ void __launch_bounds__(1024) k_first_tiles(int32_t *first, int64_t m,
+                                                      int32_t *tile_min) {
+    const int64_t base = (int64_t) blockIdx.x * kFirstTile + (int64_t) threadIdx.x * 4;
+    int x[4];
+    for (int q = 0; q < 4; q++)
+        x[q] = base + q < m ? first[base + q] : INT_MAX;
+    x[2] = min(x[2], x[3]);
+    x[1] = min(x[1], x[2]);
+    x[0] = min(x[0], x[1]);
+    int total;
+    const int later = block_suffix_min_excl(x[0], &total);
+    for (int q = 0; q < 4; q++)
+        if (base + q < m)
+            first[base + q] = min(x[q], later);
+    if (threadIdx.x == 0)
+        tile_min[blockIdx.x] = total;
+}
+
+// tile_min[b] <- the minimum over the tiles after b (INT_MAX for the last);
+// one block, at most 4 * 1024 tiles.
+__global__ void __launch_bounds__(1024) k_first_tile_mins(int32_t *tile_min, int ntiles) {
+    const int base = (int) threadIdx.x * 4;
+    int y[4];
+    for (int q = 0; q < 4; q++)
+        y[q] = base + q < ntiles ? tile_min[base + q] : INT_MAX;
+    int suf[4];
+    suf[3] = y[3];
+    suf[2] = min(y[2], suf[3]);
+    suf[1] = min(y[1], suf[2]);
+    suf[0] = min(y[0], suf[1]);
+    int total;
+    const int later = block_suffix_min_excl(suf[0], &total);
+    for (int q = 0; q < 4; q++)
+        if (base + q < ntiles)
+            tile_min[base + q] = min(q < 3 ? suf[q + 1] : INT_MAX, later);
+}
+
+__global__ void k_first_apply(int32_t *first, int64_t m, const int32_t *after, int32_t n) {
+    const int64_t c = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < m)
+        first[c] = min(min(first[c], after[c / kFirstTile]), n);
 }
 
 // ---------------------------------------------------------------- gather
 struct GridView {
     const float *rec;
     const float4 *sorted;
-    const int32_t *order, *start;
+    const int32_t *order;
+    // first[c]: the first sorted slot whose cell is c or later (cells in the
+    // walk's order), n when there is none; res^3 + 1 entries
+    const int32_t *first;
     const GridParams *g;
     int64_t n;
     float radius;
@@ -477,12 +575,6 @@ struct GridView {
     // rounded and monotone, so |d| <= radius exactly when d.d <= inside_sq
     float inside_sq;
 };
-
-// The cell of sorted slot s (kept beside the slot's power, in the sector a
-// gather reads anyway).
-__device__ __forceinline__ int cell_at(const GridView &v, int64_t s) {
-    return __float_as_int(v.sorted[2 * s + 1].z);
-}
 
 // pi r^2 as estimateIrradiance computes it (Photon.cpp:87): all in float,
 // since the reference redefines M_PI as a float literal (global.hpp:9-10).
@@ -503,25 +595,34 @@ __device__ __forceinline__ int next_slab(const uint32_t *occ, int c, int hi) {
     return hi + 1;
 }
 
-// Calls f(s) for every photon of the cells in the box [x0,x1] x [y0,y1] x
-// [z0,z1], in the reference query's order (cells by x, then y, then z; a
-// cell's photons in photon order; s indexes the cell-sorted arrays). Slabs
-// without photons are skipped before the cell table is read.
+// Calls col(a, b) for each column (cx, cy) of the box [x0,x1] x [y0,y1] x
+// [z0,z1] whose x and y slabs hold photons, in the reference query's order
+// (by x, then y): the sorted slots [a, b) are the photons of the column's
+// cells cz = z0..z1, cell after cell, each cell's in photon order -- the
+// order the reference's walk over cells by x, then y, then z takes them.
+template <class C>
+__device__ __forceinline__ void walk_columns(const GridView &v, const GridParams &g, int x0,
+                                             int x1, int y0, int y1, int z0, int z1, C &&col) {
+    for (int cx = next_slab(g.occ[0], x0, x1); cx <= x1; cx = next_slab(g.occ[0], cx + 1, x1))
+        for (int cy = next_slab(g.occ[1], y0, y1); cy <= y1;
+             cy = next_slab(g.occ[1], cy + 1, y1)) {
+            const int k0 = z0 + cy * g.res + cx * g.res * g.res;
+            const int a = v.first[k0];
+            const int b = v.first[k0 + (z1 - z0) + 1];
+            if (a < b)
+                col(a, b);
+        }
+}
+
+// Calls f(s) for every photon of the cells in the box, in the reference
+// query's order (s indexes the cell-sorted arrays).
 template <class F>
 __device__ __forceinline__ void walk_cells(const GridView &v, const GridParams &g, int x0, int x1,
                                            int y0, int y1, int z0, int z1, F &&f) {
-    for (int cx = next_slab(g.occ[0], x0, x1); cx <= x1; cx = next_slab(g.occ[0], cx + 1, x1))
-        for (int cy = next_slab(g.occ[1], y0, y1); cy <= y1;
-             cy = next_slab(g.occ[1], cy + 1, y1))
-            for (int cz = next_slab(g.occ[2], z0, z1); cz <= z1;
-                 cz = next_slab(g.occ[2], cz + 1, z1)) {
-                const int cell = cx + cy * g.res + cz * g.res * g.res;
-                int s = v.start[cell];
-                if (s < 0)
-                    continue;
-                for (; s < v.n && cell_at(v, s) == cell; s++)
-                    f(s);
-            }
+    walk_columns(v, g, x0, x1, y0, y1, z0, z1, [&](int a, int b) {
+        for (int s = a; s < b; s++)
+            f(s);
+    });
 }
 
 // The cell box of a query at pos (PhotonGrid::query, Photon.cpp:58-72).
@@ -690,25 +791,16 @@ struct CausticArgs {
     unsigned long long *dense_next; // k_caustic_dense's work counter (zeroed too)
 };
 
-// walk_cells with the photons of each cell shared out over a warp: lane l
-// takes the cell's photons l, l + 32, ... (every lane walks the same cells).
+// walk_cells with the photons of each column shared out over a warp: lane l
+// takes the column's photons l, l + 32, ... (every lane walks the same
+// columns).
 template <class F>
 __device__ __forceinline__ void walk_cells_warp(const GridView &v, const GatherBox &b, int lane,
                                                 F &&f) {
-    const GridParams &g = *v.g;
-    for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
-         cx = next_slab(g.occ[0], cx + 1, b.x1))
-        for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
-             cy = next_slab(g.occ[1], cy + 1, b.y1))
-            for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
-                 cz = next_slab(g.occ[2], cz + 1, b.z1)) {
-                const int cell = cx + cy * g.res + cz * g.res * g.res;
-                const int s0 = v.start[cell];
-                if (s0 < 0)
-                    continue;
-                for (int s = s0 + lane; s < v.n && cell_at(v, s) == cell; s += 32)
-                    f(s);
-            }
+    walk_columns(v, *v.g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int a, int e) {
+        for (int s = a + lane; s < e; s += 32)
+            f(s);
+    });
 }
 
 // The value of rank `want` (1-based) among the candidates' 32-bit keys, by a
@@ -850,34 +942,22 @@ __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a
         for (int attempt = 0; attempt < kDenseTries; attempt++) {
             const GatherBox b = sub_box(g, big, pos, t);
             int c = 0;
-            for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
-                 cx = next_slab(g.occ[0], cx + 1, b.x1))
-                for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
-                     cy = next_slab(g.occ[1], cy + 1, b.y1))
-                    for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
-                         cz = next_slab(g.occ[2], cz + 1, b.z1)) {
-                        const int cell = cx + cy * g.res + cz * g.res * g.res;
-                        const int s0 = v.start[cell];
-                        if (s0 < 0)
-                            continue;
-                        for (int base = s0;; base += 32) {
-                            const int s = base + lane;
-                            const bool in_cell = s < v.n && cell_at(v, s) == cell;
-                            if (!__any_sync(full, in_cell))
-                                break;
-                            float dist = 0.f;
-                            bool take = false;
-                            if (in_cell) {
-                                dist = dist_of(s);
-                                take = dist <= t;
-                            }
-                            const unsigned m = __ballot_sync(full, take);
-                            const int at = c + __popc(m & ((1u << lane) - 1u));
-                            if (take && at < kDenseCands)
-                                cand[at] = make_uint2(__float_as_uint(dist), (unsigned) s);
-                            c += __popc(m);
-                        }
+            walk_columns(v, g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int a0, int e0) {
+                for (int base = a0; base < e0; base += 32) {
+                    const int s = base + lane;
+                    float dist = 0.f;
+                    bool take = false;
+                    if (s < e0) {
+                        dist = dist_of(s);
+                        take = dist <= t;
                     }
+                    const unsigned m = __ballot_sync(full, take);
+                    const int at = c + __popc(m & ((1u << lane) - 1u));
+                    if (take && at < kDenseCands)
+                        cand[at] = make_uint2(__float_as_uint(dist), (unsigned) s);
+                    c += __popc(m);
+                }
+            });
             __syncwarp();
             if (c >= k && c <= kDenseCands) {
                 count = c;
@@ -951,41 +1031,28 @@ __global__ void __launch_bounds__(128) k_caustic_dense(GridView v, CausticArgs a
                                              });
             }
             const float rk = __uint_as_float(dk);
-            for (int cx = next_slab(g.occ[0], b.x0, b.x1); cx <= b.x1;
-                 cx = next_slab(g.occ[0], cx + 1, b.x1))
-                for (int cy = next_slab(g.occ[1], b.y0, b.y1); cy <= b.y1;
-                     cy = next_slab(g.occ[1], cy + 1, b.y1))
-                    for (int cz = next_slab(g.occ[2], b.z0, b.z1); cz <= b.z1;
-                         cz = next_slab(g.occ[2], cz + 1, b.z1)) {
-                        const int cell = cx + cy * g.res + cz * g.res * g.res;
-                        const int s0 = v.start[cell];
-                        if (s0 < 0)
-                            continue;
-                        for (int base = s0;; base += 32) {
-                            const int s = base + lane;
-                            const bool in_cell = s < v.n && cell_at(v, s) == cell;
-                            if (!__any_sync(full, in_cell))
-                                break;
-                            bool keep = false;
-                            V3 pw = v3(0.f);
-                            if (in_cell) {
-                                const float dist = dist_of(s);
-                                keep = dist < rk || (dist == rk && v.order[s] <= ik);
-                                if (keep) {
-                                    const float4 pa = v.sorted[2 * s];
-                                    const float4 pb = v.sorted[2 * s + 1];
-                                    pw = v3(pa.w, pb.x, pb.y);
-                                }
-                            }
-                            for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
-                                const int l = __ffs(km) - 1;
-                                const V3 w = v3(__shfl_sync(full, pw.x, l),
-                                                __shfl_sync(full, pw.y, l),
-                                                __shfl_sync(full, pw.z, l));
-                                ek = ek + w;
-                            }
+            walk_columns(v, g, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1, [&](int a0, int e0) {
+                for (int base = a0; base < e0; base += 32) {
+                    const int s = base + lane;
+                    bool keep = false;
+                    V3 pw = v3(0.f);
+                    if (s < e0) {
+                        const float dist = dist_of(s);
+                        keep = dist < rk || (dist == rk && v.order[s] <= ik);
+                        if (keep) {
+                            const float4 pa = v.sorted[2 * s];
+                            const float4 pb = v.sorted[2 * s + 1];
+                            pw = v3(pa.w, pb.x, pb.y);
                         }
                     }
+                    for (unsigned km = __ballot_sync(full, keep); km; km &= km - 1) {
+                        const int l = __ffs(km) - 1;
+                        const V3 w = v3(__shfl_sync(full, pw.x, l), __shfl_sync(full, pw.y, l),
+                                        __shfl_sync(full, pw.z, l));
+                        ek = ek + w;
+                    }
+                }
+            });
         }
         if (lane == 0) {
             const V3 c = v3(sc.x, sc.y, sc.z) * (ek / disc_area(__uint_as_float(dk)));
@@ -1148,7 +1215,7 @@ GridView view(const PhotonMap &pm) {
     v.rec = pm.rec.as<float>();
     v.sorted = pm.sorted.as<float4>();
     v.order = pm.order.as<int32_t>();
-    v.start = pm.start.as<int32_t>();
+    v.first = pm.first.as<int32_t>();
     v.g = pm.params.as<GridParams>();
     v.n = pm.n;
     v.radius = pm.radius;
@@ -1396,17 +1463,25 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     GridParams g;
     PRR_CUDA_TRY(cudaMemcpyAsync(&g, pm.params.ptr, sizeof(g), cudaMemcpyDeviceToHost, st));
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
-    const size_t cells = (size_t) g.res * g.res * g.res;
+    // the cell table with one entry past the last cell (a column's end), its
+    // entries above every slot until k_cell_table marks the occupied cells
+    const int64_t m = (int64_t) g.res * g.res * g.res + 1;
+    const int ntiles = (int) ((m + kFirstTile - 1) / kFirstTile);
     PRR_CUDA_TRY(pm.order.ensure((size_t) n * sizeof(int32_t)));
-    PRR_CUDA_TRY(pm.start.ensure(cells * sizeof(int32_t)));
-    PRR_CUDA_TRY(cudaMemsetAsync(pm.start.ptr, 0xff, cells * sizeof(int32_t), st));
+    PRR_CUDA_TRY(pm.first.ensure((size_t) m * sizeof(int32_t)));
+    PRR_CUDA_TRY(pm.tiles.ensure((size_t) ntiles * sizeof(int32_t)));
+    PRR_CUDA_TRY(cudaMemsetAsync(pm.first.ptr, 0x7f, (size_t) m * sizeof(int32_t), st));
     PRR_CUDA_TRY(pm.sorted.ensure((size_t) n * 2 * sizeof(float4)));
     k_cell_table<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(
         keys, pm.rec.as<float>(), n, pm.order.as<int32_t>(),
-        pm.start.as<int32_t>(), pm.sorted.as<float4>());
+        pm.first.as<int32_t>(), pm.sorted.as<float4>());
     k_cell_occupancy<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(keys, n,
                                                                      pm.params.as<GridParams>());
-    pm.launches += 2;
+    k_first_tiles<<<ntiles, 1024, 0, st>>>(pm.first.as<int32_t>(), m, pm.tiles.as<int32_t>());
+    k_first_tile_mins<<<1, 1024, 0, st>>>(pm.tiles.as<int32_t>(), ntiles);
+    k_first_apply<<<(unsigned) ((m + 255) / 256), 256, 0, st>>>(
+        pm.first.as<int32_t>(), m, pm.tiles.as<int32_t>(), (int32_t) n);
+    pm.launches += 5;
     PRR_CUDA_TRY(cudaGetLastError());
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     pm.res = g.res;
