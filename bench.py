@@ -752,8 +752,8 @@ def caustics_result(args, rank, world, on, steps, warmup):
                 "kernel": "k_caustic_samples + k_caustic_dense + k_caustic_film (one render call)",
                 "traffic_kernel": "k_caustic_samples",
                 "limiter": "latency and issue, not HBM: the photon grid and the scene stay in L2 "
-                           "(DRAM under 2% busy); the sample kernel issues on about 66% of "
-                           "cycles with 45% of warps resident (64 registers)",
+                           "(DRAM under 3% busy); the sample kernel issues on about 72% of "
+                           "cycles with 49% of warps resident (64 registers)",
                 "basis": "algorithmic bytes of the render + gather (gather work counted by "
                          "prr_render_caustics_counts, bytes per unit in bench.CAUSTIC_BYTES) / "
                          "its CUDA-event time",
