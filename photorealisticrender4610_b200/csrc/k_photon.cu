@@ -1121,7 +1121,7 @@ __global__ void __launch_bounds__(128, 8) k_caustic_samples(DevScene S, GridView
             if (mt.kind == kMatEmissive)
                 break;
             if (mt.kind == kMatMirror || mt.kind == kMatGlass) {
-                const Shading sd = build_shading(S, mt, in.n, in.a);
+                const Shading sd = build_shading<true>(S, mt, in.n, in.a);
                 const BSDFSample bs = delta_sample(mt, sd, -ray.d, rng);
                 if (bs.pdf < 1e-6f)
                     break;
@@ -1135,7 +1135,7 @@ __global__ void __launch_bounds__(128, 8) k_caustic_samples(DevScene S, GridView
             if constexpr (COUNT)
                 cnt_[1]++;
             const V3 albedo = mt.tex_base >= 0
-                                  ? sample_base_color(S.textures[mt.tex_base], in.a.u, in.a.v)
+                                  ? sample_base_color_ool(S.textures[mt.tex_base], in.a.u, in.a.v)
                                   : v3(mt.base[0], mt.base[1], mt.base[2]);
             const V3 scale = beta * (albedo / PRR_PI);
             const GatherBox b = gather_box(*v.g, in.p, v.radius);
