@@ -360,7 +360,8 @@ __global__ void k_gather_records(const unsigned long long *keys, const float *sr
 }
 
 // ---------------------------------------------------------------- grid
-// kOccWords 32-bit words hold one bit per slab of an axis (res <= 200)
+// kOccWords 32-bit words hold one bit per slab of an axis (res <= kMaxRes)
+constexpr int kMaxRes = 200; // PhotonGrid::build's resolution cap (Photon.cpp:44-46)
 constexpr int kOccWords = 7;
 
 struct GridParams {
@@ -403,14 +404,37 @@ __global__ void k_bounds(const float *rec, int64_t n, float *partial) {
             partial[blockIdx.x * 6 + k] = s[k][0];
 }
 
-// PhotonGrid::build's parameters (Photon.cpp:27-46), one thread.
-__global__ void k_grid_params(const float *partial, int nb, float radius, GridParams *g) {
+// PhotonGrid::build's parameters (Photon.cpp:27-46): one block folds the
+// per-block bounds (min and max are exact in any order), its first thread
+// derives the grid.
+__global__ void __launch_bounds__(256) k_grid_params(const float *partial, int nb, float radius,
+                                                     GridParams *g) {
+    __shared__ float s[6][256];
     float mn[3] = {kInf, kInf, kInf}, mx[3] = {-kInf, -kInf, -kInf};
-    for (int b = 0; b < nb; b++)
+    for (int b = threadIdx.x; b < nb; b += blockDim.x)
         for (int k = 0; k < 3; k++) {
             mn[k] = fminf(mn[k], partial[b * 6 + k]);
             mx[k] = fmaxf(mx[k], partial[b * 6 + 3 + k]);
         }
+    for (int k = 0; k < 3; k++) {
+        s[k][threadIdx.x] = mn[k];
+        s[3 + k][threadIdx.x] = mx[k];
+    }
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int) threadIdx.x < w)
+            for (int k = 0; k < 3; k++) {
+                s[k][threadIdx.x] = fminf(s[k][threadIdx.x], s[k][threadIdx.x + w]);
+                s[3 + k][threadIdx.x] = fmaxf(s[3 + k][threadIdx.x], s[3 + k][threadIdx.x + w]);
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0)
+        return;
+    for (int k = 0; k < 3; k++) {
+        mn[k] = s[k][0];
+        mx[k] = s[3 + k][0];
+    }
     for (int k = 0; k < 3; k++) {
         g->bmin[k] = mn[k] - 0.01f;
         g->bmax[k] = mx[k] + 0.01f;
@@ -420,7 +444,7 @@ __global__ void k_grid_params(const float *partial, int nb, float radius, GridPa
     const float ex = g->bmax[0] - g->bmin[0], ey = g->bmax[1] - g->bmin[1],
                 ez = g->bmax[2] - g->bmin[2];
     int res = (int) (sqrtf(ex * ex + ey * ey + ez * ez) / radius);
-    res = max(10, min(200, res));
+    res = max(10, min(kMaxRes, res));
     g->res = res;
     g->cs[0] = ex / (float) res;
     g->cs[1] = ey / (float) res;
@@ -517,8 +541,18 @@ __device__ int block_suffix_min_excl(int v, int *total) {
     return excl;
 }
 
-__global__ void __launch_bounds__(1024) k_first_tiles(int32_t *first, int64_t m,
+// Cells of the table for the grid's resolution (one past the last cell).
+__device__ __forceinline__ int64_t table_cells(const GridParams *g) {
+    const int64_t r = g->res;
+    return r * r * r + 1;
+}
+
+// Launched for the largest table; blocks past this grid's table return.
+__global__ void __launch_bounds__(1024) k_first_tiles(int32_t *first, const GridParams *g,
                                                       int32_t *tile_min) {
+    const int64_t m = table_cells(g);
+    if ((int64_t) blockIdx.x * kFirstTile >= m)
+        return;
     const int64_t base = (int64_t) blockIdx.x * kFirstTile + (int64_t) threadIdx.x * 4;
     int x[4];
     for (int q = 0; q < 4; q++)
@@ -537,7 +571,9 @@ __global__ void __launch_bounds__(1024) k_first_tiles(int32_t *first, int64_t m,
 
 // tile_min[b] <- the minimum over the tiles after b (INT_MAX for the last);
 // one block, at most 4 * 1024 tiles.
-__global__ void __launch_bounds__(1024) k_first_tile_mins(int32_t *tile_min, int ntiles) {
+__global__ void __launch_bounds__(1024) k_first_tile_mins(int32_t *tile_min,
+                                                          const GridParams *g) {
+    const int ntiles = (int) ((table_cells(g) + kFirstTile - 1) / kFirstTile);
     const int base = (int) threadIdx.x * 4;
     int y[4];
     for (int q = 0; q < 4; q++)
@@ -554,9 +590,10 @@ __global__ void __launch_bounds__(1024) k_first_tile_mins(int32_t *tile_min, int
             tile_min[base + q] = min(q < 3 ? suf[q + 1] : INT_MAX, later);
 }
 
-__global__ void k_first_apply(int32_t *first, int64_t m, const int32_t *after, int32_t n) {
+__global__ void k_first_apply(int32_t *first, const GridParams *g, const int32_t *after,
+                              int32_t n) {
     const int64_t c = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < m)
+    if (c < table_cells(g))
         first[c] = min(min(first[c], after[c / kFirstTile]), n);
 }
 
@@ -1452,7 +1489,7 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     unsigned long long *keys = pm.scratch.as<unsigned long long>();
     float *partial = reinterpret_cast<float *>((char *) pm.scratch.ptr + n2 * 8);
     k_bounds<<<nb, 256, 0, st>>>(pm.rec.as<float>(), n, partial);
-    k_grid_params<<<1, 1, 0, st>>>(partial, nb, radius, pm.params.as<GridParams>());
+    k_grid_params<<<1, 256, 0, st>>>(partial, nb, radius, pm.params.as<GridParams>());
     k_cell_keys<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(pm.rec.as<float>(), n,
                                                               pm.params.as<GridParams>(), keys);
     pm.launches += 3;
@@ -1463,12 +1500,11 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
     PRR_CUDA_TRY(cudaGetLastError());
     if (int rc = bitonic_sort(keys, n2, st, &pm.launches))
         return rc;
-    GridParams g;
-    PRR_CUDA_TRY(cudaMemcpyAsync(&g, pm.params.ptr, sizeof(g), cudaMemcpyDeviceToHost, st));
-    PRR_CUDA_TRY(cudaStreamSynchronize(st));
     // the cell table with one entry past the last cell (a column's end), its
-    // entries above every slot until k_cell_table marks the occupied cells
-    const int64_t m = (int64_t) g.res * g.res * g.res + 1;
+    // entries above every slot until k_cell_table marks the occupied cells;
+    // sized and cleared for the largest resolution, so that the host need not
+    // wait for the grid's own before it launches the rest of the build
+    const int64_t m = (int64_t) kMaxRes * kMaxRes * kMaxRes + 1;
     const int ntiles = (int) ((m + kFirstTile - 1) / kFirstTile);
     PRR_CUDA_TRY(pm.order.ensure((size_t) n * sizeof(int32_t)));
     PRR_CUDA_TRY(pm.first.ensure((size_t) m * sizeof(int32_t)));
@@ -1480,12 +1516,15 @@ int prr_photon_build(prr_photon_map *pmap, float radius, void *stream) {
         pm.first.as<int32_t>(), pm.sorted.as<float4>());
     k_cell_occupancy<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(keys, n,
                                                                      pm.params.as<GridParams>());
-    k_first_tiles<<<ntiles, 1024, 0, st>>>(pm.first.as<int32_t>(), m, pm.tiles.as<int32_t>());
-    k_first_tile_mins<<<1, 1024, 0, st>>>(pm.tiles.as<int32_t>(), ntiles);
+    const GridParams *dg = pm.params.as<GridParams>();
+    k_first_tiles<<<ntiles, 1024, 0, st>>>(pm.first.as<int32_t>(), dg, pm.tiles.as<int32_t>());
+    k_first_tile_mins<<<1, 1024, 0, st>>>(pm.tiles.as<int32_t>(), dg);
     k_first_apply<<<(unsigned) ((m + 255) / 256), 256, 0, st>>>(
-        pm.first.as<int32_t>(), m, pm.tiles.as<int32_t>(), (int32_t) n);
+        pm.first.as<int32_t>(), dg, pm.tiles.as<int32_t>(), (int32_t) n);
     pm.launches += 5;
     PRR_CUDA_TRY(cudaGetLastError());
+    GridParams g;
+    PRR_CUDA_TRY(cudaMemcpyAsync(&g, pm.params.ptr, sizeof(g), cudaMemcpyDeviceToHost, st));
     PRR_CUDA_TRY(cudaStreamSynchronize(st));
     pm.res = g.res;
     std::memcpy(pm.bmin, g.bmin, sizeof(pm.bmin));
