@@ -834,9 +834,9 @@ __global__ void __maxnreg__(48) k_wf_extend(DevScene S, Wf w, int it, int refill
     wf_extend<MULTI, STATS>(S, w, it, refill);
 }
 // The server's extend stage (paths of several requests; the request index
-// selects scene and camera) held to 56 registers: 9 resident blocks of 128
-// instead of 8 at the 64 it takes otherwise, without spills. (The one-scene
-// stage already fits in 56, and a cap there made it slower.)
+// selects scene and camera), held to 48 registers like the others: 10
+// resident blocks of 128 instead of 8 at the 64 it takes otherwise (16 bytes
+// of spills).
 __global__ void __maxnreg__(48) k_wf_extend_multi(DevScene S, Wf w, int it, int refill) {
     wf_extend<true, false>(S, w, it, refill);
 }
