@@ -352,3 +352,23 @@ def test_gather_radius_boundary_bit_exact(ref, port, cuda):
     assert (inside > 16).all()
     got16 = pm.gather(q, k_nearest=16).cpu().numpy()
     assert np.array_equal(got16.view(np.uint32), want16.view(np.uint32))
+
+
+def test_grid_large_map_sorted_in_stages(ref, cuda):
+    """A photon map whose sort needs more blocks of 2,048 keys than the
+    device holds at once (700,000 photons: 1,048,576 keys, 512 blocks) is
+    sorted a launch per stage instead of in one cooperative launch; the
+    gathers still equal the reference estimator bit for bit."""
+    rec, q = random_photons(700_000, 21)
+    pm = prr.PhotonMap().set(rec)
+    n0 = pm.launches()
+    pm.build(0.02)
+    assert pm.launches() - n0 > 20  # the staged sort, not the single launch
+    got = pm.gather(q).cpu().numpy()
+    want, res = ref.photon_estimate(rec, 0.02, q)
+    assert pm.info()[1] == res
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    small = prr.PhotonMap().set(rec[:30_000])
+    n1 = small.launches()
+    small.build(0.02)
+    assert small.launches() - n1 <= 12  # one sort launch among the build's kernels
