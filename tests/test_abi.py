@@ -169,3 +169,28 @@ def test_wavefront_config_rejected(lib, kw):
     with pytest.raises(prr.PrrError, match="wavefront config"):
         s.set_wavefront(**kw)
     s.set_wavefront(paths_per_pass=1 << 30, block_size=128, stack_smem=8)
+
+
+def test_host_sah_builder_large_mesh_threaded_passes(port):
+    """A 400,000-triangle soup (the query set's generator): the nodes of at
+    least 131,072 prims split their bounds, binning and partition passes over
+    the host threads; the tree equals the C restatement's node for node."""
+    verts, _, _ = scenes.query_set(400_000, 1, seed=5)
+    v = np.ascontiguousarray(verts, np.float32)
+    n = len(v)
+    pb = np.empty((n, 6), np.float32)
+    pa = np.empty(n, np.float32)
+    port.L.prr_oracle_triangle_prims(v, n, pb, pa)
+    ours, _ = bvh_build(pb, pa, 4)
+    m = 2 * n
+    nb = np.empty((m, 6), np.float32)
+    fc = np.empty(m, np.uint32)
+    meta = np.empty(m, np.uint32)
+    ar = np.empty(m, np.float32)
+    od = np.empty(n, np.int32)
+    nn = port.L.prr_oracle_bvh_build(pb, pa, n, 4, nb, fc, meta, ar, od)
+    assert np.array_equal(ours["bounds"], nb[:nn])
+    assert np.array_equal(ours["first_child"], fc[:nn])
+    assert np.array_equal(ours["meta"], meta[:nn])
+    assert np.array_equal(ours["area"].view(np.uint32), ar[:nn].view(np.uint32))
+    assert np.array_equal(ours["ordered"], od)
