@@ -172,9 +172,9 @@ def test_wavefront_config_rejected(lib, kw):
 
 
 def test_host_sah_builder_large_mesh_threaded_passes(port):
-    """A 400,000-triangle soup (the query set's generator): the nodes of at
-    least 131,072 prims split their bounds, binning and partition passes over
-    the host threads; the tree equals the C restatement's node for node."""
+    """A 400,000-triangle soup (the query set's generator), its subtrees built
+    on several host threads: the tree equals the C restatement's node for
+    node, areas and prim order included."""
     verts, _, _ = scenes.query_set(400_000, 1, seed=5)
     v = np.ascontiguousarray(verts, np.float32)
     n = len(v)
