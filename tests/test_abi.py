@@ -171,7 +171,7 @@ def test_wavefront_config_rejected(lib, kw):
     s.set_wavefront(paths_per_pass=1 << 30, block_size=128, stack_smem=8)
 
 
-def test_host_sah_builder_large_mesh_threaded_passes(port):
+def test_host_sah_builder_large_mesh(port):
     """A 400,000-triangle soup (the query set's generator), its subtrees built
     on several host threads: the tree equals the C restatement's node for
     node, areas and prim order included."""
